@@ -1,0 +1,328 @@
+"""ctypes view of the CPU oracle (test infrastructure only).
+
+The oracle is the C++ restatement of the reference CPU path in
+``lbm_oracle.hpp``. Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline / reference legs may import this module, and only
+as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liblbmb_oracle.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u8p = C.POINTER(C.c_uint8)
+
+COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
+MAGIC_STD = 3.0 / 16.0
+
+
+def build() -> str:
+    """Compile the oracle shared library with its Makefile (gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.lbmo_create.restype = C.c_void_p
+        L.lbmo_create.argtypes = [C.c_int, C.c_int, _ip, _ip, C.c_int, C.c_double, C.c_double,
+                                  C.c_double, _dp, _u8p, _dp, C.c_char_p, C.c_int]
+        L.lbmo_destroy.argtypes = [C.c_void_p]
+        L.lbmo_step.argtypes = [C.c_void_p, C.c_int]
+        for name in ("lbmo_stage_in", "lbmo_stage_out", "lbmo_get_force_field"):
+            getattr(L, name).argtypes = [C.c_void_p, _dp]
+        L.lbmo_init_with.argtypes = [C.c_void_p, _dp, _dp]
+        L.lbmo_read_moments.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        L.lbmo_reduce.restype = C.c_double
+        L.lbmo_reduce.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.lbmo_clear_force_field.argtypes = [C.c_void_p]
+        L.lbmo_ibm_apply.restype = C.c_int
+        L.lbmo_ibm_apply.argtypes = [C.c_void_p, _dp, _dp, C.c_long, _dp, _dp, C.c_int, C.c_double,
+                                     C.c_int, C.c_double, _dp, C.c_char_p, C.c_int]
+        L.lbmo_ibm_direct_forcing.restype = C.c_int
+        L.lbmo_ibm_direct_forcing.argtypes = [_ip, C.c_int, _u8p, _dp, _dp, _dp, _dp, C.c_long, _dp,
+                                              _dp, C.c_int, C.c_double, C.c_int, C.c_double, _dp,
+                                              _dp, C.c_char_p, C.c_int]
+        L.lbmo_marker_stencil.restype = C.c_int
+        L.lbmo_marker_stencil.argtypes = [_dp, _ip, C.c_int, C.c_int, _dp]
+        L.lbmo_scalar_enable.restype = C.c_int
+        L.lbmo_scalar_enable.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.lbmo_scalar_set.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.lbmo_scalar_get.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.lbmo_wall_rims.argtypes = [C.c_int, _ip, _ip, _dp, _u8p, _dp]
+        L.lbmo_build_tank.restype = C.c_long
+        L.lbmo_build_tank.argtypes = [_ip, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_int, C.c_double, C.c_double, C.c_int,
+                                      C.c_double, _u8p, _u8p, _dp, _dp, _dp, C.c_long, _dp, _dp,
+                                      C.c_char_p, C.c_int]
+        L.lbmo_power_qois.restype = C.c_int
+        L.lbmo_power_qois.argtypes = [C.c_double] * 5 + [_dp]
+        L.lbmo_scalar_cv.restype = C.c_double
+        L.lbmo_scalar_cv.argtypes = [_dp, _u8p, C.c_long]
+        L.lbmo_mixing_time.restype = C.c_int
+        L.lbmo_mixing_time.argtypes = [_dp, _dp, C.c_long, _dp]
+        L.lbmo_run_tank.restype = C.c_long
+        L.lbmo_run_tank.argtypes = [C.c_void_p, _dp, _dp, C.c_long, _dp, _dp, C.c_int, C.c_double,
+                                    C.c_int, C.c_double, C.c_long, C.c_long, C.c_int, _dp, _dp,
+                                    _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _as_d(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None:
+        assert a.size == n, (a.size, n)
+    return a
+
+
+DIAG_FIELDS = ("iterations", "slip_max", "slip_rms", "slip_max_rel", "slip_rms_rel", "torque",
+               "fluid_force", "marker_force", "momentum_error_rel")
+
+
+def diag_dict(v) -> dict:
+    return {"iterations": int(v[0]), "slip_max": v[1], "slip_rms": v[2], "slip_max_rel": v[3],
+            "slip_rms_rel": v[4], "torque": np.array(v[5:8]), "fluid_force": np.array(v[8:11]),
+            "marker_force": np.array(v[11:14]), "momentum_error_rel": v[14]}
+
+
+class OracleSolver:
+    """Single-part CpuScalar solver (lattice 19|27, real 32|64)."""
+
+    def __init__(self, dims, q=19, real_bits=64, collision="trt", nu=1.0 / 6.0, magic=MAGIC_STD,
+                 omega_shear=0.0, periodic=(False, False, False), force=(0.0, 0.0, 0.0),
+                 solid=None, wall_u=None):
+        L = lib()
+        self.dims = tuple(int(d) for d in dims)
+        self.n = self.dims[0] * self.dims[1] * self.dims[2]
+        self.q = q
+        dims_a = (C.c_int * 3)(*self.dims)
+        per_a = (C.c_int * 3)(*[int(bool(p)) for p in periodic])
+        force_a = np.asarray(force, dtype=np.float64)
+        self._solid = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8).ravel()
+        self._wall = None if wall_u is None else _as_d(wall_u).ravel()
+        err = C.create_string_buffer(256)
+        self.h = L.lbmo_create(q, real_bits, dims_a, per_a, COLLISION[collision], magic,
+                               omega_shear, nu, _d(force_a),
+                               None if self._solid is None else self._solid.ctypes.data_as(_u8p),
+                               _d(self._wall), err, 256)
+        if not self.h:
+            raise ValueError(err.value.decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().lbmo_destroy(self.h)
+            self.h = None
+
+    def step(self, n=1):
+        lib().lbmo_step(self.h, n)
+
+    def stage_in(self, f):
+        f = _as_d(f, self.q * self.n)
+        lib().lbmo_stage_in(self.h, _d(f))
+
+    def stage_out(self):
+        f = np.zeros(self.q * self.n)
+        lib().lbmo_stage_out(self.h, _d(f))
+        return f.reshape(self.q, self.n)
+
+    def init_with(self, rho, u):
+        rho = _as_d(rho, self.n)
+        u = _as_d(u, 3 * self.n)
+        lib().lbmo_init_with(self.h, _d(rho), _d(u))
+
+    def moments(self):
+        out = [np.zeros(self.n) for _ in range(4)]
+        lib().lbmo_read_moments(self.h, *[_d(a) for a in out])
+        return out
+
+    def reduce(self, kind, axis=0):
+        return lib().lbmo_reduce(self.h, kind, axis)
+
+    def total_mass(self):
+        return self.reduce(0) + self.reduce(1)
+
+    def clear_force_field(self):
+        lib().lbmo_clear_force_field(self.h)
+
+    def force_field(self):
+        out = np.zeros(3 * self.n)
+        lib().lbmo_get_force_field(self.h, _d(out))
+        return out.reshape(self.n, 3)
+
+    def ibm_apply(self, pos, w, center, omega, max_iterations=3, slip_tolerance=1e-2,
+                  kernel_radius=1, relaxation=1.0):
+        pos = _as_d(pos).ravel()
+        w = _as_d(w).ravel()
+        center = _as_d(center)
+        omega = _as_d(omega)
+        diag = np.zeros(15)
+        err = C.create_string_buffer(256)
+        rc = lib().lbmo_ibm_apply(self.h, _d(pos), _d(w), w.size, _d(center), _d(omega),
+                                  max_iterations, slip_tolerance, kernel_radius, relaxation,
+                                  _d(diag), err, 256)
+        if rc != 0:
+            raise ValueError(err.value.decode())
+        return diag_dict(diag)
+
+    def scalar_enable(self, diffusivity, q=None):
+        k = lib().lbmo_scalar_enable(self.h, self.q if q is None else q, diffusivity)
+        if k < 0:
+            raise ValueError("scalar enable rejected")
+        return k
+
+    def scalar_set(self, k, values):
+        v = _as_d(values, self.n)
+        lib().lbmo_scalar_set(self.h, k, _d(v))
+
+    def scalar_get(self, k):
+        out = np.zeros(self.n)
+        lib().lbmo_scalar_get(self.h, k, _d(out))
+        return out
+
+    def run_tank(self, pos, w, center, omega, steps, probe_every=1, scalar=-1,
+                 max_iterations=3, slip_tolerance=1e-2, kernel_radius=1, relaxation=1.0):
+        pos = _as_d(pos).ravel()
+        w = _as_d(w).ravel()
+        torque = np.full(steps, np.nan)
+        ff = np.full(3 * steps, np.nan)
+        cv = np.full(steps, np.nan)
+        iters = np.zeros(steps)
+        done = lib().lbmo_run_tank(self.h, _d(pos), _d(w), w.size, _d(_as_d(center)),
+                                   _d(_as_d(omega)), max_iterations, slip_tolerance,
+                                   kernel_radius, relaxation, steps, probe_every, scalar,
+                                   _d(torque), _d(ff), _d(cv), _d(iters))
+        return {"executed": int(done), "torque_lu": torque, "fluid_force": ff.reshape(steps, 3),
+                "cv": cv, "ibm_iterations": iters}
+
+
+def ibm_direct_forcing(dims, d, solid, rho, u_now, pos, w, center, omega, max_iterations=3,
+                       slip_tolerance=1e-2, kernel_radius=1, relaxation=1.0):
+    n = dims[0] * dims[1] * dims[2]
+    solid = np.ascontiguousarray(solid, dtype=np.uint8).ravel()
+    rho = _as_d(rho, n)
+    u_now = _as_d(u_now, 3 * n)
+    pos = _as_d(pos).ravel()
+    w = _as_d(w).ravel()
+    spread = np.zeros(3 * n)
+    diag = np.zeros(15)
+    err = C.create_string_buffer(256)
+    rc = lib().lbmo_ibm_direct_forcing((C.c_int * 3)(*dims), d, solid.ctypes.data_as(_u8p),
+                                       _d(rho), _d(u_now), _d(pos), _d(w), w.size,
+                                       _d(_as_d(center)), _d(_as_d(omega)), max_iterations,
+                                       slip_tolerance, kernel_radius, relaxation, _d(spread),
+                                       _d(diag), err, 256)
+    if rc != 0:
+        raise ValueError(err.value.decode())
+    return spread.reshape(n, 3), diag_dict(diag)
+
+
+def marker_stencil(p, dims, d=3, radius=1):
+    out = np.zeros(4 * 64)
+    k = lib().lbmo_marker_stencil(_d(_as_d(p)), (C.c_int * 3)(*dims), d, radius, _d(out))
+    return out[: 4 * k].reshape(k, 4)
+
+
+def wall_rims(dims, is_wall, wall_u, d=3):
+    n = dims[0] * dims[1] * dims[2]
+    solid = np.zeros(n, dtype=np.uint8)
+    wu = np.zeros(3 * n)
+    u = _as_d(wall_u, 18)
+    lib().lbmo_wall_rims(d, (C.c_int * 3)(*dims), (C.c_int * 6)(*[int(b) for b in is_wall]),
+                         _d(u), solid.ctypes.data_as(_u8p), _d(wu))
+    return solid, wu.reshape(n, 3)
+
+
+def build_tank(dims, dx, vessel_d, liquid_h, impeller_d, clearance, blades, omega_z,
+               baffle_w=0.0, baffle_t=0.0, kind=0):
+    n = dims[0] * dims[1] * dims[2]
+    err = C.create_string_buffer(256)
+    dims_a = (C.c_int * 3)(*dims)
+    m = lib().lbmo_build_tank(dims_a, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind,
+                              impeller_d, clearance, blades, omega_z, None, None, None, None,
+                              None, 0, None, None, err, 256)
+    if m < 0:
+        raise ValueError(err.value.decode())
+    solid = np.zeros(n, dtype=np.uint8)
+    baffle = np.zeros(n, dtype=np.uint8)
+    wv = np.zeros(3 * n)
+    pos = np.zeros(3 * m)
+    w = np.zeros(m)
+    center = np.zeros(3)
+    omega = np.zeros(3)
+    lib().lbmo_build_tank(dims_a, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind, impeller_d,
+                          clearance, blades, omega_z, solid.ctypes.data_as(_u8p),
+                          baffle.ctypes.data_as(_u8p), _d(wv), _d(pos), _d(w), m, _d(center),
+                          _d(omega), err, 256)
+    return {"solid": solid, "baffle": baffle, "wall_velocity": wv.reshape(n, 3),
+            "marker_pos": pos.reshape(m, 3), "marker_w": w, "center": center, "omega": omega}
+
+
+def power_qois(torque, omega, rho, d, volume):
+    out = np.zeros(5)
+    if lib().lbmo_power_qois(torque, omega, rho, d, volume, _d(out)) != 0:
+        raise ValueError("invalid power QOI inputs")
+    return dict(zip(("torque_n_m", "power_w", "rotational_speed_hz", "np", "p_over_v_w_m3"), out))
+
+
+def scalar_cv(values, include):
+    v = _as_d(values).ravel()
+    inc = np.ascontiguousarray(include, dtype=np.uint8).ravel()
+    r = lib().lbmo_scalar_cv(_d(v), inc.ctypes.data_as(_u8p), v.size)
+    return None if np.isnan(r) else r
+
+
+def mixing_time_from_cv(series):
+    t = _as_d([s[0] for s in series])
+    cv = _as_d([s[1] for s in series])
+    out = np.zeros(3)
+    if lib().lbmo_mixing_time(_d(t), _d(cv), t.size, _d(out)) != 0:
+        return None
+    return {"cv0": out[0], "t95": None if np.isnan(out[1]) else out[1],
+            "t99": None if np.isnan(out[2]) else out[2]}
+
+
+def collide_cells(q, real_bits, kind, omega_p, omega_m, omega_shear, f, rho, u, force_field=None):
+    """Collide independent cells in place; f is (q, n) float64."""
+    L = lib()
+    L.lbmo_collide_cells.restype = C.c_int
+    L.lbmo_collide_cells.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, C.c_long, _dp, _dp, _dp, _dp]
+    f = np.ascontiguousarray(f, dtype=np.float64).copy()
+    n = f.shape[1]
+    ff = None if force_field is None else _as_d(force_field, 3 * n)
+    rc = L.lbmo_collide_cells(q, real_bits, COLLISION[kind], omega_p, omega_m, omega_shear, n,
+                              _d(f), _d(_as_d(rho, n)), _d(_as_d(u, 3 * n)), _d(ff))
+    if rc != 0:
+        raise ValueError("unsupported lattice/precision")
+    return f
+
+
+def equilibrium_cells(q, real_bits, rho, u):
+    L = lib()
+    L.lbmo_equilibrium_cells.restype = C.c_int
+    L.lbmo_equilibrium_cells.argtypes = [C.c_int, C.c_int, C.c_long, _dp, _dp, _dp]
+    rho = _as_d(rho)
+    n = rho.size
+    out = np.zeros((q, n))
+    L.lbmo_equilibrium_cells(q, real_bits, n, _d(rho), _d(_as_d(u, 3 * n)), _d(out))
+    return out
