@@ -1,0 +1,225 @@
+/*
+ * lbmb.h — C ABI of the B200 (sm_100a) LBMFlow single-GPU time step.
+ *
+ * One opaque handle = one solver = one CUDA device + one stream. Every entry
+ * point returns an int status: 0 (LBMB_OK) or a negative lbmb_status; the
+ * text of the last failure on the calling thread is lbmb_last_error().
+ * Nothing throws across the ABI. Host buffers are caller-owned; device
+ * buffers are owned by the handle. A handle is not thread-safe; distinct
+ * handles may be driven from distinct threads.
+ *
+ * Arrays use the reference's compact global cell order
+ *   cell = (z * ny + y) * nx + x
+ * and populations are in the reference's deviation form (f_q - w_q),
+ * q-major: f[q * ncells + cell] (crates/lbm-core/src/fields.rs:3-15).
+ * Populations read or written through this ABI are always the reference's
+ * logical post-stream state, whatever in-place layout the device uses.
+ *
+ * Each entry point names the reference interface it replaces
+ * (path:line inside the reference project).
+ */
+#ifndef LBMB_H
+#define LBMB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lbmb_solver lbmb_solver;
+
+enum lbmb_status {
+  LBMB_OK = 0,
+  LBMB_ERR_INVALID = -1,     /* invalid argument / spec (SpecError) */
+  LBMB_ERR_CUDA = -2,        /* CUDA runtime failure */
+  LBMB_ERR_UNSUPPORTED = -3, /* UnsupportedReason::NotImplemented */
+  LBMB_ERR_DIVERGED = -4,    /* non-finite mass detected (Diverged) */
+  LBMB_ERR_STATE = -5,       /* call out of order (e.g. scalar not enabled) */
+  LBMB_ERR_NOMEM = -6        /* device allocation failed */
+};
+
+enum lbmb_collision { LBMB_BGK = 0, LBMB_TRT = 1, LBMB_CENTRAL_MOMENT = 2 };
+
+/* Population storage precision. Arithmetic is fp32 for F32/F16/BF16 and
+ * fp64 for F64. F16/BF16 store the deviation (f_q - w_q). */
+enum lbmb_storage { LBMB_STORE_F32 = 0, LBMB_STORE_F16 = 1, LBMB_STORE_BF16 = 2, LBMB_STORE_F64 = 3 };
+
+/* Backend reduction kinds (crates/lbm-core/src/params.rs:411-419). */
+enum lbmb_reduction { LBMB_RED_FLUID_CELLS = 0, LBMB_RED_MASS_DEV = 1, LBMB_RED_MOMENTUM = 2 };
+
+/* GlobalSpec subset on the hot path (crates/lbm-core/src/solver.rs:131-148). */
+typedef struct lbmb_config {
+  int32_t lattice;     /* 19 (D3Q19) or 27 (D3Q27) */
+  int32_t collision;   /* lbmb_collision */
+  int32_t storage;     /* lbmb_storage */
+  int32_t dims[3];     /* nx, ny, nz */
+  int32_t periodic[3]; /* per axis; non-periodic faces must be full solid rims */
+  int32_t device;      /* CUDA ordinal */
+  double nu;           /* lattice viscosity */
+  double magic;        /* TRT magic parameter (3/16 standard) */
+  double omega_shear;  /* central-moment shear rate in (0, 2] */
+  double force[3];     /* uniform Guo body force */
+} lbmb_config;
+
+/* DirectForcingConfig (crates/lbm-core/src/rotating_ibm.rs:106-130). */
+typedef struct lbmb_ibm_config {
+  int32_t max_iterations; /* default 3 */
+  double slip_tolerance;  /* default 1e-2 */
+  int32_t kernel_radius;  /* 1 (2-point linear) or 2 (3-point quadratic) */
+  double relaxation;      /* (0, 1], default 1 */
+} lbmb_ibm_config;
+
+/* IbmDiagnostics (crates/lbm-core/src/rotating_ibm.rs:134-153). */
+typedef struct lbmb_ibm_diag {
+  int32_t iterations;
+  double slip_max, slip_rms, slip_max_rel, slip_rms_rel;
+  double torque[3];
+  double fluid_force[3];
+  double marker_force[3];
+  double momentum_error_rel;
+} lbmb_ibm_diag;
+
+/* Impeller marker generators for lbmb_build_stirred_tank. */
+enum lbmb_impeller_kind {
+  LBMB_IMPELLER_RUSHTON = 0,    /* reference generator, geometry.rs:815-906 */
+  LBMB_IMPELLER_PITCHED = 1,    /* reference generator, 45-degree blades */
+  LBMB_IMPELLER_FLAT_BLADE = 2  /* disc + flat blades sampled at a uniform spacing */
+};
+
+/* Stirred-tank set-up (crates/lbm-core/src/geometry.rs:84-132), SI units. */
+typedef struct lbmb_tank_spec {
+  int32_t dims[3];
+  double dx_m;
+  double vessel_diameter_m;
+  double liquid_height_m;
+  int32_t baffle_count; /* 0 or 4 (wall attached) */
+  double baffle_width_m;
+  double baffle_thickness_m;
+  int32_t impeller_kind; /* lbmb_impeller_kind */
+  double impeller_diameter_m;
+  double clearance_m;
+  int32_t blade_count;
+  double omega_rad_s;          /* rotational speed (rad/s, SI) */
+  double marker_spacing_cells; /* LBMB_IMPELLER_FLAT_BLADE only */
+  double min_cells;            /* resolution floor; <= 0 -> 32 (STIRRED_TANK_MIN_CELLS) */
+} lbmb_tank_spec;
+
+/* Text of the last failure on this thread ("" if none). */
+const char* lbmb_last_error(void);
+
+/* Library version string. */
+const char* lbmb_version(void);
+
+/* Solver::try_new + Backend::alloc (solver.rs:1754-1900, backend.rs:138).
+ * solid: ncells bytes (nonzero = solid), may be NULL (all fluid).
+ * wall_u: ncells x 3 wall velocities (meaningful on solids), may be NULL.
+ * State after creation: quiescent f = 0 (rho = 1, u = 0). */
+int lbmb_create(const lbmb_config* cfg, const uint8_t* solid, const double* wall_u,
+                lbmb_solver** out);
+int lbmb_destroy(lbmb_solver* h);
+
+/* Cell count and lattice size of a handle. */
+int lbmb_shape(const lbmb_solver* h, int64_t* ncells, int32_t* q);
+
+/* Solver::init_with (solver.rs:2474-2605): f = feq(rho, u) + f_neq(grad u)
+ * from sampled fields (rho: ncells, u: ncells x 3), then moments refresh. */
+int lbmb_init_fields(lbmb_solver* h, const double* rho, const double* u);
+
+/* Backend::stage_in / stage_out (backend.rs:146-155): q-major deviation
+ * populations (Q x ncells, f64 view of the storage precision). stage_in
+ * also refreshes the cached moments, like the reference's init path. */
+int lbmb_stage_in(lbmb_solver* h, const double* f);
+int lbmb_stage_out(lbmb_solver* h, double* f);
+
+/* Solver::run (solver.rs:2283-2343): `steps` x {collide, stream, moments}
+ * (+ every enabled passive scalar, solver.rs:2113-2205). */
+int lbmb_step(lbmb_solver* h, int64_t steps);
+
+/* Solver::run_guarded (solver.rs:2346-2356): runs in chunks of check_every
+ * and checks the f64 mass after each; returns LBMB_ERR_DIVERGED with
+ * *completed = steps done at the failing check. */
+int lbmb_run_guarded(lbmb_solver* h, int64_t steps, int64_t check_every, int64_t* completed);
+
+/* Backend::read_moments (backend.rs:355-362): rho and the physical velocity
+ * (with the Guo half-force) of the current state; any pointer may be NULL.
+ * Solid cells report the values they were initialised with. */
+int lbmb_read_moments(lbmb_solver* h, double* rho, double* ux, double* uy, double* uz);
+
+/* Backend::reduce (backend.rs:347-353, 920-970): f64 accumulation over
+ * fluid cells. axis is used by LBMB_RED_MOMENTUM only. */
+int lbmb_reduce(lbmb_solver* h, int32_t kind, int32_t axis, double* out);
+
+/* Solver::total_mass_f64 (solver.rs:5114-5117). */
+int lbmb_total_mass(lbmb_solver* h, double* out);
+
+/* Solver::clear_body_force_field (solver.rs:2805-2822). */
+int lbmb_clear_body_force_field(lbmb_solver* h);
+
+/* Current per-cell force field (ncells x 3, zeros where absent). */
+int lbmb_get_force_field(lbmb_solver* h, double* out);
+
+/* RotatingBody::from_markers (rotating_ibm.rs:32-58): upload body `body`
+ * (0-based slot): n markers at lattice coordinates (n x 3), quadrature
+ * weights, rotation centre and angular velocity (rad/step). */
+int lbmb_ibm_set_body(lbmb_solver* h, int32_t body, const double* pos, const double* weight,
+                      int64_t n, const double center[3], const double omega[3]);
+
+/* Solver::apply_rotating_ibm (solver.rs:3016-3282): direct-forcing sweeps
+ * on the device; the spread is added to the force field and the
+ * diagnostics are returned. diag may be NULL. */
+int lbmb_apply_rotating_ibm(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg,
+                            lbmb_ibm_diag* diag);
+
+/* Solver::enable_scalar_distribution (solver.rs:2856-2890): q = 7 (D3Q7,
+ * cs^2 = 1/4) or the hydro lattice size (the reference's choice). */
+int lbmb_enable_scalar(lbmb_solver* h, int32_t q, double diffusivity, int32_t* index);
+
+/* Solver::set_scalar_concentration (solver.rs:2910-2966). */
+int lbmb_set_scalar_concentration(lbmb_solver* h, int32_t k, const double* c);
+
+/* Solver::gather_scalar_concentration (solver.rs:2892-2908). */
+int lbmb_gather_scalar_concentration(lbmb_solver* h, int32_t k, double* c);
+
+/* qoi::scalar_cv over fluid cells (crates/lbm-core/src/qoi.rs:507-532);
+ * *cv = NaN where the reference returns None. */
+int lbmb_scalar_cv(lbmb_solver* h, int32_t k, double* cv);
+
+/* Runner hot loop (crates/lbm-cli/src/runner.rs:1079-1129) on the device:
+ * `steps` x {clear force field, IBM of `body`, step}, recording per step
+ * torque_lu = -diag.torque[2] (runner.rs:1396-1425), the fluid force
+ * (steps x 3) and the IBM iteration count; and, if scalar >= 0, the scalar
+ * CV every probe_every steps (NaN elsewhere). Any output may be NULL.
+ * The loop is captured in CUDA graphs; nothing syncs to the host inside. */
+int lbmb_run_impeller(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg, int64_t steps,
+                      int32_t scalar, int64_t probe_every, double* torque_lu, double* fluid_force,
+                      double* cv, int32_t* ibm_iterations);
+
+/* Device time of the last lbmb_step / lbmb_run_impeller call in ms (CUDA
+ * events on the solver stream), and the hydro kernel's share of it. */
+int lbmb_last_timing(lbmb_solver* h, double* total_ms, double* hydro_ms, int64_t* hydro_launches);
+
+/* build_wall_rims (crates/lbm-core/src/solver.rs:1357-1404): one-cell solid
+ * rims on the faces with is_wall set (face order XNeg, XPos, YNeg, YPos,
+ * ZNeg, ZPos; u = 6 x 3 wall velocities); corner cells keep the fastest
+ * wall. Outputs solid (ncells) and wall_u (ncells x 3). */
+int lbmb_build_wall_rims(const int32_t dims[3], const int32_t is_wall[6], const double u[18], uint8_t* solid,
+                         double* wall_u);
+
+/* build_stirred_tank_geometry + generate_impeller_marker_set
+ * (crates/lbm-core/src/geometry.rs:207-345, 657-916): voxel flags,
+ * baffle mask, stamped wall velocity (SI) and impeller markers (lattice
+ * coordinates). Call once with marker_pos = marker_weight = NULL to read
+ * *n_markers, then again with capacity >= *n_markers. Outputs may be NULL. */
+int lbmb_build_stirred_tank(const lbmb_tank_spec* spec, uint8_t* solid, uint8_t* baffle_mask,
+                            double* wall_velocity, double* marker_pos, double* marker_weight, int64_t capacity,
+                            int64_t* n_markers, double center[3], double omega[3]);
+
+/* Synchronize the solver stream. */
+int lbmb_sync(lbmb_solver* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBMB_H */

@@ -1,0 +1,412 @@
+"""lbmflow_b200: B200 (sm_100a) LBMFlow single-GPU time step.
+
+Python mirror of the reference's stepping API (lbm-core ``Solver`` over the
+``Backend`` trait) on top of the C ABI in ``include/lbmb.h``. All compute
+runs in ``_build/liblbmb.so`` (hand-written CUDA for sm_100a); there is no
+CPU fallback: every call fails loudly when the library or a CUDA device is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liblbmb.so")
+
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6
+COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
+IMPELLER = {"rushton": 0, "pitched": 1, "flat_blade": 2}
+MAGIC_STD = 3.0 / 16.0
+RED_FLUID_CELLS, RED_MASS_DEV, RED_MOMENTUM = 0, 1, 2
+
+# Symbols the library exports; kept in sync with include/lbmb.h (checked by
+# tests/test_abi.py).
+EXPORTS = (
+    "lbmb_last_error", "lbmb_version", "lbmb_create", "lbmb_destroy", "lbmb_shape", "lbmb_init_fields",
+    "lbmb_stage_in", "lbmb_stage_out", "lbmb_step", "lbmb_run_guarded", "lbmb_read_moments", "lbmb_reduce",
+    "lbmb_total_mass", "lbmb_clear_body_force_field", "lbmb_get_force_field", "lbmb_ibm_set_body",
+    "lbmb_apply_rotating_ibm", "lbmb_enable_scalar", "lbmb_set_scalar_concentration",
+    "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
+    "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync",
+)
+
+
+class LbmbError(RuntimeError):
+    """A failed lbmb call; .code is the lbmb_status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class SpecError(LbmbError, ValueError):
+    """Invalid specification (the reference's SpecError)."""
+
+
+class UnsupportedError(LbmbError):
+    """UnsupportedReason::NotImplemented."""
+
+
+class Diverged(LbmbError):
+    """Non-finite mass detected by run_guarded; .completed steps ran."""
+
+    def __init__(self, code, msg, completed):
+        super().__init__(code, msg)
+        self.completed = completed
+
+
+class _Config(C.Structure):
+    _fields_ = [("lattice", C.c_int32), ("collision", C.c_int32), ("storage", C.c_int32),
+                ("dims", C.c_int32 * 3), ("periodic", C.c_int32 * 3), ("device", C.c_int32),
+                ("nu", C.c_double), ("magic", C.c_double), ("omega_shear", C.c_double),
+                ("force", C.c_double * 3)]
+
+
+class _IbmConfig(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("slip_tolerance", C.c_double),
+                ("kernel_radius", C.c_int32), ("relaxation", C.c_double)]
+
+
+class _IbmDiag(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("slip_max", C.c_double), ("slip_rms", C.c_double),
+                ("slip_max_rel", C.c_double), ("slip_rms_rel", C.c_double), ("torque", C.c_double * 3),
+                ("fluid_force", C.c_double * 3), ("marker_force", C.c_double * 3),
+                ("momentum_error_rel", C.c_double)]
+
+
+class _TankSpec(C.Structure):
+    _fields_ = [("dims", C.c_int32 * 3), ("dx_m", C.c_double), ("vessel_diameter_m", C.c_double),
+                ("liquid_height_m", C.c_double), ("baffle_count", C.c_int32),
+                ("baffle_width_m", C.c_double), ("baffle_thickness_m", C.c_double),
+                ("impeller_kind", C.c_int32), ("impeller_diameter_m", C.c_double),
+                ("clearance_m", C.c_double), ("blade_count", C.c_int32), ("omega_rad_s", C.c_double),
+                ("marker_spacing_cells", C.c_double), ("min_cells", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it was never built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"lbmflow_b200 CUDA library not built: {LIB_PATH} (run lbmflow_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        L.lbmb_last_error.restype = C.c_char_p
+        L.lbmb_version.restype = C.c_char_p
+        L.lbmb_create.argtypes = [C.POINTER(_Config), _u8p, _dp, C.POINTER(C.c_void_p)]
+        vp = C.c_void_p
+        L.lbmb_destroy.argtypes = [vp]
+        L.lbmb_shape.argtypes = [vp, _i64p, _i32p]
+        L.lbmb_init_fields.argtypes = [vp, _dp, _dp]
+        L.lbmb_stage_in.argtypes = [vp, _dp]
+        L.lbmb_stage_out.argtypes = [vp, _dp]
+        L.lbmb_step.argtypes = [vp, C.c_int64]
+        L.lbmb_run_guarded.argtypes = [vp, C.c_int64, C.c_int64, _i64p]
+        L.lbmb_read_moments.argtypes = [vp, _dp, _dp, _dp, _dp]
+        L.lbmb_reduce.argtypes = [vp, C.c_int32, C.c_int32, _dp]
+        L.lbmb_total_mass.argtypes = [vp, _dp]
+        L.lbmb_clear_body_force_field.argtypes = [vp]
+        L.lbmb_get_force_field.argtypes = [vp, _dp]
+        L.lbmb_ibm_set_body.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int64, _dp, _dp]
+        L.lbmb_apply_rotating_ibm.argtypes = [vp, C.c_int32, C.POINTER(_IbmConfig), C.POINTER(_IbmDiag)]
+        L.lbmb_enable_scalar.argtypes = [vp, C.c_int32, C.c_double, _i32p]
+        L.lbmb_set_scalar_concentration.argtypes = [vp, C.c_int32, _dp]
+        L.lbmb_gather_scalar_concentration.argtypes = [vp, C.c_int32, _dp]
+        L.lbmb_scalar_cv.argtypes = [vp, C.c_int32, _dp]
+        L.lbmb_run_impeller.argtypes = [vp, C.c_int32, C.POINTER(_IbmConfig), C.c_int64, C.c_int32,
+                                        C.c_int64, _dp, _dp, _dp, _i32p]
+        L.lbmb_last_timing.argtypes = [vp, _dp, _dp, _i64p]
+        L.lbmb_build_wall_rims.argtypes = [_i32p, _i32p, _dp, _u8p, _dp]
+        L.lbmb_build_stirred_tank.argtypes = [C.POINTER(_TankSpec), _u8p, _u8p, _dp, _dp, _dp, C.c_int64,
+                                              _i64p, _dp, _dp]
+        L.lbmb_sync.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc, completed=None):
+    if rc == OK:
+        return
+    msg = lib().lbmb_last_error().decode()
+    if rc == ERR_INVALID:
+        raise SpecError(rc, msg)
+    if rc == ERR_UNSUPPORTED:
+        raise UnsupportedError(rc, msg)
+    if rc == ERR_DIVERGED:
+        raise Diverged(rc, msg, completed)
+    raise LbmbError(rc, msg)
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+@dataclass
+class DirectForcingConfig:
+    """rotating_ibm.rs:106-130 (defaults: 3 sweeps, tol 1e-2, radius 1, relax 1)."""
+    max_iterations: int = 3
+    slip_tolerance: float = 1.0e-2
+    kernel_radius: int = 1
+    relaxation: float = 1.0
+
+    def _c(self):
+        return _IbmConfig(self.max_iterations, self.slip_tolerance, self.kernel_radius, self.relaxation)
+
+
+@dataclass
+class IbmDiagnostics:
+    """rotating_ibm.rs:134-153."""
+    iterations: int
+    slip_max: float
+    slip_rms: float
+    slip_max_rel: float
+    slip_rms_rel: float
+    torque: np.ndarray
+    fluid_force: np.ndarray
+    marker_force: np.ndarray
+    momentum_error_rel: float
+
+
+@dataclass
+class RotatingBody:
+    """rotating_ibm.rs:24-102: markers at lattice coordinates, Omega x r target."""
+    center: np.ndarray
+    omega: np.ndarray
+    positions: np.ndarray  # (n, 3)
+    weights: np.ndarray  # (n,)
+
+    def __post_init__(self):
+        self.center = _f64(self.center, 3)
+        self.omega = _f64(self.omega, 3)
+        self.positions = _f64(self.positions).reshape(-1, 3)
+        self.weights = _f64(self.weights).ravel()
+
+    @staticmethod
+    def circle_2d(center, radius, omega_z, n_markers, z=0.0):
+        th = 2.0 * np.pi * np.arange(n_markers) / n_markers
+        pos = np.stack([center[0] + radius * np.cos(th), center[1] + radius * np.sin(th),
+                        np.full(n_markers, z)], axis=1)
+        w = np.full(n_markers, 2.0 * np.pi * radius / n_markers)
+        return RotatingBody([center[0], center[1], z], [0.0, 0.0, omega_z], pos, w)
+
+
+class Solver:
+    """One device solver (Solver<L, T, B, H>, crates/lbm-core/src/solver.rs:1503)."""
+
+    def __init__(self, dims, lattice=19, collision="trt", storage="f32", nu=1.0 / 6.0, magic=MAGIC_STD,
+                 omega_shear=None, periodic=(False, False, False), force=(0.0, 0.0, 0.0), solid=None,
+                 wall_u=None, device=0):
+        L = lib()
+        self.dims = tuple(int(d) for d in dims)
+        self.n = self.dims[0] * self.dims[1] * self.dims[2]
+        self.q = int(lattice)
+        if omega_shear is None:
+            omega_shear = 1.0 / (3.0 * nu + 0.5)
+        cfg = _Config(int(lattice), COLLISION[collision], STORAGE[storage], (C.c_int32 * 3)(*self.dims),
+                      (C.c_int32 * 3)(*[int(bool(p)) for p in periodic]), int(device), float(nu),
+                      float(magic), float(omega_shear), (C.c_double * 3)(*[float(f) for f in force]))
+        self._solid = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8).ravel()
+        if self._solid is not None and self._solid.size != self.n:
+            raise ValueError("solid mask size does not match the grid")
+        self._wall = None if wall_u is None else _f64(wall_u, 3 * self.n)
+        h = C.c_void_p()
+        _check(L.lbmb_create(C.byref(cfg), None if self._solid is None else self._solid.ctypes.data_as(_u8p),
+                             _d(self._wall), C.byref(h)))
+        self.h = h
+        self._bodies = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lbmb_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    # --- state ------------------------------------------------------------
+    def init_with(self, rho, u):
+        _check(lib().lbmb_init_fields(self.h, _d(_f64(rho, self.n)), _d(_f64(u, 3 * self.n))))
+
+    def stage_in(self, f):
+        _check(lib().lbmb_stage_in(self.h, _d(_f64(f, self.q * self.n))))
+
+    def stage_out(self):
+        out = np.empty(self.q * self.n)
+        _check(lib().lbmb_stage_out(self.h, _d(out)))
+        return out.reshape(self.q, self.n)
+
+    # --- stepping ---------------------------------------------------------
+    def step(self):
+        self.run(1)
+
+    def run(self, steps):
+        _check(lib().lbmb_step(self.h, int(steps)))
+
+    def run_guarded(self, steps, check_every):
+        done = C.c_int64(0)
+        rc = lib().lbmb_run_guarded(self.h, int(steps), int(check_every), C.byref(done))
+        _check(rc, completed=done.value)
+        return done.value
+
+    def sync(self):
+        _check(lib().lbmb_sync(self.h))
+
+    def last_timing(self):
+        t, hy, k = C.c_double(), C.c_double(), C.c_int64()
+        _check(lib().lbmb_last_timing(self.h, C.byref(t), C.byref(hy), C.byref(k)))
+        return t.value, hy.value, k.value
+
+    # --- readback -----------------------------------------------------------
+    def read_moments(self):
+        out = [np.empty(self.n) for _ in range(4)]
+        _check(lib().lbmb_read_moments(self.h, *[_d(a) for a in out]))
+        return out
+
+    def reduce(self, kind, axis=0):
+        v = C.c_double()
+        _check(lib().lbmb_reduce(self.h, int(kind), int(axis), C.byref(v)))
+        return v.value
+
+    def total_mass_f64(self):
+        v = C.c_double()
+        _check(lib().lbmb_total_mass(self.h, C.byref(v)))
+        return v.value
+
+    def total_momentum(self):
+        return np.array([self.reduce(RED_MOMENTUM, a) for a in range(3)])
+
+    # --- forcing / IBM ------------------------------------------------------
+    def clear_body_force_field(self):
+        _check(lib().lbmb_clear_body_force_field(self.h))
+
+    def force_field(self):
+        out = np.empty(3 * self.n)
+        _check(lib().lbmb_get_force_field(self.h, _d(out)))
+        return out.reshape(self.n, 3)
+
+    def set_body(self, slot, body: RotatingBody):
+        _check(lib().lbmb_ibm_set_body(self.h, int(slot), _d(body.positions), _d(body.weights),
+                                       body.weights.size, _d(body.center), _d(body.omega)))
+        self._bodies[slot] = body
+
+    def _slot_for(self, body):
+        for k, b in self._bodies.items():
+            if b is body:
+                return k
+        slot = len(self._bodies)
+        self.set_body(slot, body)
+        return slot
+
+    def apply_rotating_ibm(self, body: RotatingBody, cfg: DirectForcingConfig = None) -> IbmDiagnostics:
+        cfg = cfg or DirectForcingConfig()
+        d = _IbmDiag()
+        _check(lib().lbmb_apply_rotating_ibm(self.h, self._slot_for(body), C.byref(cfg._c()), C.byref(d)))
+        return IbmDiagnostics(d.iterations, d.slip_max, d.slip_rms, d.slip_max_rel, d.slip_rms_rel,
+                              np.array(d.torque[:]), np.array(d.fluid_force[:]), np.array(d.marker_force[:]),
+                              d.momentum_error_rel)
+
+    def run_impeller(self, body: RotatingBody, steps, cfg: DirectForcingConfig = None, scalar=-1,
+                     probe_every=1):
+        """Runner hot loop (runner.rs:1079-1129) on the device."""
+        cfg = cfg or DirectForcingConfig()
+        torque = np.empty(steps)
+        ff = np.empty(3 * steps)
+        iters = np.empty(steps, dtype=np.int32)
+        cv = np.full(steps, np.nan) if scalar >= 0 else None
+        _check(lib().lbmb_run_impeller(self.h, self._slot_for(body), C.byref(cfg._c()), int(steps), int(scalar),
+                                       int(probe_every), _d(torque), _d(ff), _d(cv),
+                                       iters.ctypes.data_as(_i32p)))
+        return {"torque_lu": torque, "fluid_force": ff.reshape(steps, 3), "ibm_iterations": iters, "cv": cv}
+
+    # --- passive scalar -----------------------------------------------------
+    def enable_scalar_distribution(self, diffusivity, q=None):
+        k = C.c_int32()
+        _check(lib().lbmb_enable_scalar(self.h, int(self.q if q is None else q), float(diffusivity),
+                                        C.byref(k)))
+        return k.value
+
+    def set_scalar_concentration(self, k, values):
+        _check(lib().lbmb_set_scalar_concentration(self.h, int(k), _d(_f64(values, self.n))))
+
+    def gather_scalar_concentration(self, k):
+        out = np.empty(self.n)
+        _check(lib().lbmb_gather_scalar_concentration(self.h, int(k), _d(out)))
+        return out
+
+    def scalar_cv(self, k):
+        v = C.c_double()
+        _check(lib().lbmb_scalar_cv(self.h, int(k), C.byref(v)))
+        return None if np.isnan(v.value) else v.value
+
+
+def build_wall_rims(dims, is_wall, wall_u):
+    dims = [int(d) for d in dims]
+    n = dims[0] * dims[1] * dims[2]
+    solid = np.empty(n, dtype=np.uint8)
+    wu = np.empty(3 * n)
+    u = _f64(wall_u, 18)
+    _check(lib().lbmb_build_wall_rims((C.c_int32 * 3)(*dims), (C.c_int32 * 6)(*[int(bool(w)) for w in is_wall]),
+                                      _d(u), solid.ctypes.data_as(_u8p), _d(wu)))
+    return solid, wu.reshape(n, 3)
+
+
+@dataclass
+class TankSpec:
+    """Stirred-tank set-up in SI units (geometry.rs:84-132)."""
+    dims: tuple
+    dx_m: float
+    vessel_diameter_m: float
+    liquid_height_m: float
+    impeller_diameter_m: float
+    clearance_m: float
+    omega_rad_s: float
+    blade_count: int = 6
+    impeller: str = "rushton"
+    baffle_count: int = 0
+    baffle_width_m: float = 0.0
+    baffle_thickness_m: float = 0.0
+    marker_spacing_cells: float = 0.7
+    min_cells: float = 32.0
+
+    def _c(self):
+        return _TankSpec((C.c_int32 * 3)(*self.dims), self.dx_m, self.vessel_diameter_m, self.liquid_height_m,
+                         self.baffle_count, self.baffle_width_m, self.baffle_thickness_m,
+                         IMPELLER[self.impeller], self.impeller_diameter_m, self.clearance_m, self.blade_count,
+                         self.omega_rad_s, self.marker_spacing_cells, self.min_cells)
+
+
+def build_stirred_tank(spec: TankSpec):
+    L = lib()
+    c = spec._c()
+    n = spec.dims[0] * spec.dims[1] * spec.dims[2]
+    m = C.c_int64()
+    _check(L.lbmb_build_stirred_tank(C.byref(c), None, None, None, None, None, 0, C.byref(m), None, None))
+    solid = np.empty(n, dtype=np.uint8)
+    baffle = np.empty(n, dtype=np.uint8)
+    wv = np.empty(3 * n)
+    pos = np.empty(3 * m.value)
+    w = np.empty(m.value)
+    center = np.empty(3)
+    omega = np.empty(3)
+    _check(L.lbmb_build_stirred_tank(C.byref(c), solid.ctypes.data_as(_u8p), baffle.ctypes.data_as(_u8p),
+                                     _d(wv), _d(pos), _d(w), m.value, C.byref(m), _d(center), _d(omega)))
+    return {"solid": solid, "baffle": baffle, "wall_velocity": wv.reshape(n, 3),
+            "marker_pos": pos.reshape(-1, 3), "marker_w": w, "center": center, "omega": omega}

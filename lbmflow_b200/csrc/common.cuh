@@ -1,0 +1,84 @@
+// Shared device definitions: cell flags, storage codecs, small helpers.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace lbmb {
+
+// Per-cell flag byte (one byte per cell, the only per-cell array every
+// cell reads besides its populations).
+enum : uint8_t {
+  F_SOLID = 1,     // half-way bounce-back obstacle / wall rim
+  F_BOUNDARY = 2,  // fluid cell with >= 1 solid neighbour: read nbr mask
+  F_MOVING = 4,    // ... and >= 1 of them has a nonzero wall velocity
+  F_FORCED = 8,    // fluid cell inside an IBM stencil: read force slots
+};
+
+// Storage codecs: populations are stored as S and computed in A.
+template <class S>
+struct Codec;
+
+template <>
+struct Codec<float> {
+  using A = float;
+  __device__ __forceinline__ static float ld(const float* p) { return *p; }
+  __device__ __forceinline__ static void st(float* p, float v) { *p = v; }
+};
+
+template <>
+struct Codec<double> {
+  using A = double;
+  __device__ __forceinline__ static double ld(const double* p) { return *p; }
+  __device__ __forceinline__ static void st(double* p, double v) { *p = v; }
+};
+
+template <>
+struct Codec<__half> {
+  using A = float;
+  __device__ __forceinline__ static float ld(const __half* p) { return __half2float(*p); }
+  __device__ __forceinline__ static void st(__half* p, float v) { *p = __float2half_rn(v); }
+};
+
+template <>
+struct Codec<__nv_bfloat16> {
+  using A = float;
+  __device__ __forceinline__ static float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+  __device__ __forceinline__ static void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+// Force slot / wall velocity records (x, y, z, pad) in the arithmetic type.
+template <class A>
+struct Vec4 {
+  A x, y, z, w;
+};
+
+// Periodic-wrap neighbour addressing for a cell at (x, y, z). Non-periodic
+// faces are full solid rims (validated on the host), so the wrap is only
+// ever taken by periodic axes; it never leaves the grid either way.
+struct Nbr {
+  int64_t zr[3];  // z rows (z-1, z, z+1) * ny
+  int ys[3];
+  int xs[3];
+  int nx;
+  __device__ __forceinline__ Nbr(int x, int y, int z, int nx_, int ny, int nz) : nx(nx_) {
+    xs[0] = x == 0 ? nx_ - 1 : x - 1;
+    xs[1] = x;
+    xs[2] = x == nx_ - 1 ? 0 : x + 1;
+    ys[0] = y == 0 ? ny - 1 : y - 1;
+    ys[1] = y;
+    ys[2] = y == ny - 1 ? 0 : y + 1;
+    const int z0 = z == 0 ? nz - 1 : z - 1;
+    const int z2 = z == nz - 1 ? 0 : z + 1;
+    zr[0] = int64_t(z0) * ny;
+    zr[1] = int64_t(z) * ny;
+    zr[2] = int64_t(z2) * ny;
+  }
+  __device__ __forceinline__ int64_t at(int dx, int dy, int dz) const {
+    return (zr[dz + 1] + ys[dy + 1]) * int64_t(nx) + xs[dx + 1];
+  }
+};
+
+}  // namespace lbmb
