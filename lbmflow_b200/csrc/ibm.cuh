@@ -354,6 +354,7 @@ __global__ void ibm_commit_kernel(IbmArgs a, Vec4<A>* fcur, double* series_torqu
     if (series_ff)
       for (int c = 0; c < 3; ++c) series_ff[3 * s + c] = a.diag->fluid_force[c];
     if (series_iters) series_iters[s] = a.diag->iterations;
+    *step_counter = s + 1;
   }
 }
 
