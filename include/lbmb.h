@@ -215,6 +215,27 @@ int lbmb_build_stirred_tank(const lbmb_tank_spec* spec, uint8_t* solid, uint8_t*
                             double* wall_velocity, double* marker_pos, double* marker_weight, int64_t capacity,
                             int64_t* n_markers, double center[3], double omega[3]);
 
+/* No counterpart in the reference. The f64 reduction of lbmb_reduce over
+ * populations the caller already holds in device memory, for callers that
+ * cannot allocate device memory while they run (an application that owns
+ * every device byte through its own arena, a process under a hard memory
+ * quota, a stepping loop that must not call cudaMalloc/cudaFree). It
+ * allocates nothing: its block partials live in a fixed file-scope device
+ * array of about 640 KiB that every device loading this library keeps
+ * until exit.
+ *   f:      device, q-major populations f[q * plane + cell] (normal layout),
+ *           element type per `storage`; plane >= ncells.
+ *   solid:  device, ncells bytes (nonzero = solid, skipped), or NULL.
+ *   force:  host, uniform body force for the F/2 momentum term, or NULL.
+ *   out:    host, {fluid cells, sum f_dev, momentum x, y, z}.
+ *   stream: cudaStream_t to run on (NULL: the legacy default stream).
+ * ncells above 33,554,432 (2^25) is rejected with LBMB_ERR_INVALID. The
+ * first call on a device looks up the array's device address (make it
+ * before any stream capture). Calls share the array: calls that overlap on
+ * the GPU race and must be serialized by the caller. */
+int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, int64_t ncells, int64_t plane,
+                                    const uint8_t* solid, const double force[3], double out[5], void* stream);
+
 /* Synchronize the solver stream. */
 int lbmb_sync(lbmb_solver* h);
 

@@ -37,7 +37,7 @@ EXPORTS = (
     "lbmb_total_mass", "lbmb_clear_body_force_field", "lbmb_get_force_field", "lbmb_ibm_set_body",
     "lbmb_apply_rotating_ibm", "lbmb_enable_scalar", "lbmb_set_scalar_concentration",
     "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
-    "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync",
+    "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
 )
 
 
@@ -132,6 +132,8 @@ def lib():
         L.lbmb_build_stirred_tank.argtypes = [C.POINTER(_TankSpec), _u8p, _u8p, _dp, _dp, _dp, C.c_int64,
                                               _i64p, _dp, _dp]
         L.lbmb_sync.argtypes = [vp]
+        L.lbmb_reduce_populations_noalloc.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, vp, _dp,
+                                                      _dp, vp]
         _lib = L
     return _lib
 

@@ -34,7 +34,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    units = [os.path.join(SRC, "solver.cu"), os.path.join(SRC, "host_geometry.cpp")]
+    units = [os.path.join(SRC, "solver.cu"), os.path.join(SRC, "host_geometry.cpp"), os.path.join(SRC, "noalloc.cu")]
     cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + units
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
