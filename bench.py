@@ -175,7 +175,7 @@ def barrier(world):
 def run_b200(args, rank, world, local):
     import lbmflow_b200 as lb
 
-    dims, solid, body, nu = tank_case()
+    dims, solid, body, nu = tank_case(T=args.tank_T)
     q, coll, storage = 27, "cm", args.storage
     os_ = 1.0 / (3.0 * nu + 0.5)
     n_cells = dims[0] * dims[1] * dims[2]
@@ -279,7 +279,7 @@ def run_b200(args, rank, world, local):
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    dims, solid, body, nu = tank_case()
+    dims, solid, body, nu = tank_case(T=args.tank_T)
     steps = max(1, min(args.steps, args.cpu_steps))
     mlups, dt = cpu_tank_sample(dims, solid, body, nu, steps=steps, warmup=1)
     return {"impl": "reference", "metric": "MLUPS (stirred-tank runner step, D3Q27 central moment, fp32 populations)",
@@ -303,6 +303,7 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--hydro-steps", type=int, default=200)
     ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--tank-T", type=int, default=128, help="tank diameter in cells (128 = the benchmark case)")
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--variants", type=int, default=1)

@@ -15,6 +15,7 @@ enum : uint8_t {
   F_BOUNDARY = 2,  // fluid cell with >= 1 solid neighbour: read nbr mask
   F_MOVING = 4,    // ... and >= 1 of them has a nonzero wall velocity
   F_FORCED = 8,    // fluid cell inside an IBM stencil: read force slots
+  F_WRAP = 16,     // fluid cell on a periodic face: neighbours wrap around
 };
 
 // Storage codecs: populations are stored as S and computed in A.

@@ -18,6 +18,15 @@
 // collision population aimed at a solid neighbour is written back bounced
 // (plus the moving-wall term) into the slot the next step reads for the
 // reflected direction, which is exactly the reference's bounce-back value.
+//
+// Cells are split by their flag byte into three code paths:
+//   interior  (no solid neighbour, not on a periodic face): neighbour
+//             offsets are compile-time combinations of 1, nx and nx*ny;
+//   generic   (solid neighbours and/or periodic wrap): mask and wrap logic;
+//   forced    (inside an IBM stencil): handled by hydro_cells_kernel over the
+//             compact forced-cell list, after the IBM force update, unless a
+//             uniform body force makes every cell forced.
+// Element offsets q * plane + cell are 32-bit (checked on the host).
 #pragma once
 #include "common.cuh"
 #include "lattice.cuh"
@@ -29,7 +38,7 @@ enum { COLL_TRT = 0, COLL_CM = 1 };
 template <class A>
 struct HydroParams {
   void* f;                // Q planes of the storage type
-  int64_t plane;          // elements per plane
+  uint32_t plane;         // elements per plane
   const uint8_t* flags;   // per cell
   const uint32_t* nbr;    // per cell: bit q set <=> x + c_q is solid
   const Vec4<A>* wall_u;  // per cell (meaningful on solids)
@@ -37,6 +46,7 @@ struct HydroParams {
   const Vec4<A>* fprev;   // per slot: field inside the cached moments
   const Vec4<A>* fcur;    // per slot: current field (Guo source)
   int nx, ny, nz;
+  int nxy;
   A omega_p, omega_m, cp, cm, omega_shear;
   A gx, gy, gz;  // uniform body force
   int uniform_force;
@@ -45,38 +55,42 @@ struct HydroParams {
 // TRT + Guo (crates/lbm-core/src/collision.rs:123-202), BGK when
 // omega_m == omega_p. Same operand grouping as the reference; the compiler
 // may contract a*b+c into one fused rounding.
-template <int Q, class A>
-__device__ __forceinline__ void collide_trt(A (&f)[Q], A rho, A ux, A uy, A uz, A Fx, A Fy, A Fz,
-                                            bool forced, A op, A om, A cp, A cm) {
+template <int Q, bool FORCED, class A>
+__device__ __forceinline__ void collide_trt(A (&f)[Q], A rho, A ux, A uy, A uz, A Fx, A Fy, A Fz, A op, A om,
+                                            A cp, A cm) {
   using L = Lat<Q>;
   const A usq = (ux * ux + uy * uy) + uz * uz;
   const A uf = (ux * Fx + uy * Fy) + uz * Fz;
   const A drho = rho - A(1);
-  A feq[Q], src[Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
+  auto feq = [&](int q) {
     const A cu = (A(L::cx(q)) * ux + A(L::cy(q)) * uy) + A(L::cz(q)) * uz;
     const A inner = (A(3) * cu + (A(4.5) * cu) * cu) - A(1.5) * usq;
-    feq[q] = A(L::w(q)) * (drho + rho * inner);
-    if (forced) {
-      const A cf = (A(L::cx(q)) * Fx + A(L::cy(q)) * Fy) + A(L::cz(q)) * Fz;
-      src[q] = A(L::w(q)) * (A(3) * (cf - uf) + (A(9) * cu) * cf);
-    } else {
-      src[q] = A(0);
-    }
+    return A(L::w(q)) * (drho + rho * inner);
+  };
+  auto src = [&](int q) {
+    const A cu = (A(L::cx(q)) * ux + A(L::cy(q)) * uy) + A(L::cz(q)) * uz;
+    const A cf = (A(L::cx(q)) * Fx + A(L::cy(q)) * Fy) + A(L::cz(q)) * Fz;
+    return A(L::w(q)) * (A(3) * (cf - uf) + (A(9) * cu) * cf);
+  };
+  {
+    const A e0 = feq(0);
+    A v = f[0] - op * (f[0] - e0);
+    if (FORCED) v = v + cp * src(0);
+    f[0] = v;
   }
-  f[0] = (f[0] - op * (f[0] - feq[0])) + cp * src[0];
   const A half = A(0.5);
 #pragma unroll
   for (int p = 0; p < L::NPAIR; ++p) {
     const int qa = 2 * p + 1, qb = 2 * p + 2;
     const A fa = f[qa], fb = f[qb];
+    const A ea = feq(qa), eb = feq(qb);
     const A fp = half * (fa + fb), fm = half * (fa - fb);
-    const A ep = half * (feq[qa] + feq[qb]), em = half * (feq[qa] - feq[qb]);
+    const A ep = half * (ea + eb), em = half * (ea - eb);
     const A rp = op * (fp - ep), rm = om * (fm - em);
     A va = (fa - rp) - rm, vb = (fb - rp) + rm;
-    if (forced) {
-      const A sp = half * (src[qa] + src[qb]), sm = half * (src[qa] - src[qb]);
+    if (FORCED) {
+      const A sa = src(qa), sb = src(qb);
+      const A sp = half * (sa + sb), sm = half * (sa - sb);
       const A cps = cp * sp, cms = cm * sm;
       va = va + (cps + cms);
       vb = vb + (cps - cms);
@@ -112,6 +126,22 @@ __device__ __forceinline__ void cm_bwd(A& k0, A& k1, A& k2, A u) {
   k2 = fp;
 }
 
+template <class A>
+__device__ __forceinline__ void cm_fwd_all(A (&K)[3][3][3], A ux, A uy, A uz) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) cm_fwd(K[i][j][0], K[i][j][1], K[i][j][2], uz);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_fwd(K[i][0][k], K[i][1][k], K[i][2][k], uy);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_fwd(K[0][j][k], K[1][j][k], K[2][j][k], ux);
+}
+
 // D3Q27 central-moment collision with Guo forcing (kernels.rs:406-533), in
 // the arithmetic type. Post-collision moments are the reference's: order
 // 0/1 keep the population moments (+ the source), order-2 deviatoric
@@ -119,12 +149,11 @@ __device__ __forceinline__ void cm_bwd(A& k0, A& k1, A& k2, A u) {
 // and all higher moments relax at 1, the source enters with (1 - rate/2).
 // By linearity the update is applied to the non-equilibrium part:
 //   f_out = f + T^-1 [ -R T(f - feq) + (I - R/2) T(src) ].
-template <int Q, class A>
-__device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A Fx, A Fy, A Fz,
-                                           bool forced, A omega_shear) {
+template <int Q, bool FORCED, class A>
+__device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A Fx, A Fy, A Fz, A omega_shear) {
   static_assert(Q == 27, "factorised central-moment collision needs the full D3Q27 tensor basis");
   using L = Lat<Q>;
-  if (!forced && ux == A(0) && uy == A(0) && uz == A(0)) {
+  if (!FORCED && ux == A(0) && uy == A(0) && uz == A(0)) {
     // Exact-rest skip (kernels.rs:434-447): leave f untouched when every
     // population equals w (rho - 1) bitwise in the storage precision.
     bool exact = true;
@@ -135,44 +164,17 @@ __device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A
   const A usq = (ux * ux + uy * uy) + uz * uz;
   const A drho = rho - A(1);
   A K[3][3][3];
-  A S[3][3][3];
-  const A uf = (ux * Fx + uy * Fy) + uz * Fz;
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const A cu = (A(L::cx(q)) * ux + A(L::cy(q)) * uy) + A(L::cz(q)) * uz;
     const A inner = (A(3) * cu + (A(4.5) * cu) * cu) - A(1.5) * usq;
-    const A feq = A(L::w(q)) * (drho + rho * inner);
-    K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = f[q] - feq;
-    if (forced) {
-      const A cf = (A(L::cx(q)) * Fx + A(L::cy(q)) * Fy) + A(L::cz(q)) * Fz;
-      S[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = A(L::w(q)) * (A(3) * (cf - uf) + (A(9) * cu) * cf);
-    }
+    K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = f[q] - A(L::w(q)) * (drho + rho * inner);
   }
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      cm_fwd(K[i][j][0], K[i][j][1], K[i][j][2], uz);
-      if (forced) cm_fwd(S[i][j][0], S[i][j][1], S[i][j][2], uz);
-    }
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      cm_fwd(K[i][0][k], K[i][1][k], K[i][2][k], uy);
-      if (forced) cm_fwd(S[i][0][k], S[i][1][k], S[i][2][k], uy);
-    }
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      cm_fwd(K[0][j][k], K[1][j][k], K[2][j][k], ux);
-      if (forced) cm_fwd(S[0][j][k], S[1][j][k], S[2][j][k], ux);
-    }
-  // K[a][b][c] now holds the central moment with exponents (a, b, c).
+  cm_fwd_all(K, ux, uy, uz);
+  // K[a][b][c] now holds the non-equilibrium central moment (a, b, c);
+  // overwrite it with the post-collision increment.
   const A os = fmin(omega_shear * (A(1) + A(-0.16) * usq), A(2));
   const A bulk_neq = (K[2][0][0] + K[0][2][0] + K[0][0][2]) * A(1.0 / 3.0);
-  A D[3][3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -182,18 +184,22 @@ __device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A
         const int order = a + b + c;
         const bool diag = order == 2 && (a == 2 || b == 2 || c == 2);
         A d;
-        if (order <= 1) {
-          d = A(0);
-        } else if (diag) {
-          d = -os * (K[a][b][c] - bulk_neq) - bulk_neq;
-        } else if (order == 2) {
-          d = -os * K[a][b][c];
-        } else {
-          d = -K[a][b][c];
-        }
-        D[a][b][c] = d;
+        if (order <= 1) d = A(0);
+        else if (diag) d = -os * (K[a][b][c] - bulk_neq) - bulk_neq;
+        else if (order == 2) d = -os * K[a][b][c];
+        else d = -K[a][b][c];
+        K[a][b][c] = d;
       }
-  if (forced) {
+  if (FORCED) {
+    A S[3][3][3];
+    const A uf = (ux * Fx + uy * Fy) + uz * Fz;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const A cu = (A(L::cx(q)) * ux + A(L::cy(q)) * uy) + A(L::cz(q)) * uz;
+      const A cf = (A(L::cx(q)) * Fx + A(L::cy(q)) * Fy) + A(L::cz(q)) * Fz;
+      S[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = A(L::w(q)) * (A(3) * (cf - uf) + (A(9) * cu) * cf);
+    }
+    cm_fwd_all(S, ux, uy, uz);
     const A bulk_src = (S[2][0][0] + S[0][2][0] + S[0][0][2]) * A(1.0 / 3.0);
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -208,47 +214,66 @@ __device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A
           else if (diag) s = A(0.5) * bulk_src + (A(1) - A(0.5) * os) * (S[a][b][c] - bulk_src);
           else if (order == 2) s = (A(1) - A(0.5) * os) * S[a][b][c];
           else s = A(0.5) * S[a][b][c];
-          D[a][b][c] = D[a][b][c] + s;
+          K[a][b][c] = K[a][b][c] + s;
         }
   }
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) cm_bwd(D[0][j][k], D[1][j][k], D[2][j][k], ux);
+    for (int k = 0; k < 3; ++k) cm_bwd(K[0][j][k], K[1][j][k], K[2][j][k], ux);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) cm_bwd(D[i][0][k], D[i][1][k], D[i][2][k], uy);
+    for (int k = 0; k < 3; ++k) cm_bwd(K[i][0][k], K[i][1][k], K[i][2][k], uy);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) cm_bwd(D[i][j][0], D[i][j][1], D[i][j][2], uz);
+    for (int j = 0; j < 3; ++j) cm_bwd(K[i][j][0], K[i][j][1], K[i][j][2], uz);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) f[q] = f[q] + D[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1];
+  for (int q = 0; q < Q; ++q) f[q] = f[q] + K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1];
 }
 
-// Cell-local part shared by the full-grid and the cell-list kernels.
-template <int Q, class S, int COLL, bool ODD>
-__device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::A>& p, int x, int y,
-                                           int z, int64_t cell, uint8_t fl) {
+// One cell. GENERIC: solid-neighbour mask, moving walls and periodic wrap;
+// otherwise the interior fast path. FORCED: Guo source from the uniform
+// force and, on F_FORCED cells, the force slots.
+template <int Q, class S, int COLL, bool ODD, bool GENERIC, bool FORCED>
+__device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::A>& p, int x, int y, int z,
+                                           uint32_t cell, uint8_t fl) {
   using A = typename Codec<S>::A;
   using L = Lat<Q>;
   using CD = Codec<S>;
-  const Nbr nb(x, y, z, p.nx, p.ny, p.nz);
-  const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
   S* fb = static_cast<S*>(p.f);
-  const int64_t pl = p.plane;
+  const uint32_t pl = p.plane;
+  const int nx = p.nx, nxy = p.nxy;
+  uint32_t mask = 0u;
+  int xs[3], ys[3], zs[3];
+  if (GENERIC) {
+    mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
+    xs[0] = x == 0 ? p.nx - 1 : x - 1;
+    xs[1] = x;
+    xs[2] = x == p.nx - 1 ? 0 : x + 1;
+    ys[0] = y == 0 ? p.ny - 1 : y - 1;
+    ys[1] = y;
+    ys[2] = y == p.ny - 1 ? 0 : y + 1;
+    zs[0] = z == 0 ? p.nz - 1 : z - 1;
+    zs[1] = z;
+    zs[2] = z == p.nz - 1 ? 0 : z + 1;
+  }
+  auto nidx = [&](int dx, int dy, int dz) -> uint32_t {
+    if (GENERIC) return (uint32_t(zs[dz + 1]) * uint32_t(p.ny) + uint32_t(ys[dy + 1])) * uint32_t(nx) + uint32_t(xs[dx + 1]);
+    return cell + uint32_t(dx + dy * nx + dz * nxy);
+  };
   A f[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if (!ODD) {
-      f[q] = CD::ld(fb + q * pl + cell);
+      f[q] = CD::ld(fb + (q * pl + cell));
     } else {
       const int o = opp(q);
-      if ((mask >> o) & 1u)
-        f[q] = CD::ld(fb + q * pl + cell);
+      if (GENERIC && ((mask >> o) & 1u))
+        f[q] = CD::ld(fb + (q * pl + cell));
       else
-        f[q] = CD::ld(fb + o * pl + nb.at(-L::cx(q), -L::cy(q), -L::cz(q)));
+        f[q] = CD::ld(fb + (o * pl + nidx(-L::cx(q), -L::cy(q), -L::cz(q))));
     }
   }
   // Moments (kernels.rs:627-668): rho = 1 + sum f, m = sum c f.
@@ -265,23 +290,21 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
   }
   // Force: uniform + per-cell field (KParams::force_at, params.rs:386-405).
   A Fpx = A(0), Fpy = A(0), Fpz = A(0), Fcx = A(0), Fcy = A(0), Fcz = A(0);
-  bool forced = p.uniform_force != 0;
-  if (forced) {
+  if (FORCED) {
     Fpx = Fcx = p.gx;
     Fpy = Fcy = p.gy;
     Fpz = Fcz = p.gz;
-  }
-  if (fl & F_FORCED) {
-    const int32_t s = p.fslot[cell];
-    const Vec4<A> a = p.fprev[s];
-    const Vec4<A> b = p.fcur[s];
-    Fpx = Fpx + a.x;
-    Fpy = Fpy + a.y;
-    Fpz = Fpz + a.z;
-    Fcx = Fcx + b.x;
-    Fcy = Fcy + b.y;
-    Fcz = Fcz + b.z;
-    forced = true;
+    if (fl & F_FORCED) {
+      const int32_t s = p.fslot[cell];
+      const Vec4<A> a = p.fprev[s];
+      const Vec4<A> b = p.fcur[s];
+      Fpx = Fpx + a.x;
+      Fpy = Fpy + a.y;
+      Fpz = Fpz + a.z;
+      Fcx = Fcx + b.x;
+      Fcy = Fcy + b.y;
+      Fcz = Fcz + b.z;
+    }
   }
   const A rho = A(1) + dr;
   const A inv = A(1) / rho;
@@ -290,57 +313,65 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
   const A uy = (m1 + half * Fpy) * inv;
   const A uz = (m2 + half * Fpz) * inv;
   if constexpr (COLL == COLL_CM)
-    collide_cm<Q, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, forced, p.omega_shear);
+    collide_cm<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, p.omega_shear);
   else
-    collide_trt<Q, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, forced, p.omega_p, p.omega_m, p.cp, p.cm);
+    collide_trt<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, p.omega_p, p.omega_m, p.cp, p.cm);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     A v = f[q];
-    const bool wall = (mask >> q) & 1u;
     const int o = opp(q);
-    if (wall && (fl & F_MOVING)) {
-      const Vec4<A> wu = p.wall_u[nb.at(L::cx(q), L::cy(q), L::cz(q))];
+    const bool wall = GENERIC && ((mask >> q) & 1u);
+    if (GENERIC && wall && (fl & F_MOVING)) {
+      const Vec4<A> wu = p.wall_u[nidx(L::cx(q), L::cy(q), L::cz(q))];
       const A cu = (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y) + A(L::cz(o)) * wu.z;
       v = v + ((A(6) * A(L::w(o))) * rho) * cu;
     }
     if (!ODD || wall)
-      CD::st(fb + o * pl + cell, v);
+      CD::st(fb + (o * pl + cell), v);
     else
-      CD::st(fb + q * pl + nb.at(L::cx(q), L::cy(q), L::cz(q)), v);
+      CD::st(fb + (q * pl + nidx(L::cx(q), L::cy(q), L::cz(q))), v);
   }
 }
 
+template <class A>
+struct HydroOccupancy {
+  static constexpr int MIN_BLOCKS = sizeof(A) == 8 ? 2 : 4;  // <= 128 regs (fp32), <= 255 (fp64)
+};
+
 // Full-grid sweep: block = one x-row segment, grid = (x tiles, ny, nz).
-// With skip_forced, cells flagged F_FORCED are left to hydro_cells_kernel
-// (so the IBM update can overlap this launch).
-template <int Q, class S, int COLL, bool ODD>
-__global__ void __launch_bounds__(128) hydro_aa_kernel(HydroParams<typename Codec<S>::A> p,
-                                                       int skip_forced) {
+// FORCED = false skips F_FORCED cells (hydro_cells_kernel updates them after
+// the IBM force update); FORCED = true (uniform body force) forces every cell.
+template <int Q, class S, int COLL, bool ODD, bool FORCED>
+__global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
+    hydro_aa_kernel(HydroParams<typename Codec<S>::A> p) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= p.nx) return;
   const int y = blockIdx.y, z = blockIdx.z;
-  const int64_t cell = (int64_t(z) * p.ny + y) * p.nx + x;
+  const uint32_t cell = (uint32_t(z) * uint32_t(p.ny) + uint32_t(y)) * uint32_t(p.nx) + uint32_t(x);
   const uint8_t fl = p.flags[cell];
   if (fl & F_SOLID) return;
-  if (skip_forced && (fl & F_FORCED)) return;
-  hydro_cell<Q, S, COLL, ODD>(p, x, y, z, cell, fl);
+  if (!FORCED && (fl & F_FORCED)) return;
+  if (fl & (F_BOUNDARY | F_WRAP))
+    hydro_cell<Q, S, COLL, ODD, true, FORCED>(p, x, y, z, cell, fl);
+  else
+    hydro_cell<Q, S, COLL, ODD, false, FORCED>(p, x, y, z, cell, fl);
 }
 
-// Cell-list sweep (the forced cells, after the IBM force update).
+// Cell-list sweep over the forced cells (after the IBM force update).
 template <int Q, class S, int COLL, bool ODD>
-__global__ void __launch_bounds__(128) hydro_cells_kernel(HydroParams<typename Codec<S>::A> p,
-                                                          const int64_t* cells, int64_t ncells) {
+__global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
+    hydro_cells_kernel(HydroParams<typename Codec<S>::A> p, const int64_t* cells, int64_t ncells) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= ncells) return;
-  const int64_t cell = cells[i];
-  const int64_t nxy = int64_t(p.nx) * p.ny;
+  const uint32_t cell = uint32_t(cells[i]);
+  const uint32_t nxy = uint32_t(p.nxy);
   const int z = int(cell / nxy);
-  const int64_t r = cell - int64_t(z) * nxy;
-  const int y = int(r / p.nx);
-  const int x = int(r - int64_t(y) * p.nx);
+  const uint32_t r = cell - uint32_t(z) * nxy;
+  const int y = int(r / uint32_t(p.nx));
+  const int x = int(r - uint32_t(y) * uint32_t(p.nx));
   const uint8_t fl = p.flags[cell];
   if (fl & F_SOLID) return;
-  hydro_cell<Q, S, COLL, ODD>(p, x, y, z, cell, fl);
+  hydro_cell<Q, S, COLL, ODD, true, true>(p, x, y, z, cell, fl);
 }
 
 }  // namespace lbmb

@@ -302,17 +302,30 @@ __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, int swee
     last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (!last || threadIdx.x != 0) return;
+  if (!last) return;
   __threadfence();
-  double tot[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (unsigned int b = 0; b < gridDim.x; ++b) {
+  // The last block reduces every partial: thread t takes blocks t, t + B,
+  // ... in order, then a fixed tree (deterministic run to run).
+  double acc[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // 8 diag sums, 3 spread sums
+  double amax = 0.0;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
     const volatile double* p = a.part_diag + 9 * b;
-    tot[0] = fmax(tot[0], p[0]);
-    for (int k = 1; k < 9; ++k) tot[k] += p[k];
+    amax = fmax(amax, p[0]);
+    for (int k = 0; k < 8; ++k) acc[k] += p[1 + k];
   }
-  double ffs[3] = {0.0, 0.0, 0.0};
-  for (int b = 0; b < nblk_spread; ++b)
-    for (int c = 0; c < 3; ++c) ffs[c] += ((const volatile double*)a.part_spread)[3 * b + c];
+  for (int b = threadIdx.x; b < nblk_spread; b += blockDim.x)
+    for (int c = 0; c < 3; ++c) acc[8 + c] += ((const volatile double*)a.part_spread)[3 * b + c];
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0) smax_sh[threadIdx.x >> 5] = amax;
+  __shared__ double sh2[11 * (IBM_BLOCK / 32)];
+  block_sum<11>(acc, sh2);
+  if (threadIdx.x != 0) return;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) amax = fmax(amax, smax_sh[w]);
+  double tot[9];
+  tot[0] = amax;
+  for (int k = 0; k < 8; ++k) tot[1 + k] = acc[k];
+  const double ffs[3] = {acc[8], acc[9], acc[10]};
   IbmDiagDev* d = a.diag;
   for (int c = 0; c < 3; ++c) {
     d->fluid_force[c] += ffs[c];

@@ -124,8 +124,8 @@ struct Engine final : EngineBase {
   int64_t n, plane;
   int coll;  // COLL_TRT or COLL_CM
   double omega_p, omega_m;
-  cudaStream_t st = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t st = nullptr, st2 = nullptr;  // main stream, high-priority IBM stream
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork = nullptr, ev_join = nullptr;
   // device state
   DevBuf<S> f;
   DevBuf<uint8_t> flags;
@@ -163,6 +163,8 @@ struct Engine final : EngineBase {
     nz = c.dims[2];
     n = int64_t(nx) * ny * nz;
     plane = ceil_div(n, 64) * 64;
+    if (int64_t(Q) * plane >= (int64_t(1) << 31))
+      throw Error(LBMB_ERR_UNSUPPORTED, "grid too large: Q x cells must stay below 2^31 element offsets");
     coll = c.collision == LBMB_CENTRAL_MOMENT ? COLL_CM : COLL_TRT;
     double tau = 3.0 * c.nu + 0.5;
     omega_p = 1.0 / tau;
@@ -170,6 +172,13 @@ struct Engine final : EngineBase {
     if (c.collision == LBMB_TRT) omega_m = 1.0 / (c.magic / (tau - 0.5) + 0.5);  // params.rs:205-217
     CK(cudaSetDevice(c.device));
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    {
+      int lo = 0, hi = 0;
+      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      CK(cudaStreamCreateWithPriority(&st2, cudaStreamNonBlocking, hi));
+    }
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
     solid_h.assign(size_t(n), 0);
@@ -196,8 +205,12 @@ struct Engine final : EngineBase {
     if (st) cudaStreamSynchronize(st);
     bodies.clear();
     scalars.clear();
+    if (st2) cudaStreamSynchronize(st2);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
     if (st) cudaStreamDestroy(st);
   }
 
@@ -238,6 +251,9 @@ struct Engine final : EngineBase {
           uint8_t fl = 0;
           if (m) fl |= F_BOUNDARY;
           if (moving) fl |= F_MOVING;
+          if ((cfg.periodic[0] && (x == 0 || x == nx - 1)) || (cfg.periodic[1] && (y == 0 || y == ny - 1)) ||
+              (cfg.periodic[2] && (z == 0 || z == nz - 1)))
+            fl |= F_WRAP;
           flags_h[c] = fl;
           nb[c] = m;
         }
@@ -286,7 +302,8 @@ struct Engine final : EngineBase {
   HydroParams<A> hydro_params() {
     HydroParams<A> p;
     p.f = f.p;
-    p.plane = plane;
+    p.plane = uint32_t(plane);
+    p.nxy = nx * ny;
     p.flags = flags.p;
     p.nbr = nbr.p;
     p.wall_u = wall_u.p;
@@ -308,25 +325,37 @@ struct Engine final : EngineBase {
     return p;
   }
 
-  void launch_hydro(int par) {
+  template <int COLL, bool ODD>
+  void launch_hydro_t(const HydroParams<A>& p, cudaStream_t s, bool main_grid, bool cells) {
+    if (main_grid) {
+      const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
+      dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
+      if (p.uniform_force)
+        hydro_aa_kernel<Q, S, COLL, ODD, true><<<grid, block, 0, s>>>(p);
+      else
+        hydro_aa_kernel<Q, S, COLL, ODD, false><<<grid, block, 0, s>>>(p);
+      CK(cudaGetLastError());
+    }
+    if (cells && !p.uniform_force && nslots > 0) {
+      hydro_cells_kernel<Q, S, COLL, ODD><<<unsigned(ceil_div(nslots, 128)), 128, 0, s>>>(p, slot_cell.p, nslots);
+      CK(cudaGetLastError());
+    }
+  }
+
+  // One hydro step of the given parity: the full-grid sweep and (without a
+  // uniform force) the forced-cell sweep.
+  void launch_hydro(int par, cudaStream_t s = nullptr, bool main_grid = true, bool cells = true) {
+    if (!s) s = st;
     HydroParams<A> p = hydro_params();
-    const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
-    dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
     if constexpr (Q == 27) {
       if (coll == COLL_CM) {
-        if (par == 0)
-          hydro_aa_kernel<Q, S, COLL_CM, false><<<grid, block, 0, st>>>(p, 0);
-        else
-          hydro_aa_kernel<Q, S, COLL_CM, true><<<grid, block, 0, st>>>(p, 0);
-        CK(cudaGetLastError());
+        if (par == 0) launch_hydro_t<COLL_CM, false>(p, s, main_grid, cells);
+        else launch_hydro_t<COLL_CM, true>(p, s, main_grid, cells);
         return;
       }
     }
-    if (par == 0)
-      hydro_aa_kernel<Q, S, COLL_TRT, false><<<grid, block, 0, st>>>(p, 0);
-    else
-      hydro_aa_kernel<Q, S, COLL_TRT, true><<<grid, block, 0, st>>>(p, 0);
-    CK(cudaGetLastError());
+    if (par == 0) launch_hydro_t<COLL_TRT, false>(p, s, main_grid, cells);
+    else launch_hydro_t<COLL_TRT, true>(p, s, main_grid, cells);
   }
 
   // One full step on the stream: hydro, the cached-moment field refresh,
@@ -781,22 +810,23 @@ struct Engine final : EngineBase {
 
   // Device sequence of one apply_rotating_ibm call (no host sync).
   void enqueue_ibm(BodyState& B, const lbmb_ibm_config& c, double* s_torque, double* s_ff, int32_t* s_it,
-                   int64_t* counter, bool field_at_call) {
+                   int64_t* counter, bool field_at_call, cudaStream_t s_ = nullptr) {
+    cudaStream_t sx = s_ ? s_ : st;
     IbmArgs a = ibm_args(B, c);
     const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
     const unsigned gm = unsigned(std::max<int64_t>(1, ceil_div(B.nm, IBM_BLOCK)));
-    ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, st>>>(a, f.p, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz,
+    ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, sx>>>(a, f.p, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz,
                                                     parity, fcur.p, field_at_call ? 1 : 0,
                                                     double(A(cfg.force[0])), double(A(cfg.force[1])),
                                                     double(A(cfg.force[2])));
     CK(cudaGetLastError());
     for (int s = 0; s < c.max_iterations; ++s) {
-      ibm_interp_kernel<<<gm, IBM_BLOCK, 0, st>>>(a, s);
-      ibm_spread_kernel<<<gs, IBM_BLOCK, 0, st>>>(a);
-      ibm_diag_kernel<<<gm, IBM_BLOCK, 0, st>>>(a, s, int(gs));
+      ibm_interp_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s);
+      ibm_spread_kernel<<<gs, IBM_BLOCK, 0, sx>>>(a);
+      ibm_diag_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s, int(gs));
     }
     CK(cudaGetLastError());
-    ibm_commit_kernel<A><<<gs, IBM_BLOCK, 0, st>>>(a, fcur.p, s_torque, s_ff, s_it, counter);
+    ibm_commit_kernel<A><<<gs, IBM_BLOCK, 0, sx>>>(a, fcur.p, s_torque, s_ff, s_it, counter);
     CK(cudaGetLastError());
   }
 
@@ -905,13 +935,28 @@ struct Engine final : EngineBase {
     CK(cudaEventRecord(ev0, st));
     int64_t launches = 0;
     auto one_step = [&](int64_t step_index) {
+      // Fork: the IBM chain (clear -> direct forcing -> forced-cell hydro)
+      // runs on the high-priority side stream while the full-grid sweep of
+      // every other cell runs on the main stream; the two touch disjoint
+      // population slots (each cell's AA read/write set is its own).
+      CK(cudaEventRecord(ev_fork, st));
+      CK(cudaStreamWaitEvent(st2, ev_fork, 0));
       // Solver::clear_body_force_field: the IBM field is non-uniform, so the
       // cached moments keep it (F_prev) while the new field starts at zero.
-      if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st));
-      enqueue_ibm(B, c, d_torque.p, d_ff.p, d_it.p, d_counter.p, false);
+      if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st2));
+      enqueue_ibm(B, c, d_torque.p, d_ff.p, d_it.p, d_counter.p, false, st2);
       field_present = true;
       fprev_stale = true;
-      enqueue_step();
+      launch_hydro(parity, st2, false, true);
+      launch_hydro(parity, st, true, false);
+      CK(cudaEventRecord(ev_join, st2));
+      CK(cudaStreamWaitEvent(st, ev_join, 0));
+      parity ^= 1;
+      if (fprev_stale) {
+        CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
+        fprev_stale = false;
+      }
+      for (auto& sc : scalars) scalar_step(*sc);
       ++launches;
       if (k >= 0 && ((step_index + 1) % probe_every == 0 || step_index + 1 == steps))
         enqueue_cv(*scalars[k], d_cv.p + step_index, double(n - solid_count()));
