@@ -333,6 +333,15 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
   }
 }
 
+// Out-of-line generic cell update (periodic wrap, solid neighbours, moving
+// walls): compiled once per kernel so the unrolled fast paths keep the
+// instruction cache.
+template <int Q, class S, int COLL, bool ODD, bool FORCED>
+__device__ __noinline__ void hydro_cell_generic(const HydroParams<typename Codec<S>::A> p, int x, int y, int z,
+                                                uint32_t cell, uint8_t fl) {
+  hydro_cell<Q, S, COLL, ODD, true, FORCED>(p, x, y, z, cell, fl);
+}
+
 template <class A>
 struct HydroOccupancy {
   static constexpr int MIN_BLOCKS = sizeof(A) == 8 ? 2 : 4;  // <= 128 regs (fp32), <= 255 (fp64)
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN
   if (fl & F_SOLID) return;
   if (!FORCED && (fl & F_FORCED)) return;
   if (fl & (F_BOUNDARY | F_WRAP))
-    hydro_cell<Q, S, COLL, ODD, true, FORCED>(p, x, y, z, cell, fl);
+    hydro_cell_generic<Q, S, COLL, ODD, FORCED>(p, x, y, z, cell, fl);
   else
     hydro_cell<Q, S, COLL, ODD, false, FORCED>(p, x, y, z, cell, fl);
 }

@@ -1,0 +1,144 @@
+// Software-pipelined AA collide-stream with per-thread asynchronous copies.
+//
+// Persistent blocks of 128 threads walk the grid in 128-cell tiles. Each
+// thread keeps a ring of STAGES x Q population slots in shared memory (its
+// own column: [stage][q][thread]) and, while colliding the cell of tile i,
+// already has the populations of its cells in tiles i+1 .. i+STAGES-1 in
+// flight (cp.async, 4/8-byte copies). A thread only ever reads back what it
+// copied itself, so cp.async.wait_group is the only synchronisation: there
+// are no block barriers and no spin loops. The copy addresses follow the AA
+// rule of hydro.cuh (odd step: slot opp(q) of x - c_q, own slot q when that
+// neighbour is solid) as branchless selects; cells on a periodic face use
+// the out-of-line generic path, which keeps the unrolled body small enough
+// for the instruction cache. Requires 4- or 8-byte population storage.
+#pragma once
+#include "hydro.cuh"
+
+namespace lbmb {
+
+constexpr int ASYNC_TILE = 128;
+
+template <int Q, class S, int STAGES>
+constexpr size_t async_smem_bytes() {
+  return size_t(STAGES) * Q * ASYNC_TILE * sizeof(S);
+}
+
+template <class S>
+__device__ __forceinline__ void cp_async_elem(S* dst_smem, const S* src) {
+  static_assert(sizeof(S) == 4 || sizeof(S) == 8, "cp.async needs 4- or 8-byte elements");
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+  if constexpr (sizeof(S) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int Q, class S, int COLL, bool ODD, int STAGES>
+__global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
+    hydro_async_kernel(HydroParams<typename Codec<S>::A> p, int64_t ncells, int ntiles) {
+  using A = typename Codec<S>::A;
+  using L = Lat<Q>;
+  using CD = Codec<S>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  const int j = threadIdx.x;
+  S* fb = static_cast<S*>(p.f);
+  const int64_t pl = p.plane;
+  const int nx = p.nx, nxy = p.nxy;
+  auto dq = [&](int q) -> int64_t {
+    return int64_t(L::cx(q)) + int64_t(L::cy(q)) * nx + int64_t(L::cz(q)) * nxy;
+  };
+  // Cells on a periodic face take the out-of-line generic path; all other
+  // active cells go through the pipeline.
+  auto piped = [&](uint8_t fl) { return !(fl & (F_SOLID | F_FORCED | F_WRAP)); };
+  // Issue the copies of this thread's cell in tile t into ring stage s.
+  auto issue = [&](int t, int s) {
+    const int64_t cell = int64_t(t) * ASYNC_TILE + j;
+    if (t < ntiles && cell < ncells) {
+      const uint8_t fl = p.flags[cell];
+      if (piped(fl)) {
+        S* dst = sm + size_t(s) * Q * ASYNC_TILE + j;
+        const S* src0 = fb + cell;
+        if (!ODD) {
+#pragma unroll
+          for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + int64_t(q) * pl);
+        } else {
+          const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
+#pragma unroll
+          for (int q = 0; q < Q; ++q) {
+            const int o = opp(q);
+            const int64_t off = ((mask >> o) & 1u) ? int64_t(q) * pl : int64_t(o) * pl - dq(q);
+            cp_async_elem(dst + q * ASYNC_TILE, src0 + off);
+          }
+        }
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) issue(int(blockIdx.x) + s * int(gridDim.x), s);
+  int it = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    issue(t + (STAGES - 1) * int(gridDim.x), (it + STAGES - 1) % STAGES);
+    cp_async_wait<STAGES - 1>();
+    const int64_t cell = int64_t(t) * ASYNC_TILE + j;
+    if (cell >= ncells) continue;
+    const uint8_t fl = p.flags[cell];
+    if (fl & (F_SOLID | F_FORCED)) continue;
+    if (fl & F_WRAP) {
+      const int z = int(cell / nxy);
+      const int64_t r = cell - int64_t(z) * nxy;
+      const int y = int(r / nx);
+      hydro_cell_generic<Q, S, COLL, ODD, false>(p, int(r - int64_t(y) * nx), y, z, uint32_t(cell), fl);
+      continue;
+    }
+    const S* src = sm + size_t(it % STAGES) * Q * ASYNC_TILE + j;
+    A f[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) f[q] = CD::ld(src + q * ASYNC_TILE);
+    A dr = A(0), m0 = A(0), m1 = A(0), m2 = A(0);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      dr = dr + f[q];
+      if (L::cx(q) == 1) m0 = m0 + f[q];
+      if (L::cx(q) == -1) m0 = m0 - f[q];
+      if (L::cy(q) == 1) m1 = m1 + f[q];
+      if (L::cy(q) == -1) m1 = m1 - f[q];
+      if (L::cz(q) == 1) m2 = m2 + f[q];
+      if (L::cz(q) == -1) m2 = m2 - f[q];
+    }
+    const A rho = A(1) + dr;
+    const A inv = A(1) / rho;
+    const A ux = m0 * inv, uy = m1 * inv, uz = m2 * inv;
+    const A z0 = A(0);
+    if constexpr (COLL == COLL_CM)
+      collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, p.omega_shear);
+    else
+      collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, p.omega_p, p.omega_m, p.cp, p.cm);
+    const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
+    S* dst0 = fb + cell;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      A v = f[q];
+      const int o = opp(q);
+      const bool wall = (mask >> q) & 1u;
+      if (wall && (fl & F_MOVING)) {
+        const Vec4<A> wu = p.wall_u[cell + dq(q)];
+        const A cu = (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y) + A(L::cz(o)) * wu.z;
+        v = v + ((A(6) * A(L::w(o))) * rho) * cu;
+      }
+      const int64_t off = (!ODD || wall) ? int64_t(o) * pl : int64_t(q) * pl + dq(q);
+      CD::st(dst0 + off, v);
+    }
+  }
+  cp_async_wait<0>();
+}
+
+}  // namespace lbmb

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -17,6 +18,8 @@
 #include "../../include/lbmb.h"
 #include "aux.cuh"
 #include "hydro.cuh"
+#include "hydro_tma.cuh"
+#include "hydro_async.cuh"
 #include "ibm.cuh"
 #include "scalar.cuh"
 
@@ -127,7 +130,9 @@ struct Engine final : EngineBase {
   cudaStream_t st = nullptr, st2 = nullptr;  // main stream, high-priority IBM stream
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork = nullptr, ev_join = nullptr;
   // device state
-  DevBuf<S> f;
+  DevBuf<S> f_alloc;     // populations with a guard margin on both sides
+  S* fp = nullptr;       // first element of plane 0
+  int64_t margin = 0;    // guard elements before plane 0 and after the last plane
   DevBuf<uint8_t> flags;
   DevBuf<uint32_t> nbr;
   DevBuf<Vec4<A>> wall_u;
@@ -145,6 +150,13 @@ struct Engine final : EngineBase {
   // IBM
   std::vector<std::unique_ptr<BodyState>> bodies;
   DevBuf<IbmDiagDev> d_diag;
+  DevBuf<int> d_err;  // device error flag (bounded waits)
+  int sm_count = 148;
+  int64_t ntiles = 0;
+  bool rows_aligned = false;
+  int kernel_mode = 2;  // 0 direct, 1 TMA bulk-staged, 2 per-thread async pipeline
+  int tma_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int async_grid[4] = {0, 0, 0, 0};
   // reductions
   DevBuf<double> red_part, red_out;
   int red_blocks = 0;
@@ -185,13 +197,25 @@ struct Engine final : EngineBase {
     if (solid)
       for (int64_t i = 0; i < n; ++i) solid_h[i] = solid[i] ? 1 : 0;
     build_flags(wu);
-    f.alloc(size_t(Q) * plane);
-    CK(cudaMemsetAsync(f.p, 0, size_t(Q) * plane * sizeof(S), st));
+    // Guard margin: shifted TMA windows of the odd step reach up to
+    // nx*ny + nx + 1 cells (+ alignment slack and one tile) beyond a plane.
+    margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 128, 64) * 64;
+    f_alloc.alloc(size_t(Q) * plane + 2 * size_t(margin));
+    CK(cudaMemsetAsync(f_alloc.p, 0, (size_t(Q) * plane + 2 * size_t(margin)) * sizeof(S), st));
+    fp = f_alloc.p + margin;
     fslot_h.assign(size_t(n), -1);
     fslot.alloc(size_t(n));
     CK(cudaMemsetAsync(fslot.p, 0xff, size_t(n) * sizeof(int32_t), st));
     grow_slots(64);
     d_diag.alloc(1);
+    d_err.alloc(1);
+    CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
+    CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c.device));
+    ntiles = ceil_div(n, TMA_TILE);
+    rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
+    if (sizeof(S) < 4) kernel_mode = 0;  // 16-bit storage: cp.async needs 4-byte elements
+    if (const char* e = std::getenv("LBMB_KERNEL")) kernel_mode = std::atoi(e);
+    if (sizeof(S) < 4 && kernel_mode == 2) kernel_mode = 0;
     red_blocks = int(std::min<int64_t>(ceil_div(n, RED_BLOCK), 1184));
     red_part.alloc(size_t(red_blocks) * 5);
     red_out.alloc(8);
@@ -301,7 +325,7 @@ struct Engine final : EngineBase {
 
   HydroParams<A> hydro_params() {
     HydroParams<A> p;
-    p.f = f.p;
+    p.f = fp;
     p.plane = uint32_t(plane);
     p.nxy = nx * ny;
     p.flags = flags.p;
@@ -325,20 +349,70 @@ struct Engine final : EngineBase {
     return p;
   }
 
+  // TMA-staged sweep (persistent grid sized by the occupancy API).
+  template <int COLL, bool ODD, bool RA>
+  void launch_tma(const HydroParams<A>& p, cudaStream_t s) {
+    auto kern = hydro_tma_kernel<Q, S, COLL, ODD, RA>;
+    const size_t smem = tma_smem_bytes<Q, S>();
+    const int slot = (ODD ? 1 : 0) + (RA ? 2 : 0) + (COLL == COLL_CM ? 4 : 0);
+    if (tma_grid[slot] == 0) {
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TMA_TILE, smem));
+      tma_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
+    }
+    kern<<<unsigned(tma_grid[slot]), TMA_TILE, smem, s>>>(p, n, int(ntiles), d_err.p);
+    CK(cudaGetLastError());
+  }
+
+  // Per-thread cp.async pipeline (persistent grid).
+  template <int COLL, bool ODD>
+  void launch_async(const HydroParams<A>& p, cudaStream_t s) {
+    constexpr int STAGES = 3;
+    auto kern = hydro_async_kernel<Q, S, COLL, ODD, STAGES>;
+    const size_t smem = async_smem_bytes<Q, S, STAGES>();
+    const int slot = (ODD ? 1 : 0) + (COLL == COLL_CM ? 2 : 0);
+    if (async_grid[slot] == 0) {
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ASYNC_TILE, smem));
+      async_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
+    }
+    kern<<<unsigned(async_grid[slot]), ASYNC_TILE, smem, s>>>(p, n, int(ntiles));
+    CK(cudaGetLastError());
+  }
+
   template <int COLL, bool ODD>
   void launch_hydro_t(const HydroParams<A>& p, cudaStream_t s, bool main_grid, bool cells) {
     if (main_grid) {
-      const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
-      dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
-      if (p.uniform_force)
-        hydro_aa_kernel<Q, S, COLL, ODD, true><<<grid, block, 0, s>>>(p);
-      else
-        hydro_aa_kernel<Q, S, COLL, ODD, false><<<grid, block, 0, s>>>(p);
-      CK(cudaGetLastError());
+      if (!p.uniform_force && kernel_mode == 1) {
+        if (rows_aligned) launch_tma<COLL, ODD, true>(p, s);
+        else launch_tma<COLL, ODD, false>(p, s);
+      } else if (!p.uniform_force && kernel_mode == 2) {
+        if constexpr (sizeof(S) >= 4) launch_async<COLL, ODD>(p, s);
+      } else {
+        const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
+        dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
+        if (p.uniform_force)
+          hydro_aa_kernel<Q, S, COLL, ODD, true><<<grid, block, 0, s>>>(p);
+        else
+          hydro_aa_kernel<Q, S, COLL, ODD, false><<<grid, block, 0, s>>>(p);
+        CK(cudaGetLastError());
+      }
     }
     if (cells && !p.uniform_force && nslots > 0) {
       hydro_cells_kernel<Q, S, COLL, ODD><<<unsigned(ceil_div(nslots, 128)), 128, 0, s>>>(p, slot_cell.p, nslots);
       CK(cudaGetLastError());
+    }
+  }
+
+  // Raise (and clear) a device-side error reported by a bounded wait.
+  void check_device_error() {
+    int e = 0;
+    CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+      CK(cudaMemset(d_err.p, 0, sizeof(int)));
+      throw Error(LBMB_ERR_CUDA, "device wait timed out (bulk copy did not complete)");
     }
   }
 
@@ -374,7 +448,7 @@ struct Engine final : EngineBase {
     ScalarParams<A> p;
     p.h = sc.h.p;
     p.hplane = sc.hplane;
-    p.f = f.p;
+    p.f = fp;
     p.plane = plane;
     p.flags = flags.p;
     p.nbr = nbr.p;
@@ -440,6 +514,7 @@ struct Engine final : EngineBase {
     }
     CK(cudaEventRecord(ev1, st));
     CK(cudaEventSynchronize(ev1));
+    check_device_error();
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     last_total_ms = ms;
@@ -452,7 +527,7 @@ struct Engine final : EngineBase {
   void stage_in(const double* fin) override {
     DevBuf<double> tmp;
     tmp.upload(fin, size_t(Q) * n, st);
-    stage_in_kernel<Q, S><<<unsigned(ceil_div(n, 256)), 256, 0, st>>>(f.p, plane, tmp.p, n);
+    stage_in_kernel<Q, S><<<unsigned(ceil_div(n, 256)), 256, 0, st>>>(fp, plane, tmp.p, n);
     CK(cudaGetLastError());
     parity = 0;
     // Moments refresh: the cached moments now include the current field.
@@ -466,7 +541,7 @@ struct Engine final : EngineBase {
   void stage_out(double* fout) override {
     DevBuf<double> tmp;
     tmp.alloc(size_t(Q) * n);
-    stage_out_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(f.p, plane, flags.p, nbr.p, nx, ny, nz,
+    stage_out_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(fp, plane, flags.p, nbr.p, nx, ny, nz,
                                                                        parity, tmp.p, n);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(fout, tmp.p, size_t(Q) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -544,7 +619,7 @@ struct Engine final : EngineBase {
     DevBuf<double> d;
     d.alloc(size_t(4) * n);
     moments_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
-        f.p, plane, flags.p, nbr.p, nx, ny, nz, parity, fslot.p, fprev.p, A(cfg.force[0]), A(cfg.force[1]),
+        fp, plane, flags.p, nbr.p, nx, ny, nz, parity, fslot.p, fprev.p, A(cfg.force[0]), A(cfg.force[1]),
         A(cfg.force[2]), d.p, d.p + n, d.p + 2 * n, d.p + 3 * n, n);
     CK(cudaGetLastError());
     std::vector<double> h(size_t(4) * n);
@@ -560,7 +635,7 @@ struct Engine final : EngineBase {
   }
 
   void reduce_all(double out[5]) override {
-    reduce_kernel<Q, S><<<red_blocks, RED_BLOCK, 0, st>>>(f.p, plane, flags.p, nbr.p, nx, ny, nz, parity,
+    reduce_kernel<Q, S><<<red_blocks, RED_BLOCK, 0, st>>>(fp, plane, flags.p, nbr.p, nx, ny, nz, parity,
                                                          fslot.p, fcur.p, double(A(cfg.force[0])),
                                                          double(A(cfg.force[1])), double(A(cfg.force[2])),
                                                          n, red_part.p);
@@ -815,7 +890,7 @@ struct Engine final : EngineBase {
     IbmArgs a = ibm_args(B, c);
     const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
     const unsigned gm = unsigned(std::max<int64_t>(1, ceil_div(B.nm, IBM_BLOCK)));
-    ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, sx>>>(a, f.p, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz,
+    ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, sx>>>(a, fp, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz,
                                                     parity, fcur.p, field_at_call ? 1 : 0,
                                                     double(A(cfg.force[0])), double(A(cfg.force[1])),
                                                     double(A(cfg.force[2])));
@@ -992,6 +1067,7 @@ struct Engine final : EngineBase {
     for (; done < steps; ++done) one_step(done);
     CK(cudaEventRecord(ev1, st));
     CK(cudaEventSynchronize(ev1));
+    check_device_error();
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     last_total_ms = ms;
