@@ -243,6 +243,24 @@ def run_b200(args, rank, world, local):
             extra[f"{st}_hydro_gbs"] = b_lu(q, st) * n_fluid / (hv / lv * 1e-3) / 1e9
             gv.close()
         extra["fp16_over_fp32"] = extra["f16_mlups"] / (value / world)
+        # D3Q19 TRT on the same tank (the reference runner's collision), fp32
+        # and fp16-storage: runner step MLUPS and the hydro sweep's fraction
+        # of the HBM roofline (152 / 76 bytes per fluid cell).
+        peak, _ = peak_hbm()
+        for st in ("f32", "f16"):
+            gv = lb.Solver(dims, lattice=19, collision="trt", storage=st, nu=nu, solid=solid, device=local)
+            gv.run_impeller(body, 8)
+            k = max(args.steps // 2, 16)
+            gv.run_impeller(body, k)
+            tv, _, _ = gv.last_timing()
+            extra[f"d3q19_trt_{st}_mlups"] = n_cells * k / (tv * 1e-3) / 1e6
+            gv.run(args.hydro_steps)
+            hv, _, lv = gv.last_timing()
+            gbs = b_lu(19, st) * n_fluid / (hv / lv * 1e-3) / 1e9
+            extra[f"d3q19_trt_{st}_hydro_gbs"] = gbs
+            extra[f"d3q19_trt_{st}_hydro_frac"] = gbs / peak
+            gv.close()
+        extra["d3q19_fp16_over_fp32"] = extra["d3q19_trt_f16_mlups"] / extra["d3q19_trt_f32_mlups"]
     torque = out["torque_lu"]
     res = {
         "metric": "MLUPS (stirred-tank runner step, D3Q27 central moment, fp32 populations)",

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(RED_BLOCK) reduce_kernel(const S* fb, int64_t 
 }
 
 // Sum block partials in block order (single thread: deterministic).
-__global__ void reduce_finish_kernel(const double* part, int nblk, int width, double* out) {
+static __global__ void reduce_finish_kernel(const double* part, int nblk, int width, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int k = 0; k < width; ++k) {
     double s = 0.0;

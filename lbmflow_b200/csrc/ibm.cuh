@@ -157,7 +157,7 @@ __global__ void ibm_prep_kernel(IbmArgs a, const S* fb, int64_t pl, const int64_
 }
 
 // Impulse per marker from the current du (solver.rs:3118-3173).
-__global__ void ibm_interp_kernel(IbmArgs a, int sweep) {
+static __global__ void ibm_interp_kernel(IbmArgs a, int sweep) {
   const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (m >= a.nm) return;
   if (a.diag->converged) return;
@@ -220,7 +220,7 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
 }
 
 // Spread the impulses into the slots, in marker order (solver.rs:3174-3209).
-__global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) {
+static __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) {
   __shared__ double sh[3 * (IBM_BLOCK / 32)];
   if (a.diag->converged) return;
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) {
 }
 
 // Slip statistics and the sweep's global reduction (solver.rs:3211-3253).
-__global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, int sweep, int nblk_spread) {
+static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, int sweep, int nblk_spread) {
   __shared__ double sh[9 * (IBM_BLOCK / 32)];
   __shared__ double smax_sh[IBM_BLOCK / 32];
   __shared__ bool last;

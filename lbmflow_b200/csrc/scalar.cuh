@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(RED_BLOCK) scalar_cv_kernel(const A* hb, int64
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
-__global__ void scalar_cv_finish_kernel(const double* part, int nblk, int pass, double* stats, double nfluid,
+static __global__ void scalar_cv_finish_kernel(const double* part, int nblk, int pass, double* stats, double nfluid,
                                         double* cv_out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double s = 0.0;

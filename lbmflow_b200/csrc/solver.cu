@@ -1,1096 +1,14 @@
-// Host engine behind include/lbmb.h: device memory, launch sequencing,
-// CUDA graphs, validation and the C ABI.
+// C ABI behind include/lbmb.h: validation (GlobalSpec::validate), engine
+// construction and the exception-to-status translation.
 //
 // Reference boundary: trait Backend<L, T> (crates/lbm-core/src/backend.rs:
 // 126-363) driven by Solver<L, T, B, H> (crates/lbm-core/src/solver.rs:
-// 1503-1541). One engine owns one device state; the C entry points at the
-// end of this file translate exceptions into status codes.
-#include <algorithm>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <memory>
-#include <stdexcept>
-#include <string>
-#include <vector>
-
-#include "../../include/lbmb.h"
-#include "aux.cuh"
-#include "hydro.cuh"
-#include "hydro_tma.cuh"
-#include "hydro_async.cuh"
-#include "ibm.cuh"
-#include "scalar.cuh"
+// 1503-1541).
+#include "engine.cuh"
 
 namespace lbmb {
 
 thread_local std::string g_last_error;
-
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define CK(x)                                                                                   \
-  do {                                                                                          \
-    cudaError_t e_ = (x);                                                                       \
-    if (e_ != cudaSuccess)                                                                      \
-      throw ::lbmb::Error(e_ == cudaErrorMemoryAllocation ? LBMB_ERR_NOMEM : LBMB_ERR_CUDA,     \
-                          std::string(#x) + ": " + cudaGetErrorString(e_));                     \
-  } while (0)
-
-static void invalid(const std::string& m) { throw Error(LBMB_ERR_INVALID, m); }
-
-template <class T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  void alloc(size_t k) {
-    release();
-    if (k == 0) k = 1;
-    CK(cudaMalloc(&p, k * sizeof(T)));
-    n = k;
-  }
-  void upload(const T* h, size_t k, cudaStream_t st) {
-    if (k > n) alloc(k);
-    if (k) CK(cudaMemcpyAsync(p, h, k * sizeof(T), cudaMemcpyHostToDevice, st));
-  }
-  void upload(const std::vector<T>& v, cudaStream_t st) { upload(v.data(), v.size(), st); }
-};
-
-static int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
-
-struct BodyState {
-  int64_t nm = 0;
-  std::vector<double> pos, weight;
-  double center[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
-  double scale = 1.0;
-  int radius = 0;  // radius the device stencils were built for (0: none)
-  DevBuf<double> d_pos, d_weight, st_w, st_cks, cs_w, imp, mob, rmf, part_spread, part_diag;
-  DevBuf<int32_t> st_off, st_slot, bslot, cs_off, cs_marker;
-  int64_t ns = 0;
-  bool empty_stencil = false;
-};
-
-template <class A>
-struct ScalarStateT {
-  int q = 7;
-  double diffusivity = 0.0;
-  int parity = 0;
-  int64_t hplane = 0;
-  DevBuf<A> h;
-  DevBuf<double> part, stats;
-};
-
-// Type-erased engine interface.
-struct EngineBase {
-  virtual ~EngineBase() = default;
-  virtual void step(int64_t n) = 0;
-  virtual void stage_in(const double* f) = 0;
-  virtual void stage_out(double* f) = 0;
-  virtual void init_fields(const double* rho, const double* u) = 0;
-  virtual void read_moments(double* rho, double* ux, double* uy, double* uz) = 0;
-  virtual void reduce_all(double out[5]) = 0;
-  virtual void clear_force_field() = 0;
-  virtual void get_force_field(double* out) = 0;
-  virtual void ibm_set_body(int b, const double* pos, const double* w, int64_t n, const double* c,
-                            const double* om) = 0;
-  virtual void ibm_apply(int b, const lbmb_ibm_config& cfg, lbmb_ibm_diag* diag) = 0;
-  virtual int enable_scalar(int q, double d) = 0;
-  virtual void set_scalar(int k, const double* c) = 0;
-  virtual void get_scalar(int k, double* c) = 0;
-  virtual void run_impeller(int b, const lbmb_ibm_config& cfg, int64_t steps, int k, int64_t probe_every,
-                            double* torque, double* ff, double* cv, int32_t* iters) = 0;
-  virtual void sync() = 0;
-  virtual int64_t cells() const = 0;
-  virtual int q() const = 0;
-  virtual const std::vector<uint8_t>& solid() const = 0;
-  double last_total_ms = 0.0, last_hydro_ms = 0.0;
-  int64_t last_hydro_launches = 0;
-};
-
-template <int Q, class S>
-struct Engine final : EngineBase {
-  using A = typename Codec<S>::A;
-  lbmb_config cfg;
-  int nx, ny, nz;
-  int64_t n, plane;
-  int coll;  // COLL_TRT or COLL_CM
-  double omega_p, omega_m;
-  cudaStream_t st = nullptr, st2 = nullptr;  // main stream, high-priority IBM stream
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork = nullptr, ev_join = nullptr;
-  // device state
-  DevBuf<S> f_alloc;     // populations with a guard margin on both sides
-  S* fp = nullptr;       // first element of plane 0
-  int64_t margin = 0;    // guard elements before plane 0 and after the last plane
-  DevBuf<uint8_t> flags;
-  DevBuf<uint32_t> nbr;
-  DevBuf<Vec4<A>> wall_u;
-  DevBuf<int32_t> fslot;
-  int parity = 0;
-  // force slots
-  int64_t nslots = 0, slot_cap = 0;
-  std::vector<int32_t> fslot_h;  // per cell, -1 = none
-  std::vector<int64_t> slot_cell_h;
-  DevBuf<int64_t> slot_cell;
-  DevBuf<Vec4<A>> fprev, fcur;
-  DevBuf<double> s_rho, s_unow, s_du, s_spread;
-  bool field_present = false;
-  bool fprev_stale = false;
-  // IBM
-  std::vector<std::unique_ptr<BodyState>> bodies;
-  DevBuf<IbmDiagDev> d_diag;
-  DevBuf<int> d_err;  // device error flag (bounded waits)
-  int sm_count = 148;
-  int64_t ntiles = 0;
-  bool rows_aligned = false;
-  int kernel_mode = 2;  // 0 direct, 1 TMA bulk-staged, 2 per-thread async pipeline
-  int tma_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int async_grid[4] = {0, 0, 0, 0};
-  // reductions
-  DevBuf<double> red_part, red_out;
-  int red_blocks = 0;
-  // host mirrors
-  std::vector<uint8_t> solid_h, flags_h;
-  std::vector<double> init_rho_h, init_u_h;
-  // scalars
-  std::vector<std::unique_ptr<ScalarStateT<A>>> scalars;
-  // graphs
-  cudaGraphExec_t step_graph = nullptr;
-  int step_graph_len = 0;
-
-  Engine(const lbmb_config& c, const uint8_t* solid, const double* wu) : cfg(c) {
-    nx = c.dims[0];
-    ny = c.dims[1];
-    nz = c.dims[2];
-    n = int64_t(nx) * ny * nz;
-    plane = ceil_div(n, 64) * 64;
-    if (int64_t(Q) * plane >= (int64_t(1) << 31))
-      throw Error(LBMB_ERR_UNSUPPORTED, "grid too large: Q x cells must stay below 2^31 element offsets");
-    coll = c.collision == LBMB_CENTRAL_MOMENT ? COLL_CM : COLL_TRT;
-    double tau = 3.0 * c.nu + 0.5;
-    omega_p = 1.0 / tau;
-    omega_m = omega_p;
-    if (c.collision == LBMB_TRT) omega_m = 1.0 / (c.magic / (tau - 0.5) + 0.5);  // params.rs:205-217
-    CK(cudaSetDevice(c.device));
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    {
-      int lo = 0, hi = 0;
-      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-      CK(cudaStreamCreateWithPriority(&st2, cudaStreamNonBlocking, hi));
-    }
-    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
-    CK(cudaEventCreate(&ev0));
-    CK(cudaEventCreate(&ev1));
-    solid_h.assign(size_t(n), 0);
-    if (solid)
-      for (int64_t i = 0; i < n; ++i) solid_h[i] = solid[i] ? 1 : 0;
-    build_flags(wu);
-    // Guard margin: shifted TMA windows of the odd step reach up to
-    // nx*ny + nx + 1 cells (+ alignment slack and one tile) beyond a plane.
-    margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 128, 64) * 64;
-    f_alloc.alloc(size_t(Q) * plane + 2 * size_t(margin));
-    CK(cudaMemsetAsync(f_alloc.p, 0, (size_t(Q) * plane + 2 * size_t(margin)) * sizeof(S), st));
-    fp = f_alloc.p + margin;
-    fslot_h.assign(size_t(n), -1);
-    fslot.alloc(size_t(n));
-    CK(cudaMemsetAsync(fslot.p, 0xff, size_t(n) * sizeof(int32_t), st));
-    grow_slots(64);
-    d_diag.alloc(1);
-    d_err.alloc(1);
-    CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), st));
-    CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c.device));
-    ntiles = ceil_div(n, TMA_TILE);
-    rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
-    if (sizeof(S) < 4) kernel_mode = 0;  // 16-bit storage: cp.async needs 4-byte elements
-    if (const char* e = std::getenv("LBMB_KERNEL")) kernel_mode = std::atoi(e);
-    if (sizeof(S) < 4 && kernel_mode == 2) kernel_mode = 0;
-    red_blocks = int(std::min<int64_t>(ceil_div(n, RED_BLOCK), 1184));
-    red_part.alloc(size_t(red_blocks) * 5);
-    red_out.alloc(8);
-    init_rho_h.assign(size_t(n), 1.0);
-    init_u_h.assign(size_t(3 * n), 0.0);
-    CK(cudaStreamSynchronize(st));
-  }
-
-  ~Engine() override {
-    if (step_graph) cudaGraphExecDestroy(step_graph);
-    if (st) cudaStreamSynchronize(st);
-    bodies.clear();
-    scalars.clear();
-    if (st2) cudaStreamSynchronize(st2);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
-    if (st2) cudaStreamDestroy(st2);
-    if (st) cudaStreamDestroy(st);
-  }
-
-  int64_t cells() const override { return n; }
-  int q() const override { return Q; }
-  const std::vector<uint8_t>& solid() const override { return solid_h; }
-
-  int64_t idx(int x, int y, int z) const { return (int64_t(z) * ny + y) * nx + x; }
-
-  // Cell flags, solid-neighbour masks and wall velocities.
-  void build_flags(const double* wu) {
-    flags_h.assign(size_t(n), 0);
-    std::vector<uint32_t> nb(size_t(n), 0u);
-    std::vector<Vec4<A>> w(size_t(n), Vec4<A>{A(0), A(0), A(0), A(0)});
-    if (wu)
-      for (int64_t i = 0; i < n; ++i) w[i] = Vec4<A>{A(wu[3 * i]), A(wu[3 * i + 1]), A(wu[3 * i + 2]), A(0)};
-    for (int z = 0; z < nz; ++z)
-      for (int y = 0; y < ny; ++y)
-        for (int x = 0; x < nx; ++x) {
-          const int64_t c = idx(x, y, z);
-          if (solid_h[c]) {
-            flags_h[c] = F_SOLID;
-            continue;
-          }
-          uint32_t m = 0;
-          bool moving = false;
-          for (int q = 1; q < Q; ++q) {
-            int xx = x + Lat<Q>::cx(q), yy = y + Lat<Q>::cy(q), zz = z + Lat<Q>::cz(q);
-            xx = (xx + nx) % nx;
-            yy = (yy + ny) % ny;
-            zz = (zz + nz) % nz;
-            const int64_t s = idx(xx, yy, zz);
-            if (solid_h[s]) {
-              m |= 1u << q;
-              if (w[s].x != A(0) || w[s].y != A(0) || w[s].z != A(0)) moving = true;
-            }
-          }
-          uint8_t fl = 0;
-          if (m) fl |= F_BOUNDARY;
-          if (moving) fl |= F_MOVING;
-          if ((cfg.periodic[0] && (x == 0 || x == nx - 1)) || (cfg.periodic[1] && (y == 0 || y == ny - 1)) ||
-              (cfg.periodic[2] && (z == 0 || z == nz - 1)))
-            fl |= F_WRAP;
-          flags_h[c] = fl;
-          nb[c] = m;
-        }
-    flags.upload(flags_h, st);
-    nbr.upload(nb, st);
-    wall_u.upload(w, st);
-    CK(cudaStreamSynchronize(st));
-  }
-
-  void invalidate_graphs() {
-    if (step_graph) {
-      CK(cudaGraphExecDestroy(step_graph));
-      step_graph = nullptr;
-    }
-  }
-
-  // Grow the force-slot arrays, keeping content.
-  void grow_slots(int64_t need) {
-    if (need <= slot_cap) return;
-    int64_t cap = std::max<int64_t>(need, slot_cap * 2);
-    auto grow = [&](auto& buf, size_t elems_old, size_t elems_new) {
-      using E = std::remove_reference_t<decltype(*buf.p)>;
-      E* old = buf.p;
-      size_t old_n = buf.n;
-      buf.p = nullptr;
-      buf.n = 0;
-      buf.alloc(elems_new);
-      CK(cudaMemsetAsync(buf.p, 0, elems_new * sizeof(E), st));
-      if (old) {
-        CK(cudaMemcpyAsync(buf.p, old, std::min(elems_old, old_n) * sizeof(E), cudaMemcpyDeviceToDevice, st));
-        CK(cudaStreamSynchronize(st));
-        cudaFree(old);
-      }
-    };
-    grow(slot_cell, size_t(slot_cap), size_t(cap));
-    grow(fprev, size_t(slot_cap), size_t(cap));
-    grow(fcur, size_t(slot_cap), size_t(cap));
-    grow(s_rho, size_t(slot_cap), size_t(cap));
-    grow(s_unow, size_t(3 * slot_cap), size_t(3 * cap));
-    grow(s_du, size_t(3 * slot_cap), size_t(3 * cap));
-    grow(s_spread, size_t(3 * slot_cap), size_t(3 * cap));
-    slot_cap = cap;
-    invalidate_graphs();
-  }
-
-  HydroParams<A> hydro_params() {
-    HydroParams<A> p;
-    p.f = fp;
-    p.plane = uint32_t(plane);
-    p.nxy = nx * ny;
-    p.flags = flags.p;
-    p.nbr = nbr.p;
-    p.wall_u = wall_u.p;
-    p.fslot = fslot.p;
-    p.fprev = fprev.p;
-    p.fcur = fcur.p;
-    p.nx = nx;
-    p.ny = ny;
-    p.nz = nz;
-    p.omega_p = A(omega_p);
-    p.omega_m = A(omega_m);
-    p.cp = A(1.0 - omega_p / 2.0);
-    p.cm = A(1.0 - omega_m / 2.0);
-    p.omega_shear = A(cfg.omega_shear);
-    p.gx = A(cfg.force[0]);
-    p.gy = A(cfg.force[1]);
-    p.gz = A(cfg.force[2]);
-    p.uniform_force = (p.gx != A(0) || p.gy != A(0) || p.gz != A(0)) ? 1 : 0;
-    return p;
-  }
-
-  // TMA-staged sweep (persistent grid sized by the occupancy API).
-  template <int COLL, bool ODD, bool RA>
-  void launch_tma(const HydroParams<A>& p, cudaStream_t s) {
-    auto kern = hydro_tma_kernel<Q, S, COLL, ODD, RA>;
-    const size_t smem = tma_smem_bytes<Q, S>();
-    const int slot = (ODD ? 1 : 0) + (RA ? 2 : 0) + (COLL == COLL_CM ? 4 : 0);
-    if (tma_grid[slot] == 0) {
-      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      int per_sm = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TMA_TILE, smem));
-      tma_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
-    }
-    kern<<<unsigned(tma_grid[slot]), TMA_TILE, smem, s>>>(p, n, int(ntiles), d_err.p);
-    CK(cudaGetLastError());
-  }
-
-  // Per-thread cp.async pipeline (persistent grid).
-  template <int COLL, bool ODD>
-  void launch_async(const HydroParams<A>& p, cudaStream_t s) {
-    constexpr int STAGES = 3;
-    auto kern = hydro_async_kernel<Q, S, COLL, ODD, STAGES>;
-    const size_t smem = async_smem_bytes<Q, S, STAGES>();
-    const int slot = (ODD ? 1 : 0) + (COLL == COLL_CM ? 2 : 0);
-    if (async_grid[slot] == 0) {
-      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      int per_sm = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ASYNC_TILE, smem));
-      async_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
-    }
-    kern<<<unsigned(async_grid[slot]), ASYNC_TILE, smem, s>>>(p, n, int(ntiles));
-    CK(cudaGetLastError());
-  }
-
-  template <int COLL, bool ODD>
-  void launch_hydro_t(const HydroParams<A>& p, cudaStream_t s, bool main_grid, bool cells) {
-    if (main_grid) {
-      if (!p.uniform_force && kernel_mode == 1) {
-        if (rows_aligned) launch_tma<COLL, ODD, true>(p, s);
-        else launch_tma<COLL, ODD, false>(p, s);
-      } else if (!p.uniform_force && kernel_mode == 2) {
-        if constexpr (sizeof(S) >= 4) launch_async<COLL, ODD>(p, s);
-      } else {
-        const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
-        dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
-        if (p.uniform_force)
-          hydro_aa_kernel<Q, S, COLL, ODD, true><<<grid, block, 0, s>>>(p);
-        else
-          hydro_aa_kernel<Q, S, COLL, ODD, false><<<grid, block, 0, s>>>(p);
-        CK(cudaGetLastError());
-      }
-    }
-    if (cells && !p.uniform_force && nslots > 0) {
-      hydro_cells_kernel<Q, S, COLL, ODD><<<unsigned(ceil_div(nslots, 128)), 128, 0, s>>>(p, slot_cell.p, nslots);
-      CK(cudaGetLastError());
-    }
-  }
-
-  // Raise (and clear) a device-side error reported by a bounded wait.
-  void check_device_error() {
-    int e = 0;
-    CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) {
-      CK(cudaMemset(d_err.p, 0, sizeof(int)));
-      throw Error(LBMB_ERR_CUDA, "device wait timed out (bulk copy did not complete)");
-    }
-  }
-
-  // One hydro step of the given parity: the full-grid sweep and (without a
-  // uniform force) the forced-cell sweep.
-  void launch_hydro(int par, cudaStream_t s = nullptr, bool main_grid = true, bool cells = true) {
-    if (!s) s = st;
-    HydroParams<A> p = hydro_params();
-    if constexpr (Q == 27) {
-      if (coll == COLL_CM) {
-        if (par == 0) launch_hydro_t<COLL_CM, false>(p, s, main_grid, cells);
-        else launch_hydro_t<COLL_CM, true>(p, s, main_grid, cells);
-        return;
-      }
-    }
-    if (par == 0) launch_hydro_t<COLL_TRT, false>(p, s, main_grid, cells);
-    else launch_hydro_t<COLL_TRT, true>(p, s, main_grid, cells);
-  }
-
-  // One full step on the stream: hydro, the cached-moment field refresh,
-  // then the scalars (which read the moments of the new state).
-  void enqueue_step() {
-    launch_hydro(parity);
-    parity ^= 1;
-    if (fprev_stale) {
-      CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
-      fprev_stale = false;
-    }
-    for (auto& sc : scalars) scalar_step(*sc);
-  }
-
-  ScalarParams<A> scalar_params(ScalarStateT<A>& sc) {
-    ScalarParams<A> p;
-    p.h = sc.h.p;
-    p.hplane = sc.hplane;
-    p.f = fp;
-    p.plane = plane;
-    p.flags = flags.p;
-    p.nbr = nbr.p;
-    p.fslot = fslot.p;
-    p.fprev = fprev.p;
-    p.nx = nx;
-    p.ny = ny;
-    p.nz = nz;
-    p.hparity = parity;
-    p.omega = A(1.0 / ((sc.q == 7 ? Lat<7>::INV_CS2 : Lat<Q>::INV_CS2) * sc.diffusivity + 0.5));
-    p.gx = A(cfg.force[0]);
-    p.gy = A(cfg.force[1]);
-    p.gz = A(cfg.force[2]);
-    return p;
-  }
-
-  void scalar_step(ScalarStateT<A>& sc) {
-    ScalarParams<A> p = scalar_params(sc);
-    const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
-    dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
-    if (sc.q == 7) {
-      if (sc.parity == 0) scalar_step_kernel<7, Q, S, false><<<grid, block, 0, st>>>(p);
-      else scalar_step_kernel<7, Q, S, true><<<grid, block, 0, st>>>(p);
-    } else {
-      if (sc.parity == 0) scalar_step_kernel<Q, Q, S, false><<<grid, block, 0, st>>>(p);
-      else scalar_step_kernel<Q, Q, S, true><<<grid, block, 0, st>>>(p);
-    }
-    CK(cudaGetLastError());
-    sc.parity ^= 1;
-  }
-
-  void step(int64_t steps) override {
-    CK(cudaEventRecord(ev0, st));
-    int64_t launches = 0;
-    int64_t done = 0;
-    const int G = 32;
-    // Graph replay for long runs: needs parity 0 at the start, no pending
-    // force-field refresh and no scalars (whose steps are launched per step).
-    while (steps - done >= G && scalars.empty()) {
-      if (parity != 0 || fprev_stale) {
-        enqueue_step();
-        ++done;
-        ++launches;
-        continue;
-      }
-      if (!step_graph) {
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < G; ++i) enqueue_step();
-        CK(cudaStreamEndCapture(st, &g));
-        CK(cudaGraphInstantiate(&step_graph, g, 0));
-        CK(cudaGraphDestroy(g));
-        step_graph_len = G;
-        parity = 0;  // G is even
-      }
-      CK(cudaGraphLaunch(step_graph, st));
-      done += G;
-      launches += G;
-    }
-    for (; done < steps; ++done) {
-      enqueue_step();
-      ++launches;
-    }
-    CK(cudaEventRecord(ev1, st));
-    CK(cudaEventSynchronize(ev1));
-    check_device_error();
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ev0, ev1));
-    last_total_ms = ms;
-    last_hydro_ms = ms;
-    last_hydro_launches = launches;
-  }
-
-  void sync() override { CK(cudaStreamSynchronize(st)); }
-
-  void stage_in(const double* fin) override {
-    DevBuf<double> tmp;
-    tmp.upload(fin, size_t(Q) * n, st);
-    stage_in_kernel<Q, S><<<unsigned(ceil_div(n, 256)), 256, 0, st>>>(fp, plane, tmp.p, n);
-    CK(cudaGetLastError());
-    parity = 0;
-    // Moments refresh: the cached moments now include the current field.
-    if (nslots)
-      CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
-    fprev_stale = false;
-    CK(cudaStreamSynchronize(st));
-    invalidate_graphs();
-  }
-
-  void stage_out(double* fout) override {
-    DevBuf<double> tmp;
-    tmp.alloc(size_t(Q) * n);
-    stage_out_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(fp, plane, flags.p, nbr.p, nx, ny, nz,
-                                                                       parity, tmp.p, n);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(fout, tmp.p, size_t(Q) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-  }
-
-  // Solver::init_with (solver.rs:2474-2605) on the host, in the arithmetic
-  // precision, then staged in.
-  void init_fields(const double* r_in, const double* u_in) override {
-    using L = Lat<Q>;
-    std::vector<double> fh(size_t(Q) * n);
-    const A three = A(3), half = A(0.5), f45 = A(4.5), f15 = A(1.5);
-    const A tau = A(3.0 * cfg.nu + 0.5);
-    const bool per[3] = {cfg.periodic[0] != 0, cfg.periodic[1] != 0, cfg.periodic[2] != 0};
-    const int dims[3] = {nx, ny, nz};
-    for (int z = 0; z < nz; ++z)
-      for (int y = 0; y < ny; ++y)
-        for (int x = 0; x < nx; ++x) {
-          const int64_t c = idx(x, y, z);
-          const A r = A(r_in[c]);
-          const A u[3] = {A(u_in[3 * c]), A(u_in[3 * c + 1]), A(u_in[3 * c + 2])};
-          const A usq = (u[0] * u[0] + u[1] * u[1]) + u[2] * u[2];
-          const A drho = r - A(1);
-          A fq[Q];
-          for (int q = 0; q < Q; ++q) {
-            const A cu = (A(L::cx(q)) * u[0] + A(L::cy(q)) * u[1]) + A(L::cz(q)) * u[2];
-            fq[q] = A(L::w(q)) * (drho + r * (three * cu + f45 * cu * cu - f15 * usq));
-          }
-          if (!solid_h[c]) {
-            auto sample = [&](int a, int dl, A out[3]) -> bool {
-              int g[3] = {x, y, z};
-              g[a] += dl;
-              if (g[a] < 0 || g[a] >= dims[a]) {
-                if (per[a]) g[a] = (g[a] + dims[a]) % dims[a];
-                else return false;
-              }
-              const int64_t gi = idx(g[0], g[1], g[2]);
-              if (solid_h[gi]) return false;
-              for (int k = 0; k < 3; ++k) out[k] = A(u_in[3 * gi + k]);
-              return true;
-            };
-            A grad[3][3] = {};
-            for (int a = 0; a < 3; ++a) {
-              A pv[3] = {A(0), A(0), A(0)}, mv[3] = {A(0), A(0), A(0)};
-              const bool hp = sample(a, 1, pv), hm = sample(a, -1, mv);
-              for (int b = 0; b < 3; ++b) {
-                if (hp && hm) grad[a][b] = (pv[b] - mv[b]) * half;
-                else if (hp) grad[a][b] = pv[b] - u[b];
-                else if (hm) grad[a][b] = u[b] - mv[b];
-                else grad[a][b] = A(0);
-              }
-            }
-            const A div = (grad[0][0] + grad[1][1]) + grad[2][2];
-            for (int q = 0; q < Q; ++q) {
-              const A cq[3] = {A(L::cx(q)), A(L::cy(q)), A(L::cz(q))};
-              A ccgu = cq[0] * cq[0] * grad[0][0];
-              for (int a = 0; a < 3; ++a)
-                for (int b = a; b < 3; ++b) {
-                  if (a == 0 && b == 0) continue;
-                  if (a == b) ccgu = ccgu + cq[a] * cq[a] * grad[a][a];
-                  else ccgu = ccgu + cq[a] * cq[b] * (grad[a][b] + grad[b][a]);
-                }
-              const A fneq = -A(L::w(q)) * r * tau * (three * ccgu - div);
-              fq[q] = fq[q] + fneq;
-            }
-          }
-          for (int q = 0; q < Q; ++q) fh[size_t(q) * n + c] = double(fq[q]);
-          init_rho_h[c] = double(r);
-          for (int k = 0; k < 3; ++k) init_u_h[3 * c + k] = double(u[k]);
-        }
-    stage_in(fh.data());
-  }
-
-  void read_moments(double* rho, double* ux, double* uy, double* uz) override {
-    DevBuf<double> d;
-    d.alloc(size_t(4) * n);
-    moments_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
-        fp, plane, flags.p, nbr.p, nx, ny, nz, parity, fslot.p, fprev.p, A(cfg.force[0]), A(cfg.force[1]),
-        A(cfg.force[2]), d.p, d.p + n, d.p + 2 * n, d.p + 3 * n, n);
-    CK(cudaGetLastError());
-    std::vector<double> h(size_t(4) * n);
-    CK(cudaMemcpyAsync(h.data(), d.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (int64_t c = 0; c < n; ++c) {
-      const bool s = solid_h[c] != 0;
-      if (rho) rho[c] = s ? init_rho_h[c] : h[c];
-      if (ux) ux[c] = s ? init_u_h[3 * c] : h[n + c];
-      if (uy) uy[c] = s ? init_u_h[3 * c + 1] : h[2 * n + c];
-      if (uz) uz[c] = s ? init_u_h[3 * c + 2] : h[3 * n + c];
-    }
-  }
-
-  void reduce_all(double out[5]) override {
-    reduce_kernel<Q, S><<<red_blocks, RED_BLOCK, 0, st>>>(fp, plane, flags.p, nbr.p, nx, ny, nz, parity,
-                                                         fslot.p, fcur.p, double(A(cfg.force[0])),
-                                                         double(A(cfg.force[1])), double(A(cfg.force[2])),
-                                                         n, red_part.p);
-    CK(cudaGetLastError());
-    reduce_finish_kernel<<<1, 32, 0, st>>>(red_part.p, red_blocks, 5, red_out.p);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, red_out.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-  }
-
-  // Solver::clear_body_force_field (solver.rs:2805-2822): a uniform field
-  // (all cells equal) refreshes the cached moments without it; otherwise
-  // the cached moments keep the old field until the next step.
-  void clear_force_field() override {
-    if (!field_present) return;
-    bool uniform = true;
-    if (nslots > 0) {
-      std::vector<Vec4<A>> h(static_cast<size_t>(nslots));
-      CK(cudaMemcpyAsync(h.data(), fcur.p, h.size() * sizeof(Vec4<A>), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      const Vec4<A> base = (nslots == n) ? h[0] : Vec4<A>{A(0), A(0), A(0), A(0)};
-      for (auto& v : h)
-        if (!(v.x == base.x && v.y == base.y && v.z == base.z)) uniform = false;
-    }
-    field_present = false;
-    if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st));
-    if (uniform) {
-      if (nslots) CK(cudaMemsetAsync(fprev.p, 0, size_t(nslots) * sizeof(Vec4<A>), st));
-      fprev_stale = false;
-    }
-    CK(cudaStreamSynchronize(st));
-  }
-
-  void get_force_field(double* out) override {
-    std::fill(out, out + 3 * n, 0.0);
-    if (!field_present || nslots == 0) return;
-    std::vector<Vec4<A>> h(static_cast<size_t>(nslots));
-    CK(cudaMemcpyAsync(h.data(), fcur.p, h.size() * sizeof(Vec4<A>), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (int64_t s = 0; s < nslots; ++s) {
-      const int64_t c = slot_cell_h[s];
-      out[3 * c] = double(h[s].x);
-      out[3 * c + 1] = double(h[s].y);
-      out[3 * c + 2] = double(h[s].z);
-    }
-  }
-
-  // ---- IBM -------------------------------------------------------------
-  void ibm_set_body(int b, const double* pos, const double* w, int64_t nm, const double* c,
-                    const double* om) override {
-    if (b < 0 || b > 64) invalid("IBM body slot out of range");
-    if (nm <= 0) invalid("IBM body must contain at least one marker");
-    for (int64_t m = 0; m < nm; ++m) {
-      for (int a = 0; a < 3; ++a)
-        if (!std::isfinite(pos[3 * m + a])) invalid("IBM marker must have finite position and positive finite weight");
-      if (!(std::isfinite(w[m]) && w[m] > 0.0))
-        invalid("IBM marker must have finite position and positive finite weight");
-    }
-    for (int a = 0; a < 3; ++a)
-      if (!std::isfinite(c[a]) || !std::isfinite(om[a])) invalid("IBM center and omega must be finite");
-    if (int(bodies.size()) <= b) bodies.resize(size_t(b) + 1);
-    auto bs = std::make_unique<BodyState>();
-    bs->nm = nm;
-    bs->pos.assign(pos, pos + 3 * nm);
-    bs->weight.assign(w, w + nm);
-    for (int a = 0; a < 3; ++a) {
-      bs->center[a] = c[a];
-      bs->omega[a] = om[a];
-    }
-    // scale = max(max |Omega x r|, 1) (solver.rs:3090-3094)
-    double mt = 0.0;
-    for (int64_t m = 0; m < nm; ++m) {
-      const double r[3] = {pos[3 * m] - c[0], pos[3 * m + 1] - c[1], pos[3 * m + 2] - c[2]};
-      const double t[3] = {om[1] * r[2] - om[2] * r[1], om[2] * r[0] - om[0] * r[2], om[0] * r[1] - om[1] * r[0]};
-      mt = std::max(mt, std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]));
-    }
-    bs->scale = std::max(mt, 1.0);
-    bs->d_pos.upload(bs->pos, st);
-    bs->d_weight.upload(bs->weight, st);
-    bs->imp.alloc(size_t(3 * nm));
-    bs->mob.alloc(size_t(nm));
-    bs->rmf.alloc(size_t(3 * nm));
-    bs->part_diag.alloc(size_t(9 * ceil_div(nm, IBM_BLOCK)));
-    CK(cudaStreamSynchronize(st));
-    bodies[b] = std::move(bs);
-    invalidate_graphs();
-  }
-
-  static double linear_kernel(double r) { return std::max(1.0 - r, 0.0); }
-  static double quadratic_kernel(double r) {
-    if (r < 0.5) return 0.75 - r * r;
-    if (r < 1.5) return 0.5 * (1.5 - r) * (1.5 - r);
-    return 0.0;
-  }
-
-  // Marker stencils (rotating_ibm.rs:163-210) -> device CSR both ways.
-  void build_stencils(BodyState& B, int radius) {
-    const int dims[3] = {nx, ny, nz};
-    std::vector<int32_t> st_off(size_t(B.nm) + 1, 0);
-    std::vector<int64_t> st_cell;
-    std::vector<double> st_w;
-    for (int64_t m = 0; m < B.nm; ++m) {
-      std::vector<std::pair<int, double>> ax[3];
-      for (int a = 0; a < 3; ++a) {
-        const double p = B.pos[3 * m + a];
-        const long lo = long(std::floor(p)) - radius + 1, hi = long(std::floor(p)) + radius;
-        for (long i = lo; i <= hi; ++i) {
-          if (i < 0 || i >= dims[a]) continue;
-          const double r = std::fabs(p - double(i));
-          const double w = radius == 1 ? linear_kernel(r) : quadratic_kernel(r);
-          if (w != 0.0) ax[a].push_back({int(i), w});
-        }
-      }
-      if (ax[0].empty() || ax[1].empty() || ax[2].empty()) invalid("IBM marker stencil is outside the domain");
-      for (auto& px : ax[0])
-        for (auto& py : ax[1])
-          for (auto& pz : ax[2]) {
-            const int64_t c = idx(px.first, py.first, pz.first);
-            if (solid_h[c]) continue;
-            st_cell.push_back(c);
-            st_w.push_back(px.second * py.second * pz.second);
-          }
-      st_off[m + 1] = int32_t(st_cell.size());
-    }
-    // global slots for the cells (appended, never removed)
-    std::vector<int32_t> st_slot(st_cell.size());
-    int64_t need = nslots;
-    for (int64_t c : st_cell)
-      if (fslot_h[c] < 0) {
-        fslot_h[c] = -2;  // mark new
-        ++need;
-      }
-    grow_slots(need);
-    std::vector<int64_t> new_cells;
-    for (size_t k = 0; k < st_cell.size(); ++k) {
-      const int64_t c = st_cell[k];
-      if (fslot_h[c] == -2) {
-        fslot_h[c] = int32_t(nslots + int64_t(new_cells.size()));
-        new_cells.push_back(c);
-      }
-      st_slot[k] = fslot_h[c];
-    }
-    if (!new_cells.empty()) {
-      std::vector<int32_t> ids(new_cells.size());
-      for (size_t i = 0; i < new_cells.size(); ++i) {
-        ids[i] = int32_t(nslots + int64_t(i));
-        slot_cell_h.push_back(new_cells[i]);
-        flags_h[new_cells[i]] |= F_FORCED;
-      }
-      CK(cudaMemcpyAsync(slot_cell.p + nslots, new_cells.data(), new_cells.size() * sizeof(int64_t),
-                         cudaMemcpyHostToDevice, st));
-      nslots += int64_t(new_cells.size());
-      // scatter new slot ids and flags
-      for (size_t i = 0; i < new_cells.size(); ++i) {
-        CK(cudaMemcpyAsync(fslot.p + new_cells[i], &fslot_h[new_cells[i]], sizeof(int32_t), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(flags.p + new_cells[i], &flags_h[new_cells[i]], 1, cudaMemcpyHostToDevice, st));
-      }
-      CK(cudaStreamSynchronize(st));
-      invalidate_graphs();
-    }
-    // body slots and reverse CSR in marker order
-    std::vector<int32_t> local(size_t(nslots), -1);
-    std::vector<int32_t> bslot;
-    for (size_t k = 0; k < st_slot.size(); ++k)
-      if (local[st_slot[k]] < 0) {
-        local[st_slot[k]] = int32_t(bslot.size());
-        bslot.push_back(st_slot[k]);
-      }
-    const int64_t ns = int64_t(bslot.size());
-    std::vector<int32_t> cs_off(size_t(ns) + 1, 0);
-    for (size_t k = 0; k < st_slot.size(); ++k) cs_off[local[st_slot[k]] + 1]++;
-    for (int64_t i = 0; i < ns; ++i) cs_off[i + 1] += cs_off[i];
-    std::vector<int32_t> fill(cs_off.begin(), cs_off.end() - 1);
-    std::vector<int32_t> cs_marker(st_slot.size());
-    std::vector<double> cs_w(st_slot.size());
-    std::vector<double> cks(size_t(ns), 0.0);
-    for (int64_t m = 0; m < B.nm; ++m)
-      for (int32_t k = st_off[m]; k < st_off[m + 1]; ++k) {
-        const int32_t l = local[st_slot[k]];
-        cs_marker[fill[l]] = int32_t(m);
-        cs_w[fill[l]] = st_w[k];
-        fill[l]++;
-        cks[l] += st_w[k];  // cell_kernel_sum in marker order (solver.rs:3107-3116)
-      }
-    std::vector<double> st_cks(st_slot.size());
-    for (size_t k = 0; k < st_slot.size(); ++k) st_cks[k] = cks[local[st_slot[k]]];
-    B.st_off.upload(st_off, st);
-    B.st_slot.upload(st_slot, st);
-    B.st_w.upload(st_w, st);
-    B.st_cks.upload(st_cks, st);
-    B.bslot.upload(bslot, st);
-    B.cs_off.upload(cs_off, st);
-    B.cs_marker.upload(cs_marker, st);
-    B.cs_w.upload(cs_w, st);
-    B.ns = ns;
-    B.part_spread.alloc(size_t(3 * std::max<int64_t>(1, ceil_div(ns, IBM_BLOCK))));
-    B.radius = radius;
-    CK(cudaStreamSynchronize(st));
-  }
-
-  IbmArgs ibm_args(BodyState& B, const lbmb_ibm_config& c) {
-    IbmArgs a;
-    a.nm = B.nm;
-    a.pos = B.d_pos.p;
-    a.weight = B.d_weight.p;
-    a.st_off = B.st_off.p;
-    a.st_slot = B.st_slot.p;
-    a.st_w = B.st_w.p;
-    a.st_cks = B.st_cks.p;
-    a.ns = B.ns;
-    a.bslot = B.bslot.p;
-    a.cs_off = B.cs_off.p;
-    a.cs_marker = B.cs_marker.p;
-    a.cs_w = B.cs_w.p;
-    a.rho = s_rho.p;
-    a.u_now = s_unow.p;
-    a.du = s_du.p;
-    a.spread = s_spread.p;
-    a.imp = B.imp.p;
-    a.mob = B.mob.p;
-    a.rmf = B.rmf.p;
-    a.part_spread = B.part_spread.p;
-    a.part_diag = B.part_diag.p;
-    a.diag = d_diag.p;
-    for (int k = 0; k < 3; ++k) {
-      a.center[k] = B.center[k];
-      a.omega[k] = B.omega[k];
-    }
-    a.scale = B.scale;
-    a.relax = c.relaxation;
-    a.tol = c.slip_tolerance;
-    return a;
-  }
-
-  BodyState& body_for(int b, const lbmb_ibm_config& c) {
-    if (c.max_iterations <= 0) invalid("IBM max_iterations must be positive");
-    if (!(c.slip_tolerance >= 0.0 && std::isfinite(c.slip_tolerance)))
-      invalid("IBM slip_tolerance must be finite and non-negative");
-    if (!(c.relaxation > 0.0 && c.relaxation <= 1.0 && std::isfinite(c.relaxation)))
-      invalid("IBM relaxation must be finite and in (0, 1]");
-    if (c.kernel_radius != 1 && c.kernel_radius != 2) invalid("IBM kernel radius must be 1 or 2");
-    if (b < 0 || b >= int(bodies.size()) || !bodies[b]) throw Error(LBMB_ERR_STATE, "IBM body not set");
-    BodyState& B = *bodies[b];
-    if (B.radius != c.kernel_radius) build_stencils(B, c.kernel_radius);
-    return B;
-  }
-
-  // Device sequence of one apply_rotating_ibm call (no host sync).
-  void enqueue_ibm(BodyState& B, const lbmb_ibm_config& c, double* s_torque, double* s_ff, int32_t* s_it,
-                   int64_t* counter, bool field_at_call, cudaStream_t s_ = nullptr) {
-    cudaStream_t sx = s_ ? s_ : st;
-    IbmArgs a = ibm_args(B, c);
-    const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
-    const unsigned gm = unsigned(std::max<int64_t>(1, ceil_div(B.nm, IBM_BLOCK)));
-    ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, sx>>>(a, fp, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz,
-                                                    parity, fcur.p, field_at_call ? 1 : 0,
-                                                    double(A(cfg.force[0])), double(A(cfg.force[1])),
-                                                    double(A(cfg.force[2])));
-    CK(cudaGetLastError());
-    for (int s = 0; s < c.max_iterations; ++s) {
-      ibm_interp_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s);
-      ibm_spread_kernel<<<gs, IBM_BLOCK, 0, sx>>>(a);
-      ibm_diag_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s, int(gs));
-    }
-    CK(cudaGetLastError());
-    ibm_commit_kernel<A><<<gs, IBM_BLOCK, 0, sx>>>(a, fcur.p, s_torque, s_ff, s_it, counter);
-    CK(cudaGetLastError());
-  }
-
-  void ibm_apply(int b, const lbmb_ibm_config& c, lbmb_ibm_diag* out) override {
-    BodyState& B = body_for(b, c);
-    enqueue_ibm(B, c, nullptr, nullptr, nullptr, nullptr, field_present);
-    field_present = true;
-    fprev_stale = true;
-    IbmDiagDev d;
-    CK(cudaMemcpyAsync(&d, d_diag.p, sizeof(d), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (out) {
-      out->iterations = d.iterations;
-      out->slip_max = d.slip_max;
-      out->slip_rms = d.slip_rms;
-      out->slip_max_rel = d.slip_max_rel;
-      out->slip_rms_rel = d.slip_rms_rel;
-      for (int k = 0; k < 3; ++k) {
-        out->torque[k] = d.torque[k];
-        out->fluid_force[k] = d.fluid_force[k];
-        out->marker_force[k] = d.marker_force[k];
-      }
-      out->momentum_error_rel = d.momentum_error_rel;
-    }
-  }
-
-  // ---- scalars ----------------------------------------------------------
-  int enable_scalar(int q, double d) override {
-    if (!(std::isfinite(d) && d > 0.0)) invalid("scalar diffusivity must be finite > 0");
-    if (q != 7 && q != Q) invalid("scalar lattice must be D3Q7 or the hydro lattice");
-    auto sc = std::make_unique<ScalarStateT<A>>();
-    sc->q = q;
-    sc->diffusivity = d;
-    sc->hplane = plane;
-    sc->h.alloc(size_t(q) * plane);
-    CK(cudaMemsetAsync(sc->h.p, 0, size_t(q) * plane * sizeof(A), st));
-    sc->part.alloc(size_t(red_blocks));
-    sc->stats.alloc(4);
-    CK(cudaStreamSynchronize(st));
-    scalars.push_back(std::move(sc));
-    invalidate_graphs();
-    return int(scalars.size()) - 1;
-  }
-  ScalarStateT<A>& scalar(int k) {
-    if (k < 0 || k >= int(scalars.size())) throw Error(LBMB_ERR_STATE, "scalar distribution not enabled");
-    return *scalars[k];
-  }
-  void set_scalar(int k, const double* c) override {
-    auto& sc = scalar(k);
-    DevBuf<double> dc, du;
-    dc.upload(c, size_t(n), st);
-    du.upload(init_u_h, st);
-    ScalarParams<A> p = scalar_params(sc);
-    const unsigned g = unsigned(ceil_div(n, 128));
-    if (sc.q == 7) scalar_set_kernel<7, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
-    else scalar_set_kernel<Q, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
-    CK(cudaGetLastError());
-    sc.parity = 0;
-    CK(cudaStreamSynchronize(st));
-  }
-  void get_scalar(int k, double* c) override {
-    auto& sc = scalar(k);
-    DevBuf<double> dc;
-    dc.alloc(size_t(n));
-    const unsigned g = unsigned(ceil_div(n, 128));
-    if (sc.q == 7)
-      scalar_gather_kernel<7, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, dc.p, n);
-    else
-      scalar_gather_kernel<Q, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, dc.p, n);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(c, dc.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-  }
-  // Device CV of a scalar into *out (two deterministic passes).
-  void enqueue_cv(ScalarStateT<A>& sc, double* out, double nfluid) {
-    for (int pass = 0; pass < 2; ++pass) {
-      if (sc.q == 7)
-        scalar_cv_kernel<7, A><<<red_blocks, RED_BLOCK, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz,
-                                                                  sc.parity, n, pass, sc.stats.p, nfluid, sc.part.p);
-      else
-        scalar_cv_kernel<Q, A><<<red_blocks, RED_BLOCK, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz,
-                                                                  sc.parity, n, pass, sc.stats.p, nfluid, sc.part.p);
-      scalar_cv_finish_kernel<<<1, 32, 0, st>>>(sc.part.p, red_blocks, pass, sc.stats.p, nfluid, out);
-    }
-    CK(cudaGetLastError());
-  }
-
-  // ---- runner loop ------------------------------------------------------
-  void run_impeller(int b, const lbmb_ibm_config& c, int64_t steps, int k, int64_t probe_every, double* torque,
-                    double* ffo, double* cv, int32_t* iters) override {
-    BodyState& B = body_for(b, c);
-    if (k >= 0) scalar(k);
-    if (probe_every <= 0) probe_every = 1;
-    DevBuf<double> d_torque, d_ff, d_cv;
-    DevBuf<int32_t> d_it;
-    DevBuf<int64_t> d_counter;
-    d_torque.alloc(size_t(steps));
-    d_ff.alloc(size_t(3 * steps));
-    d_it.alloc(size_t(steps));
-    d_counter.alloc(1);
-    CK(cudaMemsetAsync(d_counter.p, 0, sizeof(int64_t), st));
-    if (k >= 0) {
-      d_cv.alloc(size_t(steps));
-      fill_nan(d_cv.p, steps);
-    }
-    CK(cudaEventRecord(ev0, st));
-    int64_t launches = 0;
-    auto one_step = [&](int64_t step_index) {
-      // Fork: the IBM chain (clear -> direct forcing -> forced-cell hydro)
-      // runs on the high-priority side stream while the full-grid sweep of
-      // every other cell runs on the main stream; the two touch disjoint
-      // population slots (each cell's AA read/write set is its own).
-      CK(cudaEventRecord(ev_fork, st));
-      CK(cudaStreamWaitEvent(st2, ev_fork, 0));
-      // Solver::clear_body_force_field: the IBM field is non-uniform, so the
-      // cached moments keep it (F_prev) while the new field starts at zero.
-      if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st2));
-      enqueue_ibm(B, c, d_torque.p, d_ff.p, d_it.p, d_counter.p, false, st2);
-      field_present = true;
-      fprev_stale = true;
-      launch_hydro(parity, st2, false, true);
-      launch_hydro(parity, st, true, false);
-      CK(cudaEventRecord(ev_join, st2));
-      CK(cudaStreamWaitEvent(st, ev_join, 0));
-      parity ^= 1;
-      if (fprev_stale) {
-        CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
-        fprev_stale = false;
-      }
-      for (auto& sc : scalars) scalar_step(*sc);
-      ++launches;
-      if (k >= 0 && ((step_index + 1) % probe_every == 0 || step_index + 1 == steps))
-        enqueue_cv(*scalars[k], d_cv.p + step_index, double(n - solid_count()));
-    };
-    // Graph capture of a block of G steps (parity-aligned), replayed.
-    const int64_t G = 16;
-    int64_t done = 0;
-    if (parity != 0 && steps > 0) {
-      one_step(done);
-      ++done;
-    }
-    const bool probes_every_step = (k >= 0);
-    if (!probes_every_step) {
-      cudaGraphExec_t exec = nullptr;
-      while (steps - done >= G) {
-        if (!exec) {
-          cudaGraph_t g;
-          const int par0 = parity;
-          CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-          for (int64_t i = 0; i < G; ++i) one_step(0);
-          CK(cudaStreamEndCapture(st, &g));
-          CK(cudaGraphInstantiate(&exec, g, 0));
-          CK(cudaGraphDestroy(g));
-          parity = par0;
-          launches -= G;
-        }
-        CK(cudaGraphLaunch(exec, st));
-        done += G;
-        launches += G;
-      }
-      if (exec) CK(cudaGraphExecDestroy(exec));
-    }
-    for (; done < steps; ++done) one_step(done);
-    CK(cudaEventRecord(ev1, st));
-    CK(cudaEventSynchronize(ev1));
-    check_device_error();
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ev0, ev1));
-    last_total_ms = ms;
-    last_hydro_ms = ms;
-    last_hydro_launches = launches;
-    if (torque) CK(cudaMemcpy(torque, d_torque.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
-    if (ffo) CK(cudaMemcpy(ffo, d_ff.p, size_t(3 * steps) * sizeof(double), cudaMemcpyDeviceToHost));
-    if (iters) CK(cudaMemcpy(iters, d_it.p, size_t(steps) * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    if (cv && k >= 0) CK(cudaMemcpy(cv, d_cv.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
-  }
-
-  int64_t solid_count() const {
-    int64_t s = 0;
-    for (auto v : solid_h) s += v ? 1 : 0;
-    return s;
-  }
-
-  void fill_nan(double* p, int64_t k) {
-    std::vector<double> h(size_t(k), std::nan(""));
-    CK(cudaMemcpyAsync(p, h.data(), size_t(k) * sizeof(double), cudaMemcpyHostToDevice, st));
-    CK(cudaStreamSynchronize(st));
-  }
-};
 
 // ---------------------------------------------------------------------------
 // Validation (GlobalSpec::validate, solver.rs:470-600) and construction.
@@ -1146,17 +64,17 @@ static EngineBase* make_engine(const lbmb_config& c, const uint8_t* solid, const
   validate(c, solid, wu);
   if (c.lattice == 19) {
     switch (c.storage) {
-      case LBMB_STORE_F32: return new Engine<19, float>(c, solid, wu);
-      case LBMB_STORE_F16: return new Engine<19, __half>(c, solid, wu);
-      case LBMB_STORE_BF16: return new Engine<19, __nv_bfloat16>(c, solid, wu);
-      default: return new Engine<19, double>(c, solid, wu);
+      case LBMB_STORE_F32: return make_engine_q19_f32(c, solid, wu);
+      case LBMB_STORE_F16: return make_engine_q19_f16(c, solid, wu);
+      case LBMB_STORE_BF16: return make_engine_q19_bf16(c, solid, wu);
+      default: return make_engine_q19_f64(c, solid, wu);
     }
   }
   switch (c.storage) {
-    case LBMB_STORE_F32: return new Engine<27, float>(c, solid, wu);
-    case LBMB_STORE_F16: return new Engine<27, __half>(c, solid, wu);
-    case LBMB_STORE_BF16: return new Engine<27, __nv_bfloat16>(c, solid, wu);
-    default: return new Engine<27, double>(c, solid, wu);
+    case LBMB_STORE_F32: return make_engine_q27_f32(c, solid, wu);
+    case LBMB_STORE_F16: return make_engine_q27_f16(c, solid, wu);
+    case LBMB_STORE_BF16: return make_engine_q27_bf16(c, solid, wu);
+    default: return make_engine_q27_f64(c, solid, wu);
   }
 }
 
