@@ -176,7 +176,7 @@ def run_b200(args, rank, world, local):
     import lbmflow_b200 as lb
 
     dims, solid, body, nu = tank_case(T=args.tank_T)
-    q, coll, storage = 27, "cm", args.storage
+    q, coll, storage = args.lattice, args.collision, args.storage
     os_ = 1.0 / (3.0 * nu + 0.5)
     n_cells = dims[0] * dims[1] * dims[2]
     n_fluid = int((solid == 0).sum())
@@ -322,6 +322,8 @@ def main():
     ap.add_argument("--hydro-steps", type=int, default=200)
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--tank-T", type=int, default=128, help="tank diameter in cells (128 = the benchmark case)")
+    ap.add_argument("--lattice", type=int, default=27, choices=[19, 27])
+    ap.add_argument("--collision", default="cm", choices=["cm", "trt"])
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--variants", type=int, default=1)

@@ -60,6 +60,11 @@ typedef struct lbmb_config {
   double magic;        /* TRT magic parameter (3/16 standard) */
   double omega_shear;  /* central-moment shear rate in (0, 2] */
   double force[3];     /* uniform Guo body force */
+  double smagorinsky_cs; /* 0: off (the reference's operators). > 0: Smagorinsky
+                          * LES, tau_eff = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2
+                          * |Pi_neq| / rho)) / 2 applied to the shear rate (no
+                          * reference counterpart; stabilises under-resolved
+                          * high-Re tanks) */
 } lbmb_config;
 
 /* DirectForcingConfig (crates/lbm-core/src/rotating_ibm.rs:106-130). */

@@ -345,6 +345,10 @@ struct Engine final : EngineBase {
     p.cp = A(1.0 - omega_p / 2.0);
     p.cm = A(1.0 - omega_m / 2.0);
     p.omega_shear = A(cfg.omega_shear);
+    const double cs = cfg.smagorinsky_cs;
+    p.les_c = A(cs > 0.0 ? 18.0 * std::sqrt(2.0) * cs * cs : 0.0);
+    p.tau0 = A(cfg.collision == LBMB_CENTRAL_MOMENT ? 1.0 / cfg.omega_shear : 3.0 * cfg.nu + 0.5);
+    p.magic = A(cfg.collision == LBMB_TRT ? cfg.magic : 0.0);
     p.gx = A(cfg.force[0]);
     p.gy = A(cfg.force[1]);
     p.gz = A(cfg.force[2]);

@@ -50,7 +50,59 @@ struct HydroParams {
   A omega_p, omega_m, cp, cm, omega_shear;
   A gx, gy, gz;  // uniform body force
   int uniform_force;
+  A les_c;  // 18 sqrt(2) Cs^2 (0: no LES)
+  A tau0;   // 3 nu + 1/2
+  A magic;  // TRT magic parameter (<= 0: BGK, omega_m = omega_p)
 };
+
+// Smagorinsky LES on the shear rate (no reference counterpart; off unless
+// les_c > 0). The non-equilibrium stress comes from the second moments of
+// the deviation populations, Pi = sum c c f - (rho - 1)/3 I - rho u u
+// (exact for the second-order equilibrium on D3Q19/D3Q27), and
+// tau_eff = (tau0 + sqrt(tau0^2 + les_c |Pi| / rho)) / 2.
+template <int Q, class A>
+__device__ __forceinline__ A les_tau(const A (&f)[Q], A rho, A ux, A uy, A uz, A les_c, A tau0) {
+  using L = Lat<Q>;
+  A sxx = A(0), syy = A(0), szz = A(0), sxy = A(0), sxz = A(0), syz = A(0);
+#pragma unroll
+  for (int q = 1; q < Q; ++q) {
+    const int cx = L::cx(q), cy = L::cy(q), cz = L::cz(q);
+    if (cx) sxx = sxx + f[q];
+    if (cy) syy = syy + f[q];
+    if (cz) szz = szz + f[q];
+    if (cx * cy == 1) sxy = sxy + f[q];
+    if (cx * cy == -1) sxy = sxy - f[q];
+    if (cx * cz == 1) sxz = sxz + f[q];
+    if (cx * cz == -1) sxz = sxz - f[q];
+    if (cy * cz == 1) syz = syz + f[q];
+    if (cy * cz == -1) syz = syz - f[q];
+  }
+  const A d3 = (rho - A(1)) * A(1.0 / 3.0);
+  const A pxx = sxx - d3 - rho * ux * ux, pyy = syy - d3 - rho * uy * uy, pzz = szz - d3 - rho * uz * uz;
+  const A pxy = sxy - rho * ux * uy, pxz = sxz - rho * ux * uz, pyz = syz - rho * uy * uz;
+  const A pn = sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
+  return A(0.5) * (tau0 + sqrt(tau0 * tau0 + les_c * pn / rho));
+}
+
+// Relaxation rates of one cell: the configured ones, or the LES-adjusted
+// ones (TRT keeps the magic parameter, BGK keeps omega_m = omega_p).
+template <int Q, class A>
+__device__ __forceinline__ void cell_rates(const HydroParams<A>& p, const A (&f)[Q], A rho, A ux, A uy, A uz, A& op,
+                                           A& om, A& cp, A& cm, A& os) {
+  op = p.omega_p;
+  om = p.omega_m;
+  cp = p.cp;
+  cm = p.cm;
+  os = p.omega_shear;
+  if (p.les_c > A(0)) {
+    const A te = les_tau<Q, A>(f, rho, ux, uy, uz, p.les_c, p.tau0);
+    op = A(1) / te;
+    om = p.magic > A(0) ? A(1) / (p.magic / (te - A(0.5)) + A(0.5)) : op;
+    cp = A(1) - op * A(0.5);
+    cm = A(1) - om * A(0.5);
+    os = op;
+  }
+}
 
 // TRT + Guo (crates/lbm-core/src/collision.rs:123-202), BGK when
 // omega_m == omega_p. Same operand grouping as the reference; the compiler
@@ -312,10 +364,12 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
   const A ux = (m0 + half * Fpx) * inv;
   const A uy = (m1 + half * Fpy) * inv;
   const A uz = (m2 + half * Fpz) * inv;
+  A op, om, cp, cm, os;
+  cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
   if constexpr (COLL == COLL_CM)
-    collide_cm<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, p.omega_shear);
+    collide_cm<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, os);
   else
-    collide_trt<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, p.omega_p, p.omega_m, p.cp, p.cm);
+    collide_trt<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, op, om, cp, cm);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     A v = f[q];

@@ -179,10 +179,12 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
           const A inv = A(1) / rho;
           const A ux = m0 * inv, uy = m1 * inv, uz = m2 * inv;
           const A z0 = A(0);
+          A op, om, cp, cm, os;
+          cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
           if constexpr (COLL == COLL_CM)
-            collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, p.omega_shear);
+            collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, os);
           else
-            collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, p.omega_p, p.omega_m, p.cp, p.cm);
+            collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, op, om, cp, cm);
 #pragma unroll
           for (int q = 0; q < Q; ++q) {
             A v = f[q];

@@ -27,6 +27,8 @@ static void validate(const lbmb_config& c, const uint8_t* solid, const double* w
     throw Error(LBMB_ERR_UNSUPPORTED, "central-moment collision is implemented for D3Q27");
   for (int a = 0; a < 3; ++a)
     if (!std::isfinite(c.force[a])) invalid("non-finite parameter: force");
+  if (!(std::isfinite(c.smagorinsky_cs) && c.smagorinsky_cs >= 0.0))
+    invalid("Smagorinsky constant must be finite and >= 0");
   for (int a = 0; a < 3; ++a)
     if (c.dims[a] < 3) invalid("domain too small: every axis needs >= 3 cells");
   const int64_t n = int64_t(c.dims[0]) * c.dims[1] * c.dims[2];

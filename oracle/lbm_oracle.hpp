@@ -135,6 +135,10 @@ struct StepParams {  // params.rs:302-320 (subset on the hot path)
   double omega_p = 1.0, omega_m = 1.0;
   double nu = 1.0 / 6.0;
   double force[3] = {0, 0, 0};
+  // Smagorinsky constant (0: off). Not a reference feature: an optional
+  // subgrid model of the device library that is restated here so the
+  // device path stays checkable with it switched on.
+  double smagorinsky_cs = 0.0;
 };
 
 template <class L, class T>
@@ -719,17 +723,62 @@ class Solver {
 
   void collide() {  // CpuScalar::collide (backend.rs:417-474)
     bool fon = force_on();
+    const bool les = params.smagorinsky_cs > 0.0;
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < long(n); ++c) {
       if (solid[c]) continue;
       T u[3] = {ux[c], uy[c], uz[c]};
       T fv[3];
       force_at(size_t(c), fv);
+      if (les) {
+        const KParams<T> kc = les_kparams(&f[c], rho[c], u);
+        if (kc.central_moment)
+          collide_cm_cell<L, T>(&f[c], n, rho[c], u, fv, kc);
+        else
+          collide_trt_cell<L, T>(&f[c], n, rho[c], u, fv, kc.omega_p, kc.cp, fon, kc);
+        continue;
+      }
       if (kp.central_moment)
         collide_cm_cell<L, T>(&f[c], n, rho[c], u, fv, kp);
       else
         collide_trt_cell<L, T>(&f[c], n, rho[c], u, fv, kp.omega_p, kp.cp, fon, kp);
     }
+  }
+
+  // Smagorinsky-adjusted rates of one cell: Pi_neq from the second moments
+  // of the deviation populations, Pi_neq = sum c c f_dev - (rho - 1)/3 I -
+  // rho u u; tau_eff = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 |Pi_neq| /
+  // rho)) / 2; TRT keeps its magic parameter, BGK and the central-moment
+  // shear rate take omega = 1 / tau_eff.
+  KParams<T> les_kparams(const T* fc, T rho_c, const T u[3]) const {
+    T s[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};  // xx yy zz xy xz yz
+    for (int q = 1; q < L::Q; ++q) {
+      const int cx = L::C[q][0], cy = L::C[q][1], cz = L::C[q][2];
+      const T fq = fc[size_t(q) * n];
+      if (cx) s[0] = s[0] + fq;
+      if (cy) s[1] = s[1] + fq;
+      if (cz) s[2] = s[2] + fq;
+      if (cx && cy) s[3] = cx * cy > 0 ? s[3] + fq : s[3] - fq;
+      if (cx && cz) s[4] = cx * cz > 0 ? s[4] + fq : s[4] - fq;
+      if (cy && cz) s[5] = cy * cz > 0 ? s[5] + fq : s[5] - fq;
+    }
+    const T d3 = (rho_c - T(1)) * T(1.0 / 3.0);
+    const T pxx = s[0] - d3 - rho_c * u[0] * u[0], pyy = s[1] - d3 - rho_c * u[1] * u[1];
+    const T pzz = s[2] - d3 - rho_c * u[2] * u[2];
+    const T pxy = s[3] - rho_c * u[0] * u[1], pxz = s[4] - rho_c * u[0] * u[2];
+    const T pyz = s[5] - rho_c * u[1] * u[2];
+    const T pn = std::sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + T(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
+    const double cs = params.smagorinsky_cs;
+    const T les_c = T(18.0 * std::sqrt(2.0) * cs * cs);
+    const T tau0 = T(params.collision == CENTRAL_MOMENT ? 1.0 / params.omega_shear_cfg : 3.0 * params.nu + 0.5);
+    const T te = T(0.5) * (tau0 + std::sqrt(tau0 * tau0 + les_c * pn / rho_c));
+    KParams<T> kc = kp;
+    kc.omega_p = T(1) / te;
+    kc.omega_m = params.collision == TRT ? T(1) / (T(params.magic) / (te - T(0.5)) + T(0.5)) : kc.omega_p;
+    kc.cp = T(1) - kc.omega_p * T(0.5);
+    kc.cm = T(1) - kc.omega_m * T(0.5);
+    kc.omega_shear = kc.omega_p;
+    return kc;
   }
 
   void stream() {  // stream_row (kernels.rs:547-622) over the full core

@@ -44,6 +44,7 @@ def lib():
                                   C.c_double, _dp, _u8p, _dp, C.c_char_p, C.c_int]
         L.lbmo_destroy.argtypes = [C.c_void_p]
         L.lbmo_step.argtypes = [C.c_void_p, C.c_int]
+        L.lbmo_set_smagorinsky.argtypes = [C.c_void_p, C.c_double]
         for name in ("lbmo_stage_in", "lbmo_stage_out", "lbmo_get_force_field"):
             getattr(L, name).argtypes = [C.c_void_p, _dp]
         L.lbmo_init_with.argtypes = [C.c_void_p, _dp, _dp]
@@ -110,7 +111,7 @@ class OracleSolver:
 
     def __init__(self, dims, q=19, real_bits=64, collision="trt", nu=1.0 / 6.0, magic=MAGIC_STD,
                  omega_shear=0.0, periodic=(False, False, False), force=(0.0, 0.0, 0.0),
-                 solid=None, wall_u=None):
+                 solid=None, wall_u=None, smagorinsky_cs=0.0):
         L = lib()
         self.dims = tuple(int(d) for d in dims)
         self.n = self.dims[0] * self.dims[1] * self.dims[2]
@@ -127,6 +128,8 @@ class OracleSolver:
                                _d(self._wall), err, 256)
         if not self.h:
             raise ValueError(err.value.decode())
+        if smagorinsky_cs:
+            L.lbmo_set_smagorinsky(self.h, float(smagorinsky_cs))
 
     def __del__(self):
         if getattr(self, "h", None):

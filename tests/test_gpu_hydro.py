@@ -22,13 +22,13 @@ class Pair:
     """GPU solver + oracle in the same precision (+ an f64 oracle for f32)."""
 
     def __init__(self, dims, q, prec, collision="trt", nu=0.05, periodic=(False,) * 3, force=(0, 0, 0),
-                 solid=None, wall_u=None, omega_shear=None):
+                 solid=None, wall_u=None, omega_shear=None, smagorinsky_cs=0.0):
         from oracle import oracle as o
         if omega_shear is None:
             omega_shear = 1.0 / (3.0 * nu + 0.5)
         self.prec = prec
         kw = dict(collision=collision, nu=nu, periodic=periodic, force=force, solid=solid, wall_u=wall_u,
-                  omega_shear=omega_shear)
+                  omega_shear=omega_shear, smagorinsky_cs=smagorinsky_cs)
         self.g = lb.Solver(dims, lattice=q, storage=prec, **kw)
         self.oracles = [o.OracleSolver(dims, q=q, real_bits=PREC_BITS[prec], **kw)]
         if prec == "f32":
@@ -125,6 +125,29 @@ def test_forced_channel_matches_oracle(q, coll):
     p.check(solid == 0)
     ux = p.g.read_moments()[1].reshape(12, 5, 6)[:, 2, 3]
     assert ux[6] > ux[2] > 0.0
+
+
+@pytest.mark.parametrize("q,coll", [(19, "trt"), (27, "trt"), (27, "cm"), (19, "bgk")])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_smagorinsky_cavity_matches_oracle(q, coll, prec):
+    # Under-resolved lid-driven cavity (Re 2000 on 14^3) with the optional
+    # Smagorinsky subgrid model: per-cell relaxation rates from |Pi_neq|.
+    dims, solid, wall_u, nu = cavity(14, u_lid=0.08, re=2000.0)
+    p = Pair(dims, q, prec, collision=coll, nu=nu, solid=solid, wall_u=wall_u, smagorinsky_cs=0.17)
+    p.run(45)
+    p.check(solid == 0)
+
+
+@pytest.mark.parametrize("q,coll", [(19, "trt"), (27, "cm")])
+def test_smagorinsky_forced_tgv_matches_oracle(q, coll):
+    # Periodic box with a body force on top of a Taylor-Green field, LES on.
+    dims = (10, 8, 8)
+    p = Pair(dims, q, "f64", collision=coll, nu=0.002, periodic=(True, True, True), force=(2e-6, -1e-6, 0.0),
+             smagorinsky_cs=0.2)
+    rho, u = tgv_fields(dims, amp=0.05)
+    p.init_with(rho, u)
+    p.run(25)
+    p.check(np.ones(p.n, bool))
 
 
 @pytest.mark.parametrize("q", [19, 27])
@@ -234,3 +257,5 @@ def test_invalid_specs_rejected():
         lb.Solver(dims, lattice=19, collision="cm", nu=0.1, solid=solid, wall_u=wall_u)
     with pytest.raises(lb.SpecError):
         lb.Solver(dims, nu=0.1, solid=solid, wall_u=wall_u * 10.0)
+    with pytest.raises(lb.SpecError):
+        lb.Solver(dims, nu=0.1, solid=solid, wall_u=wall_u, smagorinsky_cs=-0.1)
