@@ -241,6 +241,34 @@ int lbmb_build_stirred_tank(const lbmb_tank_spec* spec, uint8_t* solid, uint8_t*
 int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, int64_t ncells, int64_t plane,
                                     const uint8_t* solid, const double force[3], double out[5], void* stream);
 
+/* Sweep kernel of the fused collide-stream (no reference counterpart: the
+ * reference has one CPU row loop per operator). All kinds compute the same
+ * update; they differ in how populations reach the registers:
+ *   LBMB_SWEEP_DIRECT  one cell per thread, direct loads (every config);
+ *   LBMB_SWEEP_BULK    bulk asynchronous copies staged in shared memory;
+ *   LBMB_SWEEP_ASYNC   per-thread cp.async ring (4/8-byte storage);
+ *   LBMB_SWEEP_PAIR    two x-adjacent cells per thread, 2-element accesses
+ *                      and packed fp32x2 arithmetic (TRT/BGK, fp32/fp16/
+ *                      bf16 storage, even nx, no uniform body force);
+ *   LBMB_SWEEP_TILE    the pair update fed by 16-byte cp.async windows
+ *                      staged in shared memory several tiles ahead (same
+ *                      conditions as LBMB_SWEEP_PAIR);
+ *   LBMB_SWEEP_LEAN    one cell per thread with a small register footprint
+ *                      for high occupancy (TRT/BGK, fp32/fp16/bf16 storage,
+ *                      no uniform body force).
+ * A kind that cannot run the solver's configuration returns
+ * LBMB_ERR_UNSUPPORTED and leaves the current kind in place. */
+typedef enum {
+  LBMB_SWEEP_DIRECT = 0,
+  LBMB_SWEEP_BULK = 1,
+  LBMB_SWEEP_ASYNC = 2,
+  LBMB_SWEEP_PAIR = 3,
+  LBMB_SWEEP_TILE = 4,
+  LBMB_SWEEP_LEAN = 5
+} lbmb_sweep_kind;
+int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
+int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
+
 /* Synchronize the solver stream. */
 int lbmb_sync(lbmb_solver* h);
 

@@ -25,6 +25,7 @@ _i64p = C.POINTER(C.c_int64)
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6
 COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
+SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5}
 IMPELLER = {"rushton": 0, "pitched": 1, "flat_blade": 2}
 MAGIC_STD = 3.0 / 16.0
 RED_FLUID_CELLS, RED_MASS_DEV, RED_MOMENTUM = 0, 1, 2
@@ -38,6 +39,7 @@ EXPORTS = (
     "lbmb_apply_rotating_ibm", "lbmb_enable_scalar", "lbmb_set_scalar_concentration",
     "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
     "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
+    "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel",
 )
 
 
@@ -132,6 +134,8 @@ def lib():
         L.lbmb_build_stirred_tank.argtypes = [C.POINTER(_TankSpec), _u8p, _u8p, _dp, _dp, _dp, C.c_int64,
                                               _i64p, _dp, _dp]
         L.lbmb_sync.argtypes = [vp]
+        L.lbmb_set_sweep_kernel.argtypes = [vp, C.c_int32]
+        L.lbmb_get_sweep_kernel.argtypes = [vp, _i32p]
         L.lbmb_reduce_populations_noalloc.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, vp, _dp,
                                                       _dp, vp]
         _lib = L
@@ -271,6 +275,17 @@ class Solver:
 
     def sync(self):
         _check(lib().lbmb_sync(self.h))
+
+    def set_sweep_kernel(self, kind):
+        """Pick the collide-stream kernel ("direct", "bulk", "async", "pair", "tile", "lean");
+        UnsupportedError if it cannot run this configuration."""
+        _check(lib().lbmb_set_sweep_kernel(self.h, SWEEP[kind] if isinstance(kind, str) else int(kind)))
+
+    @property
+    def sweep_kernel(self):
+        k = C.c_int32()
+        _check(lib().lbmb_get_sweep_kernel(self.h, C.byref(k)))
+        return {v: n for n, v in SWEEP.items()}[k.value]
 
     def last_timing(self):
         t, hy, k = C.c_double(), C.c_double(), C.c_int64()

@@ -16,6 +16,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/lbmb.h"
@@ -23,6 +24,9 @@
 #include "hydro.cuh"
 #include "hydro_tma.cuh"
 #include "hydro_async.cuh"
+#include "hydro_pair.cuh"
+#include "hydro_tile.cuh"
+#include "hydro_lean.cuh"
 #include "ibm.cuh"
 #include "scalar.cuh"
 
@@ -115,6 +119,8 @@ struct EngineBase {
   virtual void run_impeller(int b, const lbmb_ibm_config& cfg, int64_t steps, int k, int64_t probe_every,
                             double* torque, double* ff, double* cv, int32_t* iters) = 0;
   virtual void sync() = 0;
+  virtual void set_sweep_kernel(int kind) = 0;
+  virtual int sweep_kernel() const = 0;
   virtual int64_t cells() const = 0;
   virtual int q() const = 0;
   virtual const std::vector<uint8_t>& solid() const = 0;
@@ -157,7 +163,12 @@ struct Engine final : EngineBase {
   int sm_count = 148;
   int64_t ntiles = 0;
   bool rows_aligned = false;
-  int kernel_mode = 2;  // 0 direct, 1 TMA bulk-staged, 2 per-thread async pipeline
+  int kernel_mode = 2;  // lbmb_sweep_kind
+  // tile-pipelined sweep: tiles holding a non-solid cell, window offsets
+  DevBuf<int32_t> tile_list;
+  int n_tiles_active = 0;
+  TileDirs tile_dirs[2];
+  int tile_grid[2] = {0, 0};
   int tma_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int async_grid[4] = {0, 0, 0, 0};
   // reductions
@@ -216,9 +227,12 @@ struct Engine final : EngineBase {
     CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c.device));
     ntiles = ceil_div(n, TMA_TILE);
     rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
-    if (sizeof(S) < 4) kernel_mode = 0;  // 16-bit storage: cp.async needs 4-byte elements
-    if (const char* e = std::getenv("LBMB_KERNEL")) kernel_mode = std::atoi(e);
-    if (sizeof(S) < 4 && kernel_mode == 2) kernel_mode = 0;
+    // default sweep: the pair kernel where it applies (TRT/BGK, fp32/16-bit
+    // storage, even nx, no uniform force), else cp.async (4/8-byte storage)
+    // or direct loads
+    if (sizeof(S) < 4) kernel_mode = LBMB_SWEEP_DIRECT;
+    if (std::is_same<A, float>::value && coll == COLL_TRT && nx % 2 == 0 && !has_uniform_force())
+      kernel_mode = LBMB_SWEEP_PAIR;
     red_blocks = int(std::min<int64_t>(ceil_div(n, RED_BLOCK), 1184));
     red_part.alloc(size_t(red_blocks) * 5);
     red_out.alloc(8);
@@ -288,6 +302,7 @@ struct Engine final : EngineBase {
     nbr.upload(nb, st);
     wall_u.upload(w, st);
     CK(cudaStreamSynchronize(st));
+    build_tiles();
   }
 
   void invalidate_graphs() {
@@ -389,10 +404,103 @@ struct Engine final : EngineBase {
     CK(cudaGetLastError());
   }
 
+  void set_sweep_kernel(int kind) override {
+    const bool wide = sizeof(S) >= 4;
+    const bool pair = std::is_same<A, float>::value && coll == COLL_TRT && nx % 2 == 0 && !has_uniform_force();
+    if (kind == LBMB_SWEEP_ASYNC && !wide)
+      throw Error(LBMB_ERR_UNSUPPORTED, "the cp.async sweep needs 4- or 8-byte population storage");
+    if ((kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE) && !pair)
+      throw Error(LBMB_ERR_UNSUPPORTED,
+                  "the pair sweep needs TRT/BGK, fp32/fp16/bf16 storage, even nx and no uniform body force");
+    if (kind == LBMB_SWEEP_LEAN && !lean_ok(coll))
+      throw Error(LBMB_ERR_UNSUPPORTED, "the lean sweep needs TRT/BGK, fp32/fp16/bf16 storage and no uniform body force");
+    kernel_mode = kind;
+    invalidate_graphs();
+  }
+  int sweep_kernel() const override { return kernel_mode; }
+  bool has_uniform_force() const { return cfg.force[0] != 0.0 || cfg.force[1] != 0.0 || cfg.force[2] != 0.0; }
+
+  bool lean_ok(int coll_kind) const {
+    return std::is_same<A, float>::value && coll_kind == COLL_TRT && !has_uniform_force();
+  }
+
+  template <bool ODD>
+  void launch_lean(const HydroParams<A>& p, cudaStream_t s) {
+    if constexpr (std::is_same<A, float>::value) {
+      hydro_lean_kernel<Q, S, ODD><<<unsigned(ceil_div(n, LEAN_BLOCK)), LEAN_BLOCK, 0, s>>>(p, uint32_t(n));
+      CK(cudaGetLastError());
+    }
+  }
+
+  // Whether the two-cells-per-thread kernel covers this sweep.
+  bool pair_ok(const HydroParams<A>& p, int coll_kind) const {
+    return std::is_same<A, float>::value && coll_kind == COLL_TRT && !p.uniform_force && nx % 2 == 0;
+  }
+
+  // Tile list and window offsets of the tile-pipelined sweep.
+  void build_tiles() {
+    const int64_t nt = ceil_div(n, TILE_CELLS);
+    std::vector<int32_t> list;
+    for (int64_t t = 0; t < nt; ++t) {
+      bool any = false;
+      for (int64_t c = t * TILE_CELLS; c < std::min<int64_t>(n, (t + 1) * TILE_CELLS) && !any; ++c)
+        any = !(flags_h[size_t(c)] & F_SOLID);
+      if (any) list.push_back(int32_t(t));
+    }
+    n_tiles_active = int(list.size());
+    tile_list.alloc(list.size());
+    if (!list.empty())
+      CK(cudaMemcpyAsync(tile_list.p, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    using L = Lat<Q>;
+    const int64_t E = 16 / int64_t(sizeof(S));
+    for (int q = 0; q < Q; ++q) {
+      tile_dirs[0].ws[q] = int32_t(int64_t(q) * plane);
+      tile_dirs[0].r[q] = 0;
+      const int64_t d = int64_t(L::cx(q)) + int64_t(L::cy(q)) * nx + int64_t(L::cz(q)) * nx * ny;
+      const int64_t start = int64_t(opp(q)) * plane - d;  // >= 0: plane >= n > |d|
+      tile_dirs[1].r[q] = int32_t(start % E);
+      tile_dirs[1].ws[q] = int32_t(start - start % E);
+    }
+    CK(cudaStreamSynchronize(st));
+  }
+
+  template <bool ODD>
+  void launch_tile(const HydroParams<A>& p, cudaStream_t s) {
+    if constexpr (std::is_same<A, float>::value) {
+      constexpr int STAGES = 3;
+      auto kern = hydro_tile_kernel<Q, S, ODD, STAGES>;
+      const size_t smem = tile_smem_bytes<Q, S, STAGES>();
+      if (tile_grid[ODD] == 0) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_THREADS, smem));
+        tile_grid[ODD] = int(std::max<int64_t>(1, std::min<int64_t>(n_tiles_active, int64_t(sm_count) * std::max(per_sm, 1))));
+      }
+      if (n_tiles_active == 0) return;
+      kern<<<unsigned(tile_grid[ODD]), TILE_THREADS, smem, s>>>(p, tile_list.p, n_tiles_active, tile_dirs[ODD]);
+      CK(cudaGetLastError());
+    }
+  }
+
+  template <bool ODD>
+  void launch_pair(const HydroParams<A>& p, cudaStream_t s) {
+    if constexpr (std::is_same<A, float>::value) {
+      const uint32_t npairs = uint32_t(n / 2);
+      hydro_pair_kernel<Q, S, ODD><<<unsigned(ceil_div(npairs, PAIR_BLOCK)), PAIR_BLOCK, 0, s>>>(p, npairs);
+      CK(cudaGetLastError());
+    }
+  }
+
   template <int COLL, bool ODD>
   void launch_hydro_t(const HydroParams<A>& p, cudaStream_t s, bool main_grid, bool cells) {
     if (main_grid) {
-      if (!p.uniform_force && kernel_mode == 1) {
+      if (kernel_mode == LBMB_SWEEP_PAIR && pair_ok(p, COLL)) {
+        launch_pair<ODD>(p, s);
+      } else if (kernel_mode == LBMB_SWEEP_TILE && pair_ok(p, COLL)) {
+        launch_tile<ODD>(p, s);
+      } else if (kernel_mode == LBMB_SWEEP_LEAN && lean_ok(COLL) && !p.uniform_force) {
+        launch_lean<ODD>(p, s);
+      } else if (!p.uniform_force && kernel_mode == 1) {
         if (rows_aligned) launch_tma<COLL, ODD, true>(p, s);
         else launch_tma<COLL, ODD, false>(p, s);
       } else if (!p.uniform_force && kernel_mode == 2) {

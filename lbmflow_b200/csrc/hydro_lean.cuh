@@ -1,0 +1,145 @@
+// One cell per thread AA collide-stream with a small register footprint
+// (TRT / BGK, no uniform body force, fp32 | fp16 | bf16 storage).
+//
+// The kernel is built for occupancy: a flat grid over the cells, 32-bit
+// element offsets, a branch-free pointer select for directions that bounce
+// off a solid neighbour, the pair-folded TRT algebra of hydro_pair.cuh in
+// scalar form (S = f_a + f_b and D = f_a - f_b are recomputed where they are
+// needed instead of being kept live), and single-instruction reciprocals.
+// With 16-bit storage every access is one element, so no direction needs
+// alignment handling and the odd step costs the same instructions as the
+// even one; latency is hidden by the number of resident warps.
+#pragma once
+#include "hydro_pair.cuh"
+
+namespace lbmb {
+
+constexpr int LEAN_BLOCK = 128;
+
+template <int Q>
+__device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroParams<float>& p) {
+  using L = Lat<Q>;
+  constexpr int NP = (Q - 1) / 2;
+  static_assert(pair_heads_positive<Q>(), "pair head convention");
+  float drho = f[0];
+  float jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    const int a = 2 * k + 1, b = a + 1;
+    drho += f[a] + f[b];
+    const float d = f[a] - f[b];
+    if (L::cx(a) == 1) jx += d;
+    if (L::cx(a) == -1) jx -= d;
+    if (L::cy(a) == 1) jy += d;
+    if (L::cy(a) == -1) jy -= d;
+    if (L::cz(a) == 1) jz += d;
+    if (L::cz(a) == -1) jz -= d;
+  }
+  const float rho = drho + 1.f;
+  const float inv = rcp_fast(rho);
+  const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  const float usq = ux * ux + uy * uy + uz * uz;
+  float op = p.omega_p, om = p.omega_m;
+  if (p.les_c > 0.f) {
+    float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int a = 2 * k + 1;
+      const int cx = L::cx(a), cy = L::cy(a), cz = L::cz(a);
+      const float sv = f[a] + f[a + 1];
+      if (cx) s[0] += sv;
+      if (cy) s[1] += sv;
+      if (cz) s[2] += sv;
+      if (cx && cy) s[3] += float(cx * cy) * sv;
+      if (cx && cz) s[4] += float(cx * cz) * sv;
+      if (cy && cz) s[5] += float(cy * cz) * sv;
+    }
+    const float te = les_tau_pair<Q>(s, rho, inv, ux, uy, uz, p.les_c, p.tau0);
+    op = rcp_fast(te);
+    if (p.magic > 0.f) {
+      const float l = te - 0.5f;
+      om = l * rcp_fast(p.magic + 0.5f * l);
+    } else {
+      om = op;
+    }
+  }
+  const float base = drho - 1.5f * rho * usq;
+  const float nhop = -0.5f * op, hom = 0.5f * om;
+  float oA[3], oB[3], nC[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int a = k == 0 ? 1 : (k == 1 ? 7 : 19);
+    if (a >= Q) continue;
+    const float w = float(L::w(a));
+    oA[k] = (op * w) * base;
+    oB[k] = (op * (4.5f * w)) * rho;
+    nC[k] = (om * (-3.f * w)) * rho;
+  }
+  f[0] = (1.f - op) * f[0] + (op * float(L::w(0))) * base;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    const int a = 2 * k + 1, b = a + 1;
+    const int cl = wclass<Q>(a);
+    float cu = L::cx(a) ? ux : (L::cy(a) ? uy : uz);
+    if (L::cx(a) && L::cy(a)) cu = L::cy(a) > 0 ? cu + uy : cu - uy;
+    if ((L::cx(a) || L::cy(a)) && L::cz(a)) cu = L::cz(a) > 0 ? cu + uz : cu - uz;
+    const float t = oB[cl] * (cu * cu) + oA[cl];
+    const float pn = nhop * (f[a] + f[b]) + t;     // -rp
+    const float m = nC[cl] * cu + hom * (f[a] - f[b]);  // rm
+    f[a] = (f[a] + pn) - m;
+    f[b] = (f[b] + pn) + m;
+  }
+  return rho;
+}
+
+template <int Q, class S, bool ODD>
+__global__ void __launch_bounds__(LEAN_BLOCK, 8) hydro_lean_kernel(HydroParams<float> p, uint32_t n) {
+  using L = Lat<Q>;
+  using CD = Codec<S>;
+  const uint32_t c = blockIdx.x * LEAN_BLOCK + threadIdx.x;
+  if (c >= n) return;
+  const uint32_t fl = p.flags[c];
+  if (fl & (F_SOLID | F_FORCED)) return;
+  const int nx = p.nx, nxy = p.nxy;
+  if (fl & F_WRAP) {
+    const int z = int(c / uint32_t(nxy));
+    const int r = int(c - uint32_t(z) * uint32_t(nxy));
+    const int y = r / nx;
+    hydro_cell_generic<Q, S, COLL_TRT, ODD, false>(p, r - y * nx, y, z, c, uint8_t(fl));
+    return;
+  }
+  const uint32_t mk = (fl & F_BOUNDARY) ? p.nbr[c] : 0u;
+  S* fb = static_cast<S*>(p.f);
+  const uint32_t pl = p.plane;
+  auto dq = [&](int q) { return L::cx(q) + L::cy(q) * nx + L::cz(q) * nxy; };
+  float f[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (!ODD) {
+      f[q] = CD::ld(fb + (uint32_t(q) * pl + c));
+    } else {
+      const int o = opp(q);
+      const uint32_t off = ((mk >> o) & 1u) ? uint32_t(q) * pl + c : uint32_t(o) * pl + c - uint32_t(dq(q));
+      f[q] = CD::ld(fb + off);
+    }
+  }
+  const float rho = trt_lean_collide<Q>(f, p);
+  // a fresh copy of the base pointer: keeps the compiler from holding the
+  // load addresses live across the collision to reuse them for the stores
+  S* fs = fb;
+  asm volatile("" : "+l"(fs));
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int o = opp(q);
+    float v = f[q];
+    const bool wall = (mk >> q) & 1u;
+    if (wall && (fl & F_MOVING)) {
+      const Vec4<float> wu = p.wall_u[int32_t(c) + dq(q)];
+      v += ((6.f * float(L::w(o))) * rho) * ((float(L::cx(o)) * wu.x + float(L::cy(o)) * wu.y) + float(L::cz(o)) * wu.z);
+    }
+    const uint32_t off = (!ODD || wall) ? uint32_t(o) * pl + c : uint32_t(q) * pl + c + uint32_t(dq(q));
+    CD::st(fs + off, v);
+  }
+}
+
+}  // namespace lbmb

@@ -347,6 +347,22 @@ int lbmb_last_timing(lbmb_solver* h, double* total_ms, double* hydro_ms, int64_t
   });
 }
 
+int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind) {
+  return guarded([&] {
+    NEED(h);
+    if (kind < LBMB_SWEEP_DIRECT || kind > LBMB_SWEEP_LEAN) lbmb::invalid("unknown sweep kernel kind");
+    h->e->set_sweep_kernel(kind);
+  });
+}
+
+int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind) {
+  return guarded([&] {
+    NEED(h);
+    if (!kind) lbmb::invalid("null output");
+    *kind = h->e->sweep_kernel();
+  });
+}
+
 int lbmb_sync(lbmb_solver* h) {
   return guarded([&] {
     NEED(h);

@@ -11,73 +11,9 @@ import numpy as np
 import pytest
 
 import lbmflow_b200 as lb
-from cases import TOL, cavity, rel_err, seeded_state, tgv_fields
+from cases import TOL, Pair, cavity, rel_err, seeded_state, tgv_fields
 
 pytestmark = pytest.mark.gpu
-
-PREC_BITS = {"f64": 64, "f32": 32}
-
-
-class Pair:
-    """GPU solver + oracle in the same precision (+ an f64 oracle for f32)."""
-
-    def __init__(self, dims, q, prec, collision="trt", nu=0.05, periodic=(False,) * 3, force=(0, 0, 0),
-                 solid=None, wall_u=None, omega_shear=None, smagorinsky_cs=0.0):
-        from oracle import oracle as o
-        if omega_shear is None:
-            omega_shear = 1.0 / (3.0 * nu + 0.5)
-        self.prec = prec
-        kw = dict(collision=collision, nu=nu, periodic=periodic, force=force, solid=solid, wall_u=wall_u,
-                  omega_shear=omega_shear, smagorinsky_cs=smagorinsky_cs)
-        self.g = lb.Solver(dims, lattice=q, storage=prec, **kw)
-        self.oracles = [o.OracleSolver(dims, q=q, real_bits=PREC_BITS[prec], **kw)]
-        if prec == "f32":
-            self.oracles.append(o.OracleSolver(dims, q=q, real_bits=64, **kw))
-        self.n = self.g.n
-
-    def init_with(self, rho, u):
-        self.g.init_with(rho, u)
-        for c in self.oracles:
-            c.init_with(rho, u)
-
-    def stage_in(self, f):
-        self.g.stage_in(f)
-        for c in self.oracles:
-            c.stage_in(f)
-
-    def run(self, steps):
-        self.g.run(steps)
-        for c in self.oracles:
-            c.step(steps)
-
-    def check(self, fluid):
-        """f64: populations within 1e-11 of the max population, moments
-        within 1e-10. f32: the GPU's distance to the f64 oracle is at most
-        3x the reference f32 path's own distance to it (+1e-9): the GPU is as
-        accurate as the reference CPU path in the same precision."""
-        fg = self.g.stage_out()[:, fluid]
-        rg, ug = self._mom(self.g.read_moments(), fluid)
-        c = self.oracles[0]
-        fc = c.stage_out()[:, fluid]
-        rc, uc = self._mom(c.moments(), fluid)
-        if self.prec == "f64":
-            scale = max(np.abs(fc).max(), 1e-30)
-            assert np.abs(fg - fc).max() / scale < TOL["f64"]
-            assert np.abs(rg - rc).max() < 1e-10
-            assert np.abs(ug - uc).max() / max(np.abs(uc).max(), 1e-30) < 1e-10
-            return
-        c64 = self.oracles[1]
-        f64 = c64.stage_out()[:, fluid]
-        r64, u64 = self._mom(c64.moments(), fluid)
-        for gpu, ref, exact in ((fg, fc, f64), (rg, rc, r64), (ug, uc, u64)):
-            e_gpu = np.abs(gpu - exact).max()
-            e_ref = np.abs(ref - exact).max()
-            assert e_gpu <= 3.0 * e_ref + 1e-9, (e_gpu, e_ref)
-
-    @staticmethod
-    def _mom(m, fluid):
-        return m[0][fluid], np.stack([m[1][fluid], m[2][fluid], m[3][fluid]])
-
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("steps", [1, 2, 37])
