@@ -268,6 +268,30 @@ typedef enum {
 } lbmb_sweep_kind;
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
+/* Register budget of the lean sweep per parity, as resident 128-thread
+ * blocks per SM the kernel is compiled for: 8 (64 registers), 7 (72) or 6
+ * (80). More registers avoid spills, fewer keep more warps resident; the
+ * best split depends on the lattice and storage (no reference counterpart). */
+int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
+
+/* Sweep autotuner (no reference counterpart): times every sweep kernel kind
+ * that can run this solver's configuration, and every register budget of
+ * the lean kernel, for steps_per_trial hydro steps each on the solver's own
+ * grid and state, selects the fastest and restores the populations, so the
+ * simulation continues exactly as before the call. Optional per-trial
+ * outputs (capacity entries): trial_desc[3 i] = {kind, even, odd blocks per
+ * SM (0 for kinds without a register budget)}, trial_ms[i] = ms per step.
+ * Needs one extra population buffer of device memory while it runs. */
+typedef struct {
+  int32_t kind;
+  int32_t even_blocks_per_sm;
+  int32_t odd_blocks_per_sm;
+  int32_t n_trials;
+  double best_ms_per_step;
+  double default_ms_per_step; /* the kernel in place before the call */
+} lbmb_autotune_result;
+int lbmb_autotune_sweep(lbmb_solver* h, int32_t steps_per_trial, lbmb_autotune_result* out,
+                        int32_t* trial_desc, double* trial_ms, int32_t capacity);
 
 /* Synchronize the solver stream. */
 int lbmb_sync(lbmb_solver* h);

@@ -39,7 +39,7 @@ EXPORTS = (
     "lbmb_apply_rotating_ibm", "lbmb_enable_scalar", "lbmb_set_scalar_concentration",
     "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
     "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
-    "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel",
+    "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
 )
 
 
@@ -72,6 +72,11 @@ class _Config(C.Structure):
                 ("dims", C.c_int32 * 3), ("periodic", C.c_int32 * 3), ("device", C.c_int32),
                 ("nu", C.c_double), ("magic", C.c_double), ("omega_shear", C.c_double),
                 ("force", C.c_double * 3), ("smagorinsky_cs", C.c_double)]
+
+
+class _AutotuneResult(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("even_blocks_per_sm", C.c_int32), ("odd_blocks_per_sm", C.c_int32),
+                ("n_trials", C.c_int32), ("best_ms_per_step", C.c_double), ("default_ms_per_step", C.c_double)]
 
 
 class _IbmConfig(C.Structure):
@@ -136,6 +141,8 @@ def lib():
         L.lbmb_sync.argtypes = [vp]
         L.lbmb_set_sweep_kernel.argtypes = [vp, C.c_int32]
         L.lbmb_get_sweep_kernel.argtypes = [vp, _i32p]
+        L.lbmb_set_sweep_variant.argtypes = [vp, C.c_int32, C.c_int32]
+        L.lbmb_autotune_sweep.argtypes = [vp, C.c_int32, C.POINTER(_AutotuneResult), _i32p, _dp, C.c_int32]
         L.lbmb_reduce_populations_noalloc.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, vp, _dp,
                                                       _dp, vp]
         _lib = L
@@ -280,6 +287,26 @@ class Solver:
         """Pick the collide-stream kernel ("direct", "bulk", "async", "pair", "tile", "lean");
         UnsupportedError if it cannot run this configuration."""
         _check(lib().lbmb_set_sweep_kernel(self.h, SWEEP[kind] if isinstance(kind, str) else int(kind)))
+
+    def set_sweep_variant(self, even_blocks_per_sm, odd_blocks_per_sm):
+        """Register budget of the lean sweep per parity (blocks per SM 6..8)."""
+        _check(lib().lbmb_set_sweep_variant(self.h, int(even_blocks_per_sm), int(odd_blocks_per_sm)))
+
+    def autotune_sweep(self, steps_per_trial=20):
+        """Time every applicable sweep kernel on this solver's grid and keep
+        the fastest (state preserved). Returns the choice and the trials."""
+        cap = 64
+        r = _AutotuneResult()
+        desc = np.zeros(3 * cap, dtype=np.int32)
+        ms = np.zeros(cap)
+        _check(lib().lbmb_autotune_sweep(self.h, int(steps_per_trial), C.byref(r), desc.ctypes.data_as(_i32p),
+                                         _d(ms), cap))
+        names = {v: k for k, v in SWEEP.items()}
+        trials = [(names[int(desc[3 * i])], int(desc[3 * i + 1]), int(desc[3 * i + 2]), float(ms[i]))
+                  for i in range(min(r.n_trials, cap))]
+        return {"kind": names[r.kind], "even_blocks_per_sm": r.even_blocks_per_sm,
+                "odd_blocks_per_sm": r.odd_blocks_per_sm, "best_ms_per_step": r.best_ms_per_step,
+                "default_ms_per_step": r.default_ms_per_step, "trials": trials}
 
     @property
     def sweep_kernel(self):

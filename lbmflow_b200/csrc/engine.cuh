@@ -121,6 +121,9 @@ struct EngineBase {
   virtual void sync() = 0;
   virtual void set_sweep_kernel(int kind) = 0;
   virtual int sweep_kernel() const = 0;
+  virtual void set_sweep_variant(int even, int odd) = 0;
+  virtual void autotune_sweep(int steps, lbmb_autotune_result* out, int32_t* trial_desc, double* trial_ms,
+                              int capacity) = 0;
   virtual int64_t cells() const = 0;
   virtual int q() const = 0;
   virtual const std::vector<uint8_t>& solid() const = 0;
@@ -227,12 +230,11 @@ struct Engine final : EngineBase {
     CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c.device));
     ntiles = ceil_div(n, TMA_TILE);
     rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
-    // default sweep: the pair kernel where it applies (TRT/BGK, fp32/16-bit
-    // storage, even nx, no uniform force), else cp.async (4/8-byte storage)
-    // or direct loads
+    // default sweep: the lean kernel where it applies (TRT/BGK, fp32/16-bit
+    // storage, no uniform force), else cp.async (4/8-byte storage) or direct
+    // loads
     if (sizeof(S) < 4) kernel_mode = LBMB_SWEEP_DIRECT;
-    if (std::is_same<A, float>::value && coll == COLL_TRT && nx % 2 == 0 && !has_uniform_force())
-      kernel_mode = LBMB_SWEEP_PAIR;
+    if (lean_ok(coll)) kernel_mode = LBMB_SWEEP_LEAN;
     red_blocks = int(std::min<int64_t>(ceil_div(n, RED_BLOCK), 1184));
     red_part.alloc(size_t(red_blocks) * 5);
     red_out.alloc(8);
@@ -418,17 +420,37 @@ struct Engine final : EngineBase {
     invalidate_graphs();
   }
   int sweep_kernel() const override { return kernel_mode; }
+  void set_sweep_variant(int even, int odd) override {
+    auto ok = [](int v) { return v >= 6 && v <= 8; };
+    if (!ok(even) || !ok(odd)) throw Error(LBMB_ERR_INVALID, "sweep variant: resident blocks per SM must be 6, 7 or 8");
+    lean_minb[0] = even;
+    lean_minb[1] = odd;
+    invalidate_graphs();
+  }
   bool has_uniform_force() const { return cfg.force[0] != 0.0 || cfg.force[1] != 0.0 || cfg.force[2] != 0.0; }
 
   bool lean_ok(int coll_kind) const {
     return std::is_same<A, float>::value && coll_kind == COLL_TRT && !has_uniform_force();
   }
 
+  // Register budget of the lean sweep per parity (resident blocks per SM:
+  // 8 = 64 registers, 7 = 72, 6 = 80); set by lbmb_set_sweep_variant.
+  int lean_minb[2] = {8, 6};
+
+  template <bool ODD, int MINB>
+  void launch_lean_mb(const HydroParams<A>& p, cudaStream_t s) {
+    if constexpr (std::is_same<A, float>::value) {
+      hydro_lean_kernel<Q, S, ODD, MINB><<<unsigned(ceil_div(n, LEAN_BLOCK)), LEAN_BLOCK, 0, s>>>(p, uint32_t(n));
+      CK(cudaGetLastError());
+    }
+  }
+
   template <bool ODD>
   void launch_lean(const HydroParams<A>& p, cudaStream_t s) {
-    if constexpr (std::is_same<A, float>::value) {
-      hydro_lean_kernel<Q, S, ODD><<<unsigned(ceil_div(n, LEAN_BLOCK)), LEAN_BLOCK, 0, s>>>(p, uint32_t(n));
-      CK(cudaGetLastError());
+    switch (lean_minb[ODD]) {
+      case 6: launch_lean_mb<ODD, 6>(p, s); break;
+      case 7: launch_lean_mb<ODD, 7>(p, s); break;
+      default: launch_lean_mb<ODD, 8>(p, s); break;
     }
   }
 
@@ -638,6 +660,94 @@ struct Engine final : EngineBase {
   }
 
   void sync() override { CK(cudaStreamSynchronize(st)); }
+
+  // Sweep autotuner: times every kernel kind (and, for the lean kernel,
+  // every register budget) that can run this configuration on the solver's
+  // own grid, keeps the fastest, and leaves the state untouched (the
+  // populations and parity are saved before the trials and restored after).
+  void autotune_sweep(int steps, lbmb_autotune_result* out, int32_t* trial_desc, double* trial_ms,
+                      int capacity) override {
+    if (steps < 2) throw Error(LBMB_ERR_INVALID, "autotune: steps per trial must be >= 2");
+    steps += steps & 1;  // whole even/odd pairs
+    struct Cand {
+      int kind, ev, od;
+    };
+    std::vector<Cand> cands;
+    const bool wide = sizeof(S) >= 4;
+    const bool is_f = std::is_same<A, float>::value;
+    const bool uf = has_uniform_force();
+    cands.push_back({LBMB_SWEEP_DIRECT, 0, 0});
+    if (wide && !uf) cands.push_back({LBMB_SWEEP_ASYNC, 0, 0});
+    if (!uf) cands.push_back({LBMB_SWEEP_BULK, 0, 0});
+    if (is_f && coll == COLL_TRT && nx % 2 == 0 && !uf) {
+      cands.push_back({LBMB_SWEEP_PAIR, 0, 0});
+      cands.push_back({LBMB_SWEEP_TILE, 0, 0});
+    }
+    if (lean_ok(coll))
+      for (int ev = 8; ev >= 6; --ev)
+        for (int od = 8; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
+    const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
+    const int par0 = parity;
+    const size_t fbytes = f_alloc.n * sizeof(S);
+    DevBuf<S> save;
+    save.alloc(f_alloc.n);
+    CK(cudaMemcpyAsync(save.p, f_alloc.p, fbytes, cudaMemcpyDeviceToDevice, st));
+    invalidate_graphs();
+    auto trial = [&](const Cand& cd) {
+      kernel_mode = cd.kind;
+      if (cd.kind == LBMB_SWEEP_LEAN) {
+        lean_minb[0] = cd.ev;
+        lean_minb[1] = cd.od;
+      }
+      for (int i = 0; i < 2; ++i) launch_hydro(i);  // warm-up (first launches set up grids)
+      CK(cudaEventRecord(ev0, st));
+      for (int i = 0; i < steps; ++i) launch_hydro(i & 1);
+      CK(cudaEventRecord(ev1, st));
+      CK(cudaEventSynchronize(ev1));
+      check_device_error();
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      return double(ms) / steps;
+    };
+    const double t_default = trial(Cand{kind0, ev0_, od0});
+    int best = -1;
+    double best_ms = 0.0;
+    for (size_t i = 0; i < cands.size(); ++i) {
+      const double t = trial(cands[i]);
+      if (int(i) < capacity) {
+        if (trial_desc) {
+          trial_desc[3 * i + 0] = cands[i].kind;
+          trial_desc[3 * i + 1] = cands[i].ev;
+          trial_desc[3 * i + 2] = cands[i].od;
+        }
+        if (trial_ms) trial_ms[i] = t;
+      }
+      if (best < 0 || t < best_ms) {
+        best = int(i);
+        best_ms = t;
+      }
+    }
+    kernel_mode = cands[best].kind;
+    if (kernel_mode == LBMB_SWEEP_LEAN) {
+      lean_minb[0] = cands[best].ev;
+      lean_minb[1] = cands[best].od;
+    } else {
+      lean_minb[0] = ev0_;
+      lean_minb[1] = od0;
+    }
+    CK(cudaMemcpyAsync(f_alloc.p, save.p, fbytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    parity = par0;
+    invalidate_graphs();
+    if (out) {
+      out->kind = kernel_mode;
+      out->even_blocks_per_sm = lean_minb[0];
+      out->odd_blocks_per_sm = lean_minb[1];
+      out->n_trials = int32_t(cands.size());
+      out->best_ms_per_step = best_ms;
+      out->default_ms_per_step = t_default;
+    }
+  }
 
   void stage_in(const double* fin) override {
     DevBuf<double> tmp;

@@ -92,8 +92,10 @@ __device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroPara
   return rho;
 }
 
-template <int Q, class S, bool ODD>
-__global__ void __launch_bounds__(LEAN_BLOCK, 8) hydro_lean_kernel(HydroParams<float> p, uint32_t n) {
+// MINB: resident blocks per SM the register allocation is sized for
+// (8: 64 registers, 7: 72, 6: 80).
+template <int Q, class S, bool ODD, int MINB>
+__global__ void __launch_bounds__(LEAN_BLOCK, MINB) hydro_lean_kernel(HydroParams<float> p, uint32_t n) {
   using L = Lat<Q>;
   using CD = Codec<S>;
   const uint32_t c = blockIdx.x * LEAN_BLOCK + threadIdx.x;
@@ -109,36 +111,45 @@ __global__ void __launch_bounds__(LEAN_BLOCK, 8) hydro_lean_kernel(HydroParams<f
     return;
   }
   const uint32_t mk = (fl & F_BOUNDARY) ? p.nbr[c] : 0u;
-  S* fb = static_cast<S*>(p.f);
-  const uint32_t pl = p.plane;
-  auto dq = [&](int q) { return L::cx(q) + L::cy(q) * nx + L::cz(q) * nxy; };
+  // Per-thread base pointer plus per-direction offsets that depend on the
+  // launch parameters only (uniform across the grid).
+  S* cb = static_cast<S*>(p.f) + c;
+  const int64_t pl = int64_t(p.plane);
+  // P(k): slot k of this cell; T(k): slot k of the neighbour x + c_k. The
+  // odd step reads slot opp(q) of x - c_q = T(opp(q)) and writes T(q), so
+  // loads and stores share one set of offsets.
+  auto P = [&](int k) { return int32_t(int64_t(k) * pl); };
+  auto T = [&](int k) { return int32_t(int64_t(k) * pl + (L::cx(k) + L::cy(k) * nx + L::cz(k) * nxy)); };
   float f[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if (!ODD) {
-      f[q] = CD::ld(fb + (uint32_t(q) * pl + c));
+      f[q] = CD::ld(cb + P(q));
     } else {
       const int o = opp(q);
-      const uint32_t off = ((mk >> o) & 1u) ? uint32_t(q) * pl + c : uint32_t(o) * pl + c - uint32_t(dq(q));
-      f[q] = CD::ld(fb + off);
+      f[q] = CD::ld(cb + T(o));
+      if ((mk >> o) & 1u) f[q] = CD::ld(cb + P(q));  // neighbour solid: own slot
     }
   }
   const float rho = trt_lean_collide<Q>(f, p);
-  // a fresh copy of the base pointer: keeps the compiler from holding the
-  // load addresses live across the collision to reuse them for the stores
-  S* fs = fb;
-  asm volatile("" : "+l"(fs));
+  if (fl & F_MOVING) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int o = opp(q);
+      if ((mk >> q) & 1u) {
+        const Vec4<float> wu = p.wall_u[int64_t(c) + (T(q) - P(q))];
+        f[q] += ((6.f * float(L::w(o))) * rho) *
+                ((float(L::cx(o)) * wu.x + float(L::cy(o)) * wu.y) + float(L::cz(o)) * wu.z);
+      }
+    }
+  }
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int o = opp(q);
-    float v = f[q];
-    const bool wall = (mk >> q) & 1u;
-    if (wall && (fl & F_MOVING)) {
-      const Vec4<float> wu = p.wall_u[int32_t(c) + dq(q)];
-      v += ((6.f * float(L::w(o))) * rho) * ((float(L::cx(o)) * wu.x + float(L::cy(o)) * wu.y) + float(L::cz(o)) * wu.z);
-    }
-    const uint32_t off = (!ODD || wall) ? uint32_t(o) * pl + c : uint32_t(q) * pl + c + uint32_t(dq(q));
-    CD::st(fs + off, v);
+    if (!ODD || ((mk >> q) & 1u))
+      CD::st(cb + P(o), f[q]);  // even step, or towards a wall: the own slot
+    else
+      CD::st(cb + T(q), f[q]);
   }
 }
 

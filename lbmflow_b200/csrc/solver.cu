@@ -355,6 +355,21 @@ int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind) {
   });
 }
 
+int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm) {
+  return guarded([&] {
+    NEED(h);
+    h->e->set_sweep_variant(even_blocks_per_sm, odd_blocks_per_sm);
+  });
+}
+
+int lbmb_autotune_sweep(lbmb_solver* h, int32_t steps_per_trial, lbmb_autotune_result* out,
+                        int32_t* trial_desc, double* trial_ms, int32_t capacity) {
+  return guarded([&] {
+    NEED(h);
+    h->e->autotune_sweep(steps_per_trial, out, trial_desc, trial_ms, capacity);
+  });
+}
+
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind) {
   return guarded([&] {
     NEED(h);

@@ -137,3 +137,26 @@ def test_pair_kernel_refuses_what_it_cannot_run():
         g.set_sweep_kernel("async")
     with pytest.raises(lb.SpecError):
         g.set_sweep_kernel(9)
+
+
+@pytest.mark.parametrize("prec,q", [("f32", 19), ("f16", 19), ("f32", 27), ("f64", 19)])
+def test_autotune_keeps_state_and_picks_fastest(prec, q):
+    dims, solid, wall_u, nu = cavity(16, u_lid=0.06, re=40.0)
+    g = lb.Solver(dims, lattice=q, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
+    g.run(7)  # odd parity on entry
+    before = g.stage_out()
+    r = g.autotune_sweep(steps_per_trial=6)
+    assert np.array_equal(g.stage_out(), before)
+    assert r["n_trials"] if "n_trials" in r else len(r["trials"]) >= 1
+    assert r["best_ms_per_step"] == min(t[3] for t in r["trials"])
+    assert g.sweep_kernel == r["kind"]
+    if prec == "f16":
+        assert all(t[0] != "async" for t in r["trials"])
+    if prec == "f64":
+        assert {t[0] for t in r["trials"]} == {"direct", "async", "bulk"}
+    # the tuned solver still follows the oracle
+    if prec in ("f32",):
+        p = Pair(dims, q, "f32", nu=nu, solid=solid, wall_u=wall_u)
+        p.g.autotune_sweep(steps_per_trial=4)
+        p.run(30)
+        p.check(solid == 0)
