@@ -5,9 +5,18 @@ cells on a 128 x 128 x 160 grid, flat bottom, four wall baffles of width
 T/10 and thickness 2.6 cells, a six-blade flat-blade disc turbine of
 diameter T/3 at clearance T/3 sampled by ~6k direct-forcing IBM markers at
 0.7-cell spacing, tip speed 0.05, nu for impeller Re = 2000, D3Q27
-central-moment collision, fp32 populations. One step = the reference
-runner step (clear force field -> IBM direct forcing -> collide/stream/
-moments), synthetic seeded geometry, quiescent start after a warm-up.
+central-moment collision, fp32 populations, 20k steps, with the library's
+optional Smagorinsky model (Cs = 0.1; the reference operators diverge on
+this under-resolved tank). One step = the reference runner step (clear
+force field -> IBM direct forcing -> collide/stream/moments), synthetic
+seeded geometry, quiescent start after a warm-up; the sweep kernel is
+picked by the library's autotuner on the tank itself.
+
+Besides the headline line the output carries the precision study (power
+number of the same schedule with f64 / f32 / f16 / bf16 populations for the
+D3Q27 central-moment and D3Q19 TRT forms, errors against the f64 path) and
+the throughput of every form at T = 256 (256 x 256 x 320, populations
+larger than L2).
 
 Prints one JSON line (rank 0). `--impl reference` times the reference's CPU
 path (the C++ restatement in oracle/, the reference being Rust that cannot
@@ -127,10 +136,11 @@ def peak_hbm():
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle), bounded sample
 # ---------------------------------------------------------------------------
-def cpu_tank_sample(dims, solid, body, nu, q=27, collision="cm", bits=32, steps=3, warmup=1):
+def cpu_tank_sample(dims, solid, body, nu, q=27, collision="cm", bits=32, steps=3, warmup=1, cs=0.0):
     from oracle import oracle as o
     os_ = 1.0 / (3.0 * nu + 0.5)
-    c = o.OracleSolver(dims, q=q, real_bits=bits, collision=collision, nu=nu, omega_shear=os_, solid=solid)
+    c = o.OracleSolver(dims, q=q, real_bits=bits, collision=collision, nu=nu, omega_shear=os_, solid=solid,
+                       smagorinsky_cs=cs)
     c.run_tank(body.positions, body.weights, body.center, body.omega, warmup)
     t0 = time.perf_counter()
     c.run_tank(body.positions, body.weights, body.center, body.omega, steps)
@@ -172,16 +182,87 @@ def barrier(world):
         dist.barrier()
 
 
+def power_number(torque_lu, omega, D):
+    """Np from the last-half mean torque (runner.rs:1523-1530; qoi.rs:477-505),
+    lattice units with rho = 1: P = Omega Tq, N = Omega / 2 pi, Np = P / (N^3 D^5)."""
+    t = np.asarray(torque_lu)
+    tq = float(np.mean(t[t.size // 2:]))
+    n_rev = omega / (2.0 * math.pi)
+    return omega * tq / (n_rev ** 3 * D ** 5)
+
+
+def make_solver(lb, dims, solid, nu, q, coll, storage, cs, local):
+    os_ = 1.0 / (3.0 * nu + 0.5)
+    return lb.Solver(dims, lattice=q, collision=coll, storage=storage, nu=nu, omega_shear=os_, solid=solid,
+                     device=local, smagorinsky_cs=cs)
+
+
+def qoi_study(lb, args, local, dims, solid, body, nu, D, headline_np):
+    """Np of the same runner schedule (warm-up + timed steps) in every storage
+    precision; errors against the f64 path, which the parity tests pin to the
+    C++ oracle at 1e-11."""
+    out = {}
+    omega = float(body.omega[2])
+    for q, coll, label in ((27, "cm", "d3q27_cm"), (19, "trt", "d3q19_trt")):
+        nps = {}
+        for st in ("f64", "f32", "f16", "bf16"):
+            if q == 27 and st == "f32" and headline_np is not None:
+                nps[st] = headline_np
+                continue
+            g = make_solver(lb, dims, solid, nu, q, coll, st, args.les_cs, local)
+            g.autotune_sweep(6)
+            g.run_impeller(body, max(args.warmup, 3))
+            r = g.run_impeller(body, args.steps)
+            nps[st] = power_number(r["torque_lu"], omega, D)
+            g.close()
+        ref = nps["f64"]
+        out[label] = {"Np": nps, "Np_rel_err_vs_f64": {k: abs(v - ref) / abs(ref) for k, v in nps.items()
+                                                       if k != "f64"}}
+    return out
+
+
+def throughput_study(lb, args, local, peak):
+    """Sweep throughput at the precision-variant grid (tank T = big_T,
+    populations larger than L2): hydro kernel GB/s against the HBM roofline
+    and runner-step MLUPS, autotuned kernel per configuration."""
+    dims, solid, body, nu = tank_case(T=args.big_T)
+    n_cells = dims[0] * dims[1] * dims[2]
+    n_fluid = int((solid == 0).sum())
+    res = {"grid": list(dims), "fluid_cells": n_fluid, "markers": int(body.weights.size)}
+    for q, coll in ((19, "trt"), (27, "cm")):
+        for st in ("f32", "f16", "bf16"):
+            g = make_solver(lb, dims, solid, nu, q, coll, st, args.les_cs, local)
+            tune = g.autotune_sweep(6)
+            g.run(4)
+            g.run(args.hydro_steps)
+            hms, _, L = g.last_timing()
+            per = hms / max(L, 1)
+            gbs = b_lu(q, st) * n_fluid / (per * 1e-3) / 1e9
+            g.run_impeller(body, 8)
+            g.run_impeller(body, args.big_steps)
+            tms, _, _ = g.last_timing()
+            res[f"d3q{q}_{coll}_{st}"] = {"kernel": tune["kind"], "hydro_ms": per, "hydro_gbs": gbs,
+                                          "hydro_frac": gbs / peak,
+                                          "runner_mlups": n_cells * args.big_steps / (tms * 1e-3) / 1e6}
+            g.close()
+    for q, coll in ((19, "trt"), (27, "cm")):
+        a, b = res[f"d3q{q}_{coll}_f16"], res[f"d3q{q}_{coll}_f32"]
+        res[f"d3q{q}_{coll}_fp16_over_fp32_runner"] = a["runner_mlups"] / b["runner_mlups"]
+        res[f"d3q{q}_{coll}_fp16_over_fp32_hydro"] = b["hydro_ms"] / a["hydro_ms"]
+    return res
+
+
 def run_b200(args, rank, world, local):
     import lbmflow_b200 as lb
 
     dims, solid, body, nu = tank_case(T=args.tank_T)
     q, coll, storage = args.lattice, args.collision, args.storage
-    os_ = 1.0 / (3.0 * nu + 0.5)
     n_cells = dims[0] * dims[1] * dims[2]
     n_fluid = int((solid == 0).sum())
-    g = lb.Solver(dims, lattice=q, collision=coll, storage=storage, nu=nu, omega_shear=os_, solid=solid,
-                  device=local)
+    D = args.tank_T / 3.0
+    omega = float(body.omega[2])
+    g = make_solver(lb, dims, solid, nu, q, coll, storage, args.les_cs, local)
+    tune = g.autotune_sweep(8)
     cfg = lb.DirectForcingConfig()
     # warm-up (untimed)
     g.run_impeller(body, max(args.warmup, 3))
@@ -195,6 +276,8 @@ def run_b200(args, rank, world, local):
     barrier(world)
     ms_per_step = t_ms / args.steps
     value = world * n_cells * args.steps / (t_ms * 1e-3) / 1e6
+    torque = out["torque_lu"]
+    np_head = power_number(torque, omega, D) if np.isfinite(torque).all() else None
     # hydro-kernel-only launches (same stream, CUDA events) for the roofline
     g.run(4)
     g.run(args.hydro_steps)
@@ -204,11 +287,13 @@ def run_b200(args, rank, world, local):
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = peak_hbm()
     # e2e through the reference-facing API with host buffers: per step the
-    # caller passes the rotating body (host arrays) to apply_rotating_ibm,
-    # reads the diagnostics back and advances one step.
+    # caller uploads the rotating body (host arrays), runs the IBM (its
+    # diagnostics come back to the host) and advances one step.
     e2e_steps = args.e2e_steps
-    g2 = lb.Solver(dims, lattice=q, collision=coll, storage=storage, nu=nu, omega_shear=os_, solid=solid,
-                   device=local)
+    g2 = make_solver(lb, dims, solid, nu, q, coll, storage, args.les_cs, local)
+    g2.set_sweep_kernel(tune["kind"])
+    if tune["kind"] == "lean":
+        g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
     h2d = body.positions.nbytes + body.weights.nbytes + 48
     d2h = 100
     for _ in range(3):
@@ -228,69 +313,48 @@ def run_b200(args, rank, world, local):
     e2e_s = allmax(time.perf_counter() - t0, world)
     e2e_value = world * n_cells * e2e_steps / e2e_s / 1e6
     g2.close()
-    # low-precision storage variants (same workload, short timing)
+    g.close()
     extra = {}
-    if args.variants:
-        for st in ("f16", "bf16"):
-            gv = lb.Solver(dims, lattice=q, collision=coll, storage=st, nu=nu, omega_shear=os_, solid=solid,
-                           device=local)
-            gv.run_impeller(body, 8)
-            gv.run_impeller(body, max(args.steps // 2, 16))
-            tv, _, _ = gv.last_timing()
-            extra[f"{st}_mlups"] = n_cells * max(args.steps // 2, 16) / (tv * 1e-3) / 1e6
-            gv.run(args.hydro_steps)
-            hv, _, lv = gv.last_timing()
-            extra[f"{st}_hydro_gbs"] = b_lu(q, st) * n_fluid / (hv / lv * 1e-3) / 1e9
-            gv.close()
-        extra["fp16_over_fp32"] = extra["f16_mlups"] / (value / world)
-        # D3Q19 TRT on the same tank (the reference runner's collision), fp32
-        # and fp16-storage: runner step MLUPS and the hydro sweep's fraction
-        # of the HBM roofline (152 / 76 bytes per fluid cell).
-        peak, _ = peak_hbm()
-        for st in ("f32", "f16"):
-            gv = lb.Solver(dims, lattice=19, collision="trt", storage=st, nu=nu, solid=solid, device=local)
-            gv.run_impeller(body, 8)
-            k = max(args.steps // 2, 16)
-            gv.run_impeller(body, k)
-            tv, _, _ = gv.last_timing()
-            extra[f"d3q19_trt_{st}_mlups"] = n_cells * k / (tv * 1e-3) / 1e6
-            gv.run(args.hydro_steps)
-            hv, _, lv = gv.last_timing()
-            gbs = b_lu(19, st) * n_fluid / (hv / lv * 1e-3) / 1e9
-            extra[f"d3q19_trt_{st}_hydro_gbs"] = gbs
-            extra[f"d3q19_trt_{st}_hydro_frac"] = gbs / peak
-            gv.close()
-        extra["d3q19_fp16_over_fp32"] = extra["d3q19_trt_f16_mlups"] / extra["d3q19_trt_f32_mlups"]
-    torque = out["torque_lu"]
+    if args.variants and world == 1:
+        extra["qoi_precision"] = qoi_study(lb, args, local, dims, solid, body, nu, D, np_head)
+        extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
+    kname = {"lean": "hydro_lean_kernel", "pair": "hydro_pair_kernel", "tile": "hydro_tile_kernel",
+             "async": "hydro_async_kernel", "direct": "hydro_aa_kernel", "bulk": "hydro_tma_kernel"}[tune["kind"]]
+    coll_name = {"cm": "central_moment", "trt": "trt"}[coll]
     res = {
-        "metric": "MLUPS (stirred-tank runner step, D3Q27 central moment, fp32 populations)",
+        "metric": f"MLUPS (stirred-tank runner step, D3Q{q} {coll_name}, {storage} populations)",
         "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"f32": "f32", "f16": "f16-storage/f32", "bf16": "bf16-storage/f32", "f64": "f64"}[storage],
         "data": "synthetic (seeded tank geometry, quiescent start)",
-        "config": {"workload": "tank128x128x160_d3q27_cm_ibm6k", "grid": list(dims), "cells": n_cells,
-                   "fluid_cells": n_fluid, "markers": int(body.weights.size), "lattice": "D3Q27",
-                   "collision": "central_moment", "storage": storage, "nu": nu, "u_tip": 0.05, "re": 2000,
+        "config": {"workload": f"tank{dims[0]}x{dims[1]}x{dims[2]}_d3q{q}_{coll}_ibm{body.weights.size}",
+                   "grid": list(dims), "cells": n_cells, "fluid_cells": n_fluid, "markers": int(body.weights.size),
+                   "lattice": f"D3Q{q}", "collision": coll_name, "storage": storage, "nu": nu, "u_tip": 0.05,
+                   "re": 2000, "smagorinsky_cs": args.les_cs,
+                   "les_note": "library option; without it the reference operators diverge on this "
+                               "under-resolved Re=2000 tank (D3Q27 CM at step ~2390, D3Q19 TRT at ~186)",
                    "ibm": "3 sweeps, tol 1e-2, radius 1", "top": "solid lid (reference)",
+                   "sweep_kernel": tune["kind"], "autotune": {k: tune[k] for k in
+                                                              ("even_blocks_per_sm", "odd_blocks_per_sm",
+                                                               "best_ms_per_step", "default_ms_per_step")},
                    "l2": "inputs larger than L2 (populations %.0f MB)" % (q * 4 * n_cells / 1e6),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "C ABI per step: ibm_set_body(host markers) + apply_rotating_ibm(diag to host) + step"},
-        "gpu_launches": int(12 * args.steps),
-        "roofline": {"bound": "hbm", "kernel": "hydro_aa_kernel<27,float,CM>", "achieved": achieved,
+        "gpu_launches": int(13 * args.steps),
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                      "peak_kind": peak_kind, "bytes_per_fluid_cell": b_lu(q, storage),
                      "launch_ms": per_launch_ms},
-        "qoi": {"torque_lu_last": float(torque[-1]), "finite": bool(np.isfinite(torque).all())},
+        "qoi": {"Np": np_head, "torque_lu_last": float(torque[-1]), "finite": bool(np.isfinite(torque).all())},
         "clocks": clk.summary(),
     }
     res.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu:
-        mlups, dt = cpu_tank_sample(dims, solid, body, nu, steps=args.cpu_steps)
+        mlups, dt = cpu_tank_sample(dims, solid, body, nu, steps=args.cpu_steps, cs=args.les_cs)
         res["cpu_baseline"] = {"value": mlups, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                                "sample": f"{args.cpu_steps} runner steps of the full tank, fp32, OpenMP "
                                          f"({dt:.1f} s)"}
-    g.close()
     return res
 
 
@@ -299,23 +363,27 @@ def run_reference(args, rank, world):
         return None
     dims, solid, body, nu = tank_case(T=args.tank_T)
     steps = max(1, min(args.steps, args.cpu_steps))
-    mlups, dt = cpu_tank_sample(dims, solid, body, nu, steps=steps, warmup=1)
-    return {"impl": "reference", "metric": "MLUPS (stirred-tank runner step, D3Q27 central moment, fp32 populations)",
+    q, coll = args.lattice, args.collision
+    mlups, dt = cpu_tank_sample(dims, solid, body, nu, q=q, collision=coll, steps=steps, warmup=1, cs=args.les_cs)
+    coll_name = {"cm": "central_moment", "trt": "trt"}[coll]
+    return {"impl": "reference",
+            "metric": f"MLUPS (stirred-tank runner step, D3Q{q} {coll_name}, {args.storage} populations)",
             "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": steps, "warmup": 1,
             "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded tank geometry, quiescent start)",
-            "config": {"workload": "tank128x128x160_d3q27_cm_ibm6k", "grid": list(dims)},
+            "config": {"workload": f"tank{dims[0]}x{dims[1]}x{dims[2]}_d3q{q}_{coll}_ibm{body.weights.size}",
+                       "grid": list(dims), "smagorinsky_cs": args.les_cs},
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                              "sample": f"{steps} runner steps of the full tank on the host cores (C++ "
-                                       f"restatement of the reference CpuScalar path; the Rust reference "
-                                       f"cannot be built here)"},
+                                       f"restatement of the reference CpuScalar path, OpenMP; the Rust "
+                                       f"reference cannot be built here)"},
             "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
@@ -327,6 +395,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--variants", type=int, default=1)
+    ap.add_argument("--les-cs", type=float, default=0.1, help="Smagorinsky constant (0: reference operators)")
+    ap.add_argument("--big-T", type=int, default=256, help="tank diameter of the throughput study")
+    ap.add_argument("--big-steps", type=int, default=100)
     args = ap.parse_args()
     rank, world, local = dist_init(args.gpus)
     if args.impl == "reference":
