@@ -293,6 +293,30 @@ typedef struct {
 int lbmb_autotune_sweep(lbmb_solver* h, int32_t steps_per_trial, lbmb_autotune_result* out,
                         int32_t* trial_desc, double* trial_ms, int32_t capacity);
 
+/* Batched runner for sweeps (replaces the sequential per-case loop of
+ * crates/lbm-cli/src/sweep.rs:47-106, each case being runner.rs:1079-1129).
+ * ncases solvers of one lattice and storage type (TRT/BGK, fp32/fp16/bf16,
+ * no uniform force, no scalar distributions, one device, same step parity)
+ * are advanced in lockstep: per step one launch per kernel family covers
+ * every case (IBM prep / interp / spread / diag / commit, forced cells, the
+ * full-grid sweep, the cached-field refresh), captured in CUDA graphs. Each
+ * case runs the runner step of its own body (bodies[k], NULL = body 0, set
+ * with lbmb_ibm_set_body) with cfg; per-case results equal running the case
+ * alone with the lean sweep kernel. The solvers must outlive the batch and
+ * must not be stepped on their own while a batch call runs. */
+typedef struct lbmb_batch lbmb_batch;
+int lbmb_batch_create(lbmb_solver* const* solvers, const int32_t* bodies, int32_t ncases,
+                      const lbmb_ibm_config* cfg, lbmb_batch** out);
+/* Register budget of the batched sweep picked by timing every candidate on
+ * the cases' own grids (populations restored afterwards). */
+int lbmb_batch_autotune(lbmb_batch* b, int32_t steps_per_trial, int32_t* even_blocks_per_sm,
+                        int32_t* odd_blocks_per_sm, double* best_ms_per_step);
+/* steps runner steps of every case; torque_lu (may be NULL) receives
+ * ncases x steps values, case-major (-torque_z, runner.rs:1396-1425);
+ * device_ms (may be NULL) the device time of the whole call. */
+int lbmb_batch_run(lbmb_batch* b, int64_t steps, double* torque_lu, double* device_ms);
+int lbmb_batch_destroy(lbmb_batch* b);
+
 /* Synchronize the solver stream. */
 int lbmb_sync(lbmb_solver* h);
 

@@ -40,6 +40,7 @@ EXPORTS = (
     "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
     "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
     "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
+    "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy",
 )
 
 
@@ -143,6 +144,10 @@ def lib():
         L.lbmb_get_sweep_kernel.argtypes = [vp, _i32p]
         L.lbmb_set_sweep_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.lbmb_autotune_sweep.argtypes = [vp, C.c_int32, C.POINTER(_AutotuneResult), _i32p, _dp, C.c_int32]
+        L.lbmb_batch_create.argtypes = [C.POINTER(vp), _i32p, C.c_int32, C.POINTER(_IbmConfig), C.POINTER(vp)]
+        L.lbmb_batch_autotune.argtypes = [vp, C.c_int32, _i32p, _i32p, _dp]
+        L.lbmb_batch_run.argtypes = [vp, C.c_int64, _dp, _dp]
+        L.lbmb_batch_destroy.argtypes = [vp]
         L.lbmb_reduce_populations_noalloc.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, vp, _dp,
                                                       _dp, vp]
         _lib = L
@@ -400,6 +405,43 @@ class Solver:
         v = C.c_double()
         _check(lib().lbmb_scalar_cv(self.h, int(k), C.byref(v)))
         return None if np.isnan(v.value) else v.value
+
+
+class Batch:
+    """Solvers of one lattice/storage type advanced in lockstep by batched
+    kernels (one launch per kernel family per step for every case); each case
+    runs the runner step of its own rotating body (lbmb_batch_*)."""
+
+    def __init__(self, solvers, bodies, cfg: DirectForcingConfig = None):
+        cfg = cfg or DirectForcingConfig()
+        self.solvers = list(solvers)
+        self.n = len(self.solvers)
+        slots = np.array([s._slot_for(b) for s, b in zip(self.solvers, bodies)], dtype=np.int32)
+        hs = (C.c_void_p * self.n)(*[s.h.value for s in self.solvers])
+        h = C.c_void_p()
+        _check(lib().lbmb_batch_create(C.cast(hs, C.POINTER(C.c_void_p)), slots.ctypes.data_as(_i32p), self.n,
+                                       C.byref(cfg._c()), C.byref(h)))
+        self.h = h
+
+    def autotune(self, steps_per_trial=6):
+        e, o, ms = C.c_int32(), C.c_int32(), C.c_double()
+        _check(lib().lbmb_batch_autotune(self.h, int(steps_per_trial), C.byref(e), C.byref(o), C.byref(ms)))
+        return {"even_blocks_per_sm": e.value, "odd_blocks_per_sm": o.value, "best_ms_per_step": ms.value}
+
+    def run(self, steps):
+        """Advance every case; returns (torque_lu [ncases x steps], device ms)."""
+        tq = np.empty((self.n, max(int(steps), 1)))
+        ms = C.c_double()
+        _check(lib().lbmb_batch_run(self.h, int(steps), _d(tq), C.byref(ms)))
+        return tq[:, :int(steps)], ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lbmb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def build_wall_rims(dims, is_wall, wall_u):

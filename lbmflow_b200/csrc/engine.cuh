@@ -27,6 +27,7 @@
 #include "hydro_pair.cuh"
 #include "hydro_tile.cuh"
 #include "hydro_lean.cuh"
+#include "batch.cuh"
 #include "ibm.cuh"
 #include "scalar.cuh"
 
@@ -99,6 +100,13 @@ struct ScalarStateT {
   DevBuf<double> part, stats;
 };
 
+// Type-erased batch of engines advanced in lockstep (batch.cuh).
+struct BatchBase {
+  virtual ~BatchBase() = default;
+  virtual void run(int64_t steps, double* torque, double* device_ms) = 0;
+  virtual void autotune(int steps, int32_t* even, int32_t* odd, double* best_ms) = 0;
+};
+
 // Type-erased engine interface.
 struct EngineBase {
   virtual ~EngineBase() = default;
@@ -124,6 +132,9 @@ struct EngineBase {
   virtual void set_sweep_variant(int even, int odd) = 0;
   virtual void autotune_sweep(int steps, lbmb_autotune_result* out, int32_t* trial_desc, double* trial_ms,
                               int capacity) = 0;
+  // A batch over `all` (this engine's type for every entry), one body each.
+  virtual BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
+                                const lbmb_ibm_config& cfg) = 0;
   virtual int64_t cells() const = 0;
   virtual int q() const = 0;
   virtual const std::vector<uint8_t>& solid() const = 0;
@@ -1304,6 +1315,9 @@ struct Engine final : EngineBase {
     if (cv && k >= 0) CK(cudaMemcpy(cv, d_cv.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
   }
 
+  BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
+                        const lbmb_ibm_config& cfg) override;
+
   int64_t solid_count() const {
     int64_t s = 0;
     for (auto v : solid_h) s += v ? 1 : 0;
@@ -1316,6 +1330,255 @@ struct Engine final : EngineBase {
     CK(cudaStreamSynchronize(st));
   }
 };
+
+// ---------------------------------------------------------------------------
+// Batch of engines of one (lattice, storage) type, advanced in lockstep with
+// one launch per kernel family per step (batch.cuh). The engines keep their
+// own device state and must outlive the batch.
+// ---------------------------------------------------------------------------
+template <int Q, class S>
+struct Batch final : BatchBase {
+  using E = Engine<Q, S>;
+  std::vector<E*> eng;
+  std::vector<BodyState*> bod;
+  lbmb_ibm_config cfg;
+  int ncase = 0;
+  int parity = 0;
+  int minb[2] = {8, 8};
+  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork = nullptr, ev_join = nullptr;
+  std::vector<BatchCase> cases_h;
+  DevBuf<BatchCase> cases;
+  DevBuf<int32_t> off_cells, off_bslots, off_slots, off_markers;
+  int nb_cells = 0, nb_bslots = 0, nb_slots = 0, nb_markers = 0;
+  DevBuf<double> d_torque;
+  DevBuf<int64_t> d_counter;
+
+  Batch(const std::vector<EngineBase*>& all, const int32_t* bodies, const lbmb_ibm_config& c) : cfg(c) {
+    if (all.empty()) invalid("batch needs at least one solver");
+    for (EngineBase* b : all) {
+      E* e = dynamic_cast<E*>(b);
+      if (!e) invalid("batch solvers must share lattice and storage precision");
+      if (!e->lean_ok(e->coll))
+        throw Error(LBMB_ERR_UNSUPPORTED, "batch solvers need TRT/BGK, fp32/fp16/bf16 storage, no uniform force");
+      if (!e->scalars.empty()) throw Error(LBMB_ERR_UNSUPPORTED, "batch solvers carry no scalar distributions");
+      eng.push_back(e);
+    }
+    ncase = int(eng.size());
+    parity = eng[0]->parity;
+    for (E* e : eng) {
+      if (e->parity != parity) invalid("batch solvers must be at the same step parity");
+      if (e->cfg.device != eng[0]->cfg.device) invalid("batch solvers must live on one device");
+    }
+    CK(cudaSetDevice(eng[0]->cfg.device));
+    for (int k = 0; k < ncase; ++k) {
+      eng[k]->sync();
+      bod.push_back(&eng[k]->body_for(bodies ? bodies[k] : 0, cfg));
+    }
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&st2, cudaStreamNonBlocking, hi));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    std::vector<int32_t> oc(1, 0), ob(1, 0), os(1, 0), om(1, 0);
+    for (int k = 0; k < ncase; ++k) {
+      E* e = eng[k];
+      BodyState& B = *bod[k];
+      oc.push_back(oc.back() + int32_t(ceil_div(e->n, BATCH_BLOCK)));
+      ob.push_back(ob.back() + int32_t(std::max<int64_t>(1, ceil_div(B.ns, BATCH_BLOCK))));
+      os.push_back(os.back() + int32_t(std::max<int64_t>(1, ceil_div(e->nslots, BATCH_BLOCK))));
+      om.push_back(om.back() + int32_t(std::max<int64_t>(1, ceil_div(B.nm, BATCH_BLOCK))));
+    }
+    nb_cells = oc.back();
+    nb_bslots = ob.back();
+    nb_slots = os.back();
+    nb_markers = om.back();
+    off_cells.upload(oc, st);
+    off_bslots.upload(ob, st);
+    off_slots.upload(os, st);
+    off_markers.upload(om, st);
+    cases_h.resize(size_t(ncase));
+    for (int k = 0; k < ncase; ++k) {
+      E* e = eng[k];
+      BatchCase& b = cases_h[size_t(k)];
+      b.hp = e->hydro_params();
+      b.n = uint32_t(e->n);
+      b.nx = e->nx;
+      b.ny = e->ny;
+      b.nz = e->nz;
+      b.slot_cell = e->slot_cell.p;
+      b.nslots = e->nslots;
+      b.fcur = e->fcur.p;
+      b.fprev = e->fprev.p;
+      b.ibm = e->ibm_args(*bod[size_t(k)], cfg);
+      b.gx = b.gy = b.gz = 0.0;
+      b.series_torque = nullptr;
+      b.counter = nullptr;
+    }
+    cases.upload(cases_h, st);
+    CK(cudaStreamSynchronize(st));
+  }
+
+  ~Batch() override {
+    if (st) cudaStreamSynchronize(st);
+    if (st2) cudaStreamSynchronize(st2);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st) cudaStreamDestroy(st);
+    if (st2) cudaStreamDestroy(st2);
+  }
+
+  template <bool ODD, int MB>
+  void hydro_mb() {
+    batch_hydro_kernel<Q, S, ODD, MB><<<unsigned(nb_cells), BATCH_BLOCK, 0, st>>>(cases.p, off_cells.p, ncase);
+  }
+  template <bool ODD>
+  void hydro_par() {
+    switch (minb[ODD]) {
+      case 6: hydro_mb<ODD, 6>(); break;
+      case 7: hydro_mb<ODD, 7>(); break;
+      default: hydro_mb<ODD, 8>(); break;
+    }
+  }
+  void hydro(int par) {
+    if (par) hydro_par<true>();
+    else hydro_par<false>();
+    CK(cudaGetLastError());
+  }
+
+  // One runner step of every case (runner.rs:1079-1129 per case).
+  void one_step() {
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+    batch_prep_kernel<Q, S><<<unsigned(nb_bslots), BATCH_BLOCK, 0, st2>>>(cases.p, off_bslots.p, ncase, parity);
+    for (int s = 0; s < cfg.max_iterations; ++s) {
+      batch_interp_kernel<<<unsigned(nb_markers), BATCH_BLOCK, 0, st2>>>(cases.p, off_markers.p, ncase, s);
+      batch_spread_kernel<<<unsigned(nb_bslots), BATCH_BLOCK, 0, st2>>>(cases.p, off_bslots.p, ncase);
+      batch_diag_kernel<<<unsigned(nb_markers), BATCH_BLOCK, 0, st2>>>(cases.p, off_markers.p, off_bslots.p, ncase,
+                                                                         s);
+    }
+    batch_commit_kernel<<<unsigned(nb_bslots), BATCH_BLOCK, 0, st2>>>(cases.p, off_bslots.p, ncase);
+    if (parity) batch_cells_kernel<Q, S, true><<<unsigned(nb_slots), BATCH_BLOCK, 0, st2>>>(cases.p, off_slots.p, ncase);
+    else batch_cells_kernel<Q, S, false><<<unsigned(nb_slots), BATCH_BLOCK, 0, st2>>>(cases.p, off_slots.p, ncase);
+    CK(cudaGetLastError());
+    hydro(parity);
+    CK(cudaEventRecord(ev_join, st2));
+    CK(cudaStreamWaitEvent(st, ev_join, 0));
+    batch_fprev_kernel<<<unsigned(nb_slots), BATCH_BLOCK, 0, st>>>(cases.p, off_slots.p, ncase);
+    CK(cudaGetLastError());
+    parity ^= 1;
+  }
+
+  void run(int64_t steps, double* torque, double* device_ms) override {
+    if (steps < 0) invalid("steps must be >= 0");
+    for (E* e : eng) e->sync();
+    d_torque.alloc(size_t(std::max<int64_t>(1, steps)) * size_t(ncase));
+    d_counter.alloc(size_t(ncase));
+    CK(cudaMemsetAsync(d_counter.p, 0, size_t(ncase) * sizeof(int64_t), st));
+    for (int k = 0; k < ncase; ++k) {
+      cases_h[size_t(k)].series_torque = d_torque.p + size_t(k) * size_t(std::max<int64_t>(1, steps));
+      cases_h[size_t(k)].counter = d_counter.p + k;
+    }
+    cases.upload(cases_h, st);
+    CK(cudaEventRecord(ev0, st));
+    const int64_t G = 16;
+    int64_t done = 0;
+    if (parity != 0 && steps > 0) {
+      one_step();
+      ++done;
+    }
+    cudaGraphExec_t exec = nullptr;
+    while (steps - done >= G) {
+      if (!exec) {
+        cudaGraph_t g;
+        const int par0 = parity;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int64_t i = 0; i < G; ++i) one_step();
+        CK(cudaStreamEndCapture(st, &g));
+        CK(cudaGraphInstantiate(&exec, g, 0));
+        CK(cudaGraphDestroy(g));
+        parity = par0;
+      }
+      CK(cudaGraphLaunch(exec, st));
+      done += G;
+    }
+    if (exec) CK(cudaGraphExecDestroy(exec));
+    for (; done < steps; ++done) one_step();
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (device_ms) *device_ms = ms;
+    if (torque && steps > 0)
+      CK(cudaMemcpy(torque, d_torque.p, size_t(steps) * size_t(ncase) * sizeof(double), cudaMemcpyDeviceToHost));
+    for (E* e : eng) {
+      e->check_device_error();
+      e->parity = parity;
+      e->field_present = true;
+      e->fprev_stale = false;
+      e->invalidate_graphs();
+    }
+  }
+
+  // Times the batched sweep under every register budget on the cases' own
+  // grids (populations saved and restored) and keeps the fastest.
+  void autotune(int steps, int32_t* even, int32_t* odd, double* best_ms) override {
+    if (steps < 2) invalid("autotune: steps per trial must be >= 2");
+    steps += steps & 1;
+    for (E* e : eng) e->sync();
+    std::vector<std::unique_ptr<DevBuf<S>>> save;
+    for (E* e : eng) {
+      save.emplace_back(new DevBuf<S>());
+      save.back()->alloc(e->f_alloc.n);
+      CK(cudaMemcpyAsync(save.back()->p, e->f_alloc.p, e->f_alloc.n * sizeof(S), cudaMemcpyDeviceToDevice, st));
+    }
+    double bms = 0.0;
+    int be = 8, bo = 8;
+    for (int ev = 8; ev >= 6; --ev)
+      for (int od = 8; od >= 6; --od) {
+        minb[0] = ev;
+        minb[1] = od;
+        hydro(0);
+        hydro(1);
+        CK(cudaEventRecord(ev0, st));
+        for (int i = 0; i < steps; ++i) hydro(i & 1);
+        CK(cudaEventRecord(ev1, st));
+        CK(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        const double t = double(ms) / steps;
+        if (bms == 0.0 || t < bms) {
+          bms = t;
+          be = ev;
+          bo = od;
+        }
+      }
+    minb[0] = be;
+    minb[1] = bo;
+    for (size_t k = 0; k < eng.size(); ++k)
+      CK(cudaMemcpyAsync(eng[k]->f_alloc.p, save[k]->p, eng[k]->f_alloc.n * sizeof(S), cudaMemcpyDeviceToDevice,
+                         st));
+    CK(cudaStreamSynchronize(st));
+    if (even) *even = be;
+    if (odd) *odd = bo;
+    if (best_ms) *best_ms = bms;
+  }
+};
+
+template <int Q, class S>
+BatchBase* Engine<Q, S>::make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
+                                    const lbmb_ibm_config& c) {
+  if constexpr (std::is_same<typename Codec<S>::A, float>::value) {
+    return new Batch<Q, S>(all, bodies, c);
+  } else {
+    throw Error(LBMB_ERR_UNSUPPORTED, "batch runs need fp32/fp16/bf16 population storage");
+  }
+}
 
 // Factories, one per translation unit (engine_q*_*.cu).
 EngineBase* make_engine_q19_f32(const lbmb_config&, const uint8_t*, const double*);

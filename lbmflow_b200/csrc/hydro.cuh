@@ -422,11 +422,7 @@ __global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN
 
 // Cell-list sweep over the forced cells (after the IBM force update).
 template <int Q, class S, int COLL, bool ODD>
-__global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
-    hydro_cells_kernel(HydroParams<typename Codec<S>::A> p, const int64_t* cells, int64_t ncells) {
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= ncells) return;
-  const uint32_t cell = uint32_t(cells[i]);
+__device__ __forceinline__ void forced_cell(const HydroParams<typename Codec<S>::A>& p, uint32_t cell) {
   const uint32_t nxy = uint32_t(p.nxy);
   const int z = int(cell / nxy);
   const uint32_t r = cell - uint32_t(z) * nxy;
@@ -435,6 +431,14 @@ __global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN
   const uint8_t fl = p.flags[cell];
   if (fl & F_SOLID) return;
   hydro_cell<Q, S, COLL, ODD, true, true>(p, x, y, z, cell, fl);
+}
+
+template <int Q, class S, int COLL, bool ODD>
+__global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
+    hydro_cells_kernel(HydroParams<typename Codec<S>::A> p, const int64_t* cells, int64_t ncells) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= ncells) return;
+  forced_cell<Q, S, COLL, ODD>(p, uint32_t(cells[i]));
 }
 
 }  // namespace lbmb

@@ -92,14 +92,11 @@ __device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroPara
   return rho;
 }
 
-// MINB: resident blocks per SM the register allocation is sized for
-// (8: 64 registers, 7: 72, 6: 80).
-template <int Q, class S, bool ODD, int MINB>
-__global__ void __launch_bounds__(LEAN_BLOCK, MINB) hydro_lean_kernel(HydroParams<float> p, uint32_t n) {
+// Update of one cell (c < number of cells) with the lean kernel's code.
+template <int Q, class S, bool ODD>
+__device__ __forceinline__ void lean_cell(const HydroParams<float>& p, uint32_t c) {
   using L = Lat<Q>;
   using CD = Codec<S>;
-  const uint32_t c = blockIdx.x * LEAN_BLOCK + threadIdx.x;
-  if (c >= n) return;
   const uint32_t fl = p.flags[c];
   if (fl & (F_SOLID | F_FORCED)) return;
   const int nx = p.nx, nxy = p.nxy;
@@ -151,6 +148,15 @@ __global__ void __launch_bounds__(LEAN_BLOCK, MINB) hydro_lean_kernel(HydroParam
     else
       CD::st(cb + T(q), f[q]);
   }
+}
+
+// MINB: resident blocks per SM the register allocation is sized for
+// (8: 64 registers, 7: 72, 6: 80).
+template <int Q, class S, bool ODD, int MINB>
+__global__ void __launch_bounds__(LEAN_BLOCK, MINB) hydro_lean_kernel(HydroParams<float> p, uint32_t n) {
+  const uint32_t c = blockIdx.x * LEAN_BLOCK + threadIdx.x;
+  if (c >= n) return;
+  lean_cell<Q, S, ODD>(p, c);
 }
 
 }  // namespace lbmb

@@ -103,13 +103,13 @@ __device__ __forceinline__ void load_post_stream(const S* fb, int64_t pl, int64_
 // arithmetic: 1 + sum f) and (sum c f + F/2) / rho in f64 with the force
 // field current at call time.
 template <int Q, class S>
-__global__ void ibm_prep_kernel(IbmArgs a, const S* fb, int64_t pl, const int64_t* slot_cell,
-                                const uint8_t* flags, const uint32_t* nbr, int nx, int ny, int nz,
-                                int parity, const Vec4<typename Codec<S>::A>* fcur, int field_present,
-                                double gx, double gy, double gz) {
+__device__ __forceinline__ void ibm_prep_body(const IbmArgs& a, int64_t i, const S* fb, int64_t pl,
+                                              const int64_t* slot_cell, const uint8_t* flags, const uint32_t* nbr,
+                                              int nx, int ny, int nz, int parity,
+                                              const Vec4<typename Codec<S>::A>* fcur, int field_present, double gx,
+                                              double gy, double gz) {
   using A = typename Codec<S>::A;
   using L = Lat<Q>;
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i == 0) {
     IbmDiagDev* d = a.diag;
     d->slip_max = d->slip_rms = d->slip_max_rel = d->slip_rms_rel = 0.0;
@@ -156,9 +156,17 @@ __global__ void ibm_prep_kernel(IbmArgs a, const S* fb, int64_t pl, const int64_
   }
 }
 
+template <int Q, class S>
+__global__ void ibm_prep_kernel(IbmArgs a, const S* fb, int64_t pl, const int64_t* slot_cell,
+                                const uint8_t* flags, const uint32_t* nbr, int nx, int ny, int nz,
+                                int parity, const Vec4<typename Codec<S>::A>* fcur, int field_present,
+                                double gx, double gy, double gz) {
+  ibm_prep_body<Q, S>(a, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, fb, pl, slot_cell, flags, nbr, nx, ny, nz,
+                      parity, fcur, field_present, gx, gy, gz);
+}
+
 // Impulse per marker from the current du (solver.rs:3118-3173).
-static __global__ void ibm_interp_kernel(IbmArgs a, int sweep) {
-  const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_interp_body(const IbmArgs& a, int64_t m, int sweep) {
   if (m >= a.nm) return;
   if (a.diag->converged) return;
   double t[3], r[3];
@@ -201,6 +209,10 @@ static __global__ void ibm_interp_kernel(IbmArgs a, int sweep) {
   }
 }
 
+static __global__ void ibm_interp_kernel(IbmArgs a, int sweep) {
+  ibm_interp_body(a, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, sweep);
+}
+
 template <int N>
 __device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
   // sh: N * (blockDim/32) doubles. Fixed-order warp + block tree.
@@ -220,10 +232,11 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
 }
 
 // Spread the impulses into the slots, in marker order (solver.rs:3174-3209).
-static __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) {
+// bid: block index within this body's spread grid (its partial slot).
+__device__ __forceinline__ void ibm_spread_body(const IbmArgs& a, int64_t bid) {
   __shared__ double sh[3 * (IBM_BLOCK / 32)];
   if (a.diag->converged) return;
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t i = bid * blockDim.x + threadIdx.x;
   double ff[3] = {0.0, 0.0, 0.0};
   if (i < a.ns) {
     const int32_t g = a.bslot[i];
@@ -250,16 +263,20 @@ static __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a)
   }
   block_sum<3>(ff, sh);
   if (threadIdx.x == 0)
-    for (int c = 0; c < 3; ++c) a.part_spread[3 * blockIdx.x + c] = ff[c];
+    for (int c = 0; c < 3; ++c) a.part_spread[3 * bid + c] = ff[c];
 }
 
+static __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) { ibm_spread_body(a, blockIdx.x); }
+
 // Slip statistics and the sweep's global reduction (solver.rs:3211-3253).
-static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, int sweep, int nblk_spread) {
+// bid / nblk: block index and block count of this body's diag grid.
+__device__ __forceinline__ void ibm_diag_body(const IbmArgs& a, int sweep, int nblk_spread, unsigned int bid,
+                                              unsigned int nblk) {
   __shared__ double sh[9 * (IBM_BLOCK / 32)];
   __shared__ double smax_sh[IBM_BLOCK / 32];
   __shared__ bool last;
   if (a.diag->converged) return;
-  const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t m = int64_t(bid) * blockDim.x + threadIdx.x;
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ssq, wsum, mf[3], tq[3]
   double smax = 0.0;
   if (m < a.nm) {
@@ -294,12 +311,12 @@ static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, i
   block_sum<8>(v, sh);
   if (threadIdx.x == 0) {
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) smax = fmax(smax, smax_sh[w]);
-    double* p = a.part_diag + 9 * blockIdx.x;
+    double* p = a.part_diag + 9 * bid;
     p[0] = smax;
     for (int k = 0; k < 8; ++k) p[1 + k] = v[k];
     __threadfence();
     const unsigned int t = atomicAdd(&a.diag->ticket, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == nblk - 1);
   }
   __syncthreads();
   if (!last) return;
@@ -308,7 +325,7 @@ static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, i
   // ... in order, then a fixed tree (deterministic run to run).
   double acc[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // 8 diag sums, 3 spread sums
   double amax = 0.0;
-  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+  for (unsigned int b = threadIdx.x; b < nblk; b += blockDim.x) {
     const volatile double* p = a.part_diag + 9 * b;
     amax = fmax(amax, p[0]);
     for (int k = 0; k < 8; ++k) acc[k] += p[1 + k];
@@ -347,12 +364,15 @@ static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, i
   d->ticket = 0;
 }
 
+static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, int sweep, int nblk_spread) {
+  ibm_diag_body(a, sweep, nblk_spread, blockIdx.x, gridDim.x);
+}
+
 // force field += spread in the storage arithmetic (solver.rs:3256-3279),
 // and optionally record the diagnostics of this call into per-step series.
 template <class A>
-__global__ void ibm_commit_kernel(IbmArgs a, Vec4<A>* fcur, double* series_torque, double* series_ff,
-                                  int32_t* series_iters, int64_t* step_counter) {
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ibm_commit_body(const IbmArgs& a, int64_t i, Vec4<A>* fcur, double* series_torque,
+                                                double* series_ff, int32_t* series_iters, int64_t* step_counter) {
   if (i < a.ns) {
     const int32_t g = a.bslot[i];
     Vec4<A> v = fcur[g];
@@ -369,6 +389,13 @@ __global__ void ibm_commit_kernel(IbmArgs a, Vec4<A>* fcur, double* series_torqu
     if (series_iters) series_iters[s] = a.diag->iterations;
     *step_counter = s + 1;
   }
+}
+
+template <class A>
+__global__ void ibm_commit_kernel(IbmArgs a, Vec4<A>* fcur, double* series_torque, double* series_ff,
+                                  int32_t* series_iters, int64_t* step_counter) {
+  ibm_commit_body<A>(a, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, fcur, series_torque, series_ff,
+                     series_iters, step_counter);
 }
 
 }  // namespace lbmb

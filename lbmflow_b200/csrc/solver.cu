@@ -87,6 +87,10 @@ struct lbmb_solver {
   int device = 0;
 };
 
+struct lbmb_batch {
+  std::unique_ptr<lbmb::BatchBase> b;
+};
+
 using lbmb::Error;
 
 template <class F>
@@ -376,6 +380,46 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind) {
     if (!kind) lbmb::invalid("null output");
     *kind = h->e->sweep_kernel();
   });
+}
+
+int lbmb_batch_create(lbmb_solver* const* solvers, const int32_t* bodies, int32_t ncases,
+                      const lbmb_ibm_config* cfg, lbmb_batch** out) {
+  return guarded([&] {
+    if (!solvers || !cfg || !out) lbmb::invalid("null argument");
+    if (ncases <= 0) lbmb::invalid("batch needs at least one solver");
+    std::vector<lbmb::EngineBase*> all;
+    for (int32_t k = 0; k < ncases; ++k) {
+      if (!solvers[k] || !solvers[k]->e) lbmb::invalid("null solver in batch");
+      all.push_back(solvers[k]->e.get());
+    }
+    auto* h = new lbmb_batch();
+    try {
+      h->b.reset(all.front()->make_batch(all, bodies, *cfg));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int lbmb_batch_autotune(lbmb_batch* b, int32_t steps_per_trial, int32_t* even_blocks_per_sm,
+                        int32_t* odd_blocks_per_sm, double* best_ms_per_step) {
+  return guarded([&] {
+    if (!b || !b->b) lbmb::invalid("null batch");
+    b->b->autotune(steps_per_trial, even_blocks_per_sm, odd_blocks_per_sm, best_ms_per_step);
+  });
+}
+
+int lbmb_batch_run(lbmb_batch* b, int64_t steps, double* torque_lu, double* device_ms) {
+  return guarded([&] {
+    if (!b || !b->b) lbmb::invalid("null batch");
+    b->b->run(steps, torque_lu, device_ms);
+  });
+}
+
+int lbmb_batch_destroy(lbmb_batch* b) {
+  return guarded([&] { delete b; });
 }
 
 int lbmb_sync(lbmb_solver* h) {
