@@ -252,6 +252,42 @@ def throughput_study(lb, args, local, peak):
     return res
 
 
+def sweep_study(args, rank, world, local):
+    """Batched sweep (64 seeded D3Q19 TRT fp32 tanks, T ~ U{48..128}, height
+    1.25 T, u_tip ~ U(0.02, 0.06), Re ~ U(500, 5000), seed 0x5EED): all of a
+    rank's cases in lockstep through the batched runner, autotuned; cases are
+    sharded over ranks by LPT and per-case Np gathered on rank 0. The
+    reference's sequential per-case loop is timed on a bounded sample."""
+    from lbmflow_b200 import sweep
+
+    cases = sweep.seeded_cases()
+
+    def gather(obj):
+        if world == 1:
+            return [obj]
+        import torch.distributed as dist
+        out = [None] * world
+        dist.all_gather_object(out, obj)
+        return out
+
+    res = sweep.run_sharded(cases, args.sweep_steps, rank, world, gather, mode="batch", les_cs=args.les_cs,
+                            device=local, warmup=16)
+    if rank != 0:
+        return None
+    out = {"cases": len(cases), "steps_per_case": args.sweep_steps, "cells_total": sum(c.cells for c in cases),
+           "mlups": res["mlups"], "device_ms_max_over_ranks": res["device_ms_max"],
+           "Np": res["aggregate"].get("Np"), "finite_cases": sum(1 for p in res["per_case"] if np.isfinite(p["Np"])),
+           "seed": "0x5EED", "storage": "f32", "lattice": "D3Q19 TRT", "sharding": f"LPT over {world} rank(s)"}
+    if world == 1 and args.sweep_seq_steps > 0:
+        seq = sweep.run_sweep(cases, args.sweep_seq_steps, mode="sequential", les_cs=args.les_cs, autotune=False,
+                              device=local)
+        out["sequential_sample"] = {"steps_per_case": args.sweep_seq_steps, "mlups": seq["mlups"],
+                                    "what": "one case after another (sweep.rs:61-68 order), each through the "
+                                            "device runner loop"}
+        out["batch_over_sequential"] = res["mlups"] / seq["mlups"]
+    return out
+
+
 def run_b200(args, rank, world, local):
     import lbmflow_b200 as lb
 
@@ -315,6 +351,10 @@ def run_b200(args, rank, world, local):
     g2.close()
     g.close()
     extra = {}
+    if args.sweep_steps > 0:
+        sw = sweep_study(args, rank, world, local)
+        if sw is not None:
+            extra["sweep"] = sw
     if args.variants and world == 1:
         extra["qoi_precision"] = qoi_study(lb, args, local, dims, solid, body, nu, D, np_head)
         extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
@@ -398,6 +438,9 @@ def main():
     ap.add_argument("--les-cs", type=float, default=0.1, help="Smagorinsky constant (0: reference operators)")
     ap.add_argument("--big-T", type=int, default=256, help="tank diameter of the throughput study")
     ap.add_argument("--big-steps", type=int, default=100)
+    ap.add_argument("--sweep-steps", type=int, default=5000, help="steps per case of the batched sweep (0: skip)")
+    ap.add_argument("--sweep-seq-steps", type=int, default=200,
+                    help="steps per case of the sequential-loop sample (0: skip)")
     args = ap.parse_args()
     rank, world, local = dist_init(args.gpus)
     if args.impl == "reference":

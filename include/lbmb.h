@@ -317,6 +317,38 @@ int lbmb_batch_autotune(lbmb_batch* b, int32_t steps_per_trial, int32_t* even_bl
 int lbmb_batch_run(lbmb_batch* b, int64_t steps, double* torque_lu, double* device_ms);
 int lbmb_batch_destroy(lbmb_batch* b);
 
+/* Adjoint of the runner loop (no reference counterpart: the reference has
+ * no differentiation). Runs `steps` runner steps from the solver's current
+ * state with the body's IBM at a fixed sweep count (cfg->max_iterations,
+ * slip tolerance ignored: no early exit), J = mean of the per-step torque
+ * (runner.rs:1396-1425 convention) over steps [window_begin, steps). The
+ * populations are checkpointed every checkpoint_every steps; the backward
+ * pass recomputes each segment from its checkpoint and runs the discrete
+ * adjoint of the IBM + TRT collide-stream step in reverse, giving dJ/dnu,
+ * dJ/dOmega_z (rad/step) and dJ/d(marker position) (3 per marker, NULL to
+ * skip). torque (may be NULL) receives the forward series (steps values).
+ * Needs TRT/BGK, no subgrid model, no uniform force, no scalars. The solver
+ * ends in the state after the forward run. Device memory: one population
+ * buffer per checkpoint and per step of a segment. */
+typedef struct {
+  int64_t steps;
+  int64_t window_begin;
+  int32_t checkpoint_every; /* default 100 when <= 0; rounded up to even */
+  int32_t body;
+} lbmb_adjoint_config;
+typedef struct {
+  double J;
+  double dJ_dnu;
+  double dJ_domega_z;
+  double dJ_domega_plus;  /* w.r.t. the TRT rates, for reference */
+  double dJ_domega_minus;
+  double forward_ms;      /* device time of the checkpointed forward run */
+  double adjoint_ms;      /* device time of recomputation + backward pass */
+  int64_t markers;
+} lbmb_adjoint_result;
+int lbmb_adjoint_torque(lbmb_solver* h, const lbmb_ibm_config* cfg, const lbmb_adjoint_config* ac,
+                        lbmb_adjoint_result* out, double* dJ_dpos, double* torque);
+
 /* Synchronize the solver stream. */
 int lbmb_sync(lbmb_solver* h);
 

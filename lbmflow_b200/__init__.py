@@ -40,7 +40,7 @@ EXPORTS = (
     "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
     "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
     "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
-    "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy",
+    "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy", "lbmb_adjoint_torque",
 )
 
 
@@ -78,6 +78,17 @@ class _Config(C.Structure):
 class _AutotuneResult(C.Structure):
     _fields_ = [("kind", C.c_int32), ("even_blocks_per_sm", C.c_int32), ("odd_blocks_per_sm", C.c_int32),
                 ("n_trials", C.c_int32), ("best_ms_per_step", C.c_double), ("default_ms_per_step", C.c_double)]
+
+
+class _AdjointConfig(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("window_begin", C.c_int64), ("checkpoint_every", C.c_int32),
+                ("body", C.c_int32)]
+
+
+class _AdjointResult(C.Structure):
+    _fields_ = [("J", C.c_double), ("dJ_dnu", C.c_double), ("dJ_domega_z", C.c_double),
+                ("dJ_domega_plus", C.c_double), ("dJ_domega_minus", C.c_double), ("forward_ms", C.c_double),
+                ("adjoint_ms", C.c_double), ("markers", C.c_int64)]
 
 
 class _IbmConfig(C.Structure):
@@ -148,6 +159,8 @@ def lib():
         L.lbmb_batch_autotune.argtypes = [vp, C.c_int32, _i32p, _i32p, _dp]
         L.lbmb_batch_run.argtypes = [vp, C.c_int64, _dp, _dp]
         L.lbmb_batch_destroy.argtypes = [vp]
+        L.lbmb_adjoint_torque.argtypes = [vp, C.POINTER(_IbmConfig), C.POINTER(_AdjointConfig),
+                                          C.POINTER(_AdjointResult), _dp, _dp]
         L.lbmb_reduce_populations_noalloc.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, vp, _dp,
                                                       _dp, vp]
         _lib = L
@@ -385,6 +398,25 @@ class Solver:
                                        int(probe_every), _d(torque), _d(ff), _d(cv),
                                        iters.ctypes.data_as(_i32p)))
         return {"torque_lu": torque, "fluid_force": ff.reshape(steps, 3), "ibm_iterations": iters, "cv": cv}
+
+    def adjoint_torque(self, body: RotatingBody, steps, window_begin=None, checkpoint_every=100,
+                       cfg: DirectForcingConfig = None):
+        """Gradient of J = mean torque over steps [window_begin, steps) of the
+        runner loop (fixed IBM sweep count) w.r.t. nu, Omega_z and the marker
+        positions, by the discrete adjoint with checkpointed recomputation."""
+        cfg = cfg or DirectForcingConfig()
+        if window_begin is None:
+            window_begin = steps // 2
+        slot = self._slot_for(body)
+        nm = int(np.asarray(body.weights).size)
+        ac = _AdjointConfig(int(steps), int(window_begin), int(checkpoint_every), int(slot))
+        r = _AdjointResult()
+        dpos = np.zeros(3 * max(nm, 1))
+        tq = np.zeros(int(steps))
+        _check(lib().lbmb_adjoint_torque(self.h, C.byref(cfg._c()), C.byref(ac), C.byref(r), _d(dpos), _d(tq)))
+        return {"J": r.J, "dJ_dnu": r.dJ_dnu, "dJ_domega_z": r.dJ_domega_z, "dJ_domega_plus": r.dJ_domega_plus,
+                "dJ_domega_minus": r.dJ_domega_minus, "dJ_dpos": dpos[:3 * nm].reshape(nm, 3), "torque": tq,
+                "forward_ms": r.forward_ms, "adjoint_ms": r.adjoint_ms}
 
     # --- passive scalar -----------------------------------------------------
     def enable_scalar_distribution(self, diffusivity, q=None):

@@ -28,6 +28,7 @@
 #include "hydro_tile.cuh"
 #include "hydro_lean.cuh"
 #include "batch.cuh"
+#include "adjoint.cuh"
 #include "ibm.cuh"
 #include "scalar.cuh"
 
@@ -132,6 +133,8 @@ struct EngineBase {
   virtual void set_sweep_variant(int even, int odd) = 0;
   virtual void autotune_sweep(int steps, lbmb_autotune_result* out, int32_t* trial_desc, double* trial_ms,
                               int capacity) = 0;
+  virtual void adjoint_torque(const lbmb_ibm_config& cfg, const lbmb_adjoint_config& ac, lbmb_adjoint_result* out,
+                              double* dJ_dpos, double* torque) = 0;
   // A batch over `all` (this engine's type for every entry), one body each.
   virtual BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
                                 const lbmb_ibm_config& cfg) = 0;
@@ -1317,6 +1320,258 @@ struct Engine final : EngineBase {
 
   BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
                         const lbmb_ibm_config& cfg) override;
+
+  // ---- adjoint of the runner loop ------------------------------------------
+  // One runner step (clear field -> IBM -> hydro of the forced cells on the
+  // side stream, full-grid sweep on the main stream, field refresh), eager.
+  void enqueue_runner_step(BodyState& B, const lbmb_ibm_config& c, double* s_torque, int64_t* counter) {
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+    if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st2));
+    enqueue_ibm(B, c, s_torque, nullptr, nullptr, counter, false, st2);
+    field_present = true;
+    launch_hydro(parity, st2, false, true);
+    launch_hydro(parity, st, true, false);
+    CK(cudaEventRecord(ev_join, st2));
+    CK(cudaStreamWaitEvent(st, ev_join, 0));
+    parity ^= 1;
+    if (nslots) CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
+    fprev_stale = false;
+  }
+
+  void snapshot(S* out) {
+    snapshot_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(fp, plane, flags.p, nbr.p, nx, ny, nz, parity,
+                                                                      out, n);
+    CK(cudaGetLastError());
+  }
+
+  void adjoint_torque(const lbmb_ibm_config& c0, const lbmb_adjoint_config& ac, lbmb_adjoint_result* out,
+                      double* dJ_dpos, double* torque_out) override {
+    if (coll != COLL_TRT) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint covers TRT/BGK collision");
+    if (cfg.smagorinsky_cs > 0.0) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs the subgrid model off");
+    if (has_uniform_force()) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs no uniform body force");
+    if (!scalars.empty()) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs a solver without scalars");
+    const int64_t N = ac.steps;
+    if (N < 1) invalid("adjoint: steps must be >= 1");
+    if (ac.window_begin < 0 || ac.window_begin >= N) invalid("adjoint: window_begin must be in [0, steps)");
+    int64_t K = ac.checkpoint_every > 0 ? ac.checkpoint_every : 100;
+    K += K & 1;
+    // fixed sweep count: no early exit (slip tolerance 0)
+    lbmb_ibm_config c = c0;
+    c.slip_tolerance = 0.0;
+    BodyState& B = body_for(ac.body, c);
+    const int nsweep = c.max_iterations;
+    const int64_t nseg = ceil_div(N, K);
+    const size_t fsz = size_t(Q) * size_t(plane);
+    const size_t ns3 = size_t(std::max<int64_t>(nslots, 1));
+    sync();
+    // ---- forward pass with checkpoints -------------------------------------
+    DevBuf<S> ck_f;
+    DevBuf<Vec4<A>> ck_fp;
+    ck_f.alloc(size_t(nseg) * fsz);
+    ck_fp.alloc(size_t(nseg) * ns3);
+    DevBuf<double> d_torque;
+    DevBuf<int64_t> d_counter;
+    d_torque.alloc(size_t(N));
+    d_counter.alloc(1);
+    CK(cudaMemsetAsync(d_counter.p, 0, sizeof(int64_t), st));
+    if (!field_present && nslots) CK(cudaMemsetAsync(fprev.p, 0, ns3 * sizeof(Vec4<A>), st));
+    if (fprev_stale && nslots) {
+      CK(cudaMemcpyAsync(fprev.p, fcur.p, ns3 * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
+      fprev_stale = false;
+    }
+    CK(cudaEventRecord(ev0, st));
+    for (int64_t nn = 0; nn < N; ++nn) {
+      if (nn % K == 0) {
+        snapshot(ck_f.p + size_t(nn / K) * fsz);
+        if (nslots)
+          CK(cudaMemcpyAsync(ck_fp.p + size_t(nn / K) * ns3, fprev.p, size_t(nslots) * sizeof(Vec4<A>),
+                             cudaMemcpyDeviceToDevice, st));
+      }
+      enqueue_runner_step(B, c, d_torque.p, d_counter.p);
+    }
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaEventSynchronize(ev1));
+    check_device_error();
+    float fwd_ms = 0.f;
+    CK(cudaEventElapsedTime(&fwd_ms, ev0, ev1));
+    std::vector<double> tq(static_cast<size_t>(N));
+    CK(cudaMemcpy(tq.data(), d_torque.p, size_t(N) * sizeof(double), cudaMemcpyDeviceToHost));
+    double J = 0.0;
+    for (int64_t nn = ac.window_begin; nn < N; ++nn) J += tq[size_t(nn)];
+    const double Tbar = 1.0 / double(N - ac.window_begin);
+    J *= Tbar;
+    // final state, restored after the backward pass
+    DevBuf<S> fin_f;
+    DevBuf<Vec4<A>> fin_fp;
+    fin_f.alloc(f_alloc.n);
+    fin_fp.alloc(ns3);
+    CK(cudaMemcpyAsync(fin_f.p, f_alloc.p, f_alloc.n * sizeof(S), cudaMemcpyDeviceToDevice, st));
+    if (nslots) CK(cudaMemcpyAsync(fin_fp.p, fprev.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
+    const int fin_parity = parity;
+    // ---- backward pass ----------------------------------------------------
+    DevBuf<S> seg_f;
+    DevBuf<Vec4<A>> seg_F;
+    seg_f.alloc(size_t(K) * fsz);
+    seg_F.alloc(size_t(K) * ns3);
+    DevBuf<A> lam0, lam1;
+    lam0.alloc(fsz);
+    lam1.alloc(fsz);
+    CK(cudaMemsetAsync(lam0.p, 0, fsz * sizeof(A), st));
+    CK(cudaMemsetAsync(lam1.p, 0, fsz * sizeof(A), st));
+    DevBuf<double> mu0, mu1, Fbar, dubar, ubar, rhobar, cksbar, umbar, tbar, mobbar, xbar, grad, imp_k, du_k;
+    for (DevBuf<double>* b : {&mu0, &mu1, &Fbar, &dubar, &ubar}) {
+      b->alloc(3 * ns3);
+      CK(cudaMemsetAsync(b->p, 0, 3 * ns3 * sizeof(double), st));
+    }
+    for (DevBuf<double>* b : {&rhobar, &cksbar}) {
+      b->alloc(ns3);
+      CK(cudaMemsetAsync(b->p, 0, ns3 * sizeof(double), st));
+    }
+    const size_t nm = size_t(std::max<int64_t>(B.nm, 1));
+    for (DevBuf<double>* b : {&umbar, &tbar, &xbar}) {
+      b->alloc(3 * nm);
+      CK(cudaMemsetAsync(b->p, 0, 3 * nm * sizeof(double), st));
+    }
+    mobbar.alloc(nm);
+    CK(cudaMemsetAsync(mobbar.p, 0, nm * sizeof(double), st));
+    grad.alloc(3);
+    CK(cudaMemsetAsync(grad.p, 0, 3 * sizeof(double), st));
+    imp_k.alloc(size_t(nsweep) * nm * 3);
+    du_k.alloc(size_t(nsweep) * ns3 * 3);
+    DevBuf<double> dummy_t;
+    DevBuf<int64_t> dummy_c;
+    dummy_t.alloc(size_t(K) + 1);
+    dummy_c.alloc(1);
+    A* lam_next = lam0.p;
+    A* lam_cur = lam1.p;
+    double* mu_next = mu0.p;
+    double* mu_cur = mu1.p;
+    IbmArgs a = ibm_args(B, c);
+    const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
+    const unsigned gm = unsigned(std::max<int64_t>(1, ceil_div(B.nm, IBM_BLOCK)));
+    const unsigned gc = unsigned(ceil_div(n, ADJ_BLOCK));
+    CK(cudaEventRecord(ev0, st));
+    for (int64_t seg = nseg - 1; seg >= 0; --seg) {
+      const int64_t s0 = seg * K, s1 = std::min<int64_t>(N, s0 + K);
+      // restore the checkpoint (the logical layout is the parity-0 storage)
+      CK(cudaMemcpyAsync(fp, ck_f.p + size_t(seg) * fsz, fsz * sizeof(S), cudaMemcpyDeviceToDevice, st));
+      if (nslots)
+        CK(cudaMemcpyAsync(fprev.p, ck_fp.p + size_t(seg) * ns3, size_t(nslots) * sizeof(Vec4<A>),
+                           cudaMemcpyDeviceToDevice, st));
+      parity = 0;
+      field_present = true;
+      fprev_stale = false;
+      CK(cudaMemsetAsync(dummy_c.p, 0, sizeof(int64_t), st));
+      for (int64_t nn = s0; nn < s1; ++nn) {
+        snapshot(seg_f.p + size_t(nn - s0) * fsz);
+        enqueue_runner_step(B, c, dummy_t.p, dummy_c.p);
+        if (nslots)
+          CK(cudaMemcpyAsync(seg_F.p + size_t(nn - s0) * ns3, fcur.p, size_t(nslots) * sizeof(Vec4<A>),
+                             cudaMemcpyDeviceToDevice, st));
+      }
+      for (int64_t nn = s1 - 1; nn >= s0; --nn) {
+        const S* fn = seg_f.p + size_t(nn - s0) * fsz;
+        // IBM intermediates of step nn (the forward kernels on the snapshot)
+        ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, st>>>(a, fn, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz, 0,
+                                                        fcur.p, 0, 0.0, 0.0, 0.0);
+        for (int k = 0; k < nsweep; ++k) {
+          CK(cudaMemcpyAsync(du_k.p + size_t(k) * ns3 * 3, s_du.p, size_t(nslots) * 3 * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
+          ibm_interp_kernel<<<gm, IBM_BLOCK, 0, st>>>(a, k);
+          CK(cudaMemcpyAsync(imp_k.p + size_t(k) * nm * 3, B.imp.p, size_t(B.nm) * 3 * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
+          ibm_spread_kernel<<<gs, IBM_BLOCK, 0, st>>>(a);
+        }
+        CK(cudaGetLastError());
+        AdjCollide<S> pc;
+        pc.f = fn;
+        pc.pl = plane;
+        pc.flags = flags.p;
+        pc.nbr = nbr.p;
+        pc.wall_u = wall_u.p;
+        pc.fslot = fslot.p;
+        pc.F = seg_F.p + size_t(nn - s0) * ns3;
+        pc.Fp = nn > s0 ? seg_F.p + size_t(nn - s0 - 1) * ns3 : ck_fp.p + size_t(seg) * ns3;
+        pc.lam_in = lam_next;
+        pc.lam_out = lam_cur;
+        pc.mu_in = mu_next;
+        pc.mu_out = mu_cur;
+        pc.Fbar = Fbar.p;
+        pc.grad = grad.p;
+        pc.nx = nx;
+        pc.ny = ny;
+        pc.nz = nz;
+        pc.op = omega_p;
+        pc.om = omega_m;
+        adj_collide_kernel<Q, S><<<gc, ADJ_BLOCK, 0, st>>>(pc, n);
+        CK(cudaGetLastError());
+        AdjIbm b;
+        b.a = a;
+        b.imp_k = imp_k.p;
+        b.du_k = du_k.p;
+        b.nslot = int64_t(ns3);
+        b.slot_cell = slot_cell.p;
+        b.nx = nx;
+        b.ny = ny;
+        b.radius = c.kernel_radius;
+        b.Fbar = Fbar.p;
+        b.dubar = dubar.p;
+        b.ubar = ubar.p;
+        b.rhobar = rhobar.p;
+        b.cksbar = cksbar.p;
+        b.umbar = umbar.p;
+        b.tbar = tbar.p;
+        b.mobbar = mobbar.p;
+        b.xbar = xbar.p;
+        b.grad = grad.p;
+        b.Tbar = nn >= ac.window_begin ? Tbar : 0.0;
+        for (int k = nsweep - 1; k >= 0; --k) {
+          adj_ibm_marker_kernel<<<gm, ADJ_BLOCK, 0, st>>>(b, k);
+          adj_ibm_slot_kernel<<<gs, ADJ_BLOCK, 0, st>>>(b, k);
+        }
+        adj_ibm_mob_slot_kernel<<<gs, ADJ_BLOCK, 0, st>>>(b);
+        adj_ibm_mob_marker_kernel<<<gm, ADJ_BLOCK, 0, st>>>(b);
+        adj_ibm_fbar_kernel<Q, A><<<gs, ADJ_BLOCK, 0, st>>>(b, lam_cur, plane);
+        CK(cudaGetLastError());
+        std::swap(lam_next, lam_cur);
+        std::swap(mu_next, mu_cur);
+      }
+    }
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaEventSynchronize(ev1));
+    check_device_error();
+    float adj_ms = 0.f;
+    CK(cudaEventElapsedTime(&adj_ms, ev0, ev1));
+    double gh[3];
+    CK(cudaMemcpy(gh, grad.p, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (dJ_dpos && B.nm)
+      CK(cudaMemcpy(dJ_dpos, xbar.p, size_t(B.nm) * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (torque_out) std::copy(tq.begin(), tq.end(), torque_out);
+    // restore the state at the end of the forward run
+    CK(cudaMemcpyAsync(f_alloc.p, fin_f.p, f_alloc.n * sizeof(S), cudaMemcpyDeviceToDevice, st));
+    if (nslots) CK(cudaMemcpyAsync(fprev.p, fin_fp.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    parity = fin_parity;
+    field_present = true;
+    fprev_stale = false;
+    invalidate_graphs();
+    // d omega / d nu (params.rs:205-217): omega+ = 1/(3 nu + 1/2),
+    // omega- = 1/(magic/(3 nu) + 1/2) for TRT, = omega+ for BGK
+    const double nu = cfg.nu;
+    const double dwp = -3.0 * omega_p * omega_p;
+    const double dwm = cfg.collision == LBMB_TRT ? omega_m * omega_m * cfg.magic / (3.0 * nu * nu) : dwp;
+    if (out) {
+      out->J = J;
+      out->dJ_domega_plus = gh[0];
+      out->dJ_domega_minus = gh[1];
+      out->dJ_dnu = gh[0] * dwp + gh[1] * dwm;
+      out->dJ_domega_z = gh[2];
+      out->forward_ms = fwd_ms;
+      out->adjoint_ms = adj_ms;
+      out->markers = B.nm;
+    }
+  }
 
   int64_t solid_count() const {
     int64_t s = 0;

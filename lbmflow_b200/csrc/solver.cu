@@ -422,6 +422,15 @@ int lbmb_batch_destroy(lbmb_batch* b) {
   return guarded([&] { delete b; });
 }
 
+int lbmb_adjoint_torque(lbmb_solver* h, const lbmb_ibm_config* cfg, const lbmb_adjoint_config* ac,
+                        lbmb_adjoint_result* out, double* dJ_dpos, double* torque) {
+  return guarded([&] {
+    NEED(h);
+    if (!cfg || !ac) lbmb::invalid("null argument");
+    h->e->adjoint_torque(*cfg, *ac, out, dJ_dpos, torque);
+  });
+}
+
 int lbmb_sync(lbmb_solver* h) {
   return guarded([&] {
     NEED(h);
