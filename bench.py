@@ -288,6 +288,80 @@ def sweep_study(args, rank, world, local):
     return out
 
 
+def adjoint_study(args, local):
+    """Adjoint of the runner loop on the D3Q19 TRT tank T = 96 (96 x 96 x
+    120), fp32 forward with f64 reductions, 2000 steps, a checkpoint every
+    100, J = mean torque over steps 1001-2000, fixed 3 IBM sweeps. Gradient
+    w.r.t. (nu, Omega, marker positions) checked against central differences
+    of the f64 forward on seeded random directions in (nu / nu0, Omega /
+    Omega0, x / cell), relative step 1e-4, and against the f64 adjoint. The
+    markers get a seeded jitter of at most 0.1 cell (no marker on a kink of
+    the linear IBM kernel). Re = adj_re keeps the flow laminar so that J is
+    smooth in the parameters."""
+    import lbmflow_b200 as lb
+    from lbmflow_b200 import sweep
+
+    T, steps, K = args.adj_T, args.adj_steps, 100
+    win = steps // 2
+    c = sweep.TankCase(T, 0.05, args.adj_re)
+    geo = sweep.tank_geometry(T)
+    rng = np.random.default_rng(0x5EED)
+    pos0 = geo["marker_pos"] + rng.uniform(-0.1, 0.1, size=geo["marker_pos"].shape)
+    cfg = lb.DirectForcingConfig(max_iterations=3, slip_tolerance=0.0)
+
+    def solver(storage, nu):
+        return lb.Solver(c.dims, lattice=19, collision="trt", storage=storage, nu=nu, solid=geo["solid"],
+                         device=local)
+
+    def body(omega, pos):
+        return lb.RotatingBody(geo["center"], [0.0, 0.0, omega], pos, geo["marker_w"])
+
+    g = solver("f32", c.nu)
+    r32 = g.adjoint_torque(body(c.omega, pos0), steps, win, K, cfg)
+    g.close()
+    # plain forward (graph-captured runner) for the cost ratio
+    g = solver("f32", c.nu)
+    g.run_impeller(body(c.omega, pos0), steps, cfg)
+    fwd_ms, _, _ = g.last_timing()
+    g.close()
+    g = solver("f64", c.nu)
+    r64 = g.adjoint_torque(body(c.omega, pos0), steps, win, K, cfg)
+    g.close()
+
+    def J(nu, omega, pos):
+        s_ = solver("f64", nu)
+        t = s_.run_impeller(body(omega, pos), steps, cfg)["torque_lu"]
+        s_.close()
+        return float(np.mean(t[win:]))
+
+    nm = pos0.shape[0]
+    h = 1e-4
+    errs, errs64 = [], []
+    for k in range(args.adj_dirs):
+        d = rng.normal(size=2 + 3 * nm)
+        d /= np.linalg.norm(d)
+        dn, do, dp = d[0] * c.nu, d[1] * c.omega, d[2:].reshape(nm, 3)
+        fd = (J(c.nu + h * dn, c.omega + h * do, pos0 + h * dp) -
+              J(c.nu - h * dn, c.omega - h * do, pos0 - h * dp)) / (2 * h)
+        ad32 = r32["dJ_dnu"] * dn + r32["dJ_domega_z"] * do + float(np.sum(r32["dJ_dpos"] * dp))
+        ad64 = r64["dJ_dnu"] * dn + r64["dJ_domega_z"] * do + float(np.sum(r64["dJ_dpos"] * dp))
+        errs.append(abs(ad32 - fd) / abs(fd))
+        errs64.append(abs(ad64 - fd) / abs(fd))
+    g32 = np.concatenate([[r32["dJ_dnu"], r32["dJ_domega_z"]], r32["dJ_dpos"].ravel()])
+    g64 = np.concatenate([[r64["dJ_dnu"], r64["dJ_domega_z"]], r64["dJ_dpos"].ravel()])
+    return {"grid": list(c.dims), "steps": steps, "checkpoint_every": K, "window": [win, steps],
+            "re": args.adj_re, "u_tip": 0.05, "markers": int(nm), "J_f32": r32["J"], "J_f64": r64["J"],
+            "dJ_dnu": r32["dJ_dnu"], "dJ_domega": r32["dJ_domega_z"],
+            "fd_directions": args.adj_dirs, "fd_rel_step": h,
+            "fd_rel_err_f32_adjoint_max": max(errs) if errs else None,
+            "fd_rel_err_f64_adjoint_max": max(errs64) if errs64 else None,
+            "f32_vs_f64_gradient_rel": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+            "forward_ms_runner": fwd_ms, "forward_ms_checkpointed": r32["forward_ms"],
+            "recompute_plus_adjoint_ms": r32["adjoint_ms"],
+            "cost_ratio": r32["adjoint_ms"] / fwd_ms,
+            "cost_note": "(recomputation + backward pass) / plain forward runner, device time"}
+
+
 def run_b200(args, rank, world, local):
     import lbmflow_b200 as lb
 
@@ -355,6 +429,8 @@ def run_b200(args, rank, world, local):
         sw = sweep_study(args, rank, world, local)
         if sw is not None:
             extra["sweep"] = sw
+    if args.adj_steps > 0 and world == 1:
+        extra["adjoint"] = adjoint_study(args, local)
     if args.variants and world == 1:
         extra["qoi_precision"] = qoi_study(lb, args, local, dims, solid, body, nu, D, np_head)
         extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
@@ -439,6 +515,10 @@ def main():
     ap.add_argument("--big-T", type=int, default=256, help="tank diameter of the throughput study")
     ap.add_argument("--big-steps", type=int, default=100)
     ap.add_argument("--sweep-steps", type=int, default=5000, help="steps per case of the batched sweep (0: skip)")
+    ap.add_argument("--adj-steps", type=int, default=2000, help="adjoint study steps (0: skip)")
+    ap.add_argument("--adj-T", type=int, default=96)
+    ap.add_argument("--adj-re", type=float, default=100.0)
+    ap.add_argument("--adj-dirs", type=int, default=16)
     ap.add_argument("--sweep-seq-steps", type=int, default=200,
                     help="steps per case of the sequential-loop sample (0: skip)")
     args = ap.parse_args()

@@ -97,117 +97,134 @@ __device__ __forceinline__ void adj_block_add(double (&v)[N], double* out) {
     }
 }
 
-template <int Q, class S>
-__global__ void __launch_bounds__(ADJ_BLOCK) adj_collide_kernel(AdjCollide<S> p, int64_t n) {
+// Collision + stream adjoint of one fluid cell. FORCED: the cell carries an
+// IBM force (F, Fp from its slot); otherwise both are zero and the Guo terms
+// drop out at compile time.
+template <int Q, class S, bool FORCED>
+__device__ __forceinline__ void adj_cell(const AdjCollide<S>& p, int64_t cell, uint8_t fl, double (&gsum)[2]) {
   using L = Lat<Q>;
   using A = typename Codec<S>::A;
-  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  double gsum[2] = {0.0, 0.0};
-  if (cell < n && !(p.flags[cell] & F_SOLID)) {
-    const uint8_t fl = p.flags[cell];
-    const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
-    const int64_t pl = p.pl;
-    // lambda*: reverse of the push stream with bounce-back
-    A ls[Q];
+  const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
+  const int64_t pl = p.pl;
+  // lambda*: reverse of the push stream with bounce-back
+  A ls[Q];
+  if (fl & F_WRAP) {
     int x = 0, y = 0, z = 0;
     cell_xyz(cell, p.nx, p.ny, x, y, z);
     const Nbr nb(x, y, z, p.nx, p.ny, p.nz);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      if ((mask >> q) & 1u) ls[q] = p.lam_in[opp(q) * pl + cell];
-      else ls[q] = p.lam_in[q * pl + nb.at(L::cx(q), L::cy(q), L::cz(q))];
-    }
-    A f[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) f[q] = Codec<S>::ld(p.f + q * pl + cell);
-    A F[3] = {A(0), A(0), A(0)}, Fp[3] = {A(0), A(0), A(0)};
-    int32_t g = -1;
-    if (fl & F_FORCED) {
-      g = p.fslot[cell];
-      const Vec4<A> a = p.F[g], b = p.Fp[g];
-      F[0] = a.x, F[1] = a.y, F[2] = a.z;
-      Fp[0] = b.x, Fp[1] = b.y, Fp[2] = b.z;
-    }
-    A dr = A(0), j[3] = {A(0), A(0), A(0)};
+    for (int q = 0; q < Q; ++q)
+      ls[q] = ((mask >> q) & 1u) ? p.lam_in[opp(q) * pl + cell]
+                                 : p.lam_in[q * pl + nb.at(L::cx(q), L::cy(q), L::cz(q))];
+  } else {
+    const int64_t nxy = int64_t(p.nx) * p.ny;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      dr += f[q];
-      j[0] += A(L::cx(q)) * f[q];
-      j[1] += A(L::cy(q)) * f[q];
-      j[2] += A(L::cz(q)) * f[q];
+      const int64_t d = int64_t(L::cx(q)) + int64_t(L::cy(q)) * p.nx + int64_t(L::cz(q)) * nxy;
+      ls[q] = ((mask >> q) & 1u) ? p.lam_in[opp(q) * pl + cell] : p.lam_in[q * pl + cell + d];
     }
-    const A rho = A(1) + dr, inv = A(1) / rho;
-    const A u[3] = {(j[0] + A(0.5) * Fp[0]) * inv, (j[1] + A(0.5) * Fp[1]) * inv, (j[2] + A(0.5) * Fp[2]) * inv};
-    const A usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    const A uF = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
-    const A op = A(p.op), om = A(p.om), cp = A(1) - op * A(0.5), cm = A(1) - om * A(0.5);
-    // projections of lambda* and of r = f - e + S/2
-    A lp[Q], lm[Q], rr[Q];
+  }
+  A f[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const A cu = A(L::cx(q)) * u[0] + A(L::cy(q)) * u[1] + A(L::cz(q)) * u[2];
-      const A cF = A(L::cx(q)) * F[0] + A(L::cy(q)) * F[1] + A(L::cz(q)) * F[2];
-      const A w = A(L::w(q));
-      const A e = w * (dr + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * usq));
-      const A s = w * (A(3) * (cF - uF) + A(9) * cu * cF);
-      rr[q] = f[q] - e + A(0.5) * s;
-    }
-    lp[0] = ls[0];
-    lm[0] = A(0);
+  for (int q = 0; q < Q; ++q) f[q] = Codec<S>::ld(p.f + q * pl + cell);
+  A F[3] = {A(0), A(0), A(0)}, Fp[3] = {A(0), A(0), A(0)};
+  int32_t g = -1;
+  if (FORCED) {
+    g = p.fslot[cell];
+    const Vec4<A> a = p.F[g], b = p.Fp[g];
+    F[0] = a.x, F[1] = a.y, F[2] = a.z;
+    Fp[0] = b.x, Fp[1] = b.y, Fp[2] = b.z;
+  }
+  A dr = A(0), j[3] = {A(0), A(0), A(0)};
 #pragma unroll
-    for (int k = 0; k < (Q - 1) / 2; ++k) {
-      const int a = 2 * k + 1, b = a + 1;
-      const A sp = A(0.5) * (ls[a] + ls[b]), sm = A(0.5) * (ls[a] - ls[b]);
-      lp[a] = sp, lp[b] = sp, lm[a] = sm, lm[b] = -sm;
-    }
-    A Er = A(0), E[3] = {A(0), A(0), A(0)}, B[3] = {A(0), A(0), A(0)}, gF[3] = {A(0), A(0), A(0)};
-    A dwp = A(0), dwm = A(0);
+  for (int q = 0; q < Q; ++q) {
+    dr += f[q];
+    j[0] += A(L::cx(q)) * f[q];
+    j[1] += A(L::cy(q)) * f[q];
+    j[2] += A(L::cz(q)) * f[q];
+  }
+  const A rho = A(1) + dr, inv = A(1) / rho;
+  const A u[3] = {(j[0] + A(0.5) * Fp[0]) * inv, (j[1] + A(0.5) * Fp[1]) * inv, (j[2] + A(0.5) * Fp[2]) * inv};
+  const A usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const A uF = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
+  const A op = A(p.op), om = A(p.om), cp = A(1) - op * A(0.5), cm = A(1) - om * A(0.5);
+  A Er = A(0), E[3] = {A(0), A(0), A(0)}, B[3] = {A(0), A(0), A(0)}, gF[3] = {A(0), A(0), A(0)};
+  A dwp = A(0), dwm = A(0);
+  A lp[Q], lm[Q];
+  lp[0] = ls[0];
+  lm[0] = A(0);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const A c[3] = {A(L::cx(q)), A(L::cy(q)), A(L::cz(q))};
-      const A cu = c[0] * u[0] + c[1] * u[1] + c[2] * u[2];
+  for (int k = 0; k < (Q - 1) / 2; ++k) {
+    const int a = 2 * k + 1, b = a + 1;
+    const A sp = A(0.5) * (ls[a] + ls[b]), sm = A(0.5) * (ls[a] - ls[b]);
+    lp[a] = sp, lp[b] = sp, lm[a] = sm, lm[b] = -sm;
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const A c[3] = {A(L::cx(q)), A(L::cy(q)), A(L::cz(q))};
+    const A cu = c[0] * u[0] + c[1] * u[1] + c[2] * u[2];
+    const A w = A(L::w(q));
+    const A aq = op * lp[q] + om * lm[q];
+    const A e = w * (dr + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * usq));
+    A r = f[q] - e;
+    Er += aq * w * (A(1) + A(3) * cu + A(4.5) * cu * cu - A(1.5) * usq);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) E[d] += aq * w * rho * (A(3) * c[d] + A(9) * cu * c[d] - A(3) * u[d]);
+    if (FORCED) {
       const A cF = c[0] * F[0] + c[1] * F[1] + c[2] * F[2];
-      const A w = A(L::w(q));
-      const A aq = op * lp[q] + om * lm[q];
       const A bq = cp * lp[q] + cm * lm[q];
-      Er += aq * w * (A(1) + A(3) * cu + A(4.5) * cu * cu - A(1.5) * usq);
+      r += A(0.5) * w * (A(3) * (cF - uF) + A(9) * cu * cF);
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        E[d] += aq * w * rho * (A(3) * c[d] + A(9) * cu * c[d] - A(3) * u[d]);
         B[d] += bq * w * (A(-3) * F[d] + A(9) * c[d] * cF);
         gF[d] += bq * w * (A(3) * (c[d] - u[d]) + A(9) * cu * c[d]);
       }
-      dwp -= lp[q] * rr[q];
-      dwm -= lm[q] * rr[q];
     }
-    // moving walls: f^{n+1}_{opp q}(x) gets + 6 w_{opp q} rho (c_{opp q} . u_w), rho = 1 + sum f
-    A wall = A(0);
-    if (fl & F_MOVING) {
+    dwp -= lp[q] * r;
+    dwm -= lm[q] * r;
+  }
+  // moving walls: f^{n+1}_{opp q}(x) gets + 6 w_{opp q} rho (c_{opp q} . u_w), rho = 1 + sum f
+  A wall = A(0);
+  if (fl & F_MOVING) {
+    int x = 0, y = 0, z = 0;
+    cell_xyz(cell, p.nx, p.ny, x, y, z);
+    const Nbr nb(x, y, z, p.nx, p.ny, p.nz);
 #pragma unroll
-      for (int q = 0; q < Q; ++q)
-        if ((mask >> q) & 1u) {
-          const int o = opp(q);
-          const Vec4<A> wu = p.wall_u[nb.at(L::cx(q), L::cy(q), L::cz(q))];
-          wall += ls[q] * A(6) * A(L::w(o)) * (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y + A(L::cz(o)) * wu.z);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const A aq = op * lp[q] + om * lm[q];
-      A v = ls[q] - aq + Er + wall;
-      v += (E[0] + B[0]) * (A(L::cx(q)) - u[0]) * inv + (E[1] + B[1]) * (A(L::cy(q)) - u[1]) * inv +
-           (E[2] + B[2]) * (A(L::cz(q)) - u[2]) * inv;
-      p.lam_out[q * pl + cell] = v;
-    }
-    if (g >= 0) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        p.Fbar[3 * g + d] = double(gF[d]) + p.mu_in[3 * g + d];
-        p.mu_out[3 * g + d] = double((E[d] + B[d]) * A(0.5) * inv);
+    for (int q = 0; q < Q; ++q)
+      if ((mask >> q) & 1u) {
+        const int o = opp(q);
+        const Vec4<A> wu = p.wall_u[nb.at(L::cx(q), L::cy(q), L::cz(q))];
+        wall += ls[q] * A(6) * A(L::w(o)) * (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y + A(L::cz(o)) * wu.z);
       }
+  }
+  const A G[3] = {(E[0] + B[0]) * inv, (E[1] + B[1]) * inv, (E[2] + B[2]) * inv};
+  const A base = Er + wall - (G[0] * u[0] + G[1] * u[1] + G[2] * u[2]);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const A aq = op * lp[q] + om * lm[q];
+    p.lam_out[q * pl + cell] = ls[q] - aq + base + (G[0] * A(L::cx(q)) + G[1] * A(L::cy(q)) + G[2] * A(L::cz(q)));
+  }
+  if (FORCED) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      p.Fbar[3 * g + d] = double(gF[d]) + p.mu_in[3 * g + d];
+      p.mu_out[3 * g + d] = double(G[d] * A(0.5));
     }
-    gsum[0] = double(dwp);
-    gsum[1] = double(dwm);
+  }
+  gsum[0] += double(dwp);
+  gsum[1] += double(dwm);
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(ADJ_BLOCK) adj_collide_kernel(AdjCollide<S> p, int64_t n) {
+  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double gsum[2] = {0.0, 0.0};
+  if (cell < n) {
+    const uint8_t fl = p.flags[cell];
+    if (!(fl & F_SOLID)) {
+      if (fl & F_FORCED) adj_cell<Q, S, true>(p, cell, fl, gsum);
+      else adj_cell<Q, S, false>(p, cell, fl, gsum);
+    }
   }
   adj_block_add<2>(gsum, p.grad);
 }
@@ -231,7 +248,7 @@ struct AdjIbm {
   double* mobbar;  // per marker
   double* xbar;    // per marker x3 (accumulates over steps)
   double* grad;    // [2] += dJ/dOmega_z
-  double Tbar;
+  const double* tbar_step;  // dJ/dtorque of this step (device scalar)
 };
 
 // d/dp of one axis factor of the marker kernel at distance p - i.
@@ -274,6 +291,7 @@ __device__ __forceinline__ void weight_grad(const AdjIbm& b, const double* pos, 
 // torque, then interpolation adjoint (needs dubar = adjoint of du^{k+1}).
 static __global__ void __launch_bounds__(ADJ_BLOCK) adj_ibm_marker_kernel(AdjIbm b, int k) {
   const IbmArgs& a = b.a;
+  const double Tbar = *b.tbar_step;
   const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (m >= a.nm) return;
   const double* pos = a.pos + 3 * m;
@@ -294,8 +312,8 @@ static __global__ void __launch_bounds__(ADJ_BLOCK) adj_ibm_marker_kernel(AdjIbm
     for (int c = 0; c < 3; ++c) ib[c] += w * (b.Fbar[3 * s + c] + b.dubar[3 * s + c] * ir);
   }
   // torque^k = W (r_x imp_y - r_y imp_x)
-  ib[0] += b.Tbar * W * (-r[1]);
-  ib[1] += b.Tbar * W * r[0];
+  ib[0] += Tbar * W * (-r[1]);
+  ib[1] += Tbar * W * r[0];
   const double rel = a.relax;
   double umb[3];
   for (int c = 0; c < 3; ++c) {
@@ -304,12 +322,12 @@ static __global__ void __launch_bounds__(ADJ_BLOCK) adj_ibm_marker_kernel(AdjIbm
     b.tbar[3 * m + c] += rel / mob * ib[c];
   }
   b.mobbar[m] += -(ib[0] * imp[0] + ib[1] * imp[1] + ib[2] * imp[2]) / mob;
-  double xb[3] = {b.Tbar * W * imp[1], -b.Tbar * W * imp[0], 0.0};
+  double xb[3] = {Tbar * W * imp[1], -Tbar * W * imp[0], 0.0};
   const double tq = r[0] * imp[1] - r[1] * imp[0];
   for (int32_t i = k0; i < k1; ++i) {
     const int32_t s = a.st_slot[i];
     const double ir = 1.0 / fmax(a.rho[s], 1.0e-30);
-    double wb = b.Tbar * tq;
+    double wb = Tbar * tq;
     for (int c = 0; c < 3; ++c)
       wb += imp[c] * (b.Fbar[3 * s + c] + b.dubar[3 * s + c] * ir) +
             umb[c] * (a.u_now[3 * s + c] + du[3 * s + c]);

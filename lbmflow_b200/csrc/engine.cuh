@@ -1123,8 +1123,16 @@ struct Engine final : EngineBase {
   }
 
   // Device sequence of one apply_rotating_ibm call (no host sync).
+  // Where the adjoint keeps the IBM intermediates of one step: rho, u_now
+  // (per slot), mobility (per marker), du at the start of each sweep (per
+  // slot) and each sweep's impulse (per marker).
+  struct IbmSave {
+    double *rho, *u, *mob, *du, *imp;
+    size_t ns3, nm;
+  };
+
   void enqueue_ibm(BodyState& B, const lbmb_ibm_config& c, double* s_torque, double* s_ff, int32_t* s_it,
-                   int64_t* counter, bool field_at_call, cudaStream_t s_ = nullptr) {
+                   int64_t* counter, bool field_at_call, cudaStream_t s_ = nullptr, const IbmSave* sv = nullptr) {
     cudaStream_t sx = s_ ? s_ : st;
     IbmArgs a = ibm_args(B, c);
     const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
@@ -1135,9 +1143,22 @@ struct Engine final : EngineBase {
                                                     double(A(cfg.force[2])));
     CK(cudaGetLastError());
     for (int s = 0; s < c.max_iterations; ++s) {
+      if (sv && nslots)
+        CK(cudaMemcpyAsync(sv->du + size_t(s) * sv->ns3 * 3, s_du.p, size_t(nslots) * 3 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, sx));
       ibm_interp_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s);
+      if (sv && B.nm)
+        CK(cudaMemcpyAsync(sv->imp + size_t(s) * sv->nm * 3, B.imp.p, size_t(B.nm) * 3 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, sx));
       ibm_spread_kernel<<<gs, IBM_BLOCK, 0, sx>>>(a);
       ibm_diag_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s, int(gs));
+    }
+    if (sv) {
+      if (nslots) {
+        CK(cudaMemcpyAsync(sv->rho, s_rho.p, size_t(nslots) * sizeof(double), cudaMemcpyDeviceToDevice, sx));
+        CK(cudaMemcpyAsync(sv->u, s_unow.p, size_t(nslots) * 3 * sizeof(double), cudaMemcpyDeviceToDevice, sx));
+      }
+      if (B.nm) CK(cudaMemcpyAsync(sv->mob, B.mob.p, size_t(B.nm) * sizeof(double), cudaMemcpyDeviceToDevice, sx));
     }
     CK(cudaGetLastError());
     ibm_commit_kernel<A><<<gs, IBM_BLOCK, 0, sx>>>(a, fcur.p, s_torque, s_ff, s_it, counter);
@@ -1324,11 +1345,12 @@ struct Engine final : EngineBase {
   // ---- adjoint of the runner loop ------------------------------------------
   // One runner step (clear field -> IBM -> hydro of the forced cells on the
   // side stream, full-grid sweep on the main stream, field refresh), eager.
-  void enqueue_runner_step(BodyState& B, const lbmb_ibm_config& c, double* s_torque, int64_t* counter) {
+  void enqueue_runner_step(BodyState& B, const lbmb_ibm_config& c, double* s_torque, int64_t* counter,
+                           const IbmSave* sv = nullptr) {
     CK(cudaEventRecord(ev_fork, st));
     CK(cudaStreamWaitEvent(st2, ev_fork, 0));
     if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st2));
-    enqueue_ibm(B, c, s_torque, nullptr, nullptr, counter, false, st2);
+    enqueue_ibm(B, c, s_torque, nullptr, nullptr, counter, false, st2, sv);
     field_present = true;
     launch_hydro(parity, st2, false, true);
     launch_hydro(parity, st, true, false);
@@ -1380,18 +1402,42 @@ struct Engine final : EngineBase {
       CK(cudaMemcpyAsync(fprev.p, fcur.p, ns3 * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
       fprev_stale = false;
     }
+    // Graph of one full segment (K steps; K even, so every segment starts
+    // at the same parity and the graph replays unchanged).
+    auto capture = [&](auto&& body) {
+      cudaGraph_t gr;
+      cudaGraphExec_t ex = nullptr;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      body();
+      CK(cudaStreamEndCapture(st, &gr));
+      CK(cudaGraphInstantiate(&ex, gr, 0));
+      CK(cudaGraphDestroy(gr));
+      return ex;
+    };
+    cudaGraphExec_t g_fwd = nullptr;
     CK(cudaEventRecord(ev0, st));
-    for (int64_t nn = 0; nn < N; ++nn) {
-      if (nn % K == 0) {
-        snapshot(ck_f.p + size_t(nn / K) * fsz);
-        if (nslots)
-          CK(cudaMemcpyAsync(ck_fp.p + size_t(nn / K) * ns3, fprev.p, size_t(nslots) * sizeof(Vec4<A>),
-                             cudaMemcpyDeviceToDevice, st));
+    for (int64_t seg = 0; seg < nseg; ++seg) {
+      const int64_t len = std::min<int64_t>(K, N - seg * K);
+      snapshot(ck_f.p + size_t(seg) * fsz);
+      if (nslots)
+        CK(cudaMemcpyAsync(ck_fp.p + size_t(seg) * ns3, fprev.p, size_t(nslots) * sizeof(Vec4<A>),
+                           cudaMemcpyDeviceToDevice, st));
+      if (len == K) {
+        if (!g_fwd) {
+          const int par0 = parity;
+          g_fwd = capture([&] {
+            for (int64_t i = 0; i < K; ++i) enqueue_runner_step(B, c, d_torque.p, d_counter.p);
+          });
+          parity = par0;
+        }
+        CK(cudaGraphLaunch(g_fwd, st));
+      } else {
+        for (int64_t i = 0; i < len; ++i) enqueue_runner_step(B, c, d_torque.p, d_counter.p);
       }
-      enqueue_runner_step(B, c, d_torque.p, d_counter.p);
     }
     CK(cudaEventRecord(ev1, st));
     CK(cudaEventSynchronize(ev1));
+    if (g_fwd) CK(cudaGraphExecDestroy(g_fwd));
     check_device_error();
     float fwd_ms = 0.f;
     CK(cudaEventElapsedTime(&fwd_ms, ev0, ev1));
@@ -1410,16 +1456,44 @@ struct Engine final : EngineBase {
     if (nslots) CK(cudaMemcpyAsync(fin_fp.p, fprev.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
     const int fin_parity = parity;
     // ---- backward pass ----------------------------------------------------
-    DevBuf<S> seg_f;
-    DevBuf<Vec4<A>> seg_F;
-    seg_f.alloc(size_t(K) * fsz);
-    seg_F.alloc(size_t(K) * ns3);
+    // Segments are processed last to first. The recomputation of segment
+    // j-1 (engine streams) runs while the backward steps of segment j run on
+    // two streams of their own; each side owns one of two segment buffers.
+    const size_t nm = size_t(std::max<int64_t>(B.nm, 1));
+    struct SegBuf {
+      DevBuf<S> f;
+      DevBuf<Vec4<A>> F, fp0;
+      DevBuf<double> rho, u, mob, du, imp, tb;
+    };
+    SegBuf sbuf[2];
+    for (SegBuf& b : sbuf) {
+      b.f.alloc(size_t(K) * fsz);
+      b.F.alloc(size_t(K) * ns3);
+      b.fp0.alloc(ns3);
+      b.rho.alloc(size_t(K) * ns3);
+      b.u.alloc(size_t(K) * ns3 * 3);
+      b.mob.alloc(size_t(K) * nm);
+      b.du.alloc(size_t(K) * nsweep * ns3 * 3);
+      b.imp.alloc(size_t(K) * nsweep * nm * 3);
+      b.tb.alloc(size_t(K));
+    }
+    auto save_of = [&](SegBuf& b, int64_t i) {
+      IbmSave sv;
+      sv.rho = b.rho.p + size_t(i) * ns3;
+      sv.u = b.u.p + size_t(i) * ns3 * 3;
+      sv.mob = b.mob.p + size_t(i) * nm;
+      sv.du = b.du.p + size_t(i) * nsweep * ns3 * 3;
+      sv.imp = b.imp.p + size_t(i) * nsweep * nm * 3;
+      sv.ns3 = ns3;
+      sv.nm = nm;
+      return sv;
+    };
     DevBuf<A> lam0, lam1;
     lam0.alloc(fsz);
     lam1.alloc(fsz);
     CK(cudaMemsetAsync(lam0.p, 0, fsz * sizeof(A), st));
     CK(cudaMemsetAsync(lam1.p, 0, fsz * sizeof(A), st));
-    DevBuf<double> mu0, mu1, Fbar, dubar, ubar, rhobar, cksbar, umbar, tbar, mobbar, xbar, grad, imp_k, du_k;
+    DevBuf<double> mu0, mu1, Fbar, dubar, ubar, rhobar, cksbar, umbar, tbar, mobbar, xbar, grad;
     for (DevBuf<double>* b : {&mu0, &mu1, &Fbar, &dubar, &ubar}) {
       b->alloc(3 * ns3);
       CK(cudaMemsetAsync(b->p, 0, 3 * ns3 * sizeof(double), st));
@@ -1428,7 +1502,6 @@ struct Engine final : EngineBase {
       b->alloc(ns3);
       CK(cudaMemsetAsync(b->p, 0, ns3 * sizeof(double), st));
     }
-    const size_t nm = size_t(std::max<int64_t>(B.nm, 1));
     for (DevBuf<double>* b : {&umbar, &tbar, &xbar}) {
       b->alloc(3 * nm);
       CK(cudaMemsetAsync(b->p, 0, 3 * nm * sizeof(double), st));
@@ -1437,53 +1510,56 @@ struct Engine final : EngineBase {
     CK(cudaMemsetAsync(mobbar.p, 0, nm * sizeof(double), st));
     grad.alloc(3);
     CK(cudaMemsetAsync(grad.p, 0, 3 * sizeof(double), st));
-    imp_k.alloc(size_t(nsweep) * nm * 3);
-    du_k.alloc(size_t(nsweep) * ns3 * 3);
     DevBuf<double> dummy_t;
     DevBuf<int64_t> dummy_c;
     dummy_t.alloc(size_t(K) + 1);
     dummy_c.alloc(1);
-    A* lam_next = lam0.p;
-    A* lam_cur = lam1.p;
-    double* mu_next = mu0.p;
-    double* mu_cur = mu1.p;
-    IbmArgs a = ibm_args(B, c);
+    CK(cudaStreamSynchronize(st));
+    cudaStream_t sb = nullptr, sb2 = nullptr;
+    cudaEvent_t e_fork = nullptr, e_join = nullptr, e_rec[2] = {nullptr, nullptr}, e_bwd[2] = {nullptr, nullptr};
+    CK(cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&sb2, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&e_fork, &e_join, &e_rec[0], &e_rec[1], &e_bwd[0], &e_bwd[1]})
+      CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    struct Cleanup {
+      std::vector<cudaStream_t> ss;
+      std::vector<cudaEvent_t> es;
+      std::vector<cudaGraphExec_t> gs;
+      ~Cleanup() {
+        for (auto x : ss) cudaStreamSynchronize(x);
+        for (auto g : gs)
+          if (g) cudaGraphExecDestroy(g);
+        for (auto e : es) cudaEventDestroy(e);
+        for (auto x : ss) cudaStreamDestroy(x);
+      }
+    } cleanup;
+    cleanup.ss = {sb, sb2};
+    cleanup.es = {e_fork, e_join, e_rec[0], e_rec[1], e_bwd[0], e_bwd[1]};
+    const IbmArgs a0 = ibm_args(B, c);
     const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
     const unsigned gm = unsigned(std::max<int64_t>(1, ceil_div(B.nm, IBM_BLOCK)));
     const unsigned gc = unsigned(ceil_div(n, ADJ_BLOCK));
-    CK(cudaEventRecord(ev0, st));
-    for (int64_t seg = nseg - 1; seg >= 0; --seg) {
-      const int64_t s0 = seg * K, s1 = std::min<int64_t>(N, s0 + K);
-      // restore the checkpoint (the logical layout is the parity-0 storage)
-      CK(cudaMemcpyAsync(fp, ck_f.p + size_t(seg) * fsz, fsz * sizeof(S), cudaMemcpyDeviceToDevice, st));
-      if (nslots)
-        CK(cudaMemcpyAsync(fprev.p, ck_fp.p + size_t(seg) * ns3, size_t(nslots) * sizeof(Vec4<A>),
-                           cudaMemcpyDeviceToDevice, st));
-      parity = 0;
-      field_present = true;
-      fprev_stale = false;
+    // recomputation of len steps from the restored checkpoint into b
+    auto recompute = [&](SegBuf& b, int64_t len) {
       CK(cudaMemsetAsync(dummy_c.p, 0, sizeof(int64_t), st));
-      for (int64_t nn = s0; nn < s1; ++nn) {
-        snapshot(seg_f.p + size_t(nn - s0) * fsz);
-        enqueue_runner_step(B, c, dummy_t.p, dummy_c.p);
+      for (int64_t i = 0; i < len; ++i) {
+        snapshot(b.f.p + size_t(i) * fsz);
+        const IbmSave sv = save_of(b, i);
+        enqueue_runner_step(B, c, dummy_t.p, dummy_c.p, &sv);
         if (nslots)
-          CK(cudaMemcpyAsync(seg_F.p + size_t(nn - s0) * ns3, fcur.p, size_t(nslots) * sizeof(Vec4<A>),
+          CK(cudaMemcpyAsync(b.F.p + size_t(i) * ns3, fcur.p, size_t(nslots) * sizeof(Vec4<A>),
                              cudaMemcpyDeviceToDevice, st));
       }
-      for (int64_t nn = s1 - 1; nn >= s0; --nn) {
-        const S* fn = seg_f.p + size_t(nn - s0) * fsz;
-        // IBM intermediates of step nn (the forward kernels on the snapshot)
-        ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, st>>>(a, fn, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz, 0,
-                                                        fcur.p, 0, 0.0, 0.0, 0.0);
-        for (int k = 0; k < nsweep; ++k) {
-          CK(cudaMemcpyAsync(du_k.p + size_t(k) * ns3 * 3, s_du.p, size_t(nslots) * 3 * sizeof(double),
-                             cudaMemcpyDeviceToDevice, st));
-          ibm_interp_kernel<<<gm, IBM_BLOCK, 0, st>>>(a, k);
-          CK(cudaMemcpyAsync(imp_k.p + size_t(k) * nm * 3, B.imp.p, size_t(B.nm) * 3 * sizeof(double),
-                             cudaMemcpyDeviceToDevice, st));
-          ibm_spread_kernel<<<gs, IBM_BLOCK, 0, st>>>(a);
-        }
-        CK(cudaGetLastError());
+    };
+    // backward steps of a segment of len steps held in b (stream sb)
+    auto backward = [&](SegBuf& b, int64_t len) {
+      for (int64_t i = len - 1; i >= 0; --i) {
+        const S* fn = b.f.p + size_t(i) * fsz;
+        const bool even = ((len - 1 - i) & 1) == 0;
+        A* lam_in = even ? lam0.p : lam1.p;
+        A* lam_out = even ? lam1.p : lam0.p;
+        double* mu_in = even ? mu0.p : mu1.p;
+        double* mu_out = even ? mu1.p : mu0.p;
         AdjCollide<S> pc;
         pc.f = fn;
         pc.pl = plane;
@@ -1491,12 +1567,12 @@ struct Engine final : EngineBase {
         pc.nbr = nbr.p;
         pc.wall_u = wall_u.p;
         pc.fslot = fslot.p;
-        pc.F = seg_F.p + size_t(nn - s0) * ns3;
-        pc.Fp = nn > s0 ? seg_F.p + size_t(nn - s0 - 1) * ns3 : ck_fp.p + size_t(seg) * ns3;
-        pc.lam_in = lam_next;
-        pc.lam_out = lam_cur;
-        pc.mu_in = mu_next;
-        pc.mu_out = mu_cur;
+        pc.F = b.F.p + size_t(i) * ns3;
+        pc.Fp = i > 0 ? b.F.p + size_t(i - 1) * ns3 : b.fp0.p;
+        pc.lam_in = lam_in;
+        pc.lam_out = lam_out;
+        pc.mu_in = mu_in;
+        pc.mu_out = mu_out;
         pc.Fbar = Fbar.p;
         pc.grad = grad.p;
         pc.nx = nx;
@@ -1504,40 +1580,116 @@ struct Engine final : EngineBase {
         pc.nz = nz;
         pc.op = omega_p;
         pc.om = omega_m;
-        adj_collide_kernel<Q, S><<<gc, ADJ_BLOCK, 0, st>>>(pc, n);
+        adj_collide_kernel<Q, S><<<gc, ADJ_BLOCK, 0, sb>>>(pc, n);
         CK(cudaGetLastError());
-        AdjIbm b;
-        b.a = a;
-        b.imp_k = imp_k.p;
-        b.du_k = du_k.p;
-        b.nslot = int64_t(ns3);
-        b.slot_cell = slot_cell.p;
-        b.nx = nx;
-        b.ny = ny;
-        b.radius = c.kernel_radius;
-        b.Fbar = Fbar.p;
-        b.dubar = dubar.p;
-        b.ubar = ubar.p;
-        b.rhobar = rhobar.p;
-        b.cksbar = cksbar.p;
-        b.umbar = umbar.p;
-        b.tbar = tbar.p;
-        b.mobbar = mobbar.p;
-        b.xbar = xbar.p;
-        b.grad = grad.p;
-        b.Tbar = nn >= ac.window_begin ? Tbar : 0.0;
+        const IbmSave sv = save_of(b, i);
+        AdjIbm ab;
+        ab.a = a0;
+        ab.a.rho = sv.rho;
+        ab.a.u_now = sv.u;
+        ab.a.mob = sv.mob;
+        ab.imp_k = sv.imp;
+        ab.du_k = sv.du;
+        ab.nslot = int64_t(ns3);
+        ab.slot_cell = slot_cell.p;
+        ab.nx = nx;
+        ab.ny = ny;
+        ab.radius = c.kernel_radius;
+        ab.Fbar = Fbar.p;
+        ab.dubar = dubar.p;
+        ab.ubar = ubar.p;
+        ab.rhobar = rhobar.p;
+        ab.cksbar = cksbar.p;
+        ab.umbar = umbar.p;
+        ab.tbar = tbar.p;
+        ab.mobbar = mobbar.p;
+        ab.xbar = xbar.p;
+        ab.grad = grad.p;
+        ab.tbar_step = b.tb.p + i;
         for (int k = nsweep - 1; k >= 0; --k) {
-          adj_ibm_marker_kernel<<<gm, ADJ_BLOCK, 0, st>>>(b, k);
-          adj_ibm_slot_kernel<<<gs, ADJ_BLOCK, 0, st>>>(b, k);
+          adj_ibm_marker_kernel<<<gm, ADJ_BLOCK, 0, sb>>>(ab, k);
+          adj_ibm_slot_kernel<<<gs, ADJ_BLOCK, 0, sb>>>(ab, k);
         }
-        adj_ibm_mob_slot_kernel<<<gs, ADJ_BLOCK, 0, st>>>(b);
-        adj_ibm_mob_marker_kernel<<<gm, ADJ_BLOCK, 0, st>>>(b);
-        adj_ibm_fbar_kernel<Q, A><<<gs, ADJ_BLOCK, 0, st>>>(b, lam_cur, plane);
+        adj_ibm_mob_slot_kernel<<<gs, ADJ_BLOCK, 0, sb>>>(ab);
+        adj_ibm_mob_marker_kernel<<<gm, ADJ_BLOCK, 0, sb>>>(ab);
+        adj_ibm_fbar_kernel<Q, A><<<gs, ADJ_BLOCK, 0, sb>>>(ab, lam_out, plane);
         CK(cudaGetLastError());
-        std::swap(lam_next, lam_cur);
-        std::swap(mu_next, mu_cur);
       }
+    };
+    auto capture_on = [&](cudaStream_t s0, auto&& body) {
+      cudaGraph_t gr;
+      cudaGraphExec_t ex = nullptr;
+      CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+      body();
+      CK(cudaStreamEndCapture(s0, &gr));
+      CK(cudaGraphInstantiate(&ex, gr, 0));
+      CK(cudaGraphDestroy(gr));
+      return ex;
+    };
+    cudaGraphExec_t g_rec[2] = {nullptr, nullptr}, g_bwd[2] = {nullptr, nullptr};
+    std::vector<double> tbh(static_cast<size_t>(nseg * K), 0.0);
+    for (int64_t t = ac.window_begin; t < N; ++t) tbh[size_t(t)] = Tbar;
+    bool used[2] = {false, false};
+    // stage segment seg into buffer bi on the engine streams
+    auto stage = [&](int64_t seg, int bi) {
+      SegBuf& b = sbuf[bi];
+      const int64_t len = std::min<int64_t>(K, N - seg * K);
+      if (used[bi]) CK(cudaStreamWaitEvent(st, e_bwd[bi], 0));
+      CK(cudaMemcpyAsync(fp, ck_f.p + size_t(seg) * fsz, fsz * sizeof(S), cudaMemcpyDeviceToDevice, st));
+      if (nslots) {
+        CK(cudaMemcpyAsync(fprev.p, ck_fp.p + size_t(seg) * ns3, size_t(nslots) * sizeof(Vec4<A>),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(b.fp0.p, ck_fp.p + size_t(seg) * ns3, size_t(nslots) * sizeof(Vec4<A>),
+                           cudaMemcpyDeviceToDevice, st));
+      }
+      CK(cudaMemcpyAsync(b.tb.p, tbh.data() + size_t(seg * K), size_t(len) * sizeof(double),
+                         cudaMemcpyHostToDevice, st));
+      parity = 0;
+      field_present = true;
+      fprev_stale = false;
+      if (len == K) {
+        if (!g_rec[bi]) {
+          g_rec[bi] = capture_on(st, [&] { recompute(b, K); });
+          cleanup.gs.push_back(g_rec[bi]);
+        }
+        CK(cudaGraphLaunch(g_rec[bi], st));
+        parity = 0;
+      } else {
+        recompute(b, len);
+      }
+      CK(cudaEventRecord(e_rec[bi], st));
+      used[bi] = true;
+    };
+    bool lam_in_is_0 = true;
+    auto run_back = [&](int64_t seg, int bi) {
+      SegBuf& b = sbuf[bi];
+      const int64_t len = std::min<int64_t>(K, N - seg * K);
+      CK(cudaStreamWaitEvent(sb, e_rec[bi], 0));
+      if (!lam_in_is_0) {
+        CK(cudaMemcpyAsync(lam0.p, lam1.p, fsz * sizeof(A), cudaMemcpyDeviceToDevice, sb));
+        CK(cudaMemcpyAsync(mu0.p, mu1.p, 3 * ns3 * sizeof(double), cudaMemcpyDeviceToDevice, sb));
+        lam_in_is_0 = true;
+      }
+      if (len == K) {
+        if (!g_bwd[bi]) {
+          g_bwd[bi] = capture_on(sb, [&] { backward(b, K); });
+          cleanup.gs.push_back(g_bwd[bi]);
+        }
+        CK(cudaGraphLaunch(g_bwd[bi], sb));
+      } else {
+        backward(b, len);
+        if (len & 1) lam_in_is_0 = false;
+      }
+      CK(cudaEventRecord(e_bwd[bi], sb));
+    };
+    CK(cudaEventRecord(ev0, st));
+    stage(nseg - 1, int((nseg - 1) & 1));
+    for (int64_t seg = nseg - 1; seg >= 0; --seg) {
+      if (seg - 1 >= 0) stage(seg - 1, int((seg - 1) & 1));
+      run_back(seg, int(seg & 1));
     }
+    CK(cudaStreamWaitEvent(st, e_bwd[0], 0));
+    CK(cudaStreamWaitEvent(st, e_bwd[1], 0));
     CK(cudaEventRecord(ev1, st));
     CK(cudaEventSynchronize(ev1));
     check_device_error();
