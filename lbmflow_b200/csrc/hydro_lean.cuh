@@ -117,15 +117,24 @@ __device__ __forceinline__ void lean_cell(const HydroParams<float>& p, uint32_t 
   // loads and stores share one set of offsets.
   auto P = [&](int k) { return int32_t(int64_t(k) * pl); };
   auto T = [&](int k) { return int32_t(int64_t(k) * pl + (L::cx(k) + L::cy(k) * nx + L::cz(k) * nxy)); };
+  // Odd step: a warp whose active cells have no solid neighbour (the bulk
+  // of the tank) takes straight neighbour accesses; the others test the
+  // solid-neighbour mask per direction. The vote is warp-uniform.
+  const bool clear = ODD && __all_sync(__activemask(), mk == 0u);
   float f[Q];
+  if (clear) {
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (!ODD) {
-      f[q] = CD::ld(cb + P(q));
-    } else {
-      const int o = opp(q);
-      f[q] = CD::ld(cb + T(o));
-      if ((mk >> o) & 1u) f[q] = CD::ld(cb + P(q));  // neighbour solid: own slot
+    for (int q = 0; q < Q; ++q) f[q] = CD::ld(cb + T(opp(q)));
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (!ODD) {
+        f[q] = CD::ld(cb + P(q));
+      } else {
+        const int o = opp(q);
+        f[q] = CD::ld(cb + T(o));
+        if ((mk >> o) & 1u) f[q] = CD::ld(cb + P(q));  // neighbour solid: own slot
+      }
     }
   }
   const float rho = trt_lean_collide<Q>(f, p);
@@ -140,13 +149,21 @@ __device__ __forceinline__ void lean_cell(const HydroParams<float>& p, uint32_t 
       }
     }
   }
+  // even step: a fresh copy of the base pointer keeps the compiler from
+  // holding the load addresses (the same offsets) live across the collision
+  if constexpr (!ODD) asm volatile("" : "+l"(cb));
+  if (clear) {
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int o = opp(q);
-    if (!ODD || ((mk >> q) & 1u))
-      CD::st(cb + P(o), f[q]);  // even step, or towards a wall: the own slot
-    else
-      CD::st(cb + T(q), f[q]);
+    for (int q = 0; q < Q; ++q) CD::st(cb + T(q), f[q]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int o = opp(q);
+      if (!ODD || ((mk >> q) & 1u))
+        CD::st(cb + P(o), f[q]);  // even step, or towards a wall: the own slot
+      else
+        CD::st(cb + T(q), f[q]);
+    }
   }
 }
 
