@@ -40,6 +40,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum, mean of
+# one even and one odd launch) from an ncu full-set capture of the sweep kernel
+# the autotuner picks for the form, on the tank of the given diameter.
+NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 446.65e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -459,7 +464,9 @@ def run_b200(args, rank, world, local):
                 "path": "C ABI per step: ibm_set_body(host markers) + apply_rotating_ibm(diag to host) + step"},
         "gpu_launches": int(13 * args.steps),
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": NCU_TRAFFIC.get((kname, q, coll, storage, args.tank_T)),
+                     "traffic_unit": "bytes per launch (ncu capture)", "algorithmic_bytes_per_launch": alg_bytes,
                      "peak_kind": peak_kind, "bytes_per_fluid_cell": b_lu(q, storage),
                      "launch_ms": per_launch_ms},
         "qoi": {"Np": np_head, "torque_lu_last": float(torque[-1]), "finite": bool(np.isfinite(torque).all())},
