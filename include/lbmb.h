@@ -65,6 +65,13 @@ typedef struct lbmb_config {
                           * |Pi_neq| / rho)) / 2 applied to the shear rate (no
                           * reference counterpart; stabilises under-resolved
                           * high-Re tanks) */
+  int32_t free_slip_top;  /* nonzero: the solid layer z = nz - 1 is a free-slip
+                           * (specular) wall: a population leaving a cell of
+                           * layer nz - 2 upwards with velocity (cx, cy, 1)
+                           * arrives at cell x + (cx, cy, 0) with (cx, cy, -1)
+                           * when that cell is fluid (half-way bounce-back
+                           * otherwise); no reference counterpart (the
+                           * reference tank has a no-slip lid) */
 } lbmb_config;
 
 /* DirectForcingConfig (crates/lbm-core/src/rotating_ibm.rs:106-130). */

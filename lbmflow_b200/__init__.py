@@ -72,7 +72,7 @@ class _Config(C.Structure):
     _fields_ = [("lattice", C.c_int32), ("collision", C.c_int32), ("storage", C.c_int32),
                 ("dims", C.c_int32 * 3), ("periodic", C.c_int32 * 3), ("device", C.c_int32),
                 ("nu", C.c_double), ("magic", C.c_double), ("omega_shear", C.c_double),
-                ("force", C.c_double * 3), ("smagorinsky_cs", C.c_double)]
+                ("force", C.c_double * 3), ("smagorinsky_cs", C.c_double), ("free_slip_top", C.c_int32)]
 
 
 class _AutotuneResult(C.Structure):
@@ -245,7 +245,7 @@ class Solver:
 
     def __init__(self, dims, lattice=19, collision="trt", storage="f32", nu=1.0 / 6.0, magic=MAGIC_STD,
                  omega_shear=None, periodic=(False, False, False), force=(0.0, 0.0, 0.0), solid=None,
-                 wall_u=None, device=0, smagorinsky_cs=0.0):
+                 wall_u=None, device=0, smagorinsky_cs=0.0, free_slip_top=False):
         L = lib()
         self.dims = tuple(int(d) for d in dims)
         self.n = self.dims[0] * self.dims[1] * self.dims[2]
@@ -255,7 +255,7 @@ class Solver:
         cfg = _Config(int(lattice), COLLISION[collision], STORAGE[storage], (C.c_int32 * 3)(*self.dims),
                       (C.c_int32 * 3)(*[int(bool(p)) for p in periodic]), int(device), float(nu),
                       float(magic), float(omega_shear), (C.c_double * 3)(*[float(f) for f in force]),
-                      float(smagorinsky_cs))
+                      float(smagorinsky_cs), int(bool(free_slip_top)))
         self._solid = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8).ravel()
         if self._solid is not None and self._solid.size != self.n:
             raise ValueError("solid mask size does not match the grid")

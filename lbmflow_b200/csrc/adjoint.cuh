@@ -108,14 +108,24 @@ __device__ __forceinline__ void adj_cell(const AdjCollide<S>& p, int64_t cell, u
   const int64_t pl = p.pl;
   // lambda*: reverse of the push stream with bounce-back
   A ls[Q];
-  if (fl & F_WRAP) {
+  if (fl & (F_WRAP | F_SLIP)) {
     int x = 0, y = 0, z = 0;
     cell_xyz(cell, p.nx, p.ny, x, y, z);
     const Nbr nb(x, y, z, p.nx, p.ny, p.nz);
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
-      ls[q] = ((mask >> q) & 1u) ? p.lam_in[opp(q) * pl + cell]
-                                 : p.lam_in[q * pl + nb.at(L::cx(q), L::cy(q), L::cz(q))];
+    for (int q = 0; q < Q; ++q) {
+      if ((mask >> q) & 1u) {
+        // free-slip top: the post-collision population went to the mirrored
+        // direction of the fluid partner x + (cx, cy, 0)
+        const int d = planar<Q>(q);
+        if ((mask & NBR_SLIP) && L::cz(q) == 1 && d > 0 && !((mask >> d) & 1u))
+          ls[q] = p.lam_in[mirror_z<Q>(q) * pl + nb.at(L::cx(q), L::cy(q), 0)];
+        else
+          ls[q] = p.lam_in[opp(q) * pl + cell];
+      } else {
+        ls[q] = p.lam_in[q * pl + nb.at(L::cx(q), L::cy(q), L::cz(q))];
+      }
+    }
   } else {
     const int64_t nxy = int64_t(p.nx) * p.ny;
 #pragma unroll
@@ -191,7 +201,8 @@ __device__ __forceinline__ void adj_cell(const AdjCollide<S>& p, int64_t cell, u
     const Nbr nb(x, y, z, p.nx, p.ny, p.nz);
 #pragma unroll
     for (int q = 0; q < Q; ++q)
-      if ((mask >> q) & 1u) {
+      if (((mask >> q) & 1u) &&
+          !((mask & NBR_SLIP) && L::cz(q) == 1 && planar<Q>(q) > 0 && !((mask >> planar<Q>(q)) & 1u))) {
         const int o = opp(q);
         const Vec4<A> wu = p.wall_u[nb.at(L::cx(q), L::cy(q), L::cz(q))];
         wall += ls[q] * A(6) * A(L::w(o)) * (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y + A(L::cz(o)) * wu.z);

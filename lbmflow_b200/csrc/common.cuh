@@ -16,7 +16,14 @@ enum : uint8_t {
   F_MOVING = 4,    // ... and >= 1 of them has a nonzero wall velocity
   F_FORCED = 8,    // fluid cell inside an IBM stencil: read force slots
   F_WRAP = 16,     // fluid cell on a periodic face: neighbours wrap around
+  F_SLIP = 32,     // fluid cell under a free-slip (specular) top wall
 };
+
+// Bit of the per-cell solid-neighbour mask (bits 0..Q-1 are directions)
+// marking a cell under a free-slip top wall: a link with c_z = +1 into the
+// wall reflects specularly, to direction (cx, cy, -1) of the cell
+// x + (cx, cy, 0) when that cell is fluid, and bounces back otherwise.
+constexpr uint32_t NBR_SLIP = 1u << 31;
 
 // Storage codecs: populations are stored as S and computed in A.
 template <class S>

@@ -308,6 +308,10 @@ struct Engine final : EngineBase {
           uint8_t fl = 0;
           if (m) fl |= F_BOUNDARY;
           if (moving) fl |= F_MOVING;
+          if (cfg.free_slip_top && z == nz - 2) {
+            fl |= F_SLIP | F_BOUNDARY;
+            m |= NBR_SLIP;
+          }
           if ((cfg.periodic[0] && (x == 0 || x == nx - 1)) || (cfg.periodic[1] && (y == 0 || y == ny - 1)) ||
               (cfg.periodic[2] && (z == 0 || z == nz - 1)))
             fl |= F_WRAP;

@@ -322,10 +322,17 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
       f[q] = CD::ld(fb + (q * pl + cell));
     } else {
       const int o = opp(q);
-      if (GENERIC && ((mask >> o) & 1u))
-        f[q] = CD::ld(fb + (q * pl + cell));
-      else
+      if (GENERIC && ((mask >> o) & 1u)) {
+        // source solid: bounce-back (own slot q), or under a free-slip top
+        // the mirrored population of the partner x - (cx, cy, 0)
+        const int d = planar<Q>(o);  // x - (cx, cy, 0) = x + (-cx, -cy, 0)
+        if ((mask & NBR_SLIP) && L::cz(q) == -1 && d > 0 && !((mask >> d) & 1u))
+          f[q] = CD::ld(fb + (opp(mirror_z<Q>(q)) * pl + nidx(-L::cx(q), -L::cy(q), 0)));
+        else
+          f[q] = CD::ld(fb + (q * pl + cell));
+      } else {
         f[q] = CD::ld(fb + (o * pl + nidx(-L::cx(q), -L::cy(q), -L::cz(q))));
+      }
     }
   }
   // Moments (kernels.rs:627-668): rho = 1 + sum f, m = sum c f.
@@ -375,12 +382,17 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
     A v = f[q];
     const int o = opp(q);
     const bool wall = GENERIC && ((mask >> q) & 1u);
-    if (GENERIC && wall && (fl & F_MOVING)) {
+    // free-slip top: specular to the fluid partner x + (cx, cy, 0)
+    const int d = planar<Q>(q);
+    const bool slip = GENERIC && wall && (mask & NBR_SLIP) && L::cz(q) == 1 && d > 0 && !((mask >> d) & 1u);
+    if (GENERIC && wall && !slip && (fl & F_MOVING)) {
       const Vec4<A> wu = p.wall_u[nidx(L::cx(q), L::cy(q), L::cz(q))];
       const A cu = (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y) + A(L::cz(o)) * wu.z;
       v = v + ((A(6) * A(L::w(o))) * rho) * cu;
     }
-    if (!ODD || wall)
+    if (ODD && slip)
+      CD::st(fb + (mirror_z<Q>(q) * pl + nidx(L::cx(q), L::cy(q), 0)), v);
+    else if (!ODD || wall)
       CD::st(fb + (o * pl + cell), v);
     else
       CD::st(fb + (q * pl + nidx(L::cx(q), L::cy(q), L::cz(q))), v);

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::
   };
   // Cells on a periodic face take the out-of-line generic path; all other
   // active cells go through the pipeline.
-  auto piped = [&](uint8_t fl) { return !(fl & (F_SOLID | F_FORCED | F_WRAP)); };
+  auto piped = [&](uint8_t fl) { return !(fl & (F_SOLID | F_FORCED | F_WRAP | F_SLIP)); };
   // Issue the copies of this thread's cell in tile t into ring stage s.
   auto issue = [&](int t, int s) {
     const int64_t cell = int64_t(t) * ASYNC_TILE + j;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::
     if (cell >= ncells) continue;
     const uint8_t fl = p.flags[cell];
     if (fl & (F_SOLID | F_FORCED)) continue;
-    if (fl & F_WRAP) {
+    if (fl & (F_WRAP | F_SLIP)) {
       const int z = int(cell / nxy);
       const int64_t r = cell - int64_t(z) * nxy;
       const int y = int(r / nx);

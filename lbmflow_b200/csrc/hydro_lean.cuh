@@ -100,7 +100,7 @@ __device__ __forceinline__ void lean_cell(const HydroParams<float>& p, uint32_t 
   const uint32_t fl = p.flags[c];
   if (fl & (F_SOLID | F_FORCED)) return;
   const int nx = p.nx, nxy = p.nxy;
-  if (fl & F_WRAP) {
+  if (fl & (F_WRAP | F_SLIP)) {
     const int z = int(c / uint32_t(nxy));
     const int r = int(c - uint32_t(z) * uint32_t(nxy));
     const int y = r / nx;

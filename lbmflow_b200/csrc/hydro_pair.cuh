@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) hydro_pair_kernel(HydroParams<f
   const bool act0 = !(fl0 & (F_SOLID | F_FORCED)), act1 = !(fl1 & (F_SOLID | F_FORCED));
   if (!(act0 || act1)) return;
   const int nx = p.nx, nxy = p.nxy;
-  if ((fl0 | fl1) & F_WRAP) {
+  if ((fl0 | fl1) & (F_WRAP | F_SLIP)) {
     const int z = int(c / uint32_t(nxy));
     const int r = int(c - uint32_t(z) * uint32_t(nxy));
     const int y = r / nx, x = r - y * nx;

@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3)
     const uint32_t fl0 = fl2 & 0xffu, fl1 = fl2 >> 8;
     const bool act0 = !(fl0 & (F_SOLID | F_FORCED)), act1 = !(fl1 & (F_SOLID | F_FORCED));
     if (!(act0 || act1)) continue;
-    if ((fl0 | fl1) & F_WRAP) {
+    if ((fl0 | fl1) & (F_WRAP | F_SLIP)) {
       const int z = int(c / uint32_t(nxy));
       const int r = int(c - uint32_t(z) * uint32_t(nxy));
       const int y = r / nx, x = r - y * nx;

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
     if (cell < ncells) {
       const uint8_t fl = p.flags[cell];
       if (!(fl & (F_SOLID | F_FORCED))) {
-        if (fl & F_WRAP) {
+        if (fl & (F_WRAP | F_SLIP)) {
           const int z = int(cell / nxy);
           const int64_t r = cell - int64_t(z) * nxy;
           const int y = int(r / nx);

@@ -91,10 +91,15 @@ __device__ __forceinline__ void load_post_stream(const S* fb, int64_t pl, int64_
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const int o = opp(q);
-      if ((mask >> o) & 1u)
-        f[q] = Codec<S>::ld(fb + q * pl + cell);
-      else
+      if ((mask >> o) & 1u) {
+        const int d = planar<Q>(o);
+        if ((mask & NBR_SLIP) && L::cz(q) == -1 && d > 0 && !((mask >> d) & 1u))
+          f[q] = Codec<S>::ld(fb + opp(mirror_z<Q>(q)) * pl + nb.at(-L::cx(q), -L::cy(q), 0));
+        else
+          f[q] = Codec<S>::ld(fb + q * pl + cell);
+      } else {
         f[q] = Codec<S>::ld(fb + o * pl + nb.at(-L::cx(q), -L::cy(q), -L::cz(q)));
+      }
     }
   }
 }

@@ -68,4 +68,22 @@ struct Lat<7> {
 
 __host__ __device__ constexpr int opp(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
 
+// Index of the direction with velocity (cx, cy, cz) (-1 if absent).
+template <int Q>
+__host__ __device__ constexpr int find_dir(int cx, int cy, int cz) {
+  for (int q = 0; q < Q; ++q)
+    if (Lat<Q>::cx(q) == cx && Lat<Q>::cy(q) == cy && Lat<Q>::cz(q) == cz) return q;
+  return -1;
+}
+// Mirror of direction q in z: (cx, cy, -cz).
+template <int Q>
+__host__ __device__ constexpr int mirror_z(int q) {
+  return find_dir<Q>(Lat<Q>::cx(q), Lat<Q>::cy(q), -Lat<Q>::cz(q));
+}
+// Projection of direction q on the xy plane: (cx, cy, 0) (0 = rest).
+template <int Q>
+__host__ __device__ constexpr int planar(int q) {
+  return find_dir<Q>(Lat<Q>::cx(q), Lat<Q>::cy(q), 0);
+}
+
 }  // namespace lbmb

@@ -29,6 +29,7 @@ static void validate(const lbmb_config& c, const uint8_t* solid, const double* w
     if (!std::isfinite(c.force[a])) invalid("non-finite parameter: force");
   if (!(std::isfinite(c.smagorinsky_cs) && c.smagorinsky_cs >= 0.0))
     invalid("Smagorinsky constant must be finite and >= 0");
+  if (c.free_slip_top && c.periodic[2]) invalid("a free-slip top needs a non-periodic z axis");
   for (int a = 0; a < 3; ++a)
     if (c.dims[a] < 3) invalid("domain too small: every axis needs >= 3 cells");
   const int64_t n = int64_t(c.dims[0]) * c.dims[1] * c.dims[2];

@@ -139,6 +139,11 @@ struct StepParams {  // params.rs:302-320 (subset on the hot path)
   // subgrid model of the device library that is restated here so the
   // device path stays checkable with it switched on.
   double smagorinsky_cs = 0.0;
+  // Free-slip (specular) top wall: the solid layer z = nz - 1 reflects a
+  // population (cx, cy, +1) leaving cell x into (cx, cy, -1) at x + (cx,
+  // cy, 0) when that cell is fluid (bounce-back otherwise). Not a reference
+  // feature; restated here so the device path stays checkable with it on.
+  bool free_slip_top = false;
 };
 
 template <class L, class T>
@@ -804,6 +809,27 @@ class Solver {
             }
             if (skip) continue;
             size_t si = idx(s[0], s[1], s[2]);
+            if (solid[si] && params.free_slip_top && L::C[q][2] == -1 && zz + 1 == dims[2] - 1) {
+              // pull form of the specular rule: the population arriving with
+              // (cx, cy, -1) left the partner x - (cx, cy, 0) with (cx, cy, +1)
+              long px = x - L::C[q][0], py = y - L::C[q][1];
+              bool in = true;
+              if (px < 0 || px >= dims[0]) {
+                if (periodic[0]) px = (px + dims[0]) % dims[0];
+                else in = false;
+              }
+              if (py < 0 || py >= dims[1]) {
+                if (periodic[1]) py = (py + dims[1]) % dims[1];
+                else in = false;
+              }
+              if (in && !solid[idx(px, py, zz)]) {
+                int m = 0;
+                for (int k = 0; k < L::Q; ++k)
+                  if (L::C[k][0] == L::C[q][0] && L::C[k][1] == L::C[q][1] && L::C[k][2] == 1) m = k;
+                ftmp[q * n + i] = f[size_t(m) * n + idx(px, py, zz)];
+                continue;
+              }
+            }
             if (solid[si]) {
               T fout = f[tb.opp[q] * n + i];
               const T* wu = &wall_u[3 * si];

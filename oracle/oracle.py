@@ -45,6 +45,7 @@ def lib():
         L.lbmo_destroy.argtypes = [C.c_void_p]
         L.lbmo_step.argtypes = [C.c_void_p, C.c_int]
         L.lbmo_set_smagorinsky.argtypes = [C.c_void_p, C.c_double]
+        L.lbmo_set_free_slip_top.argtypes = [C.c_void_p, C.c_int]
         for name in ("lbmo_stage_in", "lbmo_stage_out", "lbmo_get_force_field"):
             getattr(L, name).argtypes = [C.c_void_p, _dp]
         L.lbmo_init_with.argtypes = [C.c_void_p, _dp, _dp]
@@ -111,7 +112,7 @@ class OracleSolver:
 
     def __init__(self, dims, q=19, real_bits=64, collision="trt", nu=1.0 / 6.0, magic=MAGIC_STD,
                  omega_shear=0.0, periodic=(False, False, False), force=(0.0, 0.0, 0.0),
-                 solid=None, wall_u=None, smagorinsky_cs=0.0):
+                 solid=None, wall_u=None, smagorinsky_cs=0.0, free_slip_top=False):
         L = lib()
         self.dims = tuple(int(d) for d in dims)
         self.n = self.dims[0] * self.dims[1] * self.dims[2]
@@ -130,6 +131,8 @@ class OracleSolver:
             raise ValueError(err.value.decode())
         if smagorinsky_cs:
             L.lbmo_set_smagorinsky(self.h, float(smagorinsky_cs))
+        if free_slip_top:
+            L.lbmo_set_free_slip_top(self.h, 1)
 
     def __del__(self):
         if getattr(self, "h", None):

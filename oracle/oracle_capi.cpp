@@ -27,6 +27,7 @@ struct AnySolver {
   virtual const uint8_t* solid() const = 0;
   virtual int q() const = 0;
   virtual void set_smagorinsky(double cs) = 0;
+  virtual void set_free_slip_top(bool on) = 0;
 };
 
 template <class L, class T>
@@ -36,6 +37,7 @@ struct Impl final : AnySolver {
       : s(d, p, sp, so, wu) {}
   void step(int n) override { s.run(n); }
   void set_smagorinsky(double cs) override { s.params.smagorinsky_cs = cs; }
+  void set_free_slip_top(bool on) override { s.params.free_slip_top = on; }
   void stage_in(const double* f) override {
     for (size_t i = 0; i < s.f.size(); ++i) s.f[i] = T(f[i]);
     s.update_moments();
@@ -137,6 +139,8 @@ void* lbmo_create(int q, int real_bits, const int* dims, const int* periodic, in
 void lbmo_destroy(void* h) { delete static_cast<AnySolver*>(h); }
 // Switch the optional Smagorinsky subgrid model on (cs > 0) or off (0).
 void lbmo_set_smagorinsky(void* h, double cs) { static_cast<AnySolver*>(h)->set_smagorinsky(cs); }
+// Free-slip (specular) top wall on (nonzero) or off.
+void lbmo_set_free_slip_top(void* h, int on) { static_cast<AnySolver*>(h)->set_free_slip_top(on != 0); }
 void lbmo_step(void* h, int n) { static_cast<AnySolver*>(h)->step(n); }
 void lbmo_stage_in(void* h, const double* f) { static_cast<AnySolver*>(h)->stage_in(f); }
 void lbmo_stage_out(void* h, double* f) { static_cast<AnySolver*>(h)->stage_out(f); }

@@ -56,14 +56,14 @@ class Pair:
     """GPU solver + oracle in the same precision (+ an f64 oracle for f32)."""
 
     def __init__(self, dims, q, prec, collision="trt", nu=0.05, periodic=(False,) * 3, force=(0, 0, 0),
-                 solid=None, wall_u=None, omega_shear=None, smagorinsky_cs=0.0, sweep=None):
+                 solid=None, wall_u=None, omega_shear=None, smagorinsky_cs=0.0, sweep=None, free_slip_top=False):
         import lbmflow_b200 as lb
         from oracle import oracle as o
         if omega_shear is None:
             omega_shear = 1.0 / (3.0 * nu + 0.5)
         self.prec = prec
         kw = dict(collision=collision, nu=nu, periodic=periodic, force=force, solid=solid, wall_u=wall_u,
-                  omega_shear=omega_shear, smagorinsky_cs=smagorinsky_cs)
+                  omega_shear=omega_shear, smagorinsky_cs=smagorinsky_cs, free_slip_top=free_slip_top)
         self.g = lb.Solver(dims, lattice=q, storage=prec, **kw)
         if sweep is not None:
             self.g.set_sweep_kernel(sweep)

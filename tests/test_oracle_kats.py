@@ -351,3 +351,26 @@ def test_smagorinsky_model_in_oracle(oracle):
     assert np.abs(s1.stage_out() - s0.stage_out()).max() < 1e-14
     assert e2 < 0.999 * e0
     assert abs(s2.total_mass() - s0.total_mass()) < 1e-9
+
+
+def test_free_slip_top_half_channel(oracle):
+    # Force-driven flow over a no-slip bottom under a free-slip (specular) top:
+    # mass is conserved, the profile rises monotonically to the top and the
+    # shear at the top is a small fraction of the shear at the bottom (a
+    # half Poiseuille profile), while the no-slip lid gives a symmetric one.
+    dims = (4, 4, 14)
+    solid, wu = oracle.wall_rims(dims, [False, False, False, False, True, True], np.zeros(18))
+
+    def run(slip):
+        s = oracle.OracleSolver(dims, q=19, real_bits=64, nu=0.1, periodic=(True, True, False),
+                                force=(1e-6, 0.0, 0.0), solid=solid, wall_u=wu, free_slip_top=slip)
+        m0 = s.total_mass()
+        s.step(3000)
+        assert abs(s.total_mass() - m0) < 1e-10
+        return s.moments()[1].reshape(14, 4, 4)[1:13, 1, 1]
+
+    u_slip, u_lid = run(True), run(False)
+    assert np.all(np.diff(u_slip) > 0)
+    assert (u_slip[-1] - u_slip[-2]) < 0.15 * (u_slip[1] - u_slip[0])
+    assert np.allclose(u_lid, u_lid[::-1], rtol=1e-6)
+    assert u_slip[-1] > 3.0 * u_lid.max()
