@@ -1,7 +1,8 @@
 """Benchmark of the LBMFlow stirred-tank time step on B200.
 
 Workload (the single-GPU tank configuration): cylindrical tank T = 128
-cells on a 128 x 128 x 160 grid, flat bottom, four wall baffles of width
+cells on a 128 x 128 x 160 grid, flat bottom, free-slip (specular) liquid surface on top (``--lid`` for the
+reference's no-slip lid), four wall baffles of width
 T/10 and thickness 2.6 cells, a six-blade flat-blade disc turbine of
 diameter T/3 at clearance T/3 sampled by ~6k direct-forcing IBM markers at
 0.7-cell spacing, tip speed 0.05, nu for impeller Re = 2000, D3Q27
@@ -145,7 +146,7 @@ def cpu_tank_sample(dims, solid, body, nu, q=27, collision="cm", bits=32, steps=
     from oracle import oracle as o
     os_ = 1.0 / (3.0 * nu + 0.5)
     c = o.OracleSolver(dims, q=q, real_bits=bits, collision=collision, nu=nu, omega_shear=os_, solid=solid,
-                       smagorinsky_cs=cs)
+                       smagorinsky_cs=cs, free_slip_top=FREE_SLIP_TOP)
     c.run_tank(body.positions, body.weights, body.center, body.omega, warmup)
     t0 = time.perf_counter()
     c.run_tank(body.positions, body.weights, body.center, body.omega, steps)
@@ -196,33 +197,97 @@ def power_number(torque_lu, omega, D):
     return omega * tq / (n_rev ** 3 * D ** 5)
 
 
+FREE_SLIP_TOP = True
+
+
 def make_solver(lb, dims, solid, nu, q, coll, storage, cs, local):
     os_ = 1.0 / (3.0 * nu + 0.5)
     return lb.Solver(dims, lattice=q, collision=coll, storage=storage, nu=nu, omega_shear=os_, solid=solid,
-                     device=local, smagorinsky_cs=cs)
+                     device=local, smagorinsky_cs=cs, free_slip_top=FREE_SLIP_TOP)
 
 
 def qoi_study(lb, args, local, dims, solid, body, nu, D, headline_np):
-    """Np of the same runner schedule (warm-up + timed steps) in every storage
-    precision; errors against the f64 path, which the parity tests pin to the
-    C++ oracle at 1e-11."""
+    """Power number of the headline schedule (warm-up + timed steps) in every
+    storage precision, and the velocity L2 at steps 500 and 2000, each
+    against the f64 path (which the parity tests pin to the C++ oracle)."""
     out = {}
     omega = float(body.omega[2])
+    fluid = solid == 0
     for q, coll, label in ((27, "cm", "d3q27_cm"), (19, "trt", "d3q19_trt")):
-        nps = {}
+        res = {}
         for st in ("f64", "f32", "f16", "bf16"):
-            if q == 27 and st == "f32" and headline_np is not None:
-                nps[st] = headline_np
-                continue
             g = make_solver(lb, dims, solid, nu, q, coll, st, args.les_cs, local)
             g.autotune_sweep(6)
             g.run_impeller(body, max(args.warmup, 3))
-            r = g.run_impeller(body, args.steps)
-            nps[st] = power_number(r["torque_lu"], omega, D)
+            us, tq, done = {}, [], 0
+            for mark in (500, 2000, args.steps):
+                if mark > done and mark <= args.steps:
+                    tq.append(g.run_impeller(body, mark - done)["torque_lu"])
+                    done = mark
+                    if mark in (500, 2000):
+                        us[mark] = np.stack(g.read_moments()[1:4])[:, fluid]
+            tq = np.concatenate(tq)
+            res[st] = {"Np": power_number(tq, omega, D) if np.isfinite(tq).all() else None, "u": us}
             g.close()
-        ref = nps["f64"]
-        out[label] = {"Np": nps, "Np_rel_err_vs_f64": {k: abs(v - ref) / abs(ref) for k, v in nps.items()
-                                                       if k != "f64"}}
+        ref = res["f64"]
+        errs = {}
+        for st in ("f32", "f16", "bf16"):
+            r = res[st]
+            e = {"Np": abs(r["Np"] - ref["Np"]) / abs(ref["Np"]) if r["Np"] and ref["Np"] else None}
+            for mark in r["u"]:
+                e[f"velocity_L2_at_{mark}"] = float(np.linalg.norm(r["u"][mark] - ref["u"][mark]) /
+                                                    np.linalg.norm(ref["u"][mark]))
+            errs[st] = e
+        out[label] = {"Np": {k_: v["Np"] for k_, v in res.items()}, "rel_err_vs_f64": errs}
+    return out
+
+
+def mixing_study(lb, args, local):
+    """95% mixing time of a D3Q7 passive-scalar pulse (Gaussian, sigma 4
+    cells, centred on the axis just under the liquid surface) in the
+    T = mix_T tank with the D3Q27 central-moment form of the precision
+    variant, per storage precision, against the f64 path. D = mix_D
+    in lattice units: the reference's BGK advection-diffusion step needs
+    grid Peclet u_tip / D of order 10 or less to stay bounded at this tip
+    speed, so the pulse diffuses faster than in the nominal D = 1e-3 case.
+    Runs until CV <= 0.01 CV0 or mix_steps."""
+    from lbmflow_b200 import sweep
+    c = sweep.TankCase(args.mix_T, 0.05, 2000.0)
+    geo = sweep.tank_geometry(args.mix_T)
+    dims, solid = c.dims, geo["solid"]
+    body = lb.RotatingBody(geo["center"], [0.0, 0.0, c.omega], geo["marker_pos"], geo["marker_w"])
+    c0 = lb.gaussian_pulse(dims, solid, ((dims[0] - 1) / 2.0, (dims[1] - 1) / 2.0, dims[2] - 2.0), 4.0)
+    probe, chunk = 200, 5000
+    out = {"grid": list(dims), "D": args.mix_D, "sigma_cells": 4.0, "probe_every": probe,
+           "revolution_steps": 2 * math.pi / c.omega}
+    for q, coll, label in ((27, "cm", "d3q27_cm"),):
+        res = {}
+        for st in ("f64", "f32", "f16", "bf16"):
+            g = make_solver(lb, dims, solid, c.nu, q, coll, st, args.les_cs, local)
+            k = g.enable_scalar_distribution(args.mix_D, q=7)
+            g.set_scalar_concentration(k, c0)
+            cvs, done, mix = [], 0, None
+            while done < args.mix_steps:
+                r = g.run_impeller(body, chunk, scalar=k, probe_every=probe)
+                cvs.append(r["cv"])
+                done += chunk
+                cv = np.concatenate(cvs)
+                mix = lb.mixing_time_from_cv(np.arange(1, cv.size + 1, dtype=np.float64), cv)
+                if mix is None or mix["t99"] is not None or not np.isfinite(cv[np.isfinite(cv)][-1]):
+                    break
+            res[st] = mix
+            g.close()
+        ref = res["f64"]
+        errs = {}
+        for st in ("f32", "f16", "bf16"):
+            e = {}
+            for key in ("t95", "t99"):
+                a, b = (res[st] or {}).get(key), (ref or {}).get(key)
+                e[key] = abs(a - b) / b if a and b else None
+            errs[st] = e
+        out[label] = {"t95_steps": {k_: (v or {}).get("t95") for k_, v in res.items()},
+                      "t99_steps": {k_: (v or {}).get("t99") for k_, v in res.items()},
+                      "rel_err_vs_f64": errs}
     return out
 
 
@@ -438,6 +503,8 @@ def run_b200(args, rank, world, local):
         extra["adjoint"] = adjoint_study(args, local)
     if args.variants and world == 1:
         extra["qoi_precision"] = qoi_study(lb, args, local, dims, solid, body, nu, D, np_head)
+        if args.mix_steps > 0:
+            extra["mixing_precision"] = mixing_study(lb, args, local)
         extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
     kname = {"lean": "hydro_lean_kernel", "pair": "hydro_pair_kernel", "tile": "hydro_tile_kernel",
              "async": "hydro_async_kernel", "direct": "hydro_aa_kernel", "bulk": "hydro_tma_kernel"}[tune["kind"]]
@@ -454,7 +521,8 @@ def run_b200(args, rank, world, local):
                    "re": 2000, "smagorinsky_cs": args.les_cs,
                    "les_note": "library option; without it the reference operators diverge on this "
                                "under-resolved Re=2000 tank (D3Q27 CM at step ~2390, D3Q19 TRT at ~186)",
-                   "ibm": "3 sweeps, tol 1e-2, radius 1", "top": "solid lid (reference)",
+                   "ibm": "3 sweeps, tol 1e-2, radius 1",
+                   "top": "free-slip (specular) liquid surface" if FREE_SLIP_TOP else "solid lid (reference)",
                    "sweep_kernel": tune["kind"], "autotune": {k: tune[k] for k in
                                                               ("even_blocks_per_sm", "odd_blocks_per_sm",
                                                                "best_ms_per_step", "default_ms_per_step")},
@@ -495,7 +563,8 @@ def run_reference(args, rank, world):
             "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded tank geometry, quiescent start)",
             "config": {"workload": f"tank{dims[0]}x{dims[1]}x{dims[2]}_d3q{q}_{coll}_ibm{body.weights.size}",
-                       "grid": list(dims), "smagorinsky_cs": args.les_cs},
+                       "grid": list(dims), "smagorinsky_cs": args.les_cs,
+                       "top": "free-slip (specular) liquid surface" if FREE_SLIP_TOP else "solid lid (reference)"},
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                              "sample": f"{steps} runner steps of the full tank on the host cores (C++ "
                                        f"restatement of the reference CpuScalar path, OpenMP; the Rust "
@@ -526,9 +595,15 @@ def main():
     ap.add_argument("--adj-T", type=int, default=96)
     ap.add_argument("--adj-re", type=float, default=100.0)
     ap.add_argument("--adj-dirs", type=int, default=16)
+    ap.add_argument("--mix-T", type=int, default=64, help="tank diameter of the mixing-time study")
+    ap.add_argument("--mix-D", type=float, default=1e-2, help="scalar diffusivity of the mixing study (lattice)")
+    ap.add_argument("--mix-steps", type=int, default=60000, help="step cap of the mixing study (0: skip)")
+    ap.add_argument("--lid", action="store_true", help="no-slip lid (the reference's tank) instead of a free-slip top")
     ap.add_argument("--sweep-seq-steps", type=int, default=200,
                     help="steps per case of the sequential-loop sample (0: skip)")
     args = ap.parse_args()
+    global FREE_SLIP_TOP
+    FREE_SLIP_TOP = not args.lid
     rank, world, local = dist_init(args.gpus)
     if args.impl == "reference":
         res = run_reference(args, rank, world)

@@ -476,6 +476,35 @@ class Batch:
         self.close()
 
 
+def mixing_time_from_cv(times, cv):
+    """Mixing times from a CV series (crates/lbm-core/src/qoi.rs:534-556):
+    CV0 = the first finite positive value; t95 / t99 = the first time with
+    CV <= 0.05 / 0.01 CV0 (None when never reached). Returns None when no
+    finite positive CV exists."""
+    times = np.asarray(times, dtype=np.float64)
+    cv = np.asarray(cv, dtype=np.float64)
+    ok = np.isfinite(cv) & (cv > 0.0)
+    if not ok.any():
+        return None
+    cv0 = float(cv[np.argmax(ok)])
+    fin = np.isfinite(cv)
+    hit95 = fin & (cv <= 0.05 * cv0)
+    hit99 = fin & (cv <= 0.01 * cv0)
+    return {"cv0": cv0, "t95": float(times[np.argmax(hit95)]) if hit95.any() else None,
+            "t99": float(times[np.argmax(hit99)]) if hit99.any() else None}
+
+
+def gaussian_pulse(dims, solid, center, sigma):
+    """Concentration exp(-r^2 / (2 sigma^2)) around `center` (cell
+    coordinates) on the fluid cells, zero on solids."""
+    nx, ny, nz = dims
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    r2 = (x - center[0]) ** 2 + (y - center[1]) ** 2 + (z - center[2]) ** 2
+    c = np.exp(-r2.ravel() / (2.0 * sigma * sigma))
+    c[np.asarray(solid).ravel() != 0] = 0.0
+    return c
+
+
 def build_wall_rims(dims, is_wall, wall_u):
     dims = [int(d) for d in dims]
     n = dims[0] * dims[1] * dims[2]

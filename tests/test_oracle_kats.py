@@ -374,3 +374,18 @@ def test_free_slip_top_half_channel(oracle):
     assert (u_slip[-1] - u_slip[-2]) < 0.15 * (u_slip[1] - u_slip[0])
     assert np.allclose(u_lid, u_lid[::-1], rtol=1e-6)
     assert u_slip[-1] > 3.0 * u_lid.max()
+
+
+def test_library_mixing_time_matches_oracle(oracle):
+    # host-side QOI of the library (qoi.rs:534-556) against the oracle's
+    import lbmflow_b200 as lb
+    rng = np.random.default_rng(11)
+    for _ in range(20):
+        n = 30
+        t = np.cumsum(rng.uniform(0.5, 2.0, n))
+        cv = np.exp(-t / rng.uniform(2, 20)) * rng.uniform(0.5, 2.0)
+        cv[rng.integers(0, n, 3)] = np.nan
+        a = lb.mixing_time_from_cv(t, cv)
+        b = oracle.mixing_time_from_cv(list(zip(t, cv)))
+        assert a == b
+    assert lb.mixing_time_from_cv([0.0, 1.0], [np.nan, 0.0]) is None
