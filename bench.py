@@ -474,8 +474,17 @@ def run_b200(args, rank, world, local):
     g2.set_sweep_kernel(tune["kind"])
     if tune["kind"] == "lean":
         g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
-    h2d = body.positions.nbytes + body.weights.nbytes + 48
-    d2h = 100
+    # the caller's marker arrays live in pinned host memory (copied to the
+    # device by lbmb_ibm_set_body every step); the step's result is the IBM
+    # diagnostics record read back by lbmb_apply_rotating_ibm
+    import torch
+    pos_pin = torch.empty(body.positions.shape, dtype=torch.float64, pin_memory=True).numpy()
+    w_pin = torch.empty(body.weights.shape, dtype=torch.float64, pin_memory=True).numpy()
+    pos_pin[...] = body.positions
+    w_pin[...] = body.weights
+    body = lb.RotatingBody(body.center, body.omega, pos_pin, w_pin)
+    h2d = body.positions.nbytes + body.weights.nbytes
+    d2h = 128
     for _ in range(3):
         g2.clear_body_force_field()
         g2.set_body(0, body)

@@ -128,6 +128,7 @@ struct EngineBase {
   virtual void run_impeller(int b, const lbmb_ibm_config& cfg, int64_t steps, int k, int64_t probe_every,
                             double* torque, double* ff, double* cv, int32_t* iters) = 0;
   virtual void sync() = 0;
+  virtual void timing(double* total_ms, double* hydro_ms, int64_t* launches) = 0;
   virtual void set_sweep_kernel(int kind) = 0;
   virtual int sweep_kernel() const = 0;
   virtual void set_sweep_variant(int even, int odd) = 0;
@@ -668,16 +669,41 @@ struct Engine final : EngineBase {
       ++launches;
     }
     CK(cudaEventRecord(ev1, st));
-    CK(cudaEventSynchronize(ev1));
-    check_device_error();
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ev0, ev1));
-    last_total_ms = ms;
-    last_hydro_ms = ms;
-    last_hydro_launches = launches;
+    // Asynchronous: the call returns once the work is queued (every other
+    // entry point runs on the same stream, and the ones that return data
+    // synchronize). The device time is resolved when it is asked for. The
+    // bulk-copy kernel is the only one that can raise a device error flag,
+    // so its steps are checked at once.
+    pending_launches = launches;
+    timing_pending = true;
+    if (kernel_mode == LBMB_SWEEP_BULK) {
+      CK(cudaEventSynchronize(ev1));
+      check_device_error();
+    }
   }
 
-  void sync() override { CK(cudaStreamSynchronize(st)); }
+  bool timing_pending = false;
+  int64_t pending_launches = 0;
+
+  void timing(double* total_ms, double* hydro_ms, int64_t* launches) override {
+    if (timing_pending) {
+      CK(cudaEventSynchronize(ev1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      last_total_ms = ms;
+      last_hydro_ms = ms;
+      last_hydro_launches = pending_launches;
+      timing_pending = false;
+    }
+    if (total_ms) *total_ms = last_total_ms;
+    if (hydro_ms) *hydro_ms = last_hydro_ms;
+    if (launches) *launches = last_hydro_launches;
+  }
+
+  void sync() override {
+    CK(cudaStreamSynchronize(st));
+    check_device_error();
+  }
 
   // Sweep autotuner: times every kernel kind (and, for the lean kernel,
   // every register budget) that can run this configuration on the solver's
@@ -940,6 +966,28 @@ struct Engine final : EngineBase {
     for (int a = 0; a < 3; ++a)
       if (!std::isfinite(c[a]) || !std::isfinite(om[a])) invalid("IBM center and omega must be finite");
     if (int(bodies.size()) <= b) bodies.resize(size_t(b) + 1);
+    // The runner passes the same marker set every step: when the markers are
+    // unchanged the stencils and device arrays stay; only the rotation
+    // (centre, angular velocity and the slip scale) is refreshed.
+    if (BodyState* old = bodies[size_t(b)].get()) {
+      if (old->nm == nm && std::memcmp(old->pos.data(), pos, size_t(3 * nm) * sizeof(double)) == 0 &&
+          std::memcmp(old->weight.data(), w, size_t(nm) * sizeof(double)) == 0) {
+        // the marker arrays are still copied, so the device always holds
+        // what the caller passed (an asynchronous copy of the same bytes)
+        CK(cudaMemcpyAsync(old->d_pos.p, pos, size_t(3 * nm) * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(old->d_weight.p, w, size_t(nm) * sizeof(double), cudaMemcpyHostToDevice, st));
+        bool same = true;
+        for (int a = 0; a < 3; ++a) same = same && old->center[a] == c[a] && old->omega[a] == om[a];
+        if (same) return;
+        for (int a = 0; a < 3; ++a) {
+          old->center[a] = c[a];
+          old->omega[a] = om[a];
+        }
+        old->scale = body_scale(pos, nm, c, om);
+        invalidate_graphs();
+        return;
+      }
+    }
     auto bs = std::make_unique<BodyState>();
     bs->nm = nm;
     bs->pos.assign(pos, pos + 3 * nm);
@@ -948,14 +996,7 @@ struct Engine final : EngineBase {
       bs->center[a] = c[a];
       bs->omega[a] = om[a];
     }
-    // scale = max(max |Omega x r|, 1) (solver.rs:3090-3094)
-    double mt = 0.0;
-    for (int64_t m = 0; m < nm; ++m) {
-      const double r[3] = {pos[3 * m] - c[0], pos[3 * m + 1] - c[1], pos[3 * m + 2] - c[2]};
-      const double t[3] = {om[1] * r[2] - om[2] * r[1], om[2] * r[0] - om[0] * r[2], om[0] * r[1] - om[1] * r[0]};
-      mt = std::max(mt, std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]));
-    }
-    bs->scale = std::max(mt, 1.0);
+    bs->scale = body_scale(pos, nm, c, om);
     bs->d_pos.upload(bs->pos, st);
     bs->d_weight.upload(bs->weight, st);
     bs->imp.alloc(size_t(3 * nm));
@@ -965,6 +1006,17 @@ struct Engine final : EngineBase {
     CK(cudaStreamSynchronize(st));
     bodies[b] = std::move(bs);
     invalidate_graphs();
+  }
+
+  // scale = max(max |Omega x r|, 1) (solver.rs:3090-3094)
+  static double body_scale(const double* pos, int64_t nm, const double* c, const double* om) {
+    double mt = 0.0;
+    for (int64_t m = 0; m < nm; ++m) {
+      const double r[3] = {pos[3 * m] - c[0], pos[3 * m + 1] - c[1], pos[3 * m + 2] - c[2]};
+      const double t[3] = {om[1] * r[2] - om[2] * r[1], om[2] * r[0] - om[0] * r[2], om[0] * r[1] - om[1] * r[0]};
+      mt = std::max(mt, std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]));
+    }
+    return std::max(mt, 1.0);
   }
 
   static double linear_kernel(double r) { return std::max(1.0 - r, 0.0); }
@@ -1337,6 +1389,7 @@ struct Engine final : EngineBase {
     last_total_ms = ms;
     last_hydro_ms = ms;
     last_hydro_launches = launches;
+    timing_pending = false;
     if (torque) CK(cudaMemcpy(torque, d_torque.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
     if (ffo) CK(cudaMemcpy(ffo, d_ff.p, size_t(3 * steps) * sizeof(double), cudaMemcpyDeviceToHost));
     if (iters) CK(cudaMemcpy(iters, d_it.p, size_t(steps) * sizeof(int32_t), cudaMemcpyDeviceToHost));

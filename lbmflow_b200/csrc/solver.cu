@@ -346,9 +346,7 @@ int lbmb_run_impeller(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg, 
 int lbmb_last_timing(lbmb_solver* h, double* total_ms, double* hydro_ms, int64_t* hydro_launches) {
   return guarded([&] {
     if (!h || !h->e) throw Error(LBMB_ERR_INVALID, "null solver");
-    if (total_ms) *total_ms = h->e->last_total_ms;
-    if (hydro_ms) *hydro_ms = h->e->last_hydro_ms;
-    if (hydro_launches) *hydro_launches = h->e->last_hydro_launches;
+    h->e->timing(total_ms, hydro_ms, hydro_launches);
   });
 }
 
