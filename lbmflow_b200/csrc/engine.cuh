@@ -427,12 +427,12 @@ struct Engine final : EngineBase {
 
   void set_sweep_kernel(int kind) override {
     const bool wide = sizeof(S) >= 4;
-    const bool pair = std::is_same<A, float>::value && coll == COLL_TRT && nx % 2 == 0 && !has_uniform_force();
+    const bool pair = std::is_same<A, float>::value && nx % 2 == 0 && !has_uniform_force();
     if (kind == LBMB_SWEEP_ASYNC && !wide)
       throw Error(LBMB_ERR_UNSUPPORTED, "the cp.async sweep needs 4- or 8-byte population storage");
     if ((kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE) && !pair)
       throw Error(LBMB_ERR_UNSUPPORTED,
-                  "the pair sweep needs TRT/BGK, fp32/fp16/bf16 storage, even nx and no uniform body force");
+                  "the pair sweep needs fp32/fp16/bf16 storage, even nx and no uniform body force");
     if (kind == LBMB_SWEEP_LEAN && !lean_ok(coll))
       throw Error(LBMB_ERR_UNSUPPORTED, "the lean sweep needs TRT/BGK, fp32/fp16/bf16 storage and no uniform body force");
     kernel_mode = kind;
@@ -474,8 +474,8 @@ struct Engine final : EngineBase {
   }
 
   // Whether the two-cells-per-thread kernel covers this sweep.
-  bool pair_ok(const HydroParams<A>& p, int coll_kind) const {
-    return std::is_same<A, float>::value && coll_kind == COLL_TRT && !p.uniform_force && nx % 2 == 0;
+  bool pair_ok(const HydroParams<A>& p, int) const {
+    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0;
   }
 
   // Tile list and window offsets of the tile-pipelined sweep.
@@ -505,11 +505,11 @@ struct Engine final : EngineBase {
     CK(cudaStreamSynchronize(st));
   }
 
-  template <bool ODD>
+  template <bool ODD, int COLL>
   void launch_tile(const HydroParams<A>& p, cudaStream_t s) {
-    if constexpr (std::is_same<A, float>::value) {
+    if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
       constexpr int STAGES = 3;
-      auto kern = hydro_tile_kernel<Q, S, ODD, STAGES>;
+      auto kern = hydro_tile_kernel<Q, S, ODD, STAGES, COLL>;
       const size_t smem = tile_smem_bytes<Q, S, STAGES>();
       if (tile_grid[ODD] == 0) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -523,11 +523,11 @@ struct Engine final : EngineBase {
     }
   }
 
-  template <bool ODD>
+  template <bool ODD, int COLL>
   void launch_pair(const HydroParams<A>& p, cudaStream_t s) {
-    if constexpr (std::is_same<A, float>::value) {
+    if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
       const uint32_t npairs = uint32_t(n / 2);
-      hydro_pair_kernel<Q, S, ODD><<<unsigned(ceil_div(npairs, PAIR_BLOCK)), PAIR_BLOCK, 0, s>>>(p, npairs);
+      hydro_pair_kernel<Q, S, ODD, COLL><<<unsigned(ceil_div(npairs, PAIR_BLOCK)), PAIR_BLOCK, 0, s>>>(p, npairs);
       CK(cudaGetLastError());
     }
   }
@@ -536,9 +536,9 @@ struct Engine final : EngineBase {
   void launch_hydro_t(const HydroParams<A>& p, cudaStream_t s, bool main_grid, bool cells) {
     if (main_grid) {
       if (kernel_mode == LBMB_SWEEP_PAIR && pair_ok(p, COLL)) {
-        launch_pair<ODD>(p, s);
+        launch_pair<ODD, COLL>(p, s);
       } else if (kernel_mode == LBMB_SWEEP_TILE && pair_ok(p, COLL)) {
-        launch_tile<ODD>(p, s);
+        launch_tile<ODD, COLL>(p, s);
       } else if (kernel_mode == LBMB_SWEEP_LEAN && lean_ok(COLL) && !p.uniform_force) {
         launch_lean<ODD>(p, s);
       } else if (!p.uniform_force && kernel_mode == 1) {
@@ -723,7 +723,7 @@ struct Engine final : EngineBase {
     cands.push_back({LBMB_SWEEP_DIRECT, 0, 0});
     if (wide && !uf) cands.push_back({LBMB_SWEEP_ASYNC, 0, 0});
     if (!uf) cands.push_back({LBMB_SWEEP_BULK, 0, 0});
-    if (is_f && coll == COLL_TRT && nx % 2 == 0 && !uf) {
+    if (is_f && nx % 2 == 0 && !uf) {
       cands.push_back({LBMB_SWEEP_PAIR, 0, 0});
       cands.push_back({LBMB_SWEEP_TILE, 0, 0});
     }

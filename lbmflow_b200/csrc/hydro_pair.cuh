@@ -213,8 +213,171 @@ __device__ __forceinline__ float2 trt_pair_collide(float2 (&f)[Q], const HydroPa
   return rho;
 }
 
-template <int Q, class S, bool ODD>
-__global__ void __launch_bounds__(PAIR_BLOCK, 4) hydro_pair_kernel(HydroParams<float> p, uint32_t npairs) {
+// Central-moment collision (kernels.rs:406-533, no force term) of two cells
+// in float2 lanes, in the form that keeps one set of 27 values live:
+//   K = f - feq;  K <- T K (factorised central-moment transform);
+//   K <- (I - R) K  (order <= 1 kept, order-2 deviatoric at 1 - w_s, trace
+//                    and order >= 3 to zero);
+//   f' = feq + T^-1 K
+// which is the same operator as f + T^-1[-R T(f - feq)] by linearity. The
+// exact-rest skip (kernels.rs:434-447) zeroes K of a lane whose populations
+// all equal w (rho - 1), so that lane comes back unchanged.
+__device__ __forceinline__ void cm_fwd2(float2& a, float2& b, float2& c, float2 u) {
+  const float2 k0 = add2(add2(a, b), c);
+  const float2 d = sub2(c, a);
+  const float2 s = add2(c, a);
+  const float2 k1 = fma2(mul2(u, bc2(-1.f)), k0, d);
+  const float2 k2 = fma2(mul2(u, u), k0, fma2(mul2(u, bc2(-2.f)), d, s));
+  a = k0;
+  b = k1;
+  c = k2;
+}
+__device__ __forceinline__ void cm_bwd2(float2& k0, float2& k1, float2& k2, float2 u) {
+  const float2 m1 = fma2(u, k0, k1);
+  const float2 m2 = fma2(mul2(u, u), k0, fma2(mul2(u, bc2(2.f)), k1, k2));
+  const float2 fm = mul2(bc2(0.5f), sub2(m2, m1));
+  const float2 f0 = sub2(k0, m2);
+  const float2 fp = mul2(bc2(0.5f), add2(m2, m1));
+  k0 = fm;
+  k1 = f0;
+  k2 = fp;
+}
+
+template <int Q>
+__device__ __forceinline__ float2 cm_pair_collide(float2 (&f)[Q], const HydroParams<float>& p) {
+  static_assert(Q == 27, "central moments need the full D3Q27 tensor basis");
+  using L = Lat<Q>;
+  constexpr int NP = (Q - 1) / 2;
+  float2 drho = f[0], jx = bc2(0.f), jy = bc2(0.f), jz = bc2(0.f);
+  float s6[2][6] = {{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    const int a = 2 * k + 1, b = a + 1;
+    const float2 S = add2(f[a], f[b]), D = sub2(f[a], f[b]);
+    drho = add2(drho, S);
+    if (L::cx(a) == 1) jx = add2(jx, D);
+    if (L::cx(a) == -1) jx = sub2(jx, D);
+    if (L::cy(a) == 1) jy = add2(jy, D);
+    if (L::cy(a) == -1) jy = sub2(jy, D);
+    if (L::cz(a) == 1) jz = add2(jz, D);
+    if (L::cz(a) == -1) jz = sub2(jz, D);
+  }
+  const float2 rho = add2(drho, bc2(1.f));
+  const float2 inv = make_float2(rcp_fast(rho.x), rcp_fast(rho.y));
+  const float2 ux = mul2(jx, inv), uy = mul2(jy, inv), uz = mul2(jz, inv);
+  const float2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
+  float2 os = bc2(p.omega_shear);
+  if (p.les_c > 0.f) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int a = 2 * k + 1;
+      const int cx = L::cx(a), cy = L::cy(a), cz = L::cz(a);
+      const float2 S = add2(f[a], f[a + 1]);
+      const float sv[2] = {S.x, S.y};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (cx) s6[h][0] += sv[h];
+        if (cy) s6[h][1] += sv[h];
+        if (cz) s6[h][2] += sv[h];
+        if (cx && cy) s6[h][3] += float(cx * cy) * sv[h];
+        if (cx && cz) s6[h][4] += float(cx * cz) * sv[h];
+        if (cy && cz) s6[h][5] += float(cy * cz) * sv[h];
+      }
+    }
+    const float te0 = les_tau_pair<Q>(s6[0], rho.x, inv.x, ux.x, uy.x, uz.x, p.les_c, p.tau0);
+    const float te1 = les_tau_pair<Q>(s6[1], rho.y, inv.y, ux.y, uy.y, uz.y, p.les_c, p.tau0);
+    os = make_float2(rcp_fast(te0), rcp_fast(te1));
+  }
+  // exact rest (per lane): u == 0 and every population == w (rho - 1)
+  bool rest0 = ux.x == 0.f && uy.x == 0.f && uz.x == 0.f;
+  bool rest1 = ux.y == 0.f && uy.y == 0.f && uz.y == 0.f;
+  if (rest0 || rest1) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      rest0 = rest0 && (f[q].x == float(L::w(q) * (double(rho.x) - 1.0)));
+      rest1 = rest1 && (f[q].y == float(L::w(q) * (double(rho.y) - 1.0)));
+    }
+    if (rest0 && rest1) return rho;
+  }
+  auto feq = [&](int q) {
+    float2 cu = L::cx(q) ? (L::cx(q) > 0 ? ux : mul2(ux, bc2(-1.f))) : bc2(0.f);
+    if (L::cy(q)) cu = L::cy(q) > 0 ? add2(cu, uy) : sub2(cu, uy);
+    if (L::cz(q)) cu = L::cz(q) > 0 ? add2(cu, uz) : sub2(cu, uz);
+    // w (drho + rho (3 cu + 4.5 cu^2 - 1.5 u^2))
+    const float2 inner = fma2(cu, fma2(bc2(4.5f), cu, bc2(3.f)), mul2(bc2(-1.5f), usq));
+    return mul2(bc2(float(L::w(q))), fma2(rho, inner, drho));
+  };
+  float2 K[3][3][3];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = sub2(f[q], feq(q));
+  if (rest0 || rest1) {
+#pragma unroll
+    for (int i = 0; i < 27; ++i) {
+      float2& k = K[i / 9][(i / 3) % 3][i % 3];
+      if (rest0) k.x = 0.f;
+      if (rest1) k.y = 0.f;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) cm_fwd2(K[i][j][0], K[i][j][1], K[i][j][2], uz);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_fwd2(K[i][0][k], K[i][1][k], K[i][2][k], uy);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_fwd2(K[0][j][k], K[1][j][k], K[2][j][k], ux);
+  // deviatoric rate w_s (1 - 0.16 |u|^2) capped at 2
+  const float2 ws = make_float2(fminf(os.x * (1.f - 0.16f * usq.x), 2.f), fminf(os.y * (1.f - 0.16f * usq.y), 2.f));
+  const float2 keep = sub2(bc2(1.f), ws);
+  const float2 bulk = mul2(bc2(1.f / 3.f), add2(add2(K[2][0][0], K[0][2][0]), K[0][0][2]));
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int order = a + b + c;
+        const bool diag = order == 2 && (a == 2 || b == 2 || c == 2);
+        if (order <= 1) continue;
+        if (diag) K[a][b][c] = mul2(keep, sub2(K[a][b][c], bulk));
+        else if (order == 2) K[a][b][c] = mul2(keep, K[a][b][c]);
+        else K[a][b][c] = bc2(0.f);
+      }
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_bwd2(K[0][j][k], K[1][j][k], K[2][j][k], ux);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_bwd2(K[i][0][k], K[i][1][k], K[i][2][k], uy);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) cm_bwd2(K[i][j][0], K[i][j][1], K[i][j][2], uz);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const float2 v = add2(feq(q), K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1]);
+    // a lane at exact rest keeps its populations bit for bit
+    f[q].x = rest0 ? f[q].x : v.x;
+    f[q].y = rest1 ? f[q].y : v.y;
+  }
+  return rho;
+}
+
+// Collision of a pair in the chosen form.
+template <int Q, int COLL>
+__device__ __forceinline__ float2 pair_collide(float2 (&f)[Q], const HydroParams<float>& p) {
+  if constexpr (COLL == COLL_CM) return cm_pair_collide<Q>(f, p);
+  else return trt_pair_collide<Q>(f, p);
+}
+
+template <int Q, class S, bool ODD, int COLL = COLL_TRT>
+__global__ void __launch_bounds__(PAIR_BLOCK, COLL == COLL_CM ? 2 : 4) hydro_pair_kernel(HydroParams<float> p, uint32_t npairs) {
   using L = Lat<Q>;
   using IO = PairIO<S>;
   const uint32_t pi = blockIdx.x * PAIR_BLOCK + threadIdx.x;
@@ -229,8 +392,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) hydro_pair_kernel(HydroParams<f
     const int z = int(c / uint32_t(nxy));
     const int r = int(c - uint32_t(z) * uint32_t(nxy));
     const int y = r / nx, x = r - y * nx;
-    if (act0) hydro_cell_generic<Q, S, COLL_TRT, ODD, false>(p, x, y, z, c, uint8_t(fl0));
-    if (act1) hydro_cell_generic<Q, S, COLL_TRT, ODD, false>(p, x + 1, y, z, c + 1, uint8_t(fl1));
+    if (act0) hydro_cell_generic<Q, S, COLL, ODD, false>(p, x, y, z, c, uint8_t(fl0));
+    if (act1) hydro_cell_generic<Q, S, COLL, ODD, false>(p, x + 1, y, z, c + 1, uint8_t(fl1));
     return;
   }
   const uint32_t mk0 = (fl0 & F_BOUNDARY) ? p.nbr[c] : 0u;
@@ -256,7 +419,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 4) hydro_pair_kernel(HydroParams<f
       if ((mk1 >> o) & 1u) f[q].y = IO::ld1(own + 1);
     }
   }
-  const float2 rho = trt_pair_collide<Q>(f, p);
+  const float2 rho = pair_collide<Q, COLL>(f, p);
   const bool both = act0 && act1;
   const bool moving = (fl0 | fl1) & F_MOVING;
 #pragma unroll

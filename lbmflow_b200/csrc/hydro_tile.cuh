@@ -61,8 +61,8 @@ __device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
-template <int Q, class S, bool ODD, int STAGES>
-__global__ void __launch_bounds__(TILE_THREADS, 3)
+template <int Q, class S, bool ODD, int STAGES, int COLL = COLL_TRT>
+__global__ void __launch_bounds__(TILE_THREADS, COLL == COLL_CM ? 2 : 3)
     hydro_tile_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, TileDirs dirs) {
   using L = Lat<Q>;
   using W = TileWin<S>;
@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 3)
       const int z = int(c / uint32_t(nxy));
       const int r = int(c - uint32_t(z) * uint32_t(nxy));
       const int y = r / nx, x = r - y * nx;
-      if (act0) hydro_cell_generic<Q, S, COLL_TRT, ODD, false>(p, x, y, z, c, uint8_t(fl0));
-      if (act1) hydro_cell_generic<Q, S, COLL_TRT, ODD, false>(p, x + 1, y, z, c + 1, uint8_t(fl1));
+      if (act0) hydro_cell_generic<Q, S, COLL, ODD, false>(p, x, y, z, c, uint8_t(fl0));
+      if (act1) hydro_cell_generic<Q, S, COLL, ODD, false>(p, x + 1, y, z, c + 1, uint8_t(fl1));
       continue;
     }
     const uint32_t mk0 = (fl0 & F_BOUNDARY) ? p.nbr[c] : 0u;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3)
         }
       }
     }
-    const float2 rho = trt_pair_collide<Q>(f, p);
+    const float2 rho = pair_collide<Q, COLL>(f, p);
     const bool both = act0 && act1;
     const bool moving = (fl0 | fl1) & F_MOVING;
 #pragma unroll

@@ -24,7 +24,7 @@ def supported(kind, q, coll, prec, nx=14, force=False):
     if kind == "lean":
         return coll in ("trt", "bgk") and prec in ("f32", "f16", "bf16") and not force
     if kind in ("pair", "tile"):
-        return coll in ("trt", "bgk") and prec in ("f32", "f16", "bf16") and nx % 2 == 0 and not force
+        return prec in ("f32", "f16", "bf16") and nx % 2 == 0 and not force and (coll != "cm" or q == 27)
     return True
 
 
@@ -53,6 +53,14 @@ def test_smagorinsky_each_kernel_matches_oracle(kind, q):
     p.check(solid == 0)
 
 
+@pytest.mark.parametrize("kind", ["async", "pair", "tile"])
+def test_smagorinsky_central_moment_each_kernel(kind):
+    dims, solid, wall_u, nu = cavity(14, u_lid=0.08, re=2000.0)
+    p = Pair(dims, 27, "f32", collision="cm", nu=nu, solid=solid, wall_u=wall_u, smagorinsky_cs=0.17, sweep=kind)
+    p.run(45)
+    p.check(solid == 0)
+
+
 @pytest.mark.parametrize("kind", KINDS)
 def test_periodic_tgv_each_kernel(kind):
     # every cell is on or next to a periodic face at this size: wrap paths
@@ -64,14 +72,15 @@ def test_periodic_tgv_each_kernel(kind):
     p.check(np.ones(p.n, bool))
 
 
-@pytest.mark.parametrize("kind", ["pair", "tile", "lean"])
+@pytest.mark.parametrize("kind,q,coll", [("pair", 19, "trt"), ("tile", 19, "trt"), ("lean", 19, "trt"),
+                                         ("pair", 27, "cm"), ("tile", 27, "cm")])
 @pytest.mark.parametrize("prec", ["f16", "bf16"])
-def test_pair_kernel_low_precision_matches_direct(prec, kind):
+def test_pair_kernel_low_precision_matches_direct(prec, kind, q, coll):
     # Same storage, two kernels: the 16-bit rounding happens at the same
     # points, so the fields agree to a few storage ulps after 200 steps.
     dims, solid, wall_u, nu = cavity(24, re=50.0)
-    a = lb.Solver(dims, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
-    b = lb.Solver(dims, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
+    a = lb.Solver(dims, lattice=q, collision=coll, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
+    b = lb.Solver(dims, lattice=q, collision=coll, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
     a.set_sweep_kernel("direct")
     b.set_sweep_kernel(kind)
     a.run(200)
@@ -80,7 +89,7 @@ def test_pair_kernel_low_precision_matches_direct(prec, kind):
     fl = solid == 0
     eps = {"f16": 2.0 ** -10, "bf16": 2.0 ** -7}[prec]
     assert np.abs(ua - ub)[fl].max() <= 40 * eps * 0.06, np.abs(ua - ub)[fl].max()
-    ref = lb.Solver(dims, storage="f32", nu=nu, solid=solid, wall_u=wall_u)
+    ref = lb.Solver(dims, lattice=q, collision=coll, storage="f32", nu=nu, solid=solid, wall_u=wall_u)
     ref.run(200)
     ur = ref.read_moments()[1].reshape(24, 24, 24)[:, 12, 12]
     l2 = np.linalg.norm(ub.reshape(24, 24, 24)[:, 12, 12] - ur) / np.linalg.norm(ur)
@@ -132,6 +141,9 @@ def test_pair_kernel_refuses_what_it_cannot_run():
     g = lb.Solver(dims, storage="f64", nu=nu, solid=solid, wall_u=wall_u)
     with pytest.raises(lb.UnsupportedError):
         g.set_sweep_kernel("pair")
+    g = lb.Solver(dims, lattice=27, collision="cm", storage="f32", nu=nu, solid=solid, wall_u=wall_u)
+    with pytest.raises(lb.UnsupportedError):
+        g.set_sweep_kernel("lean")
     g = lb.Solver(dims, storage="f16", nu=nu, solid=solid, wall_u=wall_u)
     with pytest.raises(lb.UnsupportedError):
         g.set_sweep_kernel("async")
