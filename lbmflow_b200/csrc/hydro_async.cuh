@@ -55,6 +55,11 @@ __global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::
   auto dq = [&](int q) -> int64_t {
     return int64_t(L::cx(q)) + int64_t(L::cy(q)) * nx + int64_t(L::cz(q)) * nxy;
   };
+  // P(k): slot k of the cell; T(k): slot k of the neighbour x + c_k (the odd
+  // step reads T(opp q) and writes T(q)); both depend on launch parameters
+  // only.
+  auto P = [&](int k) -> int64_t { return int64_t(k) * pl; };
+  auto T = [&](int k) -> int64_t { return int64_t(k) * pl + dq(k); };
   // Cells on a periodic face take the out-of-line generic path; all other
   // active cells go through the pipeline.
   auto piped = [&](uint8_t fl) { return !(fl & (F_SOLID | F_FORCED | F_WRAP | F_SLIP)); };
@@ -71,11 +76,17 @@ __global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::
           for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + int64_t(q) * pl);
         } else {
           const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
+          // a warp whose cells have no solid neighbour copies straight from
+          // the neighbours (warp-uniform vote); the others select per link
+          if (__all_sync(__activemask(), mask == 0u)) {
 #pragma unroll
-          for (int q = 0; q < Q; ++q) {
-            const int o = opp(q);
-            const int64_t off = ((mask >> o) & 1u) ? int64_t(q) * pl : int64_t(o) * pl - dq(q);
-            cp_async_elem(dst + q * ASYNC_TILE, src0 + off);
+            for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + T(opp(q)));
+          } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+              const int o = opp(q);
+              cp_async_elem(dst + q * ASYNC_TILE, src0 + (((mask >> o) & 1u) ? P(q) : T(o)));
+            }
           }
         }
       }
@@ -126,18 +137,25 @@ __global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::
       collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, op, om, cp, cm);
     const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
     S* dst0 = fb + cell;
+    if (fl & F_MOVING) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      A v = f[q];
-      const int o = opp(q);
-      const bool wall = (mask >> q) & 1u;
-      if (wall && (fl & F_MOVING)) {
-        const Vec4<A> wu = p.wall_u[cell + dq(q)];
-        const A cu = (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y) + A(L::cz(o)) * wu.z;
-        v = v + ((A(6) * A(L::w(o))) * rho) * cu;
-      }
-      const int64_t off = (!ODD || wall) ? int64_t(o) * pl : int64_t(q) * pl + dq(q);
-      CD::st(dst0 + off, v);
+      for (int q = 0; q < Q; ++q)
+        if ((mask >> q) & 1u) {
+          const int o = opp(q);
+          const Vec4<A> wu = p.wall_u[cell + dq(q)];
+          const A cu = (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y) + A(L::cz(o)) * wu.z;
+          f[q] = f[q] + ((A(6) * A(L::w(o))) * rho) * cu;
+        }
+    }
+    if (!ODD) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) CD::st(dst0 + P(opp(q)), f[q]);
+    } else if (__all_sync(__activemask(), mask == 0u)) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) CD::st(dst0 + T(q), f[q]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) CD::st(dst0 + (((mask >> q) & 1u) ? P(opp(q)) : T(q)), f[q]);
     }
   }
   cp_async_wait<0>();
