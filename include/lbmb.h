@@ -275,10 +275,14 @@ typedef enum {
 } lbmb_sweep_kind;
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
-/* Register budget of the lean sweep per parity, as resident 128-thread
- * blocks per SM the kernel is compiled for: 8 (64 registers), 7 (72) or 6
- * (80). More registers avoid spills, fewer keep more warps resident; the
- * best split depends on the lattice and storage (no reference counterpart). */
+/* Launch variant of the current sweep kernel (no reference counterpart).
+ * Lean kernel: register budget per parity, as resident 128-thread blocks per
+ * SM the kernel is compiled for: 8 (64 registers), 7 (72) or 6 (80); more
+ * registers avoid spills, fewer keep more warps resident. cp.async kernel:
+ * even_blocks_per_sm = blocks per SM its persistent grid is sized for (0 =
+ * as many as fit, 1..16 capped at what fits); fewer leave room on every SM
+ * for the IBM kernels that run concurrently in a runner step;
+ * odd_blocks_per_sm is ignored. */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

@@ -419,7 +419,8 @@ struct Engine final : EngineBase {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
       int per_sm = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ASYNC_TILE, smem));
-      async_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
+      const int bps = async_bps > 0 ? std::min(async_bps, std::max(per_sm, 1)) : std::max(per_sm, 1);
+      async_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * bps)));
     }
     kern<<<unsigned(async_grid[slot]), ASYNC_TILE, smem, s>>>(p, n, int(ntiles));
     CK(cudaGetLastError());
@@ -439,7 +440,18 @@ struct Engine final : EngineBase {
     invalidate_graphs();
   }
   int sweep_kernel() const override { return kernel_mode; }
+  // Blocks per SM the persistent cp.async grid is sized for (0: as many as
+  // fit). Fewer leave room on every SM for the IBM kernels of a runner step.
+  int async_bps = 0;
+
   void set_sweep_variant(int even, int odd) override {
+    if (kernel_mode == LBMB_SWEEP_ASYNC) {
+      if (even < 0 || even > 16) throw Error(LBMB_ERR_INVALID, "sweep variant: cp.async blocks per SM must be 0..16");
+      async_bps = even;
+      for (int& g : async_grid) g = 0;
+      invalidate_graphs();
+      return;
+    }
     auto ok = [](int v) { return v >= 6 && v <= 8; };
     if (!ok(even) || !ok(odd)) throw Error(LBMB_ERR_INVALID, "sweep variant: resident blocks per SM must be 6, 7 or 8");
     lean_minb[0] = even;
