@@ -442,7 +442,14 @@ def run_b200(args, rank, world, local):
     D = args.tank_T / 3.0
     omega = float(body.omega[2])
     g = make_solver(lb, dims, solid, nu, q, coll, storage, args.les_cs, local)
-    tune = g.autotune_sweep(8)
+    if args.sweep_kernel:
+        # a fixed kernel (profiling runs: timings under a profiler would
+        # mislead the autotuner)
+        g.set_sweep_kernel(args.sweep_kernel)
+        tune = {"kind": args.sweep_kernel, "even_blocks_per_sm": 0, "odd_blocks_per_sm": 0,
+                "best_ms_per_step": None, "default_ms_per_step": None}
+    else:
+        tune = g.autotune_sweep(8)
     cfg = lb.DirectForcingConfig()
     # warm-up (untimed)
     g.run_impeller(body, max(args.warmup, 3))
@@ -607,6 +614,8 @@ def main():
     ap.add_argument("--mix-T", type=int, default=64, help="tank diameter of the mixing-time study")
     ap.add_argument("--mix-D", type=float, default=1e-2, help="scalar diffusivity of the mixing study (lattice)")
     ap.add_argument("--mix-steps", type=int, default=60000, help="step cap of the mixing study (0: skip)")
+    ap.add_argument("--sweep-kernel", default=None, choices=["direct", "bulk", "async", "pair", "tile", "lean"],
+                    help="use this sweep kernel instead of the autotuner's choice")
     ap.add_argument("--lid", action="store_true", help="no-slip lid (the reference's tank) instead of a free-slip top")
     ap.add_argument("--sweep-seq-steps", type=int, default=200,
                     help="steps per case of the sequential-loop sample (0: skip)")
