@@ -45,7 +45,7 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum, mean of
 # one even and one odd launch) from an ncu full-set capture of the sweep kernel
 # the autotuner picks for the form, on the tank of the given diameter.
-NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 446.65e6}
+NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 449.3e6}
 FALLBACK_HBM_GBS = 6650.0
 
 

@@ -280,9 +280,9 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
  * SM the kernel is compiled for: 8 (64 registers), 7 (72) or 6 (80); more
  * registers avoid spills, fewer keep more warps resident. cp.async kernel:
  * even_blocks_per_sm = blocks per SM its persistent grid is sized for (0 =
- * as many as fit, 1..16 capped at what fits); fewer leave room on every SM
- * for the IBM kernels that run concurrently in a runner step;
- * odd_blocks_per_sm is ignored. */
+ * as many as fit, 1..16 capped at what fits); odd_blocks_per_sm = block
+ * slots (0..4 x SM count, default 32) the grid leaves free in the sweep of
+ * a runner step, where the IBM kernels run concurrently on a side stream. */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

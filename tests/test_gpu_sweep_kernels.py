@@ -96,7 +96,7 @@ def test_pair_kernel_low_precision_matches_direct(prec, kind, q, coll):
     assert l2 < {"f16": 5e-3, "bf16": 5e-2}[prec], l2
 
 
-@pytest.mark.parametrize("kind", ["pair", "tile", "lean", "direct", "bulk"])
+@pytest.mark.parametrize("kind", ["pair", "tile", "lean", "direct", "bulk", "async"])
 def test_runner_loop_each_kernel_matches_oracle(kind):
     from oracle import oracle as o
     n = 28
@@ -109,6 +109,10 @@ def test_runner_loop_each_kernel_matches_oracle(kind):
     nu = 0.01
     g = lb.Solver((n, n, n), lattice=19, collision="trt", storage="f32", nu=nu, solid=solid)
     g.set_sweep_kernel(kind)
+    if kind == "async":
+        # a persistent grid smaller than the tile count, with block slots
+        # left free for the IBM chain
+        g.set_sweep_variant(1, 100)
     c = o.OracleSolver((n, n, n), q=19, real_bits=32, collision="trt", nu=nu, solid=solid)
     rg = g.run_impeller(body, 40)
     rc = c.run_tank(body.positions, body.weights, body.center, body.omega, 40)
