@@ -481,6 +481,8 @@ def run_b200(args, rank, world, local):
     g2.set_sweep_kernel(tune["kind"])
     if tune["kind"] == "lean":
         g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
+    elif tune["kind"] == "async" and tune["even_blocks_per_sm"] and storage != "f64":
+        g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
     # the caller's marker arrays live in pinned host memory (copied to the
     # device by lbmb_ibm_set_body every step); the step's result is the IBM
     # diagnostics record read back by lbmb_apply_rotating_ibm

@@ -278,11 +278,11 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
 /* Launch variant of the current sweep kernel (no reference counterpart).
  * Lean kernel: register budget per parity, as resident 128-thread blocks per
  * SM the kernel is compiled for: 8 (64 registers), 7 (72) or 6 (80); more
- * registers avoid spills, fewer keep more warps resident. cp.async kernel:
- * even_blocks_per_sm = blocks per SM its persistent grid is sized for (0 =
- * as many as fit, 1..16 capped at what fits); odd_blocks_per_sm = block
- * slots (0..4 x SM count, default 32) the grid leaves free in the sweep of
- * a runner step, where the IBM kernels run concurrently on a side stream. */
+ * registers avoid spills, fewer keep more warps resident. cp.async kernel
+ * (fp32 storage): the same per parity with 4 (128 registers, 3-tile ring,
+ * the default), 5 (96, 3 tiles) or 6 (80, 2 tiles); its persistent grid
+ * fills every resident slot, less 32 block slots in the sweep of a runner
+ * step, where the IBM kernels run concurrently on a side stream. */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

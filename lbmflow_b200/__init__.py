@@ -307,10 +307,8 @@ class Solver:
         _check(lib().lbmb_set_sweep_kernel(self.h, SWEEP[kind] if isinstance(kind, str) else int(kind)))
 
     def set_sweep_variant(self, even_blocks_per_sm, odd_blocks_per_sm):
-        """Launch variant of the current sweep kernel: for "lean" the register
-        budget per parity (resident blocks per SM 6..8); for "async" the
-        persistent grid's blocks per SM (0 = all that fit) and the block slots
-        left free for the IBM chain in a runner step (default 32)."""
+        """Register budget of the current sweep kernel per parity, as resident
+        blocks per SM: 6..8 for "lean", 4..6 for "async" (fp32 storage)."""
         _check(lib().lbmb_set_sweep_variant(self.h, int(even_blocks_per_sm), int(odd_blocks_per_sm)))
 
     def autotune_sweep(self, steps_per_trial=20):

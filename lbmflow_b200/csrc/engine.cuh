@@ -412,22 +412,31 @@ struct Engine final : EngineBase {
   // Per-thread cp.async pipeline (persistent grid). `concurrent`: the sweep
   // of a runner step, running while the IBM chain runs on the side stream;
   // its grid leaves async_reserve block slots free for that chain.
-  template <int COLL, bool ODD>
-  void launch_async(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
-    constexpr int STAGES = 3;
-    auto kern = hydro_async_kernel<Q, S, COLL, ODD, STAGES>;
+  template <int COLL, bool ODD, int MINB, int STAGES>
+  void launch_async_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    auto kern = hydro_async_kernel<Q, S, COLL, ODD, STAGES, MINB>;
     const size_t smem = async_smem_bytes<Q, S, STAGES>();
     const int slot = (ODD ? 1 : 0) + (COLL == COLL_CM ? 2 : 0) + (concurrent ? 4 : 0);
     if (async_grid[slot] == 0) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
       int per_sm = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ASYNC_TILE, smem));
-      const int bps = async_bps > 0 ? std::min(async_bps, std::max(per_sm, 1)) : std::max(per_sm, 1);
-      const int64_t slots = int64_t(sm_count) * bps - (concurrent ? async_reserve : 0);
+      const int64_t slots = int64_t(sm_count) * std::max(per_sm, 1) - (concurrent ? async_reserve : 0);
       async_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, slots)));
     }
     kern<<<unsigned(async_grid[slot]), ASYNC_TILE, smem, s>>>(p, n, int(ntiles));
     CK(cudaGetLastError());
+  }
+  template <int COLL, bool ODD>
+  void launch_async(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    if constexpr (std::is_same<A, float>::value) {
+      switch (async_minb[ODD]) {
+        case 5: launch_async_mb<COLL, ODD, 5, 3>(p, s, concurrent); return;
+        case 6: launch_async_mb<COLL, ODD, 6, 2>(p, s, concurrent); return;
+        default: break;
+      }
+    }
+    launch_async_mb<COLL, ODD, HydroOccupancy<A>::MIN_BLOCKS, 3>(p, s, concurrent);
   }
 
   void set_sweep_kernel(int kind) override {
@@ -444,23 +453,26 @@ struct Engine final : EngineBase {
     invalidate_graphs();
   }
   int sweep_kernel() const override { return kernel_mode; }
-  // Blocks per SM the persistent cp.async grid is sized for (0: as many as
-  // fit). Fewer leave room on every SM for the IBM kernels of a runner step.
-  int async_bps = 0;
+  // Register budget of the fp32 cp.async sweep per parity, as resident
+  // blocks per SM (4 = 128 registers with a 3-tile ring, 5 = 96 with 3,
+  // 6 = 80 with 2); the persistent grid fills every resident slot.
+  int async_minb[2] = {4, 4};
   // Block slots the persistent cp.async grid of a runner step leaves free
   // (out of sm_count x blocks per SM): the latency-bound IBM chain on the
   // side stream runs in them while the sweep is resident, instead of
   // waiting for the whole sweep (128^3 central-moment tank on B200: 227 ->
   // 192 us per runner step with 32).
-  int async_reserve = 32;
+  const int async_reserve = 32;
 
   void set_sweep_variant(int even, int odd) override {
     if (kernel_mode == LBMB_SWEEP_ASYNC) {
-      if (even < 0 || even > 16) throw Error(LBMB_ERR_INVALID, "sweep variant: cp.async blocks per SM must be 0..16");
-      if (odd < 0 || odd > 4 * sm_count)
-        throw Error(LBMB_ERR_INVALID, "sweep variant: cp.async reserved blocks must be 0..4 x SM count");
-      async_bps = even;
-      async_reserve = odd;
+      auto ok = [](int v) { return v >= 4 && v <= 6; };
+      if (!ok(even) || !ok(odd))
+        throw Error(LBMB_ERR_INVALID, "sweep variant: cp.async resident blocks per SM must be 4, 5 or 6");
+      if (!std::is_same<A, float>::value && (even != 4 || odd != 4))
+        throw Error(LBMB_ERR_UNSUPPORTED, "sweep variant: the fp64 cp.async sweep has one register budget (4)");
+      async_minb[0] = even;
+      async_minb[1] = odd;
       for (int& g : async_grid) g = 0;
       invalidate_graphs();
       return;
@@ -746,7 +758,14 @@ struct Engine final : EngineBase {
     const bool is_f = std::is_same<A, float>::value;
     const bool uf = has_uniform_force();
     cands.push_back({LBMB_SWEEP_DIRECT, 0, 0});
-    if (wide && !uf) cands.push_back({LBMB_SWEEP_ASYNC, 0, 0});
+    if (wide && !uf) {
+      if (is_f) {
+        for (int ev = 4; ev <= 6; ++ev)
+          for (int od = 4; od <= 6; ++od) cands.push_back({LBMB_SWEEP_ASYNC, ev, od});
+      } else {
+        cands.push_back({LBMB_SWEEP_ASYNC, 4, 4});
+      }
+    }
     if (!uf) cands.push_back({LBMB_SWEEP_BULK, 0, 0});
     if (is_f && nx % 2 == 0 && !uf) {
       cands.push_back({LBMB_SWEEP_PAIR, 0, 0});
@@ -756,6 +775,7 @@ struct Engine final : EngineBase {
       for (int ev = 8; ev >= 6; --ev)
         for (int od = 8; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
     const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
+    const int ae0 = async_minb[0], ao0 = async_minb[1];
     const int par0 = parity;
     const size_t fbytes = f_alloc.n * sizeof(S);
     DevBuf<S> save;
@@ -768,6 +788,11 @@ struct Engine final : EngineBase {
         lean_minb[0] = cd.ev;
         lean_minb[1] = cd.od;
       }
+      if (cd.kind == LBMB_SWEEP_ASYNC) {
+        async_minb[0] = cd.ev;
+        async_minb[1] = cd.od;
+        for (int& g : async_grid) g = 0;
+      }
       for (int i = 0; i < 2; ++i) launch_hydro(i);  // warm-up (first launches set up grids)
       CK(cudaEventRecord(ev0, st));
       for (int i = 0; i < steps; ++i) launch_hydro(i & 1);
@@ -778,7 +803,7 @@ struct Engine final : EngineBase {
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       return double(ms) / steps;
     };
-    const double t_default = trial(Cand{kind0, ev0_, od0});
+    const double t_default = trial(kind0 == LBMB_SWEEP_ASYNC ? Cand{kind0, ae0, ao0} : Cand{kind0, ev0_, od0});
     int best = -1;
     double best_ms = 0.0;
     for (size_t i = 0; i < cands.size(); ++i) {
@@ -804,14 +829,22 @@ struct Engine final : EngineBase {
       lean_minb[0] = ev0_;
       lean_minb[1] = od0;
     }
+    if (kernel_mode == LBMB_SWEEP_ASYNC) {
+      async_minb[0] = cands[best].ev;
+      async_minb[1] = cands[best].od;
+    } else {
+      async_minb[0] = ae0;
+      async_minb[1] = ao0;
+    }
+    for (int& g : async_grid) g = 0;
     CK(cudaMemcpyAsync(f_alloc.p, save.p, fbytes, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
     parity = par0;
     invalidate_graphs();
     if (out) {
       out->kind = kernel_mode;
-      out->even_blocks_per_sm = lean_minb[0];
-      out->odd_blocks_per_sm = lean_minb[1];
+      out->even_blocks_per_sm = kernel_mode == LBMB_SWEEP_ASYNC ? async_minb[0] : lean_minb[0];
+      out->odd_blocks_per_sm = kernel_mode == LBMB_SWEEP_ASYNC ? async_minb[1] : lean_minb[1];
       out->n_trials = int32_t(cands.size());
       out->best_ms_per_step = best_ms;
       out->default_ms_per_step = t_default;

@@ -40,8 +40,11 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int Q, class S, int COLL, bool ODD, int STAGES>
-__global__ void __launch_bounds__(ASYNC_TILE, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
+// MINB: resident blocks per SM the register allocation is sized for (fp32:
+// 4 = 128 registers, 5 = 96 (102), 6 = 80 (85); the ring of STAGES x Q x 128
+// elements per block must fit MINB times in shared memory).
+template <int Q, class S, int COLL, bool ODD, int STAGES, int MINB = HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS>
+__global__ void __launch_bounds__(ASYNC_TILE, MINB)
     hydro_async_kernel(HydroParams<typename Codec<S>::A> p, int64_t ncells, int ntiles) {
   using A = typename Codec<S>::A;
   using L = Lat<Q>;

@@ -110,9 +110,7 @@ def test_runner_loop_each_kernel_matches_oracle(kind):
     g = lb.Solver((n, n, n), lattice=19, collision="trt", storage="f32", nu=nu, solid=solid)
     g.set_sweep_kernel(kind)
     if kind == "async":
-        # a persistent grid smaller than the tile count, with block slots
-        # left free for the IBM chain
-        g.set_sweep_variant(1, 100)
+        g.set_sweep_variant(5, 6)  # 96 / 80 registers (3- / 2-tile ring)
     c = o.OracleSolver((n, n, n), q=19, real_bits=32, collision="trt", nu=nu, solid=solid)
     rg = g.run_impeller(body, 40)
     rc = c.run_tank(body.positions, body.weights, body.center, body.omega, 40)
@@ -121,6 +119,16 @@ def test_runner_loop_each_kernel_matches_oracle(kind):
     fl = solid == 0
     ug, uc = g.read_moments()[1][fl], c.moments()[1][fl]
     assert np.abs(ug - uc).max() <= 1e-5 * np.abs(uc).max()
+
+
+@pytest.mark.parametrize("budget", [(4, 4), (5, 5), (6, 6), (4, 6)])
+@pytest.mark.parametrize("q,coll", [(19, "trt"), (27, "cm")])
+def test_async_register_budgets_match_oracle(budget, q, coll):
+    dims, solid, wall_u, nu = cavity(14, u_lid=0.06, re=40.0)
+    p = Pair(dims, q, "f32", collision=coll, nu=nu, solid=solid, wall_u=wall_u, smagorinsky_cs=0.1, sweep="async")
+    p.g.set_sweep_variant(*budget)
+    p.run(23)
+    p.check(solid == 0)
 
 
 def test_lean_kernel_odd_nx_matches_oracle():
@@ -153,6 +161,11 @@ def test_pair_kernel_refuses_what_it_cannot_run():
         g.set_sweep_kernel("async")
     with pytest.raises(lb.SpecError):
         g.set_sweep_kernel(9)
+    g = lb.Solver(dims, storage="f32", nu=nu, solid=solid, wall_u=wall_u)
+    g.set_sweep_kernel("async")
+    for bad in ((3, 4), (4, 7)):
+        with pytest.raises(lb.SpecError):
+            g.set_sweep_variant(*bad)
 
 
 @pytest.mark.parametrize("prec,q", [("f32", 19), ("f16", 19), ("f32", 27), ("f64", 19)])
