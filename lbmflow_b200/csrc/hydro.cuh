@@ -28,6 +28,8 @@
 //             uniform body force makes every cell forced.
 // Element offsets q * plane + cell are 32-bit (checked on the host).
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "lattice.cuh"
 
@@ -60,7 +62,32 @@ struct HydroParams {
 // the deviation populations, Pi = sum c c f - (rho - 1)/3 I - rho u u
 // (exact for the second-order equilibrium on D3Q19/D3Q27), and
 // tau_eff = (tau0 + sqrt(tau0^2 + les_c |Pi| / rho)) / 2.
-template <int Q, class A>
+//
+// FAST (fp32 only): single-instruction square roots and reciprocals (PTX
+// .approx, a few ulp) instead of the IEEE-rounded forms, which cost a
+// slow-path branch each; fp64 keeps the IEEE forms.
+template <class A>
+__device__ __forceinline__ A fast_rcp(A x) {
+  if constexpr (std::is_same<A, float>::value) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  } else {
+    return A(1) / x;
+  }
+}
+template <class A>
+__device__ __forceinline__ A fast_sqrt(A x) {
+  if constexpr (std::is_same<A, float>::value) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  } else {
+    return sqrt(x);
+  }
+}
+
+template <int Q, class A, bool FAST = false>
 __device__ __forceinline__ A les_tau(const A (&f)[Q], A rho, A ux, A uy, A uz, A les_c, A tau0) {
   using L = Lat<Q>;
   A sxx = A(0), syy = A(0), szz = A(0), sxy = A(0), sxz = A(0), syz = A(0);
@@ -80,13 +107,19 @@ __device__ __forceinline__ A les_tau(const A (&f)[Q], A rho, A ux, A uy, A uz, A
   const A d3 = (rho - A(1)) * A(1.0 / 3.0);
   const A pxx = sxx - d3 - rho * ux * ux, pyy = syy - d3 - rho * uy * uy, pzz = szz - d3 - rho * uz * uz;
   const A pxy = sxy - rho * ux * uy, pxz = sxz - rho * ux * uz, pyz = syz - rho * uy * uz;
-  const A pn = sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
-  return A(0.5) * (tau0 + sqrt(tau0 * tau0 + les_c * pn / rho));
+  const A pn2 = (pxx * pxx + pyy * pyy + pzz * pzz) + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz);
+  if constexpr (FAST) {
+    const A pn = fast_sqrt(pn2);
+    return A(0.5) * (tau0 + fast_sqrt(tau0 * tau0 + les_c * pn * fast_rcp(rho)));
+  } else {
+    const A pn = sqrt(pn2);
+    return A(0.5) * (tau0 + sqrt(tau0 * tau0 + les_c * pn / rho));
+  }
 }
 
 // Relaxation rates of one cell: the configured ones, or the LES-adjusted
 // ones (TRT keeps the magic parameter, BGK keeps omega_m = omega_p).
-template <int Q, class A>
+template <int Q, class A, bool FAST = false>
 __device__ __forceinline__ void cell_rates(const HydroParams<A>& p, const A (&f)[Q], A rho, A ux, A uy, A uz, A& op,
                                            A& om, A& cp, A& cm, A& os) {
   op = p.omega_p;
@@ -95,9 +128,14 @@ __device__ __forceinline__ void cell_rates(const HydroParams<A>& p, const A (&f)
   cm = p.cm;
   os = p.omega_shear;
   if (p.les_c > A(0)) {
-    const A te = les_tau<Q, A>(f, rho, ux, uy, uz, p.les_c, p.tau0);
-    op = A(1) / te;
-    om = p.magic > A(0) ? A(1) / (p.magic / (te - A(0.5)) + A(0.5)) : op;
+    const A te = les_tau<Q, A, FAST>(f, rho, ux, uy, uz, p.les_c, p.tau0);
+    if constexpr (FAST) {
+      op = fast_rcp(te);
+      om = p.magic > A(0) ? (te - A(0.5)) * fast_rcp(p.magic + A(0.5) * (te - A(0.5))) : op;
+    } else {
+      op = A(1) / te;
+      om = p.magic > A(0) ? A(1) / (p.magic / (te - A(0.5)) + A(0.5)) : op;
+    }
     cp = A(1) - op * A(0.5);
     cm = A(1) - om * A(0.5);
     os = op;

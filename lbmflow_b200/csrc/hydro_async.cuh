@@ -53,16 +53,15 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
   S* sm = reinterpret_cast<S*>(smem_raw);
   const int j = threadIdx.x;
   S* fb = static_cast<S*>(p.f);
-  const int64_t pl = p.plane;
+  // 32-bit element offsets relative to the cell (the engine keeps Q x plane
+  // below 2^31). P(k): slot k of the cell; T(k): slot k of the neighbour
+  // x + c_k (the odd step reads T(opp q) and writes T(q)); both depend on
+  // launch parameters only.
+  const int32_t pl = int32_t(p.plane);
   const int nx = p.nx, nxy = p.nxy;
-  auto dq = [&](int q) -> int64_t {
-    return int64_t(L::cx(q)) + int64_t(L::cy(q)) * nx + int64_t(L::cz(q)) * nxy;
-  };
-  // P(k): slot k of the cell; T(k): slot k of the neighbour x + c_k (the odd
-  // step reads T(opp q) and writes T(q)); both depend on launch parameters
-  // only.
-  auto P = [&](int k) -> int64_t { return int64_t(k) * pl; };
-  auto T = [&](int k) -> int64_t { return int64_t(k) * pl + dq(k); };
+  auto dq = [&](int q) -> int32_t { return L::cx(q) + L::cy(q) * nx + L::cz(q) * nxy; };
+  auto P = [&](int k) -> int32_t { return k * pl; };
+  auto T = [&](int k) -> int32_t { return k * pl + dq(k); };
   // Cells on a periodic face take the out-of-line generic path; all other
   // active cells go through the pipeline.
   auto piped = [&](uint8_t fl) { return !(fl & (F_SOLID | F_FORCED | F_WRAP | F_SLIP)); };
@@ -76,7 +75,7 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
         const S* src0 = fb + cell;
         if (!ODD) {
 #pragma unroll
-          for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + int64_t(q) * pl);
+          for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + P(q));
         } else {
           const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
           // a warp whose cells have no solid neighbour copies straight from
@@ -129,11 +128,11 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
       if (L::cz(q) == -1) m2 = m2 - f[q];
     }
     const A rho = A(1) + dr;
-    const A inv = A(1) / rho;
+    const A inv = fast_rcp(rho);
     const A ux = m0 * inv, uy = m1 * inv, uz = m2 * inv;
     const A z0 = A(0);
     A op, om, cp, cm, os;
-    cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
+    cell_rates<Q, A, true>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
     if constexpr (COLL == COLL_CM)
       collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, os);
     else
