@@ -18,9 +18,12 @@ namespace lbmb {
 
 constexpr int ASYNC_TILE = 128;
 
+// Shared memory per block: the population ring [stage][q][thread], then per
+// stage and thread the solid-neighbour mask (u32) and the flags (u8) the
+// copies were issued with.
 template <int Q, class S, int STAGES>
 constexpr size_t async_smem_bytes() {
-  return size_t(STAGES) * Q * ASYNC_TILE * sizeof(S);
+  return size_t(STAGES) * ASYNC_TILE * (Q * sizeof(S) + sizeof(uint32_t) + sizeof(uint8_t));
 }
 
 template <class S>
@@ -51,6 +54,8 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
   using CD = Codec<S>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* sm = reinterpret_cast<S*>(smem_raw);
+  uint32_t* smk = reinterpret_cast<uint32_t*>(smem_raw + size_t(STAGES) * Q * ASYNC_TILE * sizeof(S));
+  uint8_t* sfl = reinterpret_cast<uint8_t*>(smk + STAGES * ASYNC_TILE);
   const int j = threadIdx.x;
   S* fb = static_cast<S*>(p.f);
   // 32-bit element offsets relative to the cell (the engine keeps Q x plane
@@ -65,45 +70,66 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
   // Cells on a periodic face take the out-of-line generic path; all other
   // active cells go through the pipeline.
   auto piped = [&](uint8_t fl) { return !(fl & (F_SOLID | F_FORCED | F_WRAP | F_SLIP)); };
-  // Issue the copies of this thread's cell in tile t into ring stage s.
-  auto issue = [&](int t, int s) {
+  // Flags of this thread's cell in tile t (solid past the grid). They are
+  // loaded one tile ahead of the copies that need them, so their latency
+  // hides behind a collision.
+  auto flags_of = [&](int t) -> uint8_t {
     const int64_t cell = int64_t(t) * ASYNC_TILE + j;
-    if (t < ntiles && cell < ncells) {
-      const uint8_t fl = p.flags[cell];
-      if (piped(fl)) {
-        S* dst = sm + size_t(s) * Q * ASYNC_TILE + j;
-        const S* src0 = fb + cell;
-        if (!ODD) {
+    return (t < ntiles && cell < ncells) ? p.flags[cell] : uint8_t(F_SOLID);
+  };
+  // Issue the copies of this thread's cell in tile t (flags fl) into ring
+  // stage s; the flags and mask go to the stage's metadata for the collision.
+  auto issue = [&](int t, int s, uint8_t fl) {
+    const int64_t cell = int64_t(t) * ASYNC_TILE + j;
+    uint32_t mk = 0u;
+    if (piped(fl)) {
+      if (fl & F_BOUNDARY) mk = p.nbr[cell];
+      S* dst = sm + size_t(s) * Q * ASYNC_TILE + j;
+      const S* src0 = fb + cell;
+      if (!ODD) {
 #pragma unroll
-          for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + P(q));
+        for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + P(q));
+      } else {
+        const uint32_t mask = mk;
+        // a warp whose cells have no solid neighbour copies straight from
+        // the neighbours (warp-uniform vote); the others select per link
+        if (__all_sync(__activemask(), mask == 0u)) {
+#pragma unroll
+          for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + T(opp(q)));
         } else {
-          const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
-          // a warp whose cells have no solid neighbour copies straight from
-          // the neighbours (warp-uniform vote); the others select per link
-          if (__all_sync(__activemask(), mask == 0u)) {
 #pragma unroll
-            for (int q = 0; q < Q; ++q) cp_async_elem(dst + q * ASYNC_TILE, src0 + T(opp(q)));
-          } else {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-              const int o = opp(q);
-              cp_async_elem(dst + q * ASYNC_TILE, src0 + (((mask >> o) & 1u) ? P(q) : T(o)));
-            }
+          for (int q = 0; q < Q; ++q) {
+            const int o = opp(q);
+            cp_async_elem(dst + q * ASYNC_TILE, src0 + (((mask >> o) & 1u) ? P(q) : T(o)));
           }
         }
       }
     }
+    smk[s * ASYNC_TILE + j] = mk;
+    sfl[s * ASYNC_TILE + j] = fl;
     cp_async_commit();
   };
+  const int G = int(gridDim.x);
+  uint8_t fl_next = flags_of(int(blockIdx.x));
 #pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) issue(int(blockIdx.x) + s * int(gridDim.x), s);
+  for (int s = 0; s < STAGES - 1; ++s) {
+    const int t = int(blockIdx.x) + s * G;
+    const uint8_t fl = fl_next;
+    fl_next = flags_of(t + G);
+    issue(t, s, fl);
+  }
   int it = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-    issue(t + (STAGES - 1) * int(gridDim.x), (it + STAGES - 1) % STAGES);
+  for (int t = blockIdx.x; t < ntiles; t += G, ++it) {
+    {
+      const int tn = t + (STAGES - 1) * G;
+      const uint8_t fl = fl_next;
+      fl_next = flags_of(tn + G);
+      issue(tn, (it + STAGES - 1) % STAGES, fl);
+    }
     cp_async_wait<STAGES - 1>();
     const int64_t cell = int64_t(t) * ASYNC_TILE + j;
-    if (cell >= ncells) continue;
-    const uint8_t fl = p.flags[cell];
+    const int stage = it % STAGES;
+    const uint8_t fl = sfl[stage * ASYNC_TILE + j];
     if (fl & (F_SOLID | F_FORCED)) continue;
     if (fl & (F_WRAP | F_SLIP)) {
       const int z = int(cell / nxy);
@@ -112,7 +138,7 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
       hydro_cell_generic<Q, S, COLL, ODD, false>(p, int(r - int64_t(y) * nx), y, z, uint32_t(cell), fl);
       continue;
     }
-    const S* src = sm + size_t(it % STAGES) * Q * ASYNC_TILE + j;
+    const S* src = sm + size_t(stage) * Q * ASYNC_TILE + j;
     A f[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) f[q] = CD::ld(src + q * ASYNC_TILE);
@@ -137,7 +163,7 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
       collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, os);
     else
       collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, op, om, cp, cm);
-    const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
+    const uint32_t mask = smk[stage * ASYNC_TILE + j];
     S* dst0 = fb + cell;
     if (fl & F_MOVING) {
 #pragma unroll
