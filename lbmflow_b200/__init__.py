@@ -265,10 +265,11 @@ class Solver:
                              _d(self._wall), C.byref(h)))
         self.h = h
         self._bodies = {}
+        self._lib = L  # kept for close() during interpreter shutdown
 
     def close(self):
         if getattr(self, "h", None):
-            lib().lbmb_destroy(self.h)
+            (getattr(self, "_lib", None) or lib()).lbmb_destroy(self.h)
             self.h = None
 
     __del__ = close
@@ -455,6 +456,7 @@ class Batch:
         _check(lib().lbmb_batch_create(C.cast(hs, C.POINTER(C.c_void_p)), slots.ctypes.data_as(_i32p), self.n,
                                        C.byref(cfg._c()), C.byref(h)))
         self.h = h
+        self._lib = lib()
 
     def autotune(self, steps_per_trial=6):
         e, o, ms = C.c_int32(), C.c_int32(), C.c_double()
@@ -470,7 +472,7 @@ class Batch:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().lbmb_batch_destroy(self.h)
+            (getattr(self, "_lib", None) or lib()).lbmb_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -144,6 +144,29 @@ __global__ void __launch_bounds__(RED_BLOCK) reduce_kernel(const S* fb, int64_t 
 }
 
 // Sum block partials in block order (single thread: deterministic).
+// clear_body_force_field on the device: *nonuniform |= any slot of the
+// field differs from the base value (slot 0 when the slots cover every
+// cell, else zero), compared component-wise like the host check.
+template <class A>
+__global__ void field_uniform_kernel(const Vec4<A>* f, int64_t nslots, int full, int* nonuniform) {
+  const Vec4<A> base = full ? f[0] : Vec4<A>{A(0), A(0), A(0), A(0)};
+  int local = 0;
+  for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nslots; s += int64_t(gridDim.x) * blockDim.x) {
+    const Vec4<A> v = f[s];
+    if (!(v.x == base.x && v.y == base.y && v.z == base.z)) local = 1;
+  }
+  if (__syncthreads_or(local) && threadIdx.x == 0) atomicOr(nonuniform, 1);
+}
+
+// Zero the field whose value the cached moments hold, when the cleared
+// field was uniform (flag from field_uniform_kernel).
+template <class A>
+__global__ void field_zero_if_uniform_kernel(Vec4<A>* f, int64_t nslots, const int* nonuniform) {
+  if (*nonuniform) return;
+  for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nslots; s += int64_t(gridDim.x) * blockDim.x)
+    f[s] = Vec4<A>{A(0), A(0), A(0), A(0)};
+}
+
 static __global__ void reduce_finish_kernel(const double* part, int nblk, int width, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int k = 0; k < width; ++k) {
