@@ -239,8 +239,16 @@ __device__ __forceinline__ void cm_fwd_all(A (&K)[3][3][3], A ux, A uy, A uz) {
 // and all higher moments relax at 1, the source enters with (1 - rate/2).
 // By linearity the update is applied to the non-equilibrium part:
 //   f_out = f + T^-1 [ -R T(f - feq) + (I - R/2) T(src) ].
-template <int Q, bool FORCED, class A>
-__device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A Fx, A Fy, A Fz, A omega_shear) {
+//
+// LES_K (unforced cells, fp32 fast math): the subgrid rate comes from the
+// transformed moments. f - feq has zero raw moments of order 0 and 1 when
+// u = j / rho, so its order-2 central moments equal the raw ones, i.e. the
+// non-equilibrium stress Pi of les_tau: K200 = Pi_xx, K110 = Pi_xy, ...
+// omega_shear = 1 / tau_eff then replaces the configured rate.
+template <int Q, bool FORCED, class A, bool LES_K = false>
+__device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A Fx, A Fy, A Fz, A omega_shear,
+                                          A les_c = A(0), A tau0 = A(0)) {
+  static_assert(!(LES_K && FORCED), "the moment-based subgrid rate needs u = j / rho");
   static_assert(Q == 27, "factorised central-moment collision needs the full D3Q27 tensor basis");
   using L = Lat<Q>;
   if (!FORCED && ux == A(0) && uy == A(0) && uz == A(0)) {
@@ -263,6 +271,14 @@ __device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A
   cm_fwd_all(K, ux, uy, uz);
   // K[a][b][c] now holds the non-equilibrium central moment (a, b, c);
   // overwrite it with the post-collision increment.
+  if constexpr (LES_K) {
+    if (les_c > A(0)) {
+      const A pxx = K[2][0][0], pyy = K[0][2][0], pzz = K[0][0][2];
+      const A pxy = K[1][1][0], pxz = K[1][0][1], pyz = K[0][1][1];
+      const A pn = fast_sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
+      omega_shear = fast_rcp(A(0.5) * (tau0 + fast_sqrt(tau0 * tau0 + les_c * pn * fast_rcp(rho))));
+    }
+  }
   const A os = fmin(omega_shear * (A(1) + A(-0.16) * usq), A(2));
   const A bulk_neq = (K[2][0][0] + K[0][2][0] + K[0][0][2]) * A(1.0 / 3.0);
 #pragma unroll

@@ -157,12 +157,20 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
     const A inv = fast_rcp(rho);
     const A ux = m0 * inv, uy = m1 * inv, uz = m2 * inv;
     const A z0 = A(0);
-    A op, om, cp, cm, os;
-    cell_rates<Q, A, true>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
-    if constexpr (COLL == COLL_CM)
-      collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, os);
-    else
+    if constexpr (COLL == COLL_CM) {
+      // subgrid rate from the transformed moments (fp32), else les_tau
+      constexpr bool LK = std::is_same<A, float>::value;
+      A os = p.omega_shear;
+      if constexpr (!LK) {
+        A op, om, cp, cm;
+        cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
+      }
+      collide_cm<Q, false, A, LK>(f, rho, ux, uy, uz, z0, z0, z0, os, p.les_c, p.tau0);
+    } else {
+      A op, om, cp, cm, os;
+      cell_rates<Q, A, true>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
       collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, op, om, cp, cm);
+    }
     const uint32_t mask = smk[stage * ASYNC_TILE + j];
     S* dst0 = fb + cell;
     if (fl & F_MOVING) {
