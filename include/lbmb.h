@@ -262,7 +262,11 @@ int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, i
  *                      conditions as LBMB_SWEEP_PAIR);
  *   LBMB_SWEEP_LEAN    one cell per thread with a small register footprint
  *                      for high occupancy (TRT/BGK, fp32/fp16/bf16 storage,
- *                      no uniform body force).
+ *                      no uniform body force);
+ *   LBMB_SWEEP_WINDOW  one cell per thread, tiles of 256 cells staged in
+ *                      shared memory by 16-byte cp.async windows several
+ *                      tiles ahead (TRT/BGK or central moment, fp32/fp16/
+ *                      bf16 storage, no uniform body force).
  * A kind that cannot run the solver's configuration returns
  * LBMB_ERR_UNSUPPORTED and leaves the current kind in place. */
 typedef enum {
@@ -271,7 +275,8 @@ typedef enum {
   LBMB_SWEEP_ASYNC = 2,
   LBMB_SWEEP_PAIR = 3,
   LBMB_SWEEP_TILE = 4,
-  LBMB_SWEEP_LEAN = 5
+  LBMB_SWEEP_LEAN = 5,
+  LBMB_SWEEP_WINDOW = 6
 } lbmb_sweep_kind;
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
@@ -282,7 +287,10 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
  * (fp32 storage): the same per parity with 4 (128 registers, 3-tile ring,
  * the default), 5 (96, 3 tiles) or 6 (80, 2 tiles); its persistent grid
  * fills every resident slot, less 32 block slots in the sweep of a runner
- * step, where the IBM kernels run concurrently on a side stream. */
+ * step, where the IBM kernels run concurrently on a side stream. Window
+ * kernel: resident 256-thread blocks per SM per parity, 2 (128 registers),
+ * 3 (80) or 4 (64, 2-tile ring); default 2 for the central moment, 3 for
+ * TRT/BGK. */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

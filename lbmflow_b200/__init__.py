@@ -25,7 +25,7 @@ _i64p = C.POINTER(C.c_int64)
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6
 COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
-SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5}
+SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5, "window": 6}
 IMPELLER = {"rushton": 0, "pitched": 1, "flat_blade": 2}
 MAGIC_STD = 3.0 / 16.0
 RED_FLUID_CELLS, RED_MASS_DEV, RED_MOMENTUM = 0, 1, 2
@@ -303,13 +303,14 @@ class Solver:
         _check(lib().lbmb_sync(self.h))
 
     def set_sweep_kernel(self, kind):
-        """Pick the collide-stream kernel ("direct", "bulk", "async", "pair", "tile", "lean");
+        """Pick the collide-stream kernel ("direct", "bulk", "async", "pair", "tile", "lean", "window");
         UnsupportedError if it cannot run this configuration."""
         _check(lib().lbmb_set_sweep_kernel(self.h, SWEEP[kind] if isinstance(kind, str) else int(kind)))
 
     def set_sweep_variant(self, even_blocks_per_sm, odd_blocks_per_sm):
         """Register budget of the current sweep kernel per parity, as resident
-        blocks per SM: 6..8 for "lean", 4..6 for "async" (fp32 storage)."""
+        blocks per SM: 6..8 for "lean", 4..6 for "async" (fp32 storage), 2..4
+        for "window" (256-thread blocks)."""
         _check(lib().lbmb_set_sweep_variant(self.h, int(even_blocks_per_sm), int(odd_blocks_per_sm)))
 
     def autotune_sweep(self, steps_per_trial=20):

@@ -27,6 +27,7 @@
 #include "hydro_pair.cuh"
 #include "hydro_tile.cuh"
 #include "hydro_lean.cuh"
+#include "hydro_window.cuh"
 #include "batch.cuh"
 #include "adjoint.cuh"
 #include "ibm.cuh"
@@ -188,6 +189,8 @@ struct Engine final : EngineBase {
   int n_tiles_active = 0;
   TileDirs tile_dirs[2];
   int tile_grid[2] = {0, 0};
+  // persistent window-kernel grid per (parity, concurrent with the IBM chain)
+  int window_grid[4] = {0, 0, 0, 0};
   int tma_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // persistent cp.async grid per (parity, collision, concurrent with the IBM chain)
   int async_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -454,6 +457,8 @@ struct Engine final : EngineBase {
     if ((kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE) && !pair)
       throw Error(LBMB_ERR_UNSUPPORTED,
                   "the pair sweep needs fp32/fp16/bf16 storage, even nx and no uniform body force");
+    if (kind == LBMB_SWEEP_WINDOW && !window_ok())
+      throw Error(LBMB_ERR_UNSUPPORTED, "the window sweep needs fp32/fp16/bf16 storage and no uniform body force");
     if (kind == LBMB_SWEEP_LEAN && !lean_ok(coll))
       throw Error(LBMB_ERR_UNSUPPORTED, "the lean sweep needs TRT/BGK, fp32/fp16/bf16 storage and no uniform body force");
     kernel_mode = kind;
@@ -484,6 +489,16 @@ struct Engine final : EngineBase {
       invalidate_graphs();
       return;
     }
+    if (kernel_mode == LBMB_SWEEP_WINDOW) {
+      auto ok = [](int v) { return v >= 2 && v <= 4; };
+      if (!ok(even) || !ok(odd))
+        throw Error(LBMB_ERR_INVALID, "sweep variant: window resident blocks per SM must be 2, 3 or 4");
+      window_minb[0] = even;
+      window_minb[1] = odd;
+      for (int& g : window_grid) g = 0;
+      invalidate_graphs();
+      return;
+    }
     auto ok = [](int v) { return v >= 6 && v <= 8; };
     if (!ok(even) || !ok(odd)) throw Error(LBMB_ERR_INVALID, "sweep variant: resident blocks per SM must be 6, 7 or 8");
     lean_minb[0] = even;
@@ -491,6 +506,8 @@ struct Engine final : EngineBase {
     invalidate_graphs();
   }
   bool has_uniform_force() const { return cfg.force[0] != 0.0 || cfg.force[1] != 0.0 || cfg.force[2] != 0.0; }
+
+  bool window_ok() const { return std::is_same<A, float>::value && !has_uniform_force(); }
 
   bool lean_ok(int coll_kind) const {
     return std::is_same<A, float>::value && coll_kind == COLL_TRT && !has_uniform_force();
@@ -549,6 +566,43 @@ struct Engine final : EngineBase {
     CK(cudaStreamSynchronize(st));
   }
 
+  // Register budget of the window kernel per parity, as resident blocks of
+  // TILE_CELLS threads per SM (2 = 128 registers, 3 = 80, 4 = 64 with a
+  // 2-deep ring); 0 = the default for the collision (CM 2, TRT 3).
+  int window_minb[2] = {0, 0};
+
+  template <int COLL, bool ODD, int MINB>
+  void launch_window_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
+      constexpr int STAGES = MINB >= 4 ? 2 : 3;
+      auto kern = hydro_window_kernel<Q, S, ODD, STAGES, COLL, MINB>;
+      const size_t smem = window_smem_bytes<Q, S, STAGES>();
+      const int slot = (ODD ? 1 : 0) + (concurrent ? 2 : 0);
+      if (window_grid[slot] == 0) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_CELLS, smem));
+        // in a runner step, leave the same thread slots free for the IBM
+        // chain as the cp.async grid does
+        const int64_t reserve = concurrent ? int64_t(async_reserve) * ASYNC_TILE / TILE_CELLS : 0;
+        const int64_t slots = int64_t(sm_count) * std::max(per_sm, 1) - reserve;
+        window_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(n_tiles_active, slots)));
+      }
+      if (n_tiles_active == 0) return;
+      kern<<<unsigned(window_grid[slot]), TILE_CELLS, smem, s>>>(p, tile_list.p, n_tiles_active, tile_dirs[ODD]);
+      CK(cudaGetLastError());
+    }
+  }
+  template <int COLL, bool ODD>
+  void launch_window(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    const int mb = window_minb[ODD] ? window_minb[ODD] : (COLL == COLL_CM ? 2 : 3);
+    switch (mb) {
+      case 2: launch_window_mb<COLL, ODD, 2>(p, s, concurrent); break;
+      case 4: launch_window_mb<COLL, ODD, 4>(p, s, concurrent); break;
+      default: launch_window_mb<COLL, ODD, 3>(p, s, concurrent); break;
+    }
+  }
+
   template <bool ODD, int COLL>
   void launch_tile(const HydroParams<A>& p, cudaStream_t s) {
     if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
@@ -581,6 +635,8 @@ struct Engine final : EngineBase {
     if (main_grid) {
       if (kernel_mode == LBMB_SWEEP_PAIR && pair_ok(p, COLL)) {
         launch_pair<ODD, COLL>(p, s);
+      } else if (kernel_mode == LBMB_SWEEP_WINDOW && window_ok() && !p.uniform_force) {
+        launch_window<COLL, ODD>(p, s, !cells);
       } else if (kernel_mode == LBMB_SWEEP_TILE && pair_ok(p, COLL)) {
         launch_tile<ODD, COLL>(p, s);
       } else if (kernel_mode == LBMB_SWEEP_LEAN && lean_ok(COLL) && !p.uniform_force) {
@@ -778,11 +834,17 @@ struct Engine final : EngineBase {
       cands.push_back({LBMB_SWEEP_PAIR, 0, 0});
       cands.push_back({LBMB_SWEEP_TILE, 0, 0});
     }
+    if (window_ok()) {
+      const int hi = coll == COLL_CM ? 3 : 4;
+      for (int ev = 2; ev <= hi; ++ev)
+        for (int od = 2; od <= hi; ++od) cands.push_back({LBMB_SWEEP_WINDOW, ev, od});
+    }
     if (lean_ok(coll))
       for (int ev = 8; ev >= 6; --ev)
         for (int od = 8; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
     const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
     const int ae0 = async_minb[0], ao0 = async_minb[1];
+    const int we0 = window_minb[0], wo0 = window_minb[1];
     const int par0 = parity;
     const size_t fbytes = f_alloc.n * sizeof(S);
     DevBuf<S> save;
@@ -800,6 +862,11 @@ struct Engine final : EngineBase {
         async_minb[1] = cd.od;
         for (int& g : async_grid) g = 0;
       }
+      if (cd.kind == LBMB_SWEEP_WINDOW) {
+        window_minb[0] = cd.ev;
+        window_minb[1] = cd.od;
+        for (int& g : window_grid) g = 0;
+      }
       for (int i = 0; i < 2; ++i) launch_hydro(i);  // warm-up (first launches set up grids)
       CK(cudaEventRecord(ev0, st));
       for (int i = 0; i < steps; ++i) launch_hydro(i & 1);
@@ -810,7 +877,9 @@ struct Engine final : EngineBase {
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       return double(ms) / steps;
     };
-    const double t_default = trial(kind0 == LBMB_SWEEP_ASYNC ? Cand{kind0, ae0, ao0} : Cand{kind0, ev0_, od0});
+    const double t_default = trial(kind0 == LBMB_SWEEP_ASYNC    ? Cand{kind0, ae0, ao0}
+                                   : kind0 == LBMB_SWEEP_WINDOW ? Cand{kind0, we0, wo0}
+                                                                : Cand{kind0, ev0_, od0});
     int best = -1;
     double best_ms = 0.0;
     for (size_t i = 0; i < cands.size(); ++i) {
@@ -843,15 +912,26 @@ struct Engine final : EngineBase {
       async_minb[0] = ae0;
       async_minb[1] = ao0;
     }
+    if (kernel_mode == LBMB_SWEEP_WINDOW) {
+      window_minb[0] = cands[best].ev;
+      window_minb[1] = cands[best].od;
+    } else {
+      window_minb[0] = we0;
+      window_minb[1] = wo0;
+    }
     for (int& g : async_grid) g = 0;
+    for (int& g : window_grid) g = 0;
     CK(cudaMemcpyAsync(f_alloc.p, save.p, fbytes, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
     parity = par0;
     invalidate_graphs();
     if (out) {
       out->kind = kernel_mode;
-      out->even_blocks_per_sm = kernel_mode == LBMB_SWEEP_ASYNC ? async_minb[0] : lean_minb[0];
-      out->odd_blocks_per_sm = kernel_mode == LBMB_SWEEP_ASYNC ? async_minb[1] : lean_minb[1];
+      const int* mb = kernel_mode == LBMB_SWEEP_ASYNC    ? async_minb
+                      : kernel_mode == LBMB_SWEEP_WINDOW ? window_minb
+                                                         : lean_minb;
+      out->even_blocks_per_sm = mb[0];
+      out->odd_blocks_per_sm = mb[1];
       out->n_trials = int32_t(cands.size());
       out->best_ms_per_step = best_ms;
       out->default_ms_per_step = t_default;

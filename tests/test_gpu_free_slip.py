@@ -35,7 +35,7 @@ def test_half_channel_matches_oracle(q, coll):
     p.check(solid == 0)
 
 
-@pytest.mark.parametrize("kind", ["direct", "bulk", "async", "pair", "tile", "lean"])
+@pytest.mark.parametrize("kind", ["direct", "bulk", "async", "pair", "tile", "lean", "window"])
 @pytest.mark.parametrize("q,coll", [(19, "trt"), (27, "cm")])
 def test_closed_box_each_kernel_matches_oracle(kind, q, coll):
     # walls on every face, free-slip top, a swirl from a seeded state: no

@@ -15,7 +15,7 @@ from cases import Pair, cavity, tgv_fields
 
 pytestmark = pytest.mark.gpu
 
-KINDS = ["direct", "bulk", "async", "pair", "tile", "lean"]
+KINDS = ["direct", "bulk", "async", "pair", "tile", "lean", "window"]
 
 
 def supported(kind, q, coll, prec, nx=14, force=False):
@@ -23,6 +23,8 @@ def supported(kind, q, coll, prec, nx=14, force=False):
         return False
     if kind == "lean":
         return coll in ("trt", "bgk") and prec in ("f32", "f16", "bf16") and not force
+    if kind == "window":
+        return prec in ("f32", "f16", "bf16") and not force
     if kind in ("pair", "tile"):
         return prec in ("f32", "f16", "bf16") and nx % 2 == 0 and not force and (coll != "cm" or q == 27)
     return True
@@ -44,7 +46,7 @@ def test_cavity_each_kernel_matches_oracle(kind, q, coll, steps):
     p.check(solid == 0)
 
 
-@pytest.mark.parametrize("kind", ["async", "pair", "tile", "lean"])
+@pytest.mark.parametrize("kind", ["async", "pair", "tile", "lean", "window"])
 @pytest.mark.parametrize("q", [19, 27])
 def test_smagorinsky_each_kernel_matches_oracle(kind, q):
     dims, solid, wall_u, nu = cavity(14, u_lid=0.08, re=2000.0)
@@ -53,7 +55,7 @@ def test_smagorinsky_each_kernel_matches_oracle(kind, q):
     p.check(solid == 0)
 
 
-@pytest.mark.parametrize("kind", ["async", "pair", "tile"])
+@pytest.mark.parametrize("kind", ["async", "pair", "tile", "window"])
 def test_smagorinsky_central_moment_each_kernel(kind):
     dims, solid, wall_u, nu = cavity(14, u_lid=0.08, re=2000.0)
     p = Pair(dims, 27, "f32", collision="cm", nu=nu, solid=solid, wall_u=wall_u, smagorinsky_cs=0.17, sweep=kind)
@@ -73,7 +75,8 @@ def test_periodic_tgv_each_kernel(kind):
 
 
 @pytest.mark.parametrize("kind,q,coll", [("pair", 19, "trt"), ("tile", 19, "trt"), ("lean", 19, "trt"),
-                                         ("pair", 27, "cm"), ("tile", 27, "cm")])
+                                         ("window", 19, "trt"), ("pair", 27, "cm"), ("tile", 27, "cm"),
+                                         ("window", 27, "cm")])
 @pytest.mark.parametrize("prec", ["f16", "bf16"])
 def test_pair_kernel_low_precision_matches_direct(prec, kind, q, coll):
     # Same storage, two kernels: the 16-bit rounding happens at the same
@@ -96,7 +99,7 @@ def test_pair_kernel_low_precision_matches_direct(prec, kind, q, coll):
     assert l2 < {"f16": 5e-3, "bf16": 5e-2}[prec], l2
 
 
-@pytest.mark.parametrize("kind", ["pair", "tile", "lean", "direct", "bulk", "async"])
+@pytest.mark.parametrize("kind", ["pair", "tile", "lean", "direct", "bulk", "async", "window"])
 def test_runner_loop_each_kernel_matches_oracle(kind):
     from oracle import oracle as o
     n = 28
@@ -111,6 +114,8 @@ def test_runner_loop_each_kernel_matches_oracle(kind):
     g.set_sweep_kernel(kind)
     if kind == "async":
         g.set_sweep_variant(5, 6)  # 96 / 80 registers (3- / 2-tile ring)
+    if kind == "window":
+        g.set_sweep_variant(4, 2)  # 64 registers (2-tile ring) / 128
     c = o.OracleSolver((n, n, n), q=19, real_bits=32, collision="trt", nu=nu, solid=solid)
     rg = g.run_impeller(body, 40)
     rc = c.run_tank(body.positions, body.weights, body.center, body.omega, 40)
@@ -131,11 +136,27 @@ def test_async_register_budgets_match_oracle(budget, q, coll):
     p.check(solid == 0)
 
 
-def test_lean_kernel_odd_nx_matches_oracle():
+@pytest.mark.parametrize("kind,q,coll", [("lean", 19, "trt"), ("window", 19, "trt"), ("window", 27, "cm")])
+def test_odd_nx_matches_oracle(kind, q, coll):
     dims, solid, wall_u, nu = cavity(13, u_lid=0.06, re=40.0)
-    p = Pair(dims, 19, "f32", nu=nu, solid=solid, wall_u=wall_u, sweep="lean")
+    p = Pair(dims, q, "f32", collision=coll, nu=nu, solid=solid, wall_u=wall_u, sweep=kind)
     p.run(21)
     p.check(solid == 0)
+
+
+@pytest.mark.parametrize("budget", [(2, 2), (3, 3), (4, 4), (2, 4)])
+@pytest.mark.parametrize("prec", ["f32", "f16"])
+def test_window_register_budgets(budget, prec):
+    dims, solid, wall_u, nu = cavity(14, u_lid=0.06, re=40.0)
+    a = lb.Solver(dims, lattice=19, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
+    b = lb.Solver(dims, lattice=19, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
+    a.set_sweep_kernel("lean")
+    b.set_sweep_kernel("window")
+    b.set_sweep_variant(*budget)
+    a.run(31)
+    b.run(31)
+    ua, ub = a.read_moments()[1], b.read_moments()[1]
+    assert np.abs(ua - ub)[solid == 0].max() <= 1e-5 * np.abs(ua).max()
 
 
 def test_pair_kernel_refuses_what_it_cannot_run():
@@ -147,12 +168,13 @@ def test_pair_kernel_refuses_what_it_cannot_run():
     assert g.sweep_kernel not in ("pair", "tile")
     dims, solid, wall_u, nu = cavity(14, re=40.0)
     g = lb.Solver(dims, storage="f32", nu=nu, solid=solid, wall_u=wall_u, force=(1e-6, 0, 0))
-    for kind in ("pair", "lean"):
+    for kind in ("pair", "lean", "window"):
         with pytest.raises(lb.UnsupportedError):
             g.set_sweep_kernel(kind)
     g = lb.Solver(dims, storage="f64", nu=nu, solid=solid, wall_u=wall_u)
-    with pytest.raises(lb.UnsupportedError):
-        g.set_sweep_kernel("pair")
+    for kind in ("pair", "window"):
+        with pytest.raises(lb.UnsupportedError):
+            g.set_sweep_kernel(kind)
     g = lb.Solver(dims, lattice=27, collision="cm", storage="f32", nu=nu, solid=solid, wall_u=wall_u)
     with pytest.raises(lb.UnsupportedError):
         g.set_sweep_kernel("lean")
