@@ -289,8 +289,8 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
  * fills every resident slot, less 32 block slots in the sweep of a runner
  * step, where the IBM kernels run concurrently on a side stream. Window
  * kernel: resident 256-thread blocks per SM per parity, 2 (128 registers),
- * 3 (80) or 4 (64, 2-tile ring); default 2 for the central moment, 3 for
- * TRT/BGK. */
+ * 3 (80) or 4 (64), with a tile ring of 3 where shared memory allows, else
+ * 2; default 2 for the central moment, 3 for TRT/BGK. */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

@@ -252,9 +252,9 @@ struct Engine final : EngineBase {
     ntiles = ceil_div(n, TMA_TILE);
     rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
     // default sweep: the lean kernel where it applies (TRT/BGK, fp32/16-bit
-    // storage, no uniform force), else cp.async (4/8-byte storage) or direct
-    // loads
-    if (sizeof(S) < 4) kernel_mode = LBMB_SWEEP_DIRECT;
+    // storage, no uniform force), else cp.async (4/8-byte storage), the
+    // window kernel (16-bit storage) or direct loads (uniform force)
+    if (sizeof(S) < 4) kernel_mode = window_ok() ? LBMB_SWEEP_WINDOW : LBMB_SWEEP_DIRECT;
     if (lean_ok(coll)) kernel_mode = LBMB_SWEEP_LEAN;
     red_blocks = int(std::min<int64_t>(ceil_div(n, RED_BLOCK), 1184));
     red_part.alloc(size_t(red_blocks) * 5);
@@ -567,14 +567,15 @@ struct Engine final : EngineBase {
   }
 
   // Register budget of the window kernel per parity, as resident blocks of
-  // TILE_CELLS threads per SM (2 = 128 registers, 3 = 80, 4 = 64 with a
-  // 2-deep ring); 0 = the default for the collision (CM 2, TRT 3).
+  // TILE_CELLS threads per SM (2 = 128 registers, 3 = 80, 4 = 64; ring
+  // depth from window_stages); 0 = the default for the collision (CM 2,
+  // TRT 3).
   int window_minb[2] = {0, 0};
 
   template <int COLL, bool ODD, int MINB>
   void launch_window_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
     if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
-      constexpr int STAGES = MINB >= 4 ? 2 : 3;
+      constexpr int STAGES = window_stages<Q, S, MINB>();
       auto kern = hydro_window_kernel<Q, S, ODD, STAGES, COLL, MINB>;
       const size_t smem = window_smem_bytes<Q, S, STAGES>();
       const int slot = (ODD ? 1 : 0) + (concurrent ? 2 : 0);

@@ -26,6 +26,16 @@ constexpr size_t window_smem_bytes() {
   return size_t(STAGES) * Q * TileWin<S>::LEN * sizeof(S);
 }
 
+// Ring depth for MINB resident blocks: 3 window sets where MINB x 3 fit in
+// about 200 KB of shared memory per SM, else 2; 2 at 4 blocks per SM (on
+// B200, deeper rings at 4 blocks ran slower).
+template <int Q, class S, int MINB>
+constexpr int window_stages() {
+  const size_t per = window_smem_bytes<Q, S, 1>();
+  const size_t fit = size_t(200 * 1024) / (size_t(MINB) * per);
+  return (MINB < 4 && fit >= 3) ? 3 : 2;
+}
+
 // MINB: resident blocks of TILE_CELLS threads per SM the register
 // allocation is sized for (2 = 128 registers, 3 = 85 -> 80, 4 = 64).
 template <int Q, class S, bool ODD, int STAGES, int COLL, int MINB>
