@@ -13,8 +13,121 @@
 // for the instruction cache. Requires 4- or 8-byte population storage.
 #pragma once
 #include "hydro.cuh"
+#include "hydro_pair.cuh"
 
 namespace lbmb {
+
+// D3Q27 central-moment collision of one fp32 cell (no force) with the
+// x-opposite populations (-1, j, k) and (+1, j, k) of the 3 x 3 x 3 tensor
+// held together in a float2 (FP[j][k] = (f(-1, j-1, k-1), f(+1, j-1, k-1)),
+// F1[j][k] = f(0, j-1, k-1)): the equilibrium of both, the z and y passes of
+// the factorised transform and the final increment run as packed FFMA2 /
+// FADD2 / FMUL2 on the pairs, the x pass and the relaxation in scalar form.
+// Same operator as collide_cm<27, false, float, true> (the subgrid rate from
+// the transformed order-2 moments), with the packed operation order.
+__device__ __forceinline__ void collide_cm_x2(float2 (&FP)[3][3], float (&F1)[3][3], float rho, float ux, float uy,
+                                              float uz, float omega_shear, float les_c, float tau0) {
+  using L = Lat<27>;
+  auto wgt = [](int nz) -> float {  // weight of a direction with nz nonzero components
+    return nz == 0 ? float(L::w(0)) : (nz == 1 ? float(L::w(1)) : (nz == 2 ? float(L::w(7)) : float(L::w(19))));
+  };
+  const float drho = rho - 1.f;
+  if (ux == 0.f && uy == 0.f && uz == 0.f) {
+    // exact-rest skip (kernels.rs:434-447)
+    bool exact = true;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int nz = (j != 1) + (k != 1);
+        const float e0 = float(double(wgt(nz)) * (double(rho) - 1.0));
+        const float e1 = float(double(wgt(nz + 1)) * (double(rho) - 1.0));
+        exact = exact && F1[j][k] == e0 && FP[j][k].x == e1 && FP[j][k].y == e1;
+      }
+    if (exact) return;
+  }
+  const float usq = (ux * ux + uy * uy) + uz * uz;
+  const float2 uxpm = make_float2(-ux, ux);
+  const float2 drho2 = bc2(drho), rho2 = bc2(rho), nusq2 = bc2(-1.5f * usq);
+  float2 KP[3][3];
+  float K1[3][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int nz = (j != 1) + (k != 1);
+      const float v = float(j - 1) * uy + float(k - 1) * uz;
+      {
+        const float inner = (3.f * v + (4.5f * v) * v) - 1.5f * usq;
+        K1[j][k] = F1[j][k] - wgt(nz) * (drho + rho * inner);
+      }
+      const float2 cu = add2(bc2(v), uxpm);
+      const float2 inner = fma2(cu, fma2(bc2(4.5f), cu, bc2(3.f)), nusq2);
+      KP[j][k] = sub2(FP[j][k], mul2(bc2(wgt(nz + 1)), fma2(rho2, inner, drho2)));
+    }
+  // forward: z, y (packed pairs + the c_x = 0 plane), x (scalar)
+  const float2 uz2 = bc2(uz), uy2 = bc2(uy);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    cm_fwd2(KP[j][0], KP[j][1], KP[j][2], uz2);
+    cm_fwd(K1[j][0], K1[j][1], K1[j][2], uz);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    cm_fwd2(KP[0][k], KP[1][k], KP[2][k], uy2);
+    cm_fwd(K1[0][k], K1[1][k], K1[2][k], uy);
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_fwd(KP[j][k].x, K1[j][k], KP[j][k].y, ux);
+  // central moment (a, b, c): a = 0 -> KP[b][c].x, a = 1 -> K1[b][c], a = 2 -> KP[b][c].y
+  auto km = [&](int a, int b, int c) -> float& { return a == 0 ? KP[b][c].x : (a == 1 ? K1[b][c] : KP[b][c].y); };
+  if (les_c > 0.f) {
+    const float pxx = km(2, 0, 0), pyy = km(0, 2, 0), pzz = km(0, 0, 2);
+    const float pxy = km(1, 1, 0), pxz = km(1, 0, 1), pyz = km(0, 1, 1);
+    const float pn = fast_sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz));
+    omega_shear = fast_rcp(0.5f * (tau0 + fast_sqrt(tau0 * tau0 + les_c * pn * fast_rcp(rho))));
+  }
+  const float os = fminf(omega_shear * (1.f + -0.16f * usq), 2.f);
+  const float bulk_neq = (km(2, 0, 0) + km(0, 2, 0) + km(0, 0, 2)) * (1.f / 3.f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int order = a + b + c;
+        const bool diag = order == 2 && (a == 2 || b == 2 || c == 2);
+        float& k = km(a, b, c);
+        if (order <= 1) k = 0.f;
+        else if (diag) k = -os * (k - bulk_neq) - bulk_neq;
+        else if (order == 2) k = -os * k;
+        else k = -k;
+      }
+  // backward: x (scalar), y, z (packed pairs + the c_x = 0 plane)
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cm_bwd(KP[j][k].x, K1[j][k], KP[j][k].y, ux);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    cm_bwd2(KP[0][k], KP[1][k], KP[2][k], uy2);
+    cm_bwd(K1[0][k], K1[1][k], K1[2][k], uy);
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    cm_bwd2(KP[j][0], KP[j][1], KP[j][2], uz2);
+    cm_bwd(K1[j][0], K1[j][1], K1[j][2], uz);
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      FP[j][k] = add2(FP[j][k], KP[j][k]);
+      F1[j][k] = F1[j][k] + K1[j][k];
+    }
+}
 
 constexpr int ASYNC_TILE = 128;
 
@@ -140,6 +253,64 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
     }
     const S* src = sm + size_t(stage) * Q * ASYNC_TILE + j;
     A f[Q];
+    if constexpr (COLL == COLL_CM && std::is_same<A, float>::value) {
+      // packed central-moment path: populations straight into the
+      // x-opposite pair layout
+      float2 FP[3][3];
+      float F1[3][3];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const float v = CD::ld(src + q * ASYNC_TILE);
+        const int jj = L::cy(q) + 1, kk = L::cz(q) + 1;
+        if (L::cx(q) == 0) F1[jj][kk] = v;
+        else if (L::cx(q) < 0) FP[jj][kk].x = v;
+        else FP[jj][kk].y = v;
+      }
+      float dr = 0.f, m0 = 0.f, m1 = 0.f, m2 = 0.f;
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          const float s3 = (FP[jj][kk].x + F1[jj][kk]) + FP[jj][kk].y;
+          dr += s3;
+          m0 += FP[jj][kk].y - FP[jj][kk].x;
+          if (jj == 2) m1 += s3;
+          if (jj == 0) m1 -= s3;
+          if (kk == 2) m2 += s3;
+          if (kk == 0) m2 -= s3;
+        }
+      const float rho = 1.f + dr;
+      const float inv = fast_rcp(rho);
+      collide_cm_x2(FP, F1, rho, m0 * inv, m1 * inv, m2 * inv, p.omega_shear, p.les_c, p.tau0);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int jj = L::cy(q) + 1, kk = L::cz(q) + 1;
+        f[q] = L::cx(q) == 0 ? F1[jj][kk] : (L::cx(q) < 0 ? FP[jj][kk].x : FP[jj][kk].y);
+      }
+      const uint32_t mask = smk[stage * ASYNC_TILE + j];
+      S* dst0 = fb + cell;
+      if (fl & F_MOVING) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+          if ((mask >> q) & 1u) {
+            const int o = opp(q);
+            const Vec4<A> wu = p.wall_u[cell + dq(q)];
+            const A cu = (A(L::cx(o)) * wu.x + A(L::cy(o)) * wu.y) + A(L::cz(o)) * wu.z;
+            f[q] = f[q] + ((A(6) * A(L::w(o))) * rho) * cu;
+          }
+      }
+      if (!ODD) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) CD::st(dst0 + P(opp(q)), f[q]);
+      } else if (__all_sync(__activemask(), mask == 0u)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) CD::st(dst0 + T(q), f[q]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) CD::st(dst0 + (((mask >> q) & 1u) ? P(opp(q)) : T(q)), f[q]);
+      }
+      continue;
+    }
 #pragma unroll
     for (int q = 0; q < Q; ++q) f[q] = CD::ld(src + q * ASYNC_TILE);
     A dr = A(0), m0 = A(0), m1 = A(0), m2 = A(0);
