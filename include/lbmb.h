@@ -282,7 +282,8 @@ int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
 /* Launch variant of the current sweep kernel (no reference counterpart).
  * Lean kernel: register budget per parity, as resident 128-thread blocks per
- * SM the kernel is compiled for: 8 (64 registers), 7 (72) or 6 (80); more
+ * SM the kernel is compiled for: 10 (48 registers), 9 (56), 8 (64), 7 (72)
+ * or 6 (80); more
  * registers avoid spills, fewer keep more warps resident. cp.async kernel
  * (fp32 storage): the same per parity with 4 (128 registers, 3-tile ring,
  * the default), 5 (96, 3 tiles) or 6 (80, 2 tiles); its persistent grid

@@ -309,7 +309,7 @@ class Solver:
 
     def set_sweep_variant(self, even_blocks_per_sm, odd_blocks_per_sm):
         """Register budget of the current sweep kernel per parity, as resident
-        blocks per SM: 6..8 for "lean", 4..6 for "async" (fp32 storage), 2..4
+        blocks per SM: 6..10 for "lean", 4..6 for "async" (fp32 storage), 2..4
         for "window" (256-thread blocks)."""
         _check(lib().lbmb_set_sweep_variant(self.h, int(even_blocks_per_sm), int(odd_blocks_per_sm)))
 

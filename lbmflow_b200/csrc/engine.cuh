@@ -499,8 +499,8 @@ struct Engine final : EngineBase {
       invalidate_graphs();
       return;
     }
-    auto ok = [](int v) { return v >= 6 && v <= 8; };
-    if (!ok(even) || !ok(odd)) throw Error(LBMB_ERR_INVALID, "sweep variant: resident blocks per SM must be 6, 7 or 8");
+    auto ok = [](int v) { return v >= 6 && v <= 10; };
+    if (!ok(even) || !ok(odd)) throw Error(LBMB_ERR_INVALID, "sweep variant: resident blocks per SM must be 6..10");
     lean_minb[0] = even;
     lean_minb[1] = odd;
     invalidate_graphs();
@@ -514,7 +514,8 @@ struct Engine final : EngineBase {
   }
 
   // Register budget of the lean sweep per parity (resident blocks per SM:
-  // 8 = 64 registers, 7 = 72, 6 = 80); set by lbmb_set_sweep_variant.
+  // 10 = 48 registers, 9 = 56, 8 = 64, 7 = 72, 6 = 80); set by
+  // lbmb_set_sweep_variant.
   int lean_minb[2] = {8, 6};
 
   template <bool ODD, int MINB>
@@ -530,6 +531,8 @@ struct Engine final : EngineBase {
     switch (lean_minb[ODD]) {
       case 6: launch_lean_mb<ODD, 6>(p, s); break;
       case 7: launch_lean_mb<ODD, 7>(p, s); break;
+      case 9: launch_lean_mb<ODD, 9>(p, s); break;
+      case 10: launch_lean_mb<ODD, 10>(p, s); break;
       default: launch_lean_mb<ODD, 8>(p, s); break;
     }
   }
@@ -841,8 +844,8 @@ struct Engine final : EngineBase {
         for (int od = 2; od <= hi; ++od) cands.push_back({LBMB_SWEEP_WINDOW, ev, od});
     }
     if (lean_ok(coll))
-      for (int ev = 8; ev >= 6; --ev)
-        for (int od = 8; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
+      for (int ev = 10; ev >= 6; --ev)
+        for (int od = 9; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
     const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
     const int ae0 = async_minb[0], ao0 = async_minb[1];
     const int we0 = window_minb[0], wo0 = window_minb[1];
