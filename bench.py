@@ -45,7 +45,7 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum, mean of
 # one even and one odd launch) from an ncu full-set capture of the sweep kernel
 # the autotuner picks for the form, on the tank of the given diameter.
-NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 449.3e6}
+NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 446.8e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -525,6 +525,7 @@ def run_b200(args, rank, world, local):
             extra["mixing_precision"] = mixing_study(lb, args, local)
         extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
     kname = {"lean": "hydro_lean_kernel", "pair": "hydro_pair_kernel", "tile": "hydro_tile_kernel",
+             "window": "hydro_window_kernel",
              "async": "hydro_async_kernel", "direct": "hydro_aa_kernel", "bulk": "hydro_tma_kernel"}[tune["kind"]]
     coll_name = {"cm": "central_moment", "trt": "trt"}[coll]
     res = {
@@ -616,7 +617,7 @@ def main():
     ap.add_argument("--mix-T", type=int, default=64, help="tank diameter of the mixing-time study")
     ap.add_argument("--mix-D", type=float, default=1e-2, help="scalar diffusivity of the mixing study (lattice)")
     ap.add_argument("--mix-steps", type=int, default=60000, help="step cap of the mixing study (0: skip)")
-    ap.add_argument("--sweep-kernel", default=None, choices=["direct", "bulk", "async", "pair", "tile", "lean"],
+    ap.add_argument("--sweep-kernel", default=None, choices=["direct", "bulk", "async", "pair", "tile", "lean", "window"],
                     help="use this sweep kernel instead of the autotuner's choice")
     ap.add_argument("--lid", action="store_true", help="no-slip lid (the reference's tank) instead of a free-slip top")
     ap.add_argument("--sweep-seq-steps", type=int, default=200,
