@@ -968,6 +968,50 @@ class Solver {
   }
 
   // --- force field / IBM (solver.rs:2805-2822, 3016-3282) ---
+  // Native strain rate of one cell (Solver::strain_rate_at, solver.rs:5393-
+  // 5447): Pi_neq = sum c c (f - feq(rho, u)) over the post-stream
+  // populations and the cached moments, corrected by +0.5 (uF + Fu) with
+  // the current force, scaled by -1 / (2 cs^2 rho tau_eff), tau_eff =
+  // 1 / omega_p. Order [S_xx, S_yy, S_zz, S_xy, S_xz, S_yz]; solids: zeros.
+  void strain_rate_at(size_t c, T out[6]) const {
+    for (int k = 0; k < 6; ++k) out[k] = T(0);
+    if (solid[c]) return;
+    const T r = rho[c];
+    const T u[3] = {ux[c], uy[c], uz[c]};
+    T feq[Q_MAX];
+    equilibrium<L, T>(kp, r, u, feq);
+    T pi[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    for (int q = 0; q < L::Q; ++q) {
+      const T fneq = f[q * n + c] - feq[q];
+      const T cx = kp.cr[q][0], cy = kp.cr[q][1], cz = kp.cr[q][2];
+      pi[0] = pi[0] + cx * cx * fneq;
+      pi[1] = pi[1] + cy * cy * fneq;
+      pi[2] = pi[2] + cz * cz * fneq;
+      pi[3] = pi[3] + cx * cy * fneq;
+      pi[4] = pi[4] + cx * cz * fneq;
+      pi[5] = pi[5] + cy * cz * fneq;
+    }
+    T fv[3];
+    force_at(c, fv);
+    const T half = T(0.5);
+    pi[0] = pi[0] + u[0] * fv[0];
+    pi[1] = pi[1] + u[1] * fv[1];
+    pi[2] = pi[2] + u[2] * fv[2];
+    pi[3] = pi[3] + half * (u[0] * fv[1] + u[1] * fv[0]);
+    pi[4] = pi[4] + half * (u[0] * fv[2] + u[2] * fv[0]);
+    pi[5] = pi[5] + half * (u[1] * fv[2] + u[2] * fv[1]);
+    const T tau_eff = T(1.0 / params.omega_p);
+    const T scale = -(T(1) / (T(2.0 / 3.0) * r * tau_eff));
+    for (int k = 0; k < 6; ++k) out[k] = pi[k] * scale;
+  }
+  // gamma_dot = sqrt(2 S:S) (Solver::gather_shear_rate, solver.rs:5588-5599)
+  T shear_rate_at(size_t c) const {
+    T s[6];
+    strain_rate_at(c, s);
+    const T ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2] + T(2.0) * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+    return std::sqrt(T(2.0) * ss);
+  }
+
   void clear_body_force_field() {
     if (!has_force_field) return;
     bool uniform = true;
@@ -1342,6 +1386,161 @@ inline bool mixing_time_from_cv(const double* t, const double* cv, size_t n, dou
   out[1] = t95;
   out[2] = t99;
   return true;
+}
+
+// ---------------------------------------------------------------------------
+// Velocity-gradient stress QOIs (crates/lbm-core/src/stress.rs), f64 over
+// f64 velocity fields in SI units. Cell index (z ny + y) nx + x.
+// ---------------------------------------------------------------------------
+struct StressCell {  // stress.rs:3-10
+  double s[6];
+  double gamma_dot, viscous_stress_pa, second_invariant_s2, von_mises_proxy_pa;
+};
+
+// velocity_gradient + neighbor_value (stress.rs:178-226): central
+// differences, one-sided next to a solid or the domain edge, zero when both
+// neighbours are missing, zero along an axis of extent 1. Not periodic.
+inline void stress_velocity_gradient(const int d[3], const double* const f[3], const uint8_t* solid, double dx,
+                                     long x, long y, long z, double g[3][3]) {
+  const long pos[3] = {x, y, z};
+  auto id = [&](long a, long b, long c) { return size_t((c * d[1] + b) * d[0] + a); };
+  for (int comp = 0; comp < 3; ++comp)
+    for (int axis = 0; axis < 3; ++axis) {
+      g[comp][axis] = 0.0;
+      if (d[axis] <= 1) continue;
+      auto nb = [&](int delta, double& v) {
+        long p[3] = {pos[0], pos[1], pos[2]};
+        p[axis] += delta;
+        if (p[axis] < 0 || p[axis] >= d[axis]) return false;
+        const size_t i = id(p[0], p[1], p[2]);
+        if (solid[i]) return false;
+        v = f[comp][i];
+        return true;
+      };
+      double pv = 0.0, mv = 0.0;
+      const bool hp = nb(1, pv), hm = nb(-1, mv);
+      const double own = f[comp][id(x, y, z)];
+      if (hp && hm) g[comp][axis] = (pv - mv) / (2.0 * dx);
+      else if (hp) g[comp][axis] = (pv - own) / dx;
+      else if (hm) g[comp][axis] = (own - mv) / dx;
+    }
+}
+
+// compute_stress_field (stress.rs:32-82); mu per cell.
+inline std::vector<StressCell> compute_stress_field(const int d[3], const double* ux, const double* uy,
+                                                    const double* uz, const uint8_t* solid, double dx,
+                                                    const double* mu) {
+  const size_t n = size_t(d[0]) * d[1] * d[2];
+  std::vector<StressCell> out(n, StressCell{{0, 0, 0, 0, 0, 0}, 0, 0, 0, 0});
+  const double* f[3] = {ux, uy, uz};
+  for (long z = 0; z < d[2]; ++z)
+    for (long y = 0; y < d[1]; ++y)
+      for (long x = 0; x < d[0]; ++x) {
+        const size_t i = size_t((z * d[1] + y) * d[0] + x);
+        if (solid[i]) continue;
+        double g[3][3];
+        stress_velocity_gradient(d, f, solid, dx, x, y, z, g);
+        const double s[6] = {g[0][0], g[1][1], g[2][2], 0.5 * (g[0][1] + g[1][0]), 0.5 * (g[0][2] + g[2][0]),
+                             0.5 * (g[1][2] + g[2][1])};
+        const double ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2] + 2.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+        const double gd = std::sqrt(2.0 * ss);
+        StressCell& o = out[i];
+        for (int k = 0; k < 6; ++k) o.s[k] = s[k];
+        o.gamma_dot = gd;
+        o.viscous_stress_pa = mu[i] * gd;
+        o.second_invariant_s2 = ss;
+        o.von_mises_proxy_pa = std::sqrt(3.0) * mu[i] * gd;
+      }
+  return out;
+}
+
+// percentile_sorted (stress.rs:296-309): linear interpolation between the
+// ranks floor / ceil of p (len - 1).
+inline double percentile_sorted(const std::vector<double>& s, double p) {
+  if (s.size() == 1) return s[0];
+  const double rank = p * double(s.size() - 1);
+  const size_t lo = size_t(std::floor(rank)), hi = size_t(std::ceil(rank));
+  if (lo == hi) return s[lo];
+  const double t = rank - double(lo);
+  return s[lo] * (1.0 - t) + s[hi] * t;
+}
+
+// percentile_summary (stress.rs:84-100): finite values only; false when
+// there is none. out = {p50, p90, p95, p99, max, fraction above threshold
+// (NaN without a threshold)}.
+inline bool percentile_summary(const double* v, size_t n, bool has_threshold, double threshold, double out[6]) {
+  std::vector<double> fin;
+  fin.reserve(n);
+  for (size_t i = 0; i < n; ++i)
+    if (std::isfinite(v[i])) fin.push_back(v[i]);
+  if (fin.empty()) return false;
+  std::sort(fin.begin(), fin.end());
+  double frac = std::nan("");
+  if (has_threshold) {
+    size_t above = 0;
+    for (double x : fin) above += x > threshold ? 1 : 0;
+    frac = double(above) / double(fin.size());
+  }
+  out[0] = percentile_sorted(fin, 0.50);
+  out[1] = percentile_sorted(fin, 0.90);
+  out[2] = percentile_sorted(fin, 0.95);
+  out[3] = percentile_sorted(fin, 0.99);
+  out[4] = fin.back();
+  out[5] = frac;
+  return true;
+}
+
+struct WallShear {  // WallShearProxy (stress.rs:22-30)
+  size_t cell_index;
+  double tau_w_pa, y_plus, u_parallel_m_s, y_m;
+  double normal[3];
+};
+
+// wall_shear_proxy + adjacent_wall_normal_and_velocity (stress.rs:102-294):
+// fluid cells with a solid among their 26 in-domain neighbours; normal =
+// normalised sum of the offsets to them, wall velocity = their mean; tau_w
+// = mu |u_parallel| / (dx / 2), y+ = y u_tau / nu. In cell order.
+inline std::vector<WallShear> wall_shear_proxy(const int d[3], const double* ux, const double* uy, const double* uz,
+                                               const uint8_t* solid, const double* wall_u, double dx, double rho,
+                                               double mu) {
+  std::vector<WallShear> out;
+  const double y_m = 0.5 * dx, nu = mu / rho;
+  for (long z = 0; z < d[2]; ++z)
+    for (long y = 0; y < d[1]; ++y)
+      for (long x = 0; x < d[0]; ++x) {
+        const size_t i = size_t((z * d[1] + y) * d[0] + x);
+        if (solid[i]) continue;
+        double nrm[3] = {0, 0, 0}, wu[3] = {0, 0, 0}, count = 0.0;
+        for (long dz = -1; dz <= 1; ++dz)
+          for (long dy = -1; dy <= 1; ++dy)
+            for (long dxo = -1; dxo <= 1; ++dxo) {
+              if (!dxo && !dy && !dz) continue;
+              const long a = x + dxo, b = y + dy, c = z + dz;
+              if (a < 0 || b < 0 || c < 0 || a >= d[0] || b >= d[1] || c >= d[2]) continue;
+              const size_t j = size_t((c * d[1] + b) * d[0] + a);
+              if (!solid[j]) continue;
+              nrm[0] += double(dxo);
+              nrm[1] += double(dy);
+              nrm[2] += double(dz);
+              for (int k = 0; k < 3; ++k) wu[k] += wall_u[3 * j + k];
+              count += 1.0;
+            }
+        if (count == 0.0) continue;
+        const double mag = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        if (mag == 0.0) continue;
+        for (int k = 0; k < 3; ++k) {
+          nrm[k] /= mag;
+          wu[k] /= count;
+        }
+        const double u[3] = {ux[i] - wu[0], uy[i] - wu[1], uz[i] - wu[2]};
+        const double un = u[0] * nrm[0] + u[1] * nrm[1] + u[2] * nrm[2];
+        const double t[3] = {u[0] - un * nrm[0], u[1] - un * nrm[1], u[2] - un * nrm[2]};
+        const double up = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const double tau = mu * up / y_m;
+        const double u_tau = std::sqrt(tau / rho);
+        out.push_back(WallShear{i, tau, y_m * u_tau / nu, up, y_m, {nrm[0], nrm[1], nrm[2]}});
+      }
+  return out;
 }
 
 }  // namespace lbmo

@@ -82,6 +82,13 @@ def lib():
         L.lbmo_run_tank.argtypes = [C.c_void_p, _dp, _dp, C.c_long, _dp, _dp, C.c_int, C.c_double,
                                     C.c_int, C.c_double, C.c_long, C.c_long, C.c_int, _dp, _dp,
                                     _dp, _dp]
+        L.lbmo_gather_strain_rate.argtypes = [C.c_void_p, _dp, _dp]
+        L.lbmo_compute_stress_field.argtypes = [_ip, _dp, _dp, _dp, _u8p, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.lbmo_percentile_summary.restype = C.c_int
+        L.lbmo_percentile_summary.argtypes = [_dp, C.c_long, C.c_int, C.c_double, _dp]
+        L.lbmo_wall_shear_proxy.restype = C.c_long
+        L.lbmo_wall_shear_proxy.argtypes = [_ip, _dp, _dp, _dp, _u8p, _dp, C.c_double, C.c_double, C.c_double,
+                                            C.c_long, C.POINTER(C.c_int64), _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -160,6 +167,13 @@ class OracleSolver:
         out = [np.zeros(self.n) for _ in range(4)]
         lib().lbmo_read_moments(self.h, *[_d(a) for a in out])
         return out
+
+    def strain_rate(self):
+        """Native strain rate (n x 6: xx yy zz xy xz yz) and shear rate
+        gamma_dot = sqrt(2 S:S) per cell (solver.rs:5393-5599)."""
+        s6, g = np.zeros(6 * self.n), np.zeros(self.n)
+        lib().lbmo_gather_strain_rate(self.h, _d(s6), _d(g))
+        return s6.reshape(self.n, 6), g
 
     def reduce(self, kind, axis=0):
         return lib().lbmo_reduce(self.h, kind, axis)
@@ -332,3 +346,52 @@ def equilibrium_cells(q, real_bits, rho, u):
     out = np.zeros((q, n))
     L.lbmo_equilibrium_cells(q, real_bits, n, _d(rho), _d(_as_d(u, 3 * n)), _d(out))
     return out
+
+
+def compute_stress_field(dims, ux, uy, uz, solid, dx, mu):
+    """stress.rs compute_stress_field (f64, SI fields, mu per cell or scalar):
+    dict of s (n x 6), gamma_dot, viscous_stress, second_invariant, von_mises."""
+    n = int(np.prod(dims))
+    d = (C.c_int * 3)(*[int(v) for v in dims])
+    mu = np.full(n, float(mu)) if np.isscalar(mu) else _as_d(mu, n)
+    sol = np.ascontiguousarray(solid, dtype=np.uint8)
+    out = {k: np.zeros(n) for k in ("gamma_dot", "viscous_stress", "second_invariant", "von_mises")}
+    s6 = np.zeros(6 * n)
+    lib().lbmo_compute_stress_field(d, _d(_as_d(ux, n)), _d(_as_d(uy, n)), _d(_as_d(uz, n)),
+                                    sol.ctypes.data_as(_u8p), float(dx), _d(mu), _d(s6), _d(out["gamma_dot"]),
+                                    _d(out["viscous_stress"]), _d(out["second_invariant"]), _d(out["von_mises"]))
+    out["s"] = s6.reshape(n, 6)
+    return out
+
+
+def percentile_summary(values, threshold=None):
+    """stress.rs percentile_summary: {p50, p90, p95, p99, max,
+    fraction_above_threshold} over the finite values, or None."""
+    v = _as_d(values)
+    out = np.zeros(6)
+    ok = lib().lbmo_percentile_summary(_d(v), v.size, 0 if threshold is None else 1,
+                                       0.0 if threshold is None else float(threshold), _d(out))
+    if not ok:
+        return None
+    keys = ("p50", "p90", "p95", "p99", "max", "fraction_above_threshold")
+    r = dict(zip(keys, out.tolist()))
+    if threshold is None:
+        r["fraction_above_threshold"] = None
+    return r
+
+
+def wall_shear_proxy(dims, ux, uy, uz, solid, wall_u, dx, rho, mu):
+    """stress.rs wall_shear_proxy: per wall-adjacent fluid cell (cell order)
+    cell_index, tau_w, y_plus, u_parallel, normal (x3)."""
+    n = int(np.prod(dims))
+    d = (C.c_int * 3)(*[int(v) for v in dims])
+    sol = np.ascontiguousarray(solid, dtype=np.uint8)
+    wu = _as_d(wall_u, 3 * n)
+    cap = n
+    cell = np.zeros(cap, dtype=np.int64)
+    tau, yp, up, nrm = np.zeros(cap), np.zeros(cap), np.zeros(cap), np.zeros(3 * cap)
+    k = lib().lbmo_wall_shear_proxy(d, _d(_as_d(ux, n)), _d(_as_d(uy, n)), _d(_as_d(uz, n)),
+                                    sol.ctypes.data_as(_u8p), _d(wu), float(dx), float(rho), float(mu), cap,
+                                    cell.ctypes.data_as(C.POINTER(C.c_int64)), _d(tau), _d(yp), _d(up), _d(nrm))
+    return {"cell_index": cell[:k], "tau_w": tau[:k], "y_plus": yp[:k], "u_parallel": up[:k],
+            "normal": nrm[:3 * k].reshape(k, 3)}

@@ -28,6 +28,7 @@ struct AnySolver {
   virtual int q() const = 0;
   virtual void set_smagorinsky(double cs) = 0;
   virtual void set_free_slip_top(bool on) = 0;
+  virtual void strain_rate(double* s6, double* gamma) const = 0;
 };
 
 template <class L, class T>
@@ -72,6 +73,15 @@ struct Impl final : AnySolver {
   size_t cells() const override { return s.n; }
   const uint8_t* solid() const override { return s.solid.data(); }
   int q() const override { return L::Q; }
+  void strain_rate(double* s6, double* gamma) const override {
+    for (size_t c = 0; c < s.n; ++c) {
+      T v[6];
+      s.strain_rate_at(c, v);
+      if (s6)
+        for (int k = 0; k < 6; ++k) s6[6 * c + k] = double(v[k]);
+      if (gamma) gamma[c] = double(s.shear_rate_at(c));
+    }
+  }
 };
 
 void set_err(char* err, int len, const char* msg) {
@@ -314,6 +324,47 @@ long lbmo_run_tank(void* h, const double* pos, const double* w, long nm, const d
     }
   }
   return executed;
+}
+
+// Native strain rate and shear rate of every cell (solver.rs:5464-5599).
+void lbmo_gather_strain_rate(void* h, double* s6, double* gamma) {
+  static_cast<AnySolver*>(h)->strain_rate(s6, gamma);
+}
+
+// stress.rs compute_stress_field over SI velocity fields; any output NULL.
+void lbmo_compute_stress_field(const int* dims, const double* ux, const double* uy, const double* uz,
+                               const uint8_t* solid, double dx, const double* mu, double* s6, double* gamma,
+                               double* vstress, double* s2, double* vm) {
+  const auto st = compute_stress_field(dims, ux, uy, uz, solid, dx, mu);
+  for (size_t i = 0; i < st.size(); ++i) {
+    if (s6)
+      for (int k = 0; k < 6; ++k) s6[6 * i + k] = st[i].s[k];
+    if (gamma) gamma[i] = st[i].gamma_dot;
+    if (vstress) vstress[i] = st[i].viscous_stress_pa;
+    if (s2) s2[i] = st[i].second_invariant_s2;
+    if (vm) vm[i] = st[i].von_mises_proxy_pa;
+  }
+}
+
+// stress.rs percentile_summary; 1 with out filled, 0 when no finite value.
+int lbmo_percentile_summary(const double* v, long n, int has_threshold, double threshold, double* out) {
+  return percentile_summary(v, size_t(n), has_threshold != 0, threshold, out) ? 1 : 0;
+}
+
+// stress.rs wall_shear_proxy; returns the count, fills up to capacity
+// entries (cell, tau_w, y+, |u_par|, normal x3).
+long lbmo_wall_shear_proxy(const int* dims, const double* ux, const double* uy, const double* uz,
+                           const uint8_t* solid, const double* wall_u, double dx, double rho, double mu,
+                           long capacity, int64_t* cell, double* tau, double* yplus, double* upar, double* normal) {
+  const auto w = wall_shear_proxy(dims, ux, uy, uz, solid, wall_u, dx, rho, mu);
+  for (size_t i = 0; i < w.size() && long(i) < capacity; ++i) {
+    cell[i] = int64_t(w[i].cell_index);
+    tau[i] = w[i].tau_w_pa;
+    yplus[i] = w[i].y_plus;
+    upar[i] = w[i].u_parallel_m_s;
+    for (int k = 0; k < 3; ++k) normal[3 * i + k] = w[i].normal[k];
+  }
+  return long(w.size());
 }
 
 }  // extern "C"
