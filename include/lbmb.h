@@ -171,6 +171,59 @@ int lbmb_clear_body_force_field(lbmb_solver* h);
 /* Current per-cell force field (ncells x 3, zeros where absent). */
 int lbmb_get_force_field(lbmb_solver* h, double* out);
 
+/* ---- Shear-rate and stress QOIs ----------------------------------------- */
+
+/* Solver::gather_strain_rate / gather_shear_rate (solver.rs:5464-5480,
+ * 5588-5599; per cell solver.rs:5393-5447): the native strain rate from the
+ * non-equilibrium second moment of the current post-stream populations and
+ * the cached moments, Pi_neq + 0.5 (uF + Fu), scaled by
+ * -1 / (2 cs^2 rho tau_eff) with tau_eff = 1 / omega+ (lattice units).
+ * s6 = n x 6 [S_xx, S_yy, S_zz, S_xy, S_xz, S_yz], gamma = n values of
+ * sqrt(2 S:S); either may be NULL. Solid cells report zeros. */
+int lbmb_gather_strain_rate(lbmb_solver* h, double* s6, double* gamma);
+
+/* stress.rs compute_stress_field (stress.rs:32-82) on the cached velocity in
+ * SI units (lattice velocity x dx_m / dt_s), as the bioprocess runner calls
+ * it (runner.rs:1648-1676) with a uniform viscosity mu_pa_s: central
+ * differences, one-sided next to a solid or the domain edge (not periodic),
+ * s6 = n x 6 strain-rate tensor, gamma = gamma_dot [1/s], viscous =
+ * mu gamma_dot [Pa]; any output may be NULL; solid cells report zeros. */
+int lbmb_stress_field(lbmb_solver* h, double dx_m, double dt_s, double mu_pa_s, double* s6, double* gamma,
+                      double* viscous);
+
+/* stress.rs PercentileSummary (stress.rs:12-20) with the number of finite
+ * values it is taken over; valid = 0 when there is none (the reference's
+ * None). fraction_above_threshold is NaN without a threshold. */
+typedef struct {
+  double p50, p90, p95, p99, max;
+  double fraction_above_threshold;
+  int64_t count;
+  int32_t valid;
+} lbmb_percentiles;
+
+/* The stress QOI of write_stress_and_wall_outputs (runner.rs:1648-1690):
+ * percentile_summary (stress.rs:84-100) of gamma_dot and of the viscous
+ * stress over the fluid cells, sorted on the device. Thresholds: NaN for
+ * none (the runner passes 0). device_ms (may be NULL): device time of the
+ * moments, stress field, sort and counts. */
+int lbmb_stress_summary(lbmb_solver* h, double dx_m, double dt_s, double mu_pa_s, double gamma_threshold,
+                        double tau_threshold, lbmb_percentiles* gamma, lbmb_percentiles* viscous,
+                        double* device_ms);
+
+/* stress.rs WallShearProxy (stress.rs:22-30). */
+typedef struct {
+  int64_t cell_index;
+  double tau_w_pa, y_plus, u_parallel_m_s, y_m;
+  double normal[3];
+} lbmb_wall_shear;
+
+/* stress.rs wall_shear_proxy (stress.rs:102-165, 228-294): every fluid cell
+ * with a solid among its 26 in-domain neighbours, in cell order; the wall
+ * velocity is the solver's wall velocity x dx_m / dt_s. Writes up to
+ * capacity entries to out (may be NULL) and the total to *count. */
+int lbmb_wall_shear_proxy(lbmb_solver* h, double dx_m, double dt_s, double rho_kg_m3, double mu_pa_s,
+                          lbmb_wall_shear* out, int64_t capacity, int64_t* count);
+
 /* RotatingBody::from_markers (rotating_ibm.rs:32-58): upload body `body`
  * (0-based slot): n markers at lattice coordinates (n x 3), quadrature
  * weights, rotation centre and angular velocity (rad/step). */

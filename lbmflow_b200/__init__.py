@@ -41,6 +41,7 @@ EXPORTS = (
     "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
     "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
     "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy", "lbmb_adjoint_torque",
+    "lbmb_gather_strain_rate", "lbmb_stress_field", "lbmb_stress_summary", "lbmb_wall_shear_proxy",
 )
 
 
@@ -103,6 +104,24 @@ class _IbmDiag(C.Structure):
                 ("momentum_error_rel", C.c_double)]
 
 
+class _Percentiles(C.Structure):
+    _fields_ = [("p50", C.c_double), ("p90", C.c_double), ("p95", C.c_double), ("p99", C.c_double),
+                ("max", C.c_double), ("fraction_above_threshold", C.c_double), ("count", C.c_int64),
+                ("valid", C.c_int32)]
+
+    def as_dict(self):
+        if not self.valid:
+            return None
+        f = self.fraction_above_threshold
+        return {"p50": self.p50, "p90": self.p90, "p95": self.p95, "p99": self.p99, "max": self.max,
+                "fraction_above_threshold": None if np.isnan(f) else f, "count": self.count}
+
+
+class _WallShear(C.Structure):
+    _fields_ = [("cell_index", C.c_int64), ("tau_w_pa", C.c_double), ("y_plus", C.c_double),
+                ("u_parallel_m_s", C.c_double), ("y_m", C.c_double), ("normal", C.c_double * 3)]
+
+
 class _TankSpec(C.Structure):
     _fields_ = [("dims", C.c_int32 * 3), ("dx_m", C.c_double), ("vessel_diameter_m", C.c_double),
                 ("liquid_height_m", C.c_double), ("baffle_count", C.c_int32),
@@ -151,6 +170,12 @@ def lib():
         L.lbmb_build_stirred_tank.argtypes = [C.POINTER(_TankSpec), _u8p, _u8p, _dp, _dp, _dp, C.c_int64,
                                               _i64p, _dp, _dp]
         L.lbmb_sync.argtypes = [vp]
+        L.lbmb_gather_strain_rate.argtypes = [vp, _dp, _dp]
+        L.lbmb_stress_field.argtypes = [vp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
+        L.lbmb_stress_summary.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                          C.POINTER(_Percentiles), C.POINTER(_Percentiles), _dp]
+        L.lbmb_wall_shear_proxy.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                            C.POINTER(_WallShear), C.c_int64, _i64p]
         L.lbmb_set_sweep_kernel.argtypes = [vp, C.c_int32]
         L.lbmb_get_sweep_kernel.argtypes = [vp, _i32p]
         L.lbmb_set_sweep_variant.argtypes = [vp, C.c_int32, C.c_int32]
@@ -360,6 +385,50 @@ class Solver:
         return np.array([self.reduce(RED_MOMENTUM, a) for a in range(3)])
 
     # --- forcing / IBM ------------------------------------------------------
+    # --- shear-rate and stress QOIs ---------------------------------------
+    def strain_rate(self):
+        """Native strain rate (n x 6: xx yy zz xy xz yz) and shear rate
+        sqrt(2 S:S) per cell in lattice units (Solver::gather_strain_rate /
+        gather_shear_rate, solver.rs:5464-5599)."""
+        s6, g = np.empty(6 * self.n), np.empty(self.n)
+        _check(lib().lbmb_gather_strain_rate(self.h, _d(s6), _d(g)))
+        return s6.reshape(self.n, 6), g
+
+    def stress_field(self, dx_m, dt_s, mu_pa_s):
+        """stress.rs compute_stress_field on the SI velocity (u x dx/dt):
+        strain-rate tensor (n x 6), gamma_dot [1/s], viscous stress [Pa]."""
+        s6, g, v = np.empty(6 * self.n), np.empty(self.n), np.empty(self.n)
+        _check(lib().lbmb_stress_field(self.h, float(dx_m), float(dt_s), float(mu_pa_s), _d(s6), _d(g), _d(v)))
+        return {"s": s6.reshape(self.n, 6), "gamma_dot": g, "viscous_stress": v}
+
+    def stress_summary(self, dx_m, dt_s, mu_pa_s, gamma_threshold=0.0, tau_threshold=0.0):
+        """Percentile summaries of gamma_dot and viscous stress over the fluid
+        cells (runner.rs:1648-1690; thresholds None for none). Returns
+        (gamma, viscous, device_ms); a summary is None without fluid values."""
+        pg, pt, ms = _Percentiles(), _Percentiles(), C.c_double()
+        tg = float("nan") if gamma_threshold is None else float(gamma_threshold)
+        tt = float("nan") if tau_threshold is None else float(tau_threshold)
+        _check(lib().lbmb_stress_summary(self.h, float(dx_m), float(dt_s), float(mu_pa_s), tg, tt, C.byref(pg),
+                                         C.byref(pt), C.byref(ms)))
+        return pg.as_dict(), pt.as_dict(), ms.value
+
+    def wall_shear_proxy(self, dx_m, dt_s, rho_kg_m3, mu_pa_s):
+        """stress.rs wall_shear_proxy: wall-adjacent fluid cells in cell order
+        with tau_w [Pa], y+, |u_parallel| [m/s] and the unit wall normal."""
+        cnt = C.c_int64()
+        _check(lib().lbmb_wall_shear_proxy(self.h, float(dx_m), float(dt_s), float(rho_kg_m3), float(mu_pa_s),
+                                           None, 0, C.byref(cnt)))
+        k = cnt.value
+        buf = (_WallShear * max(k, 1))()
+        _check(lib().lbmb_wall_shear_proxy(self.h, float(dx_m), float(dt_s), float(rho_kg_m3), float(mu_pa_s),
+                                           buf, k, C.byref(cnt)))
+        a = np.ctypeslib.as_array(buf)[:k] if k else None
+        if k == 0:
+            return {"cell_index": np.zeros(0, np.int64), "tau_w": np.zeros(0), "y_plus": np.zeros(0),
+                    "u_parallel": np.zeros(0), "normal": np.zeros((0, 3))}
+        return {"cell_index": a["cell_index"].copy(), "tau_w": a["tau_w_pa"].copy(), "y_plus": a["y_plus"].copy(),
+                "u_parallel": a["u_parallel_m_s"].copy(), "normal": np.array(a["normal"]).reshape(k, 3)}
+
     def clear_body_force_field(self):
         _check(lib().lbmb_clear_body_force_field(self.h))
 

@@ -32,6 +32,7 @@
 #include "adjoint.cuh"
 #include "ibm.cuh"
 #include "scalar.cuh"
+#include "stress.cuh"
 
 namespace lbmb {
 
@@ -141,6 +142,12 @@ struct EngineBase {
   virtual BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
                                 const lbmb_ibm_config& cfg) = 0;
   virtual int64_t cells() const = 0;
+  virtual void strain_rate(double* s6, double* gamma) = 0;
+  virtual void stress_field(double dx, double dt, double mu, double* s6, double* gamma, double* viscous) = 0;
+  virtual void stress_summary(double dx, double dt, double mu, double t_gamma, double t_tau, lbmb_percentiles* pg,
+                              lbmb_percentiles* pt, double* device_ms) = 0;
+  virtual void wall_shear(double dx, double dt, double rho, double mu, lbmb_wall_shear* out, int64_t capacity,
+                          int64_t* count) = 0;
   virtual int q() const = 0;
   virtual const std::vector<uint8_t>& solid() const = 0;
   double last_total_ms = 0.0, last_hydro_ms = 0.0;
@@ -1101,6 +1108,176 @@ struct Engine final : EngineBase {
       fprev_stale = false;
     }
     CK(cudaStreamSynchronize(st));
+  }
+
+  // ---- shear-rate and stress QOIs (stress.cuh) ---------------------------
+  void strain_rate(double* s6, double* gamma) override {
+    DevBuf<double> d6, dg;
+    if (s6) d6.alloc(size_t(6) * n);
+    if (gamma) dg.alloc(size_t(n));
+    strain_rate_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
+        fp, plane, flags.p, nbr.p, nx, ny, nz, parity, fslot.p, fprev.p, fcur.p, field_present ? 1 : 0,
+        A(cfg.force[0]), A(cfg.force[1]), A(cfg.force[2]), A(1.0 / omega_p), s6 ? d6.p : nullptr,
+        gamma ? dg.p : nullptr, n);
+    CK(cudaGetLastError());
+    if (s6) CK(cudaMemcpyAsync(s6, d6.p, size_t(6) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (gamma) CK(cudaMemcpyAsync(gamma, dg.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+
+  // cached velocity moments (lattice units) into u3 = [ux | uy | uz]
+  void velocity_moments(DevBuf<double>& u3) {
+    u3.alloc(size_t(3) * n);
+    moments_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
+        fp, plane, flags.p, nbr.p, nx, ny, nz, parity, fslot.p, fprev.p, A(cfg.force[0]), A(cfg.force[1]),
+        A(cfg.force[2]), nullptr, u3.p, u3.p + n, u3.p + 2 * n, n);
+    CK(cudaGetLastError());
+  }
+  static void check_si(double dx, double dt, double mu) {
+    if (!(std::isfinite(dx) && dx > 0.0)) invalid("stress: dx_m must be finite and positive");
+    if (!(std::isfinite(dt) && dt > 0.0)) invalid("stress: dt_s must be finite and positive");
+    if (!(std::isfinite(mu) && mu > 0.0)) invalid("stress: mu_pa_s must be finite and positive");
+  }
+
+  void stress_field(double dx, double dt, double mu, double* s6, double* gamma, double* viscous) override {
+    check_si(dx, dt, mu);
+    DevBuf<double> u3, d6, dg, dv;
+    velocity_moments(u3);
+    if (s6) d6.alloc(size_t(6) * n);
+    if (gamma) dg.alloc(size_t(n));
+    if (viscous) dv.alloc(size_t(n));
+    stress_field_kernel<<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
+        u3.p, u3.p + n, u3.p + 2 * n, flags.p, nx, ny, nz, dx, dx / dt, mu, s6 ? d6.p : nullptr,
+        gamma ? dg.p : nullptr, viscous ? dv.p : nullptr, nullptr, nullptr, n);
+    CK(cudaGetLastError());
+    if (s6) CK(cudaMemcpyAsync(s6, d6.p, size_t(6) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (gamma) CK(cudaMemcpyAsync(gamma, dg.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (viscous) CK(cudaMemcpyAsync(viscous, dv.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+
+  // runner.rs:1648-1690: percentile summaries of gamma_dot and mu gamma_dot
+  // over the fluid cells (thresholds: NaN for none).
+  void stress_summary(double dx, double dt, double mu, double t_gamma, double t_tau, lbmb_percentiles* pg,
+                      lbmb_percentiles* pt, double* device_ms) override {
+    check_si(dx, dt, mu);
+    DevBuf<double> u3, key, sorted;
+    DevBuf<unsigned long long> cnt;
+    cnt.alloc(3);
+    key.alloc(size_t(n));
+    sorted.alloc(size_t(n));
+    size_t tmp_bytes = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, key.p, sorted.p, int(n), 0, 64, st));
+    DevBuf<unsigned char> tmp;
+    tmp.alloc(std::max<size_t>(tmp_bytes, 1));
+    CK(cudaMemsetAsync(cnt.p, 0, 3 * sizeof(unsigned long long), st));
+    CK(cudaEventRecord(ev0, st));
+    velocity_moments(u3);
+    stress_field_kernel<<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(u3.p, u3.p + n, u3.p + 2 * n, flags.p, nx, ny,
+                                                                    nz, dx, dx / dt, mu, nullptr, nullptr, nullptr,
+                                                                    key.p, cnt.p, n);
+    CK(cudaGetLastError());
+    CK(cub::DeviceRadixSort::SortKeys(tmp.p, tmp_bytes, key.p, sorted.p, int(n), 0, 64, st));
+    unsigned long long k = 0;
+    CK(cudaMemcpyAsync(&k, cnt.p, sizeof(k), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const bool hg = std::isfinite(t_gamma), ht = std::isfinite(t_tau);
+    if (k > 0) {
+      const unsigned g = unsigned(ceil_div(int64_t(k), 128));
+      if (hg) count_above_kernel<<<g, 128, 0, st>>>(sorted.p, int64_t(k), 1.0, t_gamma, cnt.p + 1);
+      if (ht) count_above_kernel<<<g, 128, 0, st>>>(sorted.p, int64_t(k), mu, t_tau, cnt.p + 2);
+      CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ev1, st));
+    unsigned long long above[2] = {0, 0};
+    CK(cudaMemcpyAsync(above, cnt.p + 1, sizeof(above), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventSynchronize(ev1));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (device_ms) *device_ms = ms;
+    // percentile_sorted (stress.rs:296-309) on ranks read back one by one
+    auto at = [&](int64_t i) {
+      double v = 0.0;
+      CK(cudaMemcpy(&v, sorted.p + i, sizeof(double), cudaMemcpyDeviceToHost));
+      return v;
+    };
+    auto fill = [&](lbmb_percentiles* o, double scale, bool has_t, unsigned long long nab) {
+      if (!o) return;
+      *o = lbmb_percentiles{};
+      o->count = int64_t(k);
+      o->valid = k > 0 ? 1 : 0;
+      o->fraction_above_threshold = std::nan("");
+      if (k == 0) return;
+      auto pct = [&](double p) {
+        if (k == 1) return scale * at(0);
+        const double rank = p * double(k - 1);
+        const int64_t lo = int64_t(std::floor(rank)), hi = int64_t(std::ceil(rank));
+        if (lo == hi) return scale * at(lo);
+        const double t = rank - double(lo);
+        return (scale * at(lo)) * (1.0 - t) + (scale * at(hi)) * t;
+      };
+      o->p50 = pct(0.50);
+      o->p90 = pct(0.90);
+      o->p95 = pct(0.95);
+      o->p99 = pct(0.99);
+      o->max = scale * at(int64_t(k) - 1);
+      if (has_t) o->fraction_above_threshold = double(nab) / double(k);
+    };
+    fill(pg, 1.0, hg, above[0]);
+    fill(pt, mu, ht, above[1]);
+  }
+
+  void wall_shear(double dx, double dt, double rho, double mu, lbmb_wall_shear* out, int64_t capacity,
+                  int64_t* count) override {
+    check_si(dx, dt, mu);
+    if (!(std::isfinite(rho) && rho > 0.0)) invalid("wall shear: rho_kg_m3 must be finite and positive");
+    DevBuf<double> u3, tau, yp, up, nrm, vals;
+    DevBuf<uint8_t> flag;
+    DevBuf<int64_t> idx, sel;
+    DevBuf<int> nsel;
+    velocity_moments(u3);
+    tau.alloc(size_t(n));
+    yp.alloc(size_t(n));
+    up.alloc(size_t(n));
+    nrm.alloc(size_t(3) * n);
+    flag.alloc(size_t(n));
+    idx.alloc(size_t(n));
+    sel.alloc(size_t(n));
+    nsel.alloc(1);
+    const unsigned g = unsigned(ceil_div(n, 128));
+    wall_shear_kernel<A><<<g, 128, 0, st>>>(u3.p, u3.p + n, u3.p + 2 * n, flags.p, wall_u.p, nx, ny, nz, dx, dx / dt,
+                                            rho, mu, flag.p, tau.p, yp.p, up.p, nrm.p, n);
+    iota_kernel<<<g, 128, 0, st>>>(idx.p, n);
+    CK(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    CK(cub::DeviceSelect::Flagged(nullptr, tmp_bytes, idx.p, flag.p, sel.p, nsel.p, int(n), st));
+    DevBuf<unsigned char> tmp;
+    tmp.alloc(std::max<size_t>(tmp_bytes, 1));
+    CK(cub::DeviceSelect::Flagged(tmp.p, tmp_bytes, idx.p, flag.p, sel.p, nsel.p, int(n), st));
+    int m = 0;
+    CK(cudaMemcpyAsync(&m, nsel.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (count) *count = m;
+    const int64_t k = std::min<int64_t>(m, std::max<int64_t>(capacity, 0));
+    if (!out || k == 0) return;
+    vals.alloc(size_t(7) * k);
+    gather_wall_kernel<<<unsigned(ceil_div(k, 128)), 128, 0, st>>>(sel.p, k, tau.p, yp.p, up.p, nrm.p, vals.p);
+    CK(cudaGetLastError());
+    std::vector<int64_t> hi(static_cast<size_t>(k));
+    std::vector<double> hv(static_cast<size_t>(7 * k));
+    CK(cudaMemcpyAsync(hi.data(), sel.p, size_t(k) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hv.data(), vals.p, size_t(7) * k * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < k; ++i) {
+      lbmb_wall_shear& w = out[i];
+      w.cell_index = hi[size_t(i)];
+      w.tau_w_pa = hv[size_t(7 * i)];
+      w.y_plus = hv[size_t(7 * i + 1)];
+      w.u_parallel_m_s = hv[size_t(7 * i + 2)];
+      w.y_m = 0.5 * dx;
+      for (int a = 0; a < 3; ++a) w.normal[a] = hv[size_t(7 * i + 3 + a)];
+    }
   }
 
   void get_force_field(double* out) override {

@@ -256,6 +256,39 @@ int lbmb_get_force_field(lbmb_solver* h, double* out) {
   });
 }
 
+int lbmb_gather_strain_rate(lbmb_solver* h, double* s6, double* gamma) {
+  return guarded([&] {
+    NEED(h);
+    h->e->strain_rate(s6, gamma);
+  });
+}
+
+int lbmb_stress_field(lbmb_solver* h, double dx_m, double dt_s, double mu_pa_s, double* s6, double* gamma,
+                      double* viscous) {
+  return guarded([&] {
+    NEED(h);
+    h->e->stress_field(dx_m, dt_s, mu_pa_s, s6, gamma, viscous);
+  });
+}
+
+int lbmb_stress_summary(lbmb_solver* h, double dx_m, double dt_s, double mu_pa_s, double gamma_threshold,
+                        double tau_threshold, lbmb_percentiles* gamma, lbmb_percentiles* viscous,
+                        double* device_ms) {
+  return guarded([&] {
+    NEED(h);
+    h->e->stress_summary(dx_m, dt_s, mu_pa_s, gamma_threshold, tau_threshold, gamma, viscous, device_ms);
+  });
+}
+
+int lbmb_wall_shear_proxy(lbmb_solver* h, double dx_m, double dt_s, double rho_kg_m3, double mu_pa_s,
+                          lbmb_wall_shear* out, int64_t capacity, int64_t* count) {
+  return guarded([&] {
+    NEED(h);
+    if (!count) throw Error(LBMB_ERR_INVALID, "null count");
+    h->e->wall_shear(dx_m, dt_s, rho_kg_m3, mu_pa_s, out, capacity, count);
+  });
+}
+
 int lbmb_ibm_set_body(lbmb_solver* h, int32_t body, const double* pos, const double* weight, int64_t n,
                       const double center[3], const double omega[3]) {
   return guarded([&] {
