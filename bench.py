@@ -155,6 +155,38 @@ def cpu_tank_sample(dims, solid, body, nu, q=27, collision="cm", bits=32, steps=
     return n * steps / dt / 1e6, dt
 
 
+def shear_study(g, dims, solid, nu, T, q, storage):
+    """The bioprocess runner's stress QOI (runner.rs:1648-1690) on the final
+    headline state: gamma_dot and viscous-stress percentiles over the fluid
+    cells, on the device (moments, f64 finite differences, device sort) and
+    through the oracle's restatement of stress.rs on the same velocity (the
+    CPU leg, single thread). Units: a water-filled 1 m vessel (dx = 1 / T m,
+    nu = 1e-6 m^2/s, mu = 1e-3 Pa s; dt from nu_lattice = nu dt / dx^2)."""
+    from oracle import oracle as o
+    dx = 1.0 / T
+    dt = nu * dx * dx / 1.0e-6
+    mu = 1.0e-3
+    g.stress_summary(dx, dt, mu)  # warm-up (first-call set-up)
+    runs = [g.stress_summary(dx, dt, mu, 0.0, 0.0) for _ in range(3)]
+    gam, tau, _ = runs[-1]
+    dev_ms = min(r[2] for r in runs)
+    _, ux, uy, uz = g.read_moments()
+    vs = dx / dt
+    t0 = time.perf_counter()
+    ref = o.compute_stress_field(dims, ux * vs, uy * vs, uz * vs, solid, dx, mu)
+    fl = solid == 0
+    rg = o.percentile_summary(ref["gamma_dot"][fl], 0.0)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    n_fluid = int(fl.sum())
+    pop_bytes = q * {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}[storage] * n_fluid
+    return {"what": "gamma_dot / viscous-stress percentiles over fluid cells (stress.rs, runner.rs:1648-1690)",
+            "units": {"dx_m": dx, "dt_s": dt, "mu_pa_s": mu}, "fluid_cells": n_fluid,
+            "gamma_dot_1_s": gam, "viscous_stress_pa": tau, "device_ms": dev_ms,
+            "device_populations_gbs": pop_bytes / (dev_ms * 1e-3) / 1e9,
+            "cpu_ms": cpu_ms, "cpu_kind": "port (oracle restatement, 1 thread, same velocity field)",
+            "p95_rel_diff_vs_cpu": abs(gam["p95"] - rg["p95"]) / rg["p95"]}
+
+
 # ---------------------------------------------------------------------------
 # Distributed plumbing (replicas: one independent tank per GPU)
 # ---------------------------------------------------------------------------
@@ -511,8 +543,10 @@ def run_b200(args, rank, world, local):
     e2e_s = allmax(time.perf_counter() - t0, world)
     e2e_value = world * n_cells * e2e_steps / e2e_s / 1e6
     g2.close()
-    g.close()
     extra = {}
+    if world == 1 and args.shear:
+        extra["shear_qoi"] = shear_study(g, dims, solid, nu, args.tank_T, q, storage)
+    g.close()
     if args.sweep_steps > 0:
         sw = sweep_study(args, rank, world, local)
         if sw is not None:
@@ -605,6 +639,7 @@ def main():
     ap.add_argument("--collision", default="cm", choices=["cm", "trt"])
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shear", type=int, default=1, help="stress QOI study on the final state (0: skip)")
     ap.add_argument("--variants", type=int, default=1)
     ap.add_argument("--les-cs", type=float, default=0.1, help="Smagorinsky constant (0: reference operators)")
     ap.add_argument("--big-T", type=int, default=256, help="tank diameter of the throughput study")
