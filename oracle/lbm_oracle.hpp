@@ -1543,4 +1543,124 @@ inline std::vector<WallShear> wall_shear_proxy(const int d[3], const double* ux,
   return out;
 }
 
+// ---------------------------------------------------------------------------
+// Oxygen transfer and uptake sources (crates/lbm-core/src/oxygen.rs:72-216,
+// reaction.rs:57-137) over flat f64 arrays. Each returns 0 on success or an
+// error code (the reference's Err variants): 1 invalid cell volume, 2
+// invalid transfer inputs / kL, 3 invalid time step, 4 negative or
+// non-finite C_L before the uptake, 5 invalid uptake-model parameters.
+// ---------------------------------------------------------------------------
+struct OxygenDiag {  // OxygenDiagnostics (oxygen.rs:18-23)
+  size_t clipped_cells = 0;
+  double clipped_fraction = 0.0, min_before_clip = 0.0;
+};
+
+inline OxygenDiag clip_negative_concentrations(double* v, size_t n) {  // oxygen.rs:193-216
+  OxygenDiag d;
+  double mn = INFINITY;
+  for (size_t i = 0; i < n; ++i) {
+    const double before = v[i];
+    if (before < mn) mn = before;
+    if (v[i] < 0.0) {
+      v[i] = 0.0;
+      ++d.clipped_cells;
+    }
+  }
+  d.clipped_fraction = n == 0 ? 0.0 : double(d.clipped_cells) / double(n);
+  d.min_before_clip = std::isfinite(mn) ? mn : 0.0;
+  return d;
+}
+
+// henry_equilibrium (oxygen.rs:72-87); NaN on invalid input
+inline double henry_equilibrium(double h, double p) {
+  if (!(std::isfinite(h) && h > 0.0) || !(std::isfinite(p) && p >= 0.0)) return std::nan("");
+  return h * p;
+}
+
+// interfacial_area_density (oxygen.rs:89-115); NaN on invalid input
+inline double interfacial_area_density(double phi, const double g[3], double width) {
+  if (!(std::isfinite(phi) && phi >= 0.0 && phi <= 1.0) || !(std::isfinite(width) && width > 0.0))
+    return std::nan("");
+  const double ga = std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  if (!std::isfinite(ga)) return std::nan("");
+  return 6.0 * ga * phi * (1.0 - phi) * (4.0 / width);
+}
+
+struct OxygenLedger {  // OxygenFluxLedger (oxygen.rs:25-31)
+  double cumulative_mol = 0.0, last_step_mol = 0.0, source_integral_mol_s = 0.0;
+  size_t active_interface_cells = 0;
+};
+
+// apply_interfacial_flux_sources + oxygen_source_step (oxygen.rs:124-191);
+// kL of a Constant / Calibrated model.
+inline int apply_interfacial_flux_sources(double* c, const double* c_star, const double* area, const double* vol,
+                                          size_t n, double dt, double kl, OxygenLedger& ledger, OxygenDiag& diag) {
+  if (!(std::isfinite(dt) && dt >= 0.0)) return 3;
+  double integral = 0.0;
+  size_t active = 0;
+  for (size_t i = 0; i < n; ++i) {
+    if (!(std::isfinite(vol[i]) && vol[i] > 0.0)) return 1;
+    if (!(std::isfinite(c[i]) && std::isfinite(c_star[i]) && std::isfinite(area[i]) && area[i] >= 0.0)) return 2;
+    if (!(std::isfinite(kl) && kl > 0.0)) return 2;
+    const double source = kl * area[i] * (c_star[i] - c[i]);
+    if (area[i] > 0.0) ++active;
+    c[i] += source * dt;
+    integral += source * vol[i];
+  }
+  diag = clip_negative_concentrations(c, n);
+  ledger.source_integral_mol_s = integral;
+  ledger.last_step_mol = integral * dt;
+  ledger.cumulative_mol += ledger.last_step_mol;
+  ledger.active_interface_cells = active;
+  return 0;
+}
+
+struct OurModel {  // OurModel (reaction.rs:7-21); kind 0 Constant, 1 Monod, 2 CellDensityScaled
+  int kind = 0;
+  double our = 0.0, our_max = 0.0, ks = 0.0, c_ref = 0.0, specific_our = 0.0;
+};
+
+// oxygen_uptake_rate (reaction.rs:57-93): 0 and the rate, or an error code
+inline int oxygen_uptake_rate(const OurModel& m, double c, const double* density, double& rate) {
+  if (!(std::isfinite(c) && c >= 0.0)) return 4;
+  auto nonneg = [](double v) { return std::isfinite(v) && v >= 0.0; };
+  if (m.kind == 0) {
+    if (!nonneg(m.our)) return 5;
+    rate = m.our;
+  } else if (m.kind == 1) {
+    if (!nonneg(m.our_max)) return 5;
+    if (!(std::isfinite(m.ks) && m.ks > 0.0 && std::isfinite(m.c_ref) && m.c_ref > 0.0)) return 5;
+    const double cs = c / m.c_ref;
+    rate = m.our_max * cs / (m.ks + cs);
+  } else {
+    if (!nonneg(m.specific_our)) return 5;
+    if (!density || !nonneg(*density)) return 5;
+    rate = m.specific_our * *density;
+  }
+  return 0;
+}
+
+struct OurLedger {  // OurLedger (reaction.rs:23-27)
+  double cumulative_kmol_consumed = 0.0, last_step_kmol_consumed = 0.0;
+};
+
+// apply_oxygen_reaction_source (reaction.rs:95-137)
+inline int apply_oxygen_reaction_source(double* c, const double* vol, size_t n, double dt, const OurModel& m,
+                                        const double* density, OurLedger& ledger, OxygenDiag& diag) {
+  if (!(std::isfinite(dt) && dt >= 0.0)) return 3;
+  double consumed = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    if (!(std::isfinite(vol[i]) && vol[i] > 0.0)) return 1;
+    double rate = 0.0;
+    const int e = oxygen_uptake_rate(m, c[i], density ? density + i : nullptr, rate);
+    if (e) return e;
+    c[i] -= rate * dt;
+    consumed += rate * vol[i] * dt;
+  }
+  diag = clip_negative_concentrations(c, n);
+  ledger.last_step_kmol_consumed = consumed;
+  ledger.cumulative_kmol_consumed += consumed;
+  return 0;
+}
+
 }  // namespace lbmo

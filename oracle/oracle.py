@@ -89,6 +89,14 @@ def lib():
         L.lbmo_wall_shear_proxy.restype = C.c_long
         L.lbmo_wall_shear_proxy.argtypes = [_ip, _dp, _dp, _dp, _u8p, _dp, C.c_double, C.c_double, C.c_double,
                                             C.c_long, C.POINTER(C.c_int64), _dp, _dp, _dp, _dp]
+        L.lbmo_interfacial_flux.restype = C.c_int
+        L.lbmo_interfacial_flux.argtypes = [_dp, _dp, _dp, _dp, C.c_long, C.c_double, C.c_double, _dp, _dp]
+        L.lbmo_oxygen_uptake.restype = C.c_int
+        L.lbmo_oxygen_uptake.argtypes = [_dp, _dp, C.c_long, C.c_double, C.c_int, _dp, _dp, _dp, _dp]
+        L.lbmo_henry_equilibrium.restype = C.c_double
+        L.lbmo_henry_equilibrium.argtypes = [C.c_double, C.c_double]
+        L.lbmo_interfacial_area_density.restype = C.c_double
+        L.lbmo_interfacial_area_density.argtypes = [C.c_double, _dp, C.c_double]
         _lib = L
     return _lib
 
@@ -395,3 +403,53 @@ def wall_shear_proxy(dims, ux, uy, uz, solid, wall_u, dx, rho, mu):
                                     cell.ctypes.data_as(C.POINTER(C.c_int64)), _d(tau), _d(yp), _d(up), _d(nrm))
     return {"cell_index": cell[:k], "tau_w": tau[:k], "y_plus": yp[:k], "u_parallel": up[:k],
             "normal": nrm[:3 * k].reshape(k, 3)}
+
+
+OUR_KIND = {"constant": 0, "monod": 1, "cell_density_scaled": 2}
+
+
+def _diag(d):
+    return {"clipped_cells": int(d[0]), "clipped_fraction": d[1], "min_before_clip": d[2]}
+
+
+def interfacial_flux(c, c_star, area, volume, dt, kl, cumulative=0.0):
+    """oxygen.rs apply_interfacial_flux_sources on a copy of c: (c_new,
+    ledger, diag), or raises ValueError with the error code."""
+    c = _as_d(c).copy()
+    n = c.size
+    ledger = np.array([cumulative, 0.0, 0.0, 0.0])
+    diag = np.zeros(3)
+    cs = np.full(n, float(c_star)) if np.isscalar(c_star) else _as_d(c_star, n)
+    vol = np.full(n, float(volume)) if np.isscalar(volume) else _as_d(volume, n)
+    e = lib().lbmo_interfacial_flux(_d(c), _d(cs), _d(_as_d(area, n)), _d(vol), n, float(dt), float(kl), _d(ledger),
+                                    _d(diag))
+    if e:
+        raise ValueError(f"oxygen source error {e}")
+    return c, {"cumulative_mol": ledger[0], "last_step_mol": ledger[1], "source_integral_mol_s": ledger[2],
+               "active_interface_cells": int(ledger[3])}, _diag(diag)
+
+
+def oxygen_uptake(c, volume, dt, kind="constant", our=0.0, our_max=0.0, ks=0.0, c_ref=0.0, specific_our=0.0,
+                  density=None, cumulative=0.0):
+    """reaction.rs apply_oxygen_reaction_source on a copy of c."""
+    c = _as_d(c).copy()
+    n = c.size
+    vol = np.full(n, float(volume)) if np.isscalar(volume) else _as_d(volume, n)
+    ledger = np.array([cumulative, 0.0])
+    diag = np.zeros(3)
+    params = np.array([our, our_max, ks, c_ref, specific_our], dtype=np.float64)
+    dens = None if density is None else _as_d(density, n)
+    e = lib().lbmo_oxygen_uptake(_d(c), _d(vol), n, float(dt), OUR_KIND[kind], _d(params), _d(dens), _d(ledger),
+                                 _d(diag))
+    if e:
+        raise ValueError(f"reaction source error {e}")
+    return c, {"cumulative_kmol_consumed": ledger[0], "last_step_kmol_consumed": ledger[1]}, _diag(diag)
+
+
+def henry_equilibrium(h, p):
+    return lib().lbmo_henry_equilibrium(float(h), float(p))
+
+
+def interfacial_area_density(phi, grad, width):
+    return lib().lbmo_interfacial_area_density(float(phi), _d(_as_d(grad, 3)), float(width))
+

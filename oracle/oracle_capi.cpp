@@ -367,6 +367,54 @@ long lbmo_wall_shear_proxy(const int* dims, const double* ux, const double* uy, 
   return long(w.size());
 }
 
+// oxygen.rs / reaction.rs over f64 arrays (c updated in place). ledger in /
+// out: {cumulative, last step, source integral, active cells} for the
+// transfer, {cumulative, last step} for the uptake; diag out: {clipped
+// cells, clipped fraction, min before clip}. Returns 0 or the error code.
+int lbmo_interfacial_flux(double* c, const double* c_star, const double* area, const double* vol, long n, double dt,
+                          double kl, double* ledger, double* diag) {
+  OxygenLedger l;
+  l.cumulative_mol = ledger[0];
+  OxygenDiag d;
+  const int e = apply_interfacial_flux_sources(c, c_star, area, vol, size_t(n), dt, kl, l, d);
+  if (e) return e;
+  ledger[0] = l.cumulative_mol;
+  ledger[1] = l.last_step_mol;
+  ledger[2] = l.source_integral_mol_s;
+  ledger[3] = double(l.active_interface_cells);
+  diag[0] = double(d.clipped_cells);
+  diag[1] = d.clipped_fraction;
+  diag[2] = d.min_before_clip;
+  return 0;
+}
+
+int lbmo_oxygen_uptake(double* c, const double* vol, long n, double dt, int kind, const double* params,
+                       const double* density, double* ledger, double* diag) {
+  OurModel m;
+  m.kind = kind;
+  m.our = params[0];
+  m.our_max = params[1];
+  m.ks = params[2];
+  m.c_ref = params[3];
+  m.specific_our = params[4];
+  OurLedger l;
+  l.cumulative_kmol_consumed = ledger[0];
+  OxygenDiag d;
+  const int e = apply_oxygen_reaction_source(c, vol, size_t(n), dt, m, density, l, d);
+  if (e) return e;
+  ledger[0] = l.cumulative_kmol_consumed;
+  ledger[1] = l.last_step_kmol_consumed;
+  diag[0] = double(d.clipped_cells);
+  diag[1] = d.clipped_fraction;
+  diag[2] = d.min_before_clip;
+  return 0;
+}
+
+double lbmo_henry_equilibrium(double h, double p) { return henry_equilibrium(h, p); }
+double lbmo_interfacial_area_density(double phi, const double* g, double w) {
+  return interfacial_area_density(phi, g, w);
+}
+
 }  // extern "C"
 
 extern "C" {
