@@ -246,6 +246,55 @@ int lbmb_set_scalar_concentration(lbmb_solver* h, int32_t k, const double* c);
 /* Solver::gather_scalar_concentration (solver.rs:2892-2908). */
 int lbmb_gather_scalar_concentration(lbmb_solver* h, int32_t k, double* c);
 
+/* ---- Oxygen transfer and uptake sources on a scalar --------------------- */
+
+/* OxygenDiagnostics (oxygen.rs:18-23) of the negative clip. */
+typedef struct {
+  int64_t clipped_cells;
+  double clipped_fraction;
+  double min_before_clip;
+} lbmb_oxygen_diag;
+
+/* OxygenFluxLedger (oxygen.rs:25-31); cumulative_mol is read and updated. */
+typedef struct {
+  double cumulative_mol, last_step_mol, source_integral_mol_s;
+  int64_t active_interface_cells;
+} lbmb_oxygen_ledger;
+
+/* OurLedger (reaction.rs:23-27); cumulative_kmol_consumed is read and updated. */
+typedef struct {
+  double cumulative_kmol_consumed, last_step_kmol_consumed;
+} lbmb_our_ledger;
+
+/* OurModel (reaction.rs:7-21). */
+typedef enum { LBMB_OUR_CONSTANT = 0, LBMB_OUR_MONOD = 1, LBMB_OUR_CELL_DENSITY = 2 } lbmb_our_kind;
+typedef struct {
+  int32_t kind;
+  double our_kmol_m3_s;                 /* constant */
+  double our_max, ks, c_ref;            /* Monod: our_max (C/c_ref) / (ks + C/c_ref) */
+  double specific_our;                  /* cell-density scaled: specific_our x density */
+} lbmb_our_model;
+
+/* The reference's composition gather_scalar_concentration ->
+ * apply_interfacial_flux_sources (oxygen.rs:124-191, kL of a constant or
+ * calibrated model) -> set_scalar_concentration, on the device for scalar
+ * k: C += kL a (C* - C) dt over every cell, negative values clipped to 0,
+ * the scalar reset to the equilibrium of the new C with the current
+ * velocity. c_star / cell_volume: n values or NULL for the uniform value;
+ * area_density: n values (1/m). Invalid inputs return LBMB_ERR_INVALID and
+ * leave the scalar unchanged. Solid cells hold concentration 0 here (the
+ * reference keeps the value last set there). */
+int lbmb_scalar_interfacial_flux(lbmb_solver* h, int32_t k, const double* c_star, double c_star_uniform,
+                                 const double* area_density, const double* cell_volume, double cell_volume_uniform,
+                                 double dt_s, double kl_m_s, lbmb_oxygen_ledger* ledger, lbmb_oxygen_diag* diag);
+
+/* Same composition with apply_oxygen_reaction_source (reaction.rs:95-137):
+ * C -= OUR(C) dt, clip, ledger of kmol consumed. cell_density: n values,
+ * required by LBMB_OUR_CELL_DENSITY, else ignored (may be NULL). */
+int lbmb_scalar_oxygen_uptake(lbmb_solver* h, int32_t k, const lbmb_our_model* model, const double* cell_density,
+                              const double* cell_volume, double cell_volume_uniform, double dt_s,
+                              lbmb_our_ledger* ledger, lbmb_oxygen_diag* diag);
+
 /* qoi::scalar_cv over fluid cells (crates/lbm-core/src/qoi.rs:507-532);
  * *cv = NaN where the reference returns None. */
 int lbmb_scalar_cv(lbmb_solver* h, int32_t k, double* cv);

@@ -42,6 +42,7 @@ EXPORTS = (
     "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
     "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy", "lbmb_adjoint_torque",
     "lbmb_gather_strain_rate", "lbmb_stress_field", "lbmb_stress_summary", "lbmb_wall_shear_proxy",
+    "lbmb_scalar_interfacial_flux", "lbmb_scalar_oxygen_uptake",
 )
 
 
@@ -117,6 +118,31 @@ class _Percentiles(C.Structure):
                 "fraction_above_threshold": None if np.isnan(f) else f, "count": self.count}
 
 
+class _OxygenDiag(C.Structure):
+    _fields_ = [("clipped_cells", C.c_int64), ("clipped_fraction", C.c_double), ("min_before_clip", C.c_double)]
+
+    def as_dict(self):
+        return {"clipped_cells": self.clipped_cells, "clipped_fraction": self.clipped_fraction,
+                "min_before_clip": self.min_before_clip}
+
+
+class _OxygenLedger(C.Structure):
+    _fields_ = [("cumulative_mol", C.c_double), ("last_step_mol", C.c_double),
+                ("source_integral_mol_s", C.c_double), ("active_interface_cells", C.c_int64)]
+
+
+class _OurLedger(C.Structure):
+    _fields_ = [("cumulative_kmol_consumed", C.c_double), ("last_step_kmol_consumed", C.c_double)]
+
+
+class _OurModel(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("our_kmol_m3_s", C.c_double), ("our_max", C.c_double), ("ks", C.c_double),
+                ("c_ref", C.c_double), ("specific_our", C.c_double)]
+
+
+OUR_KIND = {"constant": 0, "monod": 1, "cell_density_scaled": 2}
+
+
 class _WallShear(C.Structure):
     _fields_ = [("cell_index", C.c_int64), ("tau_w_pa", C.c_double), ("y_plus", C.c_double),
                 ("u_parallel_m_s", C.c_double), ("y_m", C.c_double), ("normal", C.c_double * 3)]
@@ -171,6 +197,10 @@ def lib():
                                               _i64p, _dp, _dp]
         L.lbmb_sync.argtypes = [vp]
         L.lbmb_gather_strain_rate.argtypes = [vp, _dp, _dp]
+        L.lbmb_scalar_interfacial_flux.argtypes = [vp, C.c_int32, _dp, C.c_double, _dp, _dp, C.c_double, C.c_double,
+                                                   C.c_double, C.POINTER(_OxygenLedger), C.POINTER(_OxygenDiag)]
+        L.lbmb_scalar_oxygen_uptake.argtypes = [vp, C.c_int32, C.POINTER(_OurModel), _dp, _dp, C.c_double,
+                                                C.c_double, C.POINTER(_OurLedger), C.POINTER(_OxygenDiag)]
         L.lbmb_stress_field.argtypes = [vp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         L.lbmb_stress_summary.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                           C.POINTER(_Percentiles), C.POINTER(_Percentiles), _dp]
@@ -385,6 +415,39 @@ class Solver:
         return np.array([self.reduce(RED_MOMENTUM, a) for a in range(3)])
 
     # --- forcing / IBM ------------------------------------------------------
+    # --- oxygen transfer and uptake on a scalar --------------------------
+    def apply_interfacial_flux_sources(self, scalar, area_density, c_star, cell_volume, dt_s, kl_m_s,
+                                       cumulative_mol=0.0):
+        """oxygen.rs apply_interfacial_flux_sources on scalar `scalar` (gather,
+        C += kL a (C* - C) dt, clip, set). c_star / cell_volume: per-cell
+        arrays or one value. Returns (ledger, diagnostics)."""
+        led, dg = _OxygenLedger(), _OxygenDiag()
+        led.cumulative_mol = float(cumulative_mol)
+        cs = None if np.isscalar(c_star) else _f64(c_star, self.n)
+        vol = None if np.isscalar(cell_volume) else _f64(cell_volume, self.n)
+        _check(lib().lbmb_scalar_interfacial_flux(
+            self.h, int(scalar), _d(cs), float(c_star) if cs is None else 0.0, _d(_f64(area_density, self.n)),
+            _d(vol), float(cell_volume) if vol is None else 0.0, float(dt_s), float(kl_m_s), C.byref(led),
+            C.byref(dg)))
+        return ({"cumulative_mol": led.cumulative_mol, "last_step_mol": led.last_step_mol,
+                 "source_integral_mol_s": led.source_integral_mol_s,
+                 "active_interface_cells": led.active_interface_cells}, dg.as_dict())
+
+    def apply_oxygen_reaction_source(self, scalar, cell_volume, dt_s, kind="constant", our=0.0, our_max=0.0, ks=0.0,
+                                     c_ref=0.0, specific_our=0.0, cell_density=None, cumulative_kmol=0.0):
+        """reaction.rs apply_oxygen_reaction_source on scalar `scalar`
+        (gather, C -= OUR(C) dt, clip, set). Returns (ledger, diagnostics)."""
+        m = _OurModel(OUR_KIND[kind], float(our), float(our_max), float(ks), float(c_ref), float(specific_our))
+        led, dg = _OurLedger(), _OxygenDiag()
+        led.cumulative_kmol_consumed = float(cumulative_kmol)
+        vol = None if np.isscalar(cell_volume) else _f64(cell_volume, self.n)
+        dens = None if cell_density is None else _f64(cell_density, self.n)
+        _check(lib().lbmb_scalar_oxygen_uptake(self.h, int(scalar), C.byref(m), _d(dens), _d(vol),
+                                               float(cell_volume) if vol is None else 0.0, float(dt_s),
+                                               C.byref(led), C.byref(dg)))
+        return ({"cumulative_kmol_consumed": led.cumulative_kmol_consumed,
+                 "last_step_kmol_consumed": led.last_step_kmol_consumed}, dg.as_dict())
+
     # --- shear-rate and stress QOIs ---------------------------------------
     def strain_rate(self):
         """Native strain rate (n x 6: xx yy zz xy xz yz) and shear rate

@@ -143,6 +143,8 @@ struct EngineBase {
                                 const lbmb_ibm_config& cfg) = 0;
   virtual int64_t cells() const = 0;
   virtual void strain_rate(double* s6, double* gamma) = 0;
+  virtual void scalar_oxygen(int k, const OxygenSourceArgs& a, double* sum, lbmb_oxygen_diag* diag,
+                             int64_t* active) = 0;
   virtual void stress_field(double dx, double dt, double mu, double* s6, double* gamma, double* viscous) = 0;
   virtual void stress_summary(double dx, double dt, double mu, double t_gamma, double t_tau, lbmb_percentiles* pg,
                               lbmb_percentiles* pt, double* device_ms) = 0;
@@ -1670,6 +1672,71 @@ struct Engine final : EngineBase {
     CK(cudaMemcpyAsync(c, dc.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
   }
+  // Oxygen transfer / uptake on scalar k (the gather -> host source ->
+  // set composition of the reference, on the device). a's arrays are host
+  // pointers (n values each, or null); *sum = the source integral.
+  void scalar_oxygen(int k, const OxygenSourceArgs& a0, double* sum, lbmb_oxygen_diag* diag,
+                     int64_t* active) override {
+    auto& sc = scalar(k);
+    OxygenSourceArgs a = a0;
+    DevBuf<double> dc, cs, ar, vo, de, du, part;
+    DevBuf<int> err;
+    DevBuf<unsigned long long> cnt;
+    if (a0.cstar) cs.upload(a0.cstar, size_t(n), st);
+    if (a0.area) ar.upload(a0.area, size_t(n), st);
+    if (a0.vol) vo.upload(a0.vol, size_t(n), st);
+    if (a0.density) de.upload(a0.density, size_t(n), st);
+    a.cstar = a0.cstar ? cs.p : nullptr;
+    a.area = a0.area ? ar.p : nullptr;
+    a.vol = a0.vol ? vo.p : nullptr;
+    a.density = a0.density ? de.p : nullptr;
+    dc.alloc(size_t(n));
+    const unsigned g = unsigned(ceil_div(n, 128));
+    if (sc.q == 7)
+      scalar_gather_kernel<7, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, dc.p, n);
+    else
+      scalar_gather_kernel<Q, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, dc.p, n);
+    const int64_t nb = ceil_div(n, OXY_BLOCK);
+    part.alloc(size_t(2 * nb));
+    err.alloc(1);
+    cnt.alloc(2);
+    CK(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(cnt.p, 0, 2 * sizeof(unsigned long long), st));
+    oxygen_source_kernel<<<unsigned(nb), OXY_BLOCK, 0, st>>>(dc.p, a, err.p, part.p, cnt.p, n);
+    CK(cudaGetLastError());
+    int e = 0;
+    unsigned long long hc[2] = {0, 0};
+    std::vector<double> hp(static_cast<size_t>(2 * nb));
+    CK(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hc, cnt.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (e & 1) invalid("cell volume must be finite and positive");
+    if (e & 2) invalid("oxygen transfer source inputs must be finite (C_L, C*, area density >= 0)");
+    if (e & 4) invalid("oxygen concentration must be finite and non-negative before the uptake");
+    if (e & 8) invalid("cell density must be finite and non-negative");
+    double s = 0.0, mn = INFINITY;
+    for (int64_t b = 0; b < nb; ++b) {
+      s += hp[size_t(2 * b)];
+      if (hp[size_t(2 * b + 1)] < mn) mn = hp[size_t(2 * b + 1)];
+    }
+    if (sum) *sum = s;
+    if (active) *active = int64_t(hc[0]);
+    if (diag) {
+      diag->clipped_cells = int64_t(hc[1]);
+      diag->clipped_fraction = n == 0 ? 0.0 : double(hc[1]) / double(n);
+      diag->min_before_clip = std::isfinite(mn) ? mn : 0.0;
+    }
+    // set_scalar_concentration: equilibrium of the new C at the current u
+    du.upload(init_u_h, st);
+    ScalarParams<A> p = scalar_params(sc);
+    if (sc.q == 7) scalar_set_kernel<7, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
+    else scalar_set_kernel<Q, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
+    CK(cudaGetLastError());
+    sc.parity = 0;
+    CK(cudaStreamSynchronize(st));
+  }
+
   // Device CV of a scalar into *out (two deterministic passes).
   void enqueue_cv(ScalarStateT<A>& sc, double* out, double nfluid) {
     for (int pass = 0; pass < 2; ++pass) {

@@ -230,4 +230,84 @@ static __global__ void scalar_cv_finish_kernel(const double* part, int nblk, int
   stats[1] = cv;
 }
 
+// Oxygen transfer (oxygen.rs:124-191) or uptake (reaction.rs:57-137) on a
+// gathered concentration array, in place, followed by the negative clip
+// (oxygen.rs:193-216). Per block: the f64 sum of the source integral (mol/s
+// for the transfer, kmol consumed for the uptake) and the minimum before
+// the clip, in a fixed tree order; counts of active interface cells and of
+// clipped cells; error bits (1 cell volume, 2 transfer inputs, 4 C_L < 0
+// or not finite before the uptake, 8 cell density).
+struct OxygenSourceArgs {
+  int mode;  // 0 transfer, 1 uptake
+  double dt, kl, cstar_u, vol_u;
+  const double *cstar, *area, *vol, *density;
+  int our_kind;  // 0 constant, 1 Monod, 2 cell-density scaled
+  double our, our_max, ks, c_ref, specific_our;
+};
+
+constexpr int OXY_BLOCK = 256;
+
+static __global__ void __launch_bounds__(OXY_BLOCK)
+    oxygen_source_kernel(double* c, OxygenSourceArgs a, int* err, double* part, unsigned long long* cnt, int64_t n) {
+  __shared__ double ssum[OXY_BLOCK], smin[OXY_BLOCK];
+  const int64_t i = int64_t(blockIdx.x) * OXY_BLOCK + threadIdx.x;
+  double contrib = 0.0, before = INFINITY;
+  int active = 0, clipped = 0, e = 0;
+  if (i < n) {
+    const double v = a.vol ? a.vol[i] : a.vol_u;
+    double ci = c[i];
+    if (!(isfinite(v) && v > 0.0)) e |= 1;
+    if (a.mode == 0) {
+      const double cs = a.cstar ? a.cstar[i] : a.cstar_u;
+      const double ar = a.area[i];
+      if (!(isfinite(ci) && isfinite(cs) && isfinite(ar) && ar >= 0.0)) e |= 2;
+      const double source = a.kl * ar * (cs - ci);
+      active = ar > 0.0;
+      ci += source * a.dt;
+      contrib = source * v;
+    } else {
+      double rate = 0.0;
+      if (!(isfinite(ci) && ci >= 0.0)) e |= 4;
+      if (a.our_kind == 0) {
+        rate = a.our;
+      } else if (a.our_kind == 1) {
+        const double cs = ci / a.c_ref;
+        rate = a.our_max * cs / (a.ks + cs);
+      } else {
+        const double d = a.density[i];
+        if (!(isfinite(d) && d >= 0.0)) e |= 8;
+        rate = a.specific_our * d;
+      }
+      ci -= rate * a.dt;
+      contrib = rate * v * a.dt;
+    }
+    before = ci;
+    if (ci < 0.0) {
+      ci = 0.0;
+      clipped = 1;
+    }
+    c[i] = ci;
+  }
+  if (e) atomicOr(err, e);
+  ssum[threadIdx.x] = contrib;
+  smin[threadIdx.x] = before;
+  __syncthreads();
+  for (int s = OXY_BLOCK / 2; s > 0; s >>= 1) {
+    if (int(threadIdx.x) < s) {
+      ssum[threadIdx.x] += ssum[threadIdx.x + s];
+      smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = ssum[0];
+    part[2 * blockIdx.x + 1] = smin[0];
+  }
+  const unsigned ba = __ballot_sync(0xffffffffu, active), bc = __ballot_sync(0xffffffffu, clipped);
+  if ((threadIdx.x & 31) == 0) {
+    if (ba) atomicAdd(cnt, (unsigned long long)__popc(ba));
+    if (bc) atomicAdd(cnt + 1, (unsigned long long)__popc(bc));
+  }
+}
+
 }  // namespace lbmb

@@ -256,6 +256,76 @@ int lbmb_get_force_field(lbmb_solver* h, double* out) {
   });
 }
 
+int lbmb_scalar_interfacial_flux(lbmb_solver* h, int32_t k, const double* c_star, double c_star_uniform,
+                                 const double* area_density, const double* cell_volume, double cell_volume_uniform,
+                                 double dt_s, double kl_m_s, lbmb_oxygen_ledger* ledger, lbmb_oxygen_diag* diag) {
+  return guarded([&] {
+    NEED(h);
+    if (!area_density) lbmb::invalid("area_density must hold one value per cell");
+    if (!(std::isfinite(dt_s) && dt_s >= 0.0)) lbmb::invalid("oxygen source time step must be finite and non-negative");
+    if (!(std::isfinite(kl_m_s) && kl_m_s > 0.0)) lbmb::invalid("kL must be finite and positive");
+    lbmb::OxygenSourceArgs a{};
+    a.mode = 0;
+    a.dt = dt_s;
+    a.kl = kl_m_s;
+    a.cstar_u = c_star_uniform;
+    a.vol_u = cell_volume_uniform;
+    a.cstar = c_star;
+    a.area = area_density;
+    a.vol = cell_volume;
+    double sum = 0.0;
+    int64_t active = 0;
+    h->e->scalar_oxygen(k, a, &sum, diag, &active);
+    if (ledger) {
+      ledger->source_integral_mol_s = sum;
+      ledger->last_step_mol = sum * dt_s;
+      ledger->cumulative_mol += ledger->last_step_mol;
+      ledger->active_interface_cells = active;
+    }
+  });
+}
+
+int lbmb_scalar_oxygen_uptake(lbmb_solver* h, int32_t k, const lbmb_our_model* model, const double* cell_density,
+                              const double* cell_volume, double cell_volume_uniform, double dt_s,
+                              lbmb_our_ledger* ledger, lbmb_oxygen_diag* diag) {
+  return guarded([&] {
+    NEED(h);
+    if (!model) lbmb::invalid("null uptake model");
+    if (!(std::isfinite(dt_s) && dt_s >= 0.0)) lbmb::invalid("reaction time step must be finite and non-negative");
+    auto nonneg = [](double v) { return std::isfinite(v) && v >= 0.0; };
+    lbmb::OxygenSourceArgs a{};
+    a.mode = 1;
+    a.dt = dt_s;
+    a.vol_u = cell_volume_uniform;
+    a.vol = cell_volume;
+    a.our_kind = model->kind;
+    if (model->kind == LBMB_OUR_CONSTANT) {
+      if (!nonneg(model->our_kmol_m3_s)) lbmb::invalid("our_kmol_m3_s must be finite and non-negative");
+      a.our = model->our_kmol_m3_s;
+    } else if (model->kind == LBMB_OUR_MONOD) {
+      if (!nonneg(model->our_max)) lbmb::invalid("our_max must be finite and non-negative");
+      if (!(std::isfinite(model->ks) && model->ks > 0.0 && std::isfinite(model->c_ref) && model->c_ref > 0.0))
+        lbmb::invalid("Monod parameters must be finite and positive where dimensional");
+      a.our_max = model->our_max;
+      a.ks = model->ks;
+      a.c_ref = model->c_ref;
+    } else if (model->kind == LBMB_OUR_CELL_DENSITY) {
+      if (!nonneg(model->specific_our)) lbmb::invalid("specific_our must be finite and non-negative");
+      if (!cell_density) lbmb::invalid("cell-density-scaled OUR requires a cell density field");
+      a.specific_our = model->specific_our;
+      a.density = cell_density;
+    } else {
+      lbmb::invalid("unknown uptake model kind");
+    }
+    double sum = 0.0;
+    h->e->scalar_oxygen(k, a, &sum, diag, nullptr);
+    if (ledger) {
+      ledger->last_step_kmol_consumed = sum;
+      ledger->cumulative_kmol_consumed += sum;
+    }
+  });
+}
+
 int lbmb_gather_strain_rate(lbmb_solver* h, double* s6, double* gamma) {
   return guarded([&] {
     NEED(h);
