@@ -187,6 +187,47 @@ def shear_study(g, dims, solid, nu, T, q, storage):
             "p95_rel_diff_vs_cpu": abs(gam["p95"] - rg["p95"]) / rg["p95"]}
 
 
+def oxygen_study(g, dims, solid, T):
+    """Oxygen transfer on a D3Q7 scalar of the final headline state (the
+    reference composition gather -> apply_interfacial_flux_sources -> set,
+    oxygen.rs:124-191): Henry C* = 1.3e-5 x 21 kPa, kL = 2e-4 m/s, interface
+    area density 1/dx on the top fluid layer, dx = 1/T m, dt = 1 ms. Timed
+    through the public call (host arrays in, ledger out) against the
+    oracle's restatement of the host function on the same arrays."""
+    from oracle import oracle as o
+    n = dims[0] * dims[1] * dims[2]
+    dx = 1.0 / T
+    fl = solid == 0
+    z = np.arange(n) // (dims[0] * dims[1])
+    top = int(z[fl].max())
+    import torch
+    area = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()  # caller's array in pinned memory
+    area[...] = np.where(fl & (z == top), 1.0 / dx, 0.0)
+    k = g.enable_scalar_distribution(1e-2, q=7)
+    g.set_scalar_concentration(k, np.where(fl, 0.05, 0.0))
+    c_star, kl, vol, dt = 1.3e-5 * 21000.0, 2.0e-4, dx ** 3, 1.0e-3
+    g.apply_interfacial_flux_sources(k, area, c_star, vol, dt, kl)  # warm-up
+    g.sync()
+    times = []
+    for _ in range(7):
+        t0 = time.perf_counter()
+        led, diag = g.apply_interfacial_flux_sources(k, area, c_star, vol, dt, kl)
+        times.append((time.perf_counter() - t0) * 1e3)
+    dev_ms = float(np.median(times))
+    c = g.gather_scalar_concentration(k)
+    led, diag = g.apply_interfacial_flux_sources(k, area, c_star, vol, dt, kl)  # on the state c holds
+    t0 = time.perf_counter()
+    _, led_c, _ = o.interfacial_flux(c, c_star, area, vol, dt, kl)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    return {"what": "kL a (C* - C) transfer step on a D3Q7 scalar, gather + source + clip + set (oxygen.rs)",
+            "cells": n, "interface_cells": led["active_interface_cells"], "source_integral_mol_s":
+            led["source_integral_mol_s"], "call_ms": dev_ms,
+            "call_path": "C ABI, median of 7 calls, host area array (pinned) uploaded every call (8 B per cell)",
+            "cpu_ms": cpu_ms, "cpu_kind": "port (oracle restatement of the host function, 1 thread, source only)",
+            "ledger_rel_diff_vs_cpu": abs(led["source_integral_mol_s"] - led_c["source_integral_mol_s"]) /
+            abs(led_c["source_integral_mol_s"])}
+
+
 # ---------------------------------------------------------------------------
 # Distributed plumbing (replicas: one independent tank per GPU)
 # ---------------------------------------------------------------------------
@@ -546,6 +587,7 @@ def run_b200(args, rank, world, local):
     extra = {}
     if world == 1 and args.shear:
         extra["shear_qoi"] = shear_study(g, dims, solid, nu, args.tank_T, q, storage)
+        extra["oxygen_transfer"] = oxygen_study(g, dims, solid, args.tank_T)
     g.close()
     if args.sweep_steps > 0:
         sw = sweep_study(args, rank, world, local)

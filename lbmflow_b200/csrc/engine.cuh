@@ -209,6 +209,17 @@ struct Engine final : EngineBase {
   // host mirrors
   std::vector<uint8_t> solid_h, flags_h;
   std::vector<double> init_rho_h, init_u_h;
+  // device copy of init_u_h (the velocity the scalar equilibrium uses on
+  // solid cells), refreshed when init_u_h changes
+  DevBuf<double> d_init_u;
+  bool d_init_u_ok = false;
+  const double* init_u_dev() {
+    if (!d_init_u_ok) {
+      d_init_u.upload(init_u_h, st);
+      d_init_u_ok = true;
+    }
+    return d_init_u.p;
+  }
   // scalars
   std::vector<std::unique_ptr<ScalarStateT<A>>> scalars;
   // graphs
@@ -1038,6 +1049,7 @@ struct Engine final : EngineBase {
           for (int q = 0; q < Q; ++q) fh[size_t(q) * n + c] = double(fq[q]);
           init_rho_h[c] = double(r);
           for (int k = 0; k < 3; ++k) init_u_h[3 * c + k] = double(u[k]);
+          d_init_u_ok = false;
         }
     stage_in(fh.data());
   }
@@ -1648,13 +1660,12 @@ struct Engine final : EngineBase {
   }
   void set_scalar(int k, const double* c) override {
     auto& sc = scalar(k);
-    DevBuf<double> dc, du;
+    DevBuf<double> dc;
     dc.upload(c, size_t(n), st);
-    du.upload(init_u_h, st);
     ScalarParams<A> p = scalar_params(sc);
     const unsigned g = unsigned(ceil_div(n, 128));
-    if (sc.q == 7) scalar_set_kernel<7, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
-    else scalar_set_kernel<Q, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
+    if (sc.q == 7) scalar_set_kernel<7, Q, S><<<g, 128, 0, st>>>(p, dc.p, init_u_dev(), n);
+    else scalar_set_kernel<Q, Q, S><<<g, 128, 0, st>>>(p, dc.p, init_u_dev(), n);
     CK(cudaGetLastError());
     sc.parity = 0;
     CK(cudaStreamSynchronize(st));
@@ -1679,7 +1690,7 @@ struct Engine final : EngineBase {
                      int64_t* active) override {
     auto& sc = scalar(k);
     OxygenSourceArgs a = a0;
-    DevBuf<double> dc, cs, ar, vo, de, du, part;
+    DevBuf<double> dc, cs, ar, vo, de, part;
     DevBuf<int> err;
     DevBuf<unsigned long long> cnt;
     if (a0.cstar) cs.upload(a0.cstar, size_t(n), st);
@@ -1728,10 +1739,9 @@ struct Engine final : EngineBase {
       diag->min_before_clip = std::isfinite(mn) ? mn : 0.0;
     }
     // set_scalar_concentration: equilibrium of the new C at the current u
-    du.upload(init_u_h, st);
     ScalarParams<A> p = scalar_params(sc);
-    if (sc.q == 7) scalar_set_kernel<7, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
-    else scalar_set_kernel<Q, Q, S><<<g, 128, 0, st>>>(p, dc.p, du.p, n);
+    if (sc.q == 7) scalar_set_kernel<7, Q, S><<<g, 128, 0, st>>>(p, dc.p, init_u_dev(), n);
+    else scalar_set_kernel<Q, Q, S><<<g, 128, 0, st>>>(p, dc.p, init_u_dev(), n);
     CK(cudaGetLastError());
     sc.parity = 0;
     CK(cudaStreamSynchronize(st));
