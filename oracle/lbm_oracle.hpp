@@ -684,6 +684,12 @@ class Solver {
   std::vector<T> wall_u;  // n x 3
   bool has_force_field = false;
   std::vector<T> force_field;  // n x 3
+  // Per-cell relaxation field (Solver::set_omega_field, solver.rs:4443-4473):
+  // TRT takes omega+ = field, c+ = 1 - omega+/2 (omega- unchanged,
+  // kernels.rs:151-156); the central moment takes its shear rate from it
+  // (kernels.rs:481).
+  bool has_omega_field = false;
+  std::vector<T> omega_field;
   std::vector<Scalar<T>> scalars;
   uint64_t time = 0;
 
@@ -735,6 +741,17 @@ class Solver {
       T u[3] = {ux[c], uy[c], uz[c]};
       T fv[3];
       force_at(size_t(c), fv);
+      if (has_omega_field) {
+        const T op = omega_field[c];
+        if (kp.central_moment) {
+          KParams<T> kc = kp;
+          kc.omega_shear = op;
+          collide_cm_cell<L, T>(&f[c], n, rho[c], u, fv, kc);
+        } else {
+          collide_trt_cell<L, T>(&f[c], n, rho[c], u, fv, op, T(1) - op / T(2.0), fon, kp);
+        }
+        continue;
+      }
       if (les) {
         const KParams<T> kc = les_kparams(&f[c], rho[c], u);
         if (kc.central_moment)
@@ -1004,6 +1021,131 @@ class Solver {
     const T scale = -(T(1) / (T(2.0 / 3.0) * r * tau_eff));
     for (int k = 0; k < 6; ++k) out[k] = pi[k] * scale;
   }
+  void set_omega_field(const double* v) {
+    if (!v) {
+      has_omega_field = false;
+      omega_field.clear();
+      return;
+    }
+    omega_field.assign(n, T(0));
+    for (size_t i = 0; i < n; ++i) omega_field[i] = T(v[i]);
+    has_omega_field = true;
+  }
+
+  // Velocity gradient g[i][j] = du_i/dx_j of one cell
+  // (Solver::gather_velocity_gradient, solver.rs:5482-5582): symmetric
+  // off-diagonal part from the native strain rate, diagonal and rotation
+  // from velocity differences: central between fluid cells, the half-way
+  // wall stencil -4/3 w + u + 1/3 u(+1) (mirrored) next to a solid (whose
+  // wall velocity counts), one-sided at a non-periodic domain edge,
+  // periodic faces wrapped. Solid cells: zeros.
+  void velocity_gradient_at(size_t c, T out[3][3]) const {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[i][j] = T(0);
+    if (solid[c]) return;
+    T st[6];
+    strain_rate_at(c, st);
+    T sm[3][3];
+    sm[0][0] = st[0];
+    sm[1][1] = st[1];
+    sm[2][2] = st[2];
+    sm[0][1] = sm[1][0] = st[3];
+    sm[0][2] = sm[2][0] = st[4];
+    sm[1][2] = sm[2][1] = st[5];
+    const long x = long(c % size_t(dims[0])), y = long((c / size_t(dims[0])) % size_t(dims[1])),
+               z = long(c / (size_t(dims[0]) * size_t(dims[1])));
+    const T own[3] = {ux[c], uy[c], uz[c]};
+    // neighbour along axis a by da: 0 none, 1 fluid (v), 2 solid (wall velocity v)
+    auto nb = [&](int a, int da, T v[3]) {
+      long pp[3] = {x, y, z};
+      pp[a] += da;
+      if (pp[a] < 0 || pp[a] >= dims[a]) {
+        if (!periodic[a]) return 0;
+        pp[a] = (pp[a] + dims[a]) % dims[a];
+      }
+      const size_t j = idx(pp[0], pp[1], pp[2]);
+      if (solid[j]) {
+        for (int k = 0; k < 3; ++k) v[k] = wall_u[3 * j + k];
+        return 2;
+      }
+      v[0] = ux[j];
+      v[1] = uy[j];
+      v[2] = uz[j];
+      return 1;
+    };
+    T fd[3][3];
+    for (int comp = 0; comp < 3; ++comp)
+      for (int a = 0; a < 3; ++a) {
+        T pv[3], mv[3];
+        const int hp = nb(a, 1, pv), hm = nb(a, -1, mv);
+        T v = T(0);
+        if (hp == 1 && hm == 1) v = (pv[comp] - mv[comp]) * T(0.5);
+        else if (hp == 1 && hm == 2) v = -T(4.0 / 3.0) * mv[comp] + own[comp] + T(1.0 / 3.0) * pv[comp];
+        else if (hp == 2 && hm == 1) v = T(4.0 / 3.0) * pv[comp] - own[comp] - T(1.0 / 3.0) * mv[comp];
+        else if (hp == 1 && hm == 0) v = pv[comp] - own[comp];
+        else if (hp == 0 && hm == 1) v = own[comp] - mv[comp];
+        fd[comp][a] = v;
+      }
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        out[r][q] = r == q ? fd[r][q] : sm[r][q] + T(0.5) * (fd[r][q] - fd[q][r]);
+  }
+
+  // WaleLes::update (les.rs:120-211), Cw = 0.325, Delta = 1: nu_t from the
+  // velocity gradient, optional tau_eff bound, omega+ field installed for
+  // the next collision. diag = {clipped cells, clipped fraction, max nu_t
+  // before clipping, tau_eff_max (NaN), nu_t_max (NaN)}.
+  void wale_update(bool has_max, double tau_eff_max, std::vector<T>& nu_t, double diag[5]) {
+    const T cwd = T(0.325) * T(1.0);
+    const T cw_delta_sq = cwd * cwd;
+    const T nu0 = T(params.nu);
+    const T tau0 = T(0.5) + T(3.0) * nu0;
+    const T nu_t_max = has_max ? (T(tau_eff_max) - tau0) / T(3.0) : T(0);
+    nu_t.assign(n, T(0));
+    std::vector<double> om(n);
+    size_t clipped = 0;
+    T max_before = T(0);
+    for (size_t i = 0; i < n; ++i) {
+      T g[3][3];
+      velocity_gradient_at(i, g);
+      T sr[3][3], g2[3][3], sd[3][3];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) sr[a][b] = T(0.5) * (g[a][b] + g[b][a]);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          g2[a][b] = T(0);
+          for (int k = 0; k < 3; ++k) g2[a][b] = g2[a][b] + g[a][k] * g[k][b];
+        }
+      const T tr = g2[0][0] + g2[1][1] + g2[2][2];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          sd[a][b] = T(0.5) * (g2[a][b] + g2[b][a]);
+          if (a == b) sd[a][b] = sd[a][b] - tr / T(3.0);
+        }
+      T ss = T(0), sdsd = T(0);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          ss = ss + sr[a][b] * sr[a][b];
+          sdsd = sdsd + sd[a][b] * sd[a][b];
+        }
+      const T denom = std::pow(ss, T(2.5)) + std::pow(sdsd, T(1.25));
+      T nut = denom > T(0) ? cw_delta_sq * std::pow(sdsd, T(1.5)) / denom : T(0);
+      max_before = std::max(max_before, nut);
+      if (has_max && nut > nu_t_max) {
+        ++clipped;
+        nut = nu_t_max;
+      }
+      nu_t[i] = nut;
+      om[i] = double(T(1) / (T(3.0) * (nu0 + nut) + T(0.5)));
+    }
+    set_omega_field(om.data());
+    diag[0] = double(clipped);
+    diag[1] = n == 0 ? 0.0 : double(T(double(clipped)) / T(double(n)));
+    diag[2] = double(max_before);
+    diag[3] = has_max ? tau_eff_max : std::nan("");
+    diag[4] = has_max ? double(nu_t_max) : std::nan("");
+  }
+
   // gamma_dot = sqrt(2 S:S) (Solver::gather_shear_rate, solver.rs:5588-5599)
   T shear_rate_at(size_t c) const {
     T s[6];

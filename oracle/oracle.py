@@ -83,6 +83,9 @@ def lib():
                                     C.c_int, C.c_double, C.c_long, C.c_long, C.c_int, _dp, _dp,
                                     _dp, _dp]
         L.lbmo_gather_strain_rate.argtypes = [C.c_void_p, _dp, _dp]
+        L.lbmo_set_omega_field.argtypes = [C.c_void_p, _dp]
+        L.lbmo_gather_velocity_gradient.argtypes = [C.c_void_p, _dp]
+        L.lbmo_wale_update.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
         L.lbmo_compute_stress_field.argtypes = [_ip, _dp, _dp, _dp, _u8p, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp]
         L.lbmo_percentile_summary.restype = C.c_int
         L.lbmo_percentile_summary.argtypes = [_dp, C.c_long, C.c_int, C.c_double, _dp]
@@ -175,6 +178,27 @@ class OracleSolver:
         out = [np.zeros(self.n) for _ in range(4)]
         lib().lbmo_read_moments(self.h, *[_d(a) for a in out])
         return out
+
+    def set_omega_field(self, omega):
+        """Solver::set_omega_field (None clears)."""
+        lib().lbmo_set_omega_field(self.h, None if omega is None else _d(_as_d(omega, self.n)))
+
+    def velocity_gradient(self):
+        """Solver::gather_velocity_gradient: n x 3 x 3, g[i][j] = du_i/dx_j."""
+        g = np.zeros(9 * self.n)
+        lib().lbmo_gather_velocity_gradient(self.h, _d(g))
+        return g.reshape(self.n, 3, 3)
+
+    def wale_update(self, tau_eff_max=None):
+        """WaleLes::update (Cw 0.325): nu_t per cell and diagnostics; the
+        omega+ field is installed for the next collision."""
+        nu_t, diag = np.zeros(self.n), np.zeros(5)
+        lib().lbmo_wale_update(self.h, float("nan") if tau_eff_max is None else float(tau_eff_max), _d(nu_t),
+                               _d(diag))
+        return nu_t, {"clipped_cells": int(diag[0]), "clipped_fraction": diag[1],
+                      "max_nu_t_before_clipping": diag[2],
+                      "tau_eff_max": None if np.isnan(diag[3]) else diag[3],
+                      "nu_t_max": None if np.isnan(diag[4]) else diag[4]}
 
     def strain_rate(self):
         """Native strain rate (n x 6: xx yy zz xy xz yz) and shear rate

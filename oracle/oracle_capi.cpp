@@ -29,6 +29,9 @@ struct AnySolver {
   virtual void set_smagorinsky(double cs) = 0;
   virtual void set_free_slip_top(bool on) = 0;
   virtual void strain_rate(double* s6, double* gamma) const = 0;
+  virtual void set_omega_field(const double* v) = 0;
+  virtual void velocity_gradient(double* g9) const = 0;
+  virtual void wale(bool has_max, double tau_max, double* nu_t, double* diag) = 0;
 };
 
 template <class L, class T>
@@ -73,6 +76,20 @@ struct Impl final : AnySolver {
   size_t cells() const override { return s.n; }
   const uint8_t* solid() const override { return s.solid.data(); }
   int q() const override { return L::Q; }
+  void set_omega_field(const double* v) override { s.set_omega_field(v); }
+  void velocity_gradient(double* g9) const override {
+    for (size_t c = 0; c < s.n; ++c) {
+      T g[3][3];
+      s.velocity_gradient_at(c, g);
+      for (int i = 0; i < 9; ++i) g9[9 * c + i] = double(g[i / 3][i % 3]);
+    }
+  }
+  void wale(bool has_max, double tau_max, double* nu_t, double* diag) override {
+    std::vector<T> v;
+    s.wale_update(has_max, tau_max, v, diag);
+    if (nu_t)
+      for (size_t c = 0; c < s.n; ++c) nu_t[c] = double(v[c]);
+  }
   void strain_rate(double* s6, double* gamma) const override {
     for (size_t c = 0; c < s.n; ++c) {
       T v[6];
@@ -324,6 +341,15 @@ long lbmo_run_tank(void* h, const double* pos, const double* w, long nm, const d
     }
   }
   return executed;
+}
+
+// Solver::set_omega_field (NULL clears), gather_velocity_gradient (n x 9,
+// row-major g[i][j] = du_i/dx_j) and WaleLes::update (tau_eff_max NaN for
+// no bound; diag: 5 values).
+void lbmo_set_omega_field(void* h, const double* v) { static_cast<AnySolver*>(h)->set_omega_field(v); }
+void lbmo_gather_velocity_gradient(void* h, double* g9) { static_cast<AnySolver*>(h)->velocity_gradient(g9); }
+void lbmo_wale_update(void* h, double tau_eff_max, double* nu_t, double* diag) {
+  static_cast<AnySolver*>(h)->wale(std::isfinite(tau_eff_max), tau_eff_max, nu_t, diag);
 }
 
 // Native strain rate and shear rate of every cell (solver.rs:5464-5599).
