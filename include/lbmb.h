@@ -171,6 +171,40 @@ int lbmb_clear_body_force_field(lbmb_solver* h);
 /* Current per-cell force field (ncells x 3, zeros where absent). */
 int lbmb_get_force_field(lbmb_solver* h, double* out);
 
+/* ---- Per-cell relaxation field and WALE LES ------------------------------ */
+
+/* Solver::set_omega_field (solver.rs:4443-4473): a per-cell relaxation
+ * rate (n values; NULL removes it) for the following collisions: TRT/BGK
+ * take omega+ = field and c+ = 1 - omega+/2 with omega- unchanged
+ * (kernels.rs:151-156), the central moment takes it as its shear rate
+ * (kernels.rs:481). Not combined with smagorinsky_cs > 0; the pair and
+ * tile sweep kernels do not take it (a solver on one of them moves to its
+ * default kernel), nor do batches and the adjoint. */
+int lbmb_set_omega_field(lbmb_solver* h, const double* omega);
+
+/* Solver::gather_velocity_gradient (solver.rs:5482-5582): n x 9 row-major,
+ * g[i][j] = du_i/dx_j (lattice units); symmetric off-diagonal part from the
+ * native strain rate, diagonal and rotation from velocity differences with
+ * the half-way wall stencil; solid cells zero. */
+int lbmb_gather_velocity_gradient(lbmb_solver* h, double* g9);
+
+/* WaleLesDiagnostics (les.rs:19-31). tau_eff_max and nu_t_max are NaN
+ * without a bound. */
+typedef struct {
+  int64_t clipped_cells;
+  double clipped_fraction;
+  double max_nu_t_before_clipping;
+  double tau_eff_max;
+  double nu_t_max;
+} lbmb_wale_diag;
+
+/* WaleLes::update (les.rs:120-211; Cw = 0.325, Delta = 1): WALE eddy
+ * viscosity nu_t from the velocity gradient, clipped at
+ * (tau_eff_max - tau0) / 3 when tau_eff_max is not NaN, and the field
+ * omega+ = 1 / (3 (nu + nu_t) + 1/2) installed for the next collision on
+ * the device (one-step lag). nu_t (n values) may be NULL. */
+int lbmb_wale_update(lbmb_solver* h, double tau_eff_max, double* nu_t, lbmb_wale_diag* diag);
+
 /* ---- Shear-rate and stress QOIs ----------------------------------------- */
 
 /* Solver::gather_strain_rate / gather_shear_rate (solver.rs:5464-5480,

@@ -42,7 +42,8 @@ EXPORTS = (
     "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
     "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy", "lbmb_adjoint_torque",
     "lbmb_gather_strain_rate", "lbmb_stress_field", "lbmb_stress_summary", "lbmb_wall_shear_proxy",
-    "lbmb_scalar_interfacial_flux", "lbmb_scalar_oxygen_uptake",
+    "lbmb_scalar_interfacial_flux", "lbmb_scalar_oxygen_uptake", "lbmb_set_omega_field",
+    "lbmb_gather_velocity_gradient", "lbmb_wale_update",
 )
 
 
@@ -116,6 +117,11 @@ class _Percentiles(C.Structure):
         f = self.fraction_above_threshold
         return {"p50": self.p50, "p90": self.p90, "p95": self.p95, "p99": self.p99, "max": self.max,
                 "fraction_above_threshold": None if np.isnan(f) else f, "count": self.count}
+
+
+class _WaleDiag(C.Structure):
+    _fields_ = [("clipped_cells", C.c_int64), ("clipped_fraction", C.c_double),
+                ("max_nu_t_before_clipping", C.c_double), ("tau_eff_max", C.c_double), ("nu_t_max", C.c_double)]
 
 
 class _OxygenDiag(C.Structure):
@@ -197,6 +203,9 @@ def lib():
                                               _i64p, _dp, _dp]
         L.lbmb_sync.argtypes = [vp]
         L.lbmb_gather_strain_rate.argtypes = [vp, _dp, _dp]
+        L.lbmb_set_omega_field.argtypes = [vp, _dp]
+        L.lbmb_gather_velocity_gradient.argtypes = [vp, _dp]
+        L.lbmb_wale_update.argtypes = [vp, C.c_double, _dp, C.POINTER(_WaleDiag)]
         L.lbmb_scalar_interfacial_flux.argtypes = [vp, C.c_int32, _dp, C.c_double, _dp, _dp, C.c_double, C.c_double,
                                                    C.c_double, C.POINTER(_OxygenLedger), C.POINTER(_OxygenDiag)]
         L.lbmb_scalar_oxygen_uptake.argtypes = [vp, C.c_int32, C.POINTER(_OurModel), _dp, _dp, C.c_double,
@@ -415,6 +424,29 @@ class Solver:
         return np.array([self.reduce(RED_MOMENTUM, a) for a in range(3)])
 
     # --- forcing / IBM ------------------------------------------------------
+    # --- per-cell relaxation field and WALE -------------------------------
+    def set_omega_field(self, omega):
+        """Solver::set_omega_field: per-cell omega+ (TRT/BGK) or shear rate
+        (central moment) for the following collisions; None removes it."""
+        _check(lib().lbmb_set_omega_field(self.h, None if omega is None else _d(_f64(omega, self.n))))
+
+    def velocity_gradient(self):
+        """Solver::gather_velocity_gradient: n x 3 x 3, g[i][j] = du_i/dx_j."""
+        g = np.empty(9 * self.n)
+        _check(lib().lbmb_gather_velocity_gradient(self.h, _d(g)))
+        return g.reshape(self.n, 3, 3)
+
+    def wale_update(self, tau_eff_max=None):
+        """WaleLes::update (Cw 0.325): nu_t per cell and diagnostics; the
+        omega+ field is installed on the device for the next collision."""
+        nu_t, d = np.empty(self.n), _WaleDiag()
+        _check(lib().lbmb_wale_update(self.h, float("nan") if tau_eff_max is None else float(tau_eff_max), _d(nu_t),
+                                      C.byref(d)))
+        return nu_t, {"clipped_cells": d.clipped_cells, "clipped_fraction": d.clipped_fraction,
+                      "max_nu_t_before_clipping": d.max_nu_t_before_clipping,
+                      "tau_eff_max": None if np.isnan(d.tau_eff_max) else d.tau_eff_max,
+                      "nu_t_max": None if np.isnan(d.nu_t_max) else d.nu_t_max}
+
     # --- oxygen transfer and uptake on a scalar --------------------------
     def apply_interfacial_flux_sources(self, scalar, area_density, c_star, cell_volume, dt_s, kl_m_s,
                                        cumulative_mol=0.0):

@@ -143,6 +143,9 @@ struct EngineBase {
                                 const lbmb_ibm_config& cfg) = 0;
   virtual int64_t cells() const = 0;
   virtual void strain_rate(double* s6, double* gamma) = 0;
+  virtual void set_omega_field(const double* omega) = 0;
+  virtual void velocity_gradient(double* g9) = 0;
+  virtual void wale_update(double tau_eff_max, double* nu_t, lbmb_wale_diag* diag) = 0;
   virtual void scalar_oxygen(int k, const OxygenSourceArgs& a, double* sum, lbmb_oxygen_diag* diag,
                              int64_t* active) = 0;
   virtual void stress_field(double dx, double dt, double mu, double* s6, double* gamma, double* viscous) = 0;
@@ -395,6 +398,7 @@ struct Engine final : EngineBase {
 
   HydroParams<A> hydro_params() {
     HydroParams<A> p;
+    p.omega_field = omega_on ? omega_dev.p : nullptr;
     p.f = fp;
     p.plane = uint32_t(plane);
     p.nxy = nx * ny;
@@ -472,6 +476,8 @@ struct Engine final : EngineBase {
   void set_sweep_kernel(int kind) override {
     const bool wide = sizeof(S) >= 4;
     const bool pair = std::is_same<A, float>::value && nx % 2 == 0 && !has_uniform_force();
+    if (omega_on && !omega_kind_ok(kind))
+      throw Error(LBMB_ERR_UNSUPPORTED, "the pair and tile sweeps do not take a relaxation field");
     if (kind == LBMB_SWEEP_ASYNC && !wide)
       throw Error(LBMB_ERR_UNSUPPORTED, "the cp.async sweep needs 4- or 8-byte population storage");
     if ((kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE) && !pair)
@@ -559,7 +565,7 @@ struct Engine final : EngineBase {
 
   // Whether the two-cells-per-thread kernel covers this sweep.
   bool pair_ok(const HydroParams<A>& p, int) const {
-    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0;
+    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0 && !p.omega_field;
   }
 
   // Tile list and window offsets of the tile-pipelined sweep.
@@ -854,7 +860,7 @@ struct Engine final : EngineBase {
       }
     }
     if (!uf) cands.push_back({LBMB_SWEEP_BULK, 0, 0});
-    if (is_f && nx % 2 == 0 && !uf) {
+    if (is_f && nx % 2 == 0 && !uf && !omega_on) {
       cands.push_back({LBMB_SWEEP_PAIR, 0, 0});
       cands.push_back({LBMB_SWEEP_TILE, 0, 0});
     }
@@ -1125,18 +1131,126 @@ struct Engine final : EngineBase {
   }
 
   // ---- shear-rate and stress QOIs (stress.cuh) ---------------------------
+  StrainArgs<S> strain_args() {
+    StrainArgs<S> a;
+    a.fb = fp;
+    a.pl = plane;
+    a.flags = flags.p;
+    a.nbr = nbr.p;
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.parity = parity;
+    a.fslot = fslot.p;
+    a.fprev = fprev.p;
+    a.fcur = fcur.p;
+    a.field_present = field_present ? 1 : 0;
+    a.gx = A(cfg.force[0]);
+    a.gy = A(cfg.force[1]);
+    a.gz = A(cfg.force[2]);
+    a.tau_eff = A(1.0 / omega_p);
+    return a;
+  }
+
   void strain_rate(double* s6, double* gamma) override {
     DevBuf<double> d6, dg;
     if (s6) d6.alloc(size_t(6) * n);
     if (gamma) dg.alloc(size_t(n));
-    strain_rate_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
-        fp, plane, flags.p, nbr.p, nx, ny, nz, parity, fslot.p, fprev.p, fcur.p, field_present ? 1 : 0,
-        A(cfg.force[0]), A(cfg.force[1]), A(cfg.force[2]), A(1.0 / omega_p), s6 ? d6.p : nullptr,
-        gamma ? dg.p : nullptr, n);
+    strain_rate_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(strain_args(), s6 ? d6.p : nullptr,
+                                                                        gamma ? dg.p : nullptr, n);
     CK(cudaGetLastError());
     if (s6) CK(cudaMemcpyAsync(s6, d6.p, size_t(6) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (gamma) CK(cudaMemcpyAsync(gamma, dg.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+  }
+
+  // ---- per-cell relaxation field and WALE (les.rs) -------------------------
+  DevBuf<A> omega_dev;
+  bool omega_on = false;
+
+  // Kinds without the field: the two-cells-per-thread pair and tile kernels.
+  bool omega_kind_ok(int kind) const { return !(kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE); }
+  void omega_install() {
+    if (cfg.smagorinsky_cs > 0.0)
+      throw Error(LBMB_ERR_UNSUPPORTED, "a relaxation field and the Smagorinsky option cannot be combined");
+    omega_on = true;
+    if (!omega_kind_ok(kernel_mode)) kernel_mode = lean_ok(coll) ? LBMB_SWEEP_LEAN : default_kernel();
+    invalidate_graphs();
+  }
+  int default_kernel() const {
+    if (lean_ok(coll)) return LBMB_SWEEP_LEAN;
+    if (sizeof(S) >= 4 && !has_uniform_force()) return LBMB_SWEEP_ASYNC;
+    if (sizeof(S) < 4 && window_ok()) return LBMB_SWEEP_WINDOW;
+    return LBMB_SWEEP_DIRECT;
+  }
+
+  void set_omega_field(const double* omega) override {
+    if (!omega) {
+      omega_on = false;
+      invalidate_graphs();
+      return;
+    }
+    for (int64_t c = 0; c < n; ++c)
+      if (!std::isfinite(omega[c])) invalid("omega field values must be finite");
+    std::vector<A> h(static_cast<size_t>(n));
+    for (int64_t c = 0; c < n; ++c) h[size_t(c)] = A(omega[c]);
+    if (omega_dev.n != size_t(n)) omega_dev.alloc(size_t(n));
+    CK(cudaMemcpyAsync(omega_dev.p, h.data(), h.size() * sizeof(A), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    omega_install();
+  }
+
+  void velocity_gradient(double* g9) override {
+    DevBuf<double> u3, dg;
+    velocity_moments(u3);
+    dg.alloc(size_t(9) * n);
+    wale_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
+        strain_args(), u3.p, wall_u.p, cfg.periodic[0], cfg.periodic[1], cfg.periodic[2], A(cfg.nu), 0, A(0), dg.p,
+        nullptr, nullptr, nullptr, nullptr, n);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(g9, dg.p, size_t(9) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+
+  // WaleLes::update (les.rs:120-211): nu_t and the omega+ field, installed
+  // for the next collision without leaving the device.
+  void wale_update(double tau_eff_max, double* nu_t, lbmb_wale_diag* diag) override {
+    if (cfg.smagorinsky_cs > 0.0)
+      throw Error(LBMB_ERR_UNSUPPORTED, "WALE and the Smagorinsky option cannot be combined");
+    const bool clip = !std::isnan(tau_eff_max);
+    const A nu0 = A(cfg.nu);
+    const A tau0 = A(0.5) + A(3.0) * nu0;
+    A nu_t_max = A(0);
+    if (clip) {
+      if (!(std::isfinite(tau_eff_max) && tau_eff_max > 0.5)) invalid("tau_eff_max must be finite and greater than 0.5");
+      if (A(tau_eff_max) < tau0) invalid("tau_eff_max must be at least the laminar tau for this solver");
+      nu_t_max = (A(tau_eff_max) - tau0) / A(3.0);
+    }
+    DevBuf<double> u3, dnu;
+    DevBuf<unsigned long long> cnt;
+    cnt.alloc(2);
+    CK(cudaMemsetAsync(cnt.p, 0, 2 * sizeof(unsigned long long), st));
+    velocity_moments(u3);
+    if (nu_t) dnu.alloc(size_t(n));
+    if (omega_dev.n != size_t(n)) omega_dev.alloc(size_t(n));
+    wale_kernel<Q, S><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(
+        strain_args(), u3.p, wall_u.p, cfg.periodic[0], cfg.periodic[1], cfg.periodic[2], nu0, clip ? 1 : 0,
+        nu_t_max, nullptr, nu_t ? dnu.p : nullptr, omega_dev.p, cnt.p, cnt.p + 1, n);
+    CK(cudaGetLastError());
+    unsigned long long hc[2] = {0, 0};
+    CK(cudaMemcpyAsync(hc, cnt.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    if (nu_t) CK(cudaMemcpyAsync(nu_t, dnu.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    omega_install();
+    if (diag) {
+      double mx = 0.0;
+      std::memcpy(&mx, &hc[1], sizeof(double));
+      diag->clipped_cells = int64_t(hc[0]);
+      diag->clipped_fraction = n == 0 ? 0.0 : double(A(double(hc[0])) / A(double(n)));
+      diag->max_nu_t_before_clipping = mx;
+      diag->tau_eff_max = clip ? tau_eff_max : std::nan("");
+      diag->nu_t_max = clip ? double(nu_t_max) : std::nan("");
+    }
   }
 
   // cached velocity moments (lattice units) into u3 = [ux | uy | uz]
@@ -1883,6 +1997,7 @@ struct Engine final : EngineBase {
   void adjoint_torque(const lbmb_ibm_config& c0, const lbmb_adjoint_config& ac, lbmb_adjoint_result* out,
                       double* dJ_dpos, double* torque_out) override {
     if (coll != COLL_TRT) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint covers TRT/BGK collision");
+    if (omega_on) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs uniform relaxation rates (no omega field)");
     if (cfg.smagorinsky_cs > 0.0) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs the subgrid model off");
     if (has_uniform_force()) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs no uniform body force");
     if (!scalars.empty()) throw Error(LBMB_ERR_UNSUPPORTED, "the adjoint needs a solver without scalars");
@@ -2282,6 +2397,7 @@ struct Batch final : BatchBase {
       if (!e->lean_ok(e->coll))
         throw Error(LBMB_ERR_UNSUPPORTED, "batch solvers need TRT/BGK, fp32/fp16/bf16 storage, no uniform force");
       if (!e->scalars.empty()) throw Error(LBMB_ERR_UNSUPPORTED, "batch solvers carry no scalar distributions");
+      if (e->omega_on) throw Error(LBMB_ERR_UNSUPPORTED, "batch solvers carry no relaxation field");
       eng.push_back(e);
     }
     ncase = int(eng.size());

@@ -55,6 +55,10 @@ struct HydroParams {
   A les_c;  // 18 sqrt(2) Cs^2 (0: no LES)
   A tau0;   // 3 nu + 1/2
   A magic;  // TRT magic parameter (<= 0: BGK, omega_m = omega_p)
+  // Per-cell relaxation field (Solver::set_omega_field; null when off): TRT
+  // takes omega+ = field, c+ = 1 - omega+/2 with omega- unchanged
+  // (kernels.rs:151-156), the central moment its shear rate (kernels.rs:481).
+  const A* omega_field;
 };
 
 // Smagorinsky LES on the shear rate (no reference counterpart; off unless
@@ -121,12 +125,18 @@ __device__ __forceinline__ A les_tau(const A (&f)[Q], A rho, A ux, A uy, A uz, A
 // ones (TRT keeps the magic parameter, BGK keeps omega_m = omega_p).
 template <int Q, class A, bool FAST = false>
 __device__ __forceinline__ void cell_rates(const HydroParams<A>& p, const A (&f)[Q], A rho, A ux, A uy, A uz, A& op,
-                                           A& om, A& cp, A& cm, A& os) {
+                                           A& om, A& cp, A& cm, A& os, int64_t cell) {
   op = p.omega_p;
   om = p.omega_m;
   cp = p.cp;
   cm = p.cm;
   os = p.omega_shear;
+  if (p.omega_field) {
+    op = p.omega_field[cell];
+    cp = A(1) - op / A(2);
+    os = op;
+    return;
+  }
   if (p.les_c > A(0)) {
     const A te = les_tau<Q, A, FAST>(f, rho, ux, uy, uz, p.les_c, p.tau0);
     if constexpr (FAST) {
@@ -426,7 +436,7 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
   const A uy = (m1 + half * Fpy) * inv;
   const A uz = (m2 + half * Fpz) * inv;
   A op, om, cp, cm, os;
-  cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
+  cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell);
   if constexpr (COLL == COLL_CM)
     collide_cm<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, os);
   else

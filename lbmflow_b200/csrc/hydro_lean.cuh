@@ -17,7 +17,7 @@ namespace lbmb {
 constexpr int LEAN_BLOCK = 128;
 
 template <int Q>
-__device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroParams<float>& p) {
+__device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroParams<float>& p, int64_t cell) {
   using L = Lat<Q>;
   constexpr int NP = (Q - 1) / 2;
   static_assert(pair_heads_positive<Q>(), "pair head convention");
@@ -39,7 +39,7 @@ __device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroPara
   const float inv = rcp_fast(rho);
   const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
   const float usq = ux * ux + uy * uy + uz * uz;
-  float op = p.omega_p, om = p.omega_m;
+  float op = p.omega_field ? p.omega_field[cell] : p.omega_p, om = p.omega_m;
   if (p.les_c > 0.f) {
     float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
@@ -137,7 +137,7 @@ __device__ __forceinline__ void lean_cell(const HydroParams<float>& p, uint32_t 
       }
     }
   }
-  const float rho = trt_lean_collide<Q>(f, p);
+  const float rho = trt_lean_collide<Q>(f, p, int64_t(c));
   if (fl & F_MOVING) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {

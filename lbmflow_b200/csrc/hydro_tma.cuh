@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
           const A ux = m0 * inv, uy = m1 * inv, uz = m2 * inv;
           const A z0 = A(0);
           A op, om, cp, cm, os;
-          cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os);
+          cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, int64_t(cell));
           if constexpr (COLL == COLL_CM)
             collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, os);
           else

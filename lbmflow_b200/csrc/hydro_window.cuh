@@ -113,10 +113,11 @@ __global__ void __launch_bounds__(TILE_CELLS, MINB)
       }
       rho = 1.f + dr;
       const float inv = fast_rcp(rho);
-      collide_cm<Q, false, float, true>(f, rho, m0 * inv, m1 * inv, m2 * inv, 0.f, 0.f, 0.f, p.omega_shear, p.les_c,
+      collide_cm<Q, false, float, true>(f, rho, m0 * inv, m1 * inv, m2 * inv, 0.f, 0.f, 0.f,
+                                        p.omega_field ? p.omega_field[c] : p.omega_shear, p.les_c,
                                         p.tau0);
     } else {
-      rho = trt_lean_collide<Q>(f, p);
+      rho = trt_lean_collide<Q>(f, p, int64_t(c));
     }
     if (fl & F_MOVING) {
 #pragma unroll

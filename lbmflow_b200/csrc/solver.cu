@@ -326,6 +326,28 @@ int lbmb_scalar_oxygen_uptake(lbmb_solver* h, int32_t k, const lbmb_our_model* m
   });
 }
 
+int lbmb_set_omega_field(lbmb_solver* h, const double* omega) {
+  return guarded([&] {
+    NEED(h);
+    h->e->set_omega_field(omega);
+  });
+}
+
+int lbmb_gather_velocity_gradient(lbmb_solver* h, double* g9) {
+  return guarded([&] {
+    NEED(h);
+    if (!g9) lbmb::invalid("null output");
+    h->e->velocity_gradient(g9);
+  });
+}
+
+int lbmb_wale_update(lbmb_solver* h, double tau_eff_max, double* nu_t, lbmb_wale_diag* diag) {
+  return guarded([&] {
+    NEED(h);
+    h->e->wale_update(tau_eff_max, nu_t, diag);
+  });
+}
+
 int lbmb_gather_strain_rate(lbmb_solver* h, double* s6, double* gamma) {
   return guarded([&] {
     NEED(h);
