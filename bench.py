@@ -522,6 +522,10 @@ def run_b200(args, rank, world, local):
         tune = {"kind": args.sweep_kernel, "even_blocks_per_sm": 0, "odd_blocks_per_sm": 0,
                 "best_ms_per_step": None, "default_ms_per_step": None}
     else:
+        # tune on a developed flow: on the quiescent start the central-moment
+        # exact-rest skip makes every kernel unrepresentatively cheap
+        if args.tune_after > 0:
+            g.run_impeller(body, args.tune_after)
         tune = g.autotune_sweep(8)
     cfg = lb.DirectForcingConfig()
     # warm-up (untimed)
@@ -615,12 +619,15 @@ def run_b200(args, rank, world, local):
                    "lattice": f"D3Q{q}", "collision": coll_name, "storage": storage, "nu": nu, "u_tip": 0.05,
                    "re": 2000, "smagorinsky_cs": args.les_cs,
                    "les_note": "library option; without it the reference operators diverge on this "
-                               "under-resolved Re=2000 tank (D3Q27 CM at step ~2390, D3Q19 TRT at ~186)",
+                               "under-resolved Re=2000 tank (D3Q27 CM at step ~2390, D3Q19 TRT at ~186); "
+                               "the reference's WALE closure (lbmb_wale_update every 10 steps) also keeps "
+                               "it finite but is a host-driven per-step call outside the runner loop",
                    "ibm": "3 sweeps, tol 1e-2, radius 1",
                    "top": "free-slip (specular) liquid surface" if FREE_SLIP_TOP else "solid lid (reference)",
                    "sweep_kernel": tune["kind"], "autotune": {k: tune[k] for k in
                                                               ("even_blocks_per_sm", "odd_blocks_per_sm",
-                                                               "best_ms_per_step", "default_ms_per_step")},
+                                                               "best_ms_per_step", "default_ms_per_step")}
+                   | {"tuned_after_runner_steps": args.tune_after},
                    "l2": "inputs larger than L2 (populations %.0f MB)" % (q * 4 * n_cells / 1e6),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -675,6 +682,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--hydro-steps", type=int, default=200)
+    ap.add_argument("--tune-after", type=int, default=300,
+                    help="untimed runner steps before the autotuner runs (developed flow)")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--tank-T", type=int, default=128, help="tank diameter in cells (128 = the benchmark case)")
     ap.add_argument("--lattice", type=int, default=27, choices=[19, 27])

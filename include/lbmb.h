@@ -177,9 +177,10 @@ int lbmb_get_force_field(lbmb_solver* h, double* out);
  * rate (n values; NULL removes it) for the following collisions: TRT/BGK
  * take omega+ = field and c+ = 1 - omega+/2 with omega- unchanged
  * (kernels.rs:151-156), the central moment takes it as its shear rate
- * (kernels.rs:481). Not combined with smagorinsky_cs > 0; the pair and
- * tile sweep kernels do not take it (a solver on one of them moves to its
- * default kernel), nor do batches and the adjoint. */
+ * (kernels.rs:481). Not combined with smagorinsky_cs > 0. While a field
+ * is set the sweep runs on the direct, bulk or window kernel (a solver on
+ * another kind moves to window, or direct where window cannot run);
+ * batches and the adjoint do not take it. */
 int lbmb_set_omega_field(lbmb_solver* h, const double* omega);
 
 /* Solver::gather_velocity_gradient (solver.rs:5482-5582): n x 9 row-major,

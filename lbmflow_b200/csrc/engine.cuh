@@ -398,7 +398,6 @@ struct Engine final : EngineBase {
 
   HydroParams<A> hydro_params() {
     HydroParams<A> p;
-    p.omega_field = omega_on ? omega_dev.p : nullptr;
     p.f = fp;
     p.plane = uint32_t(plane);
     p.nxy = nx * ny;
@@ -439,7 +438,7 @@ struct Engine final : EngineBase {
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TMA_TILE, smem));
       tma_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
     }
-    kern<<<unsigned(tma_grid[slot]), TMA_TILE, smem, s>>>(p, n, int(ntiles), d_err.p);
+    kern<<<unsigned(tma_grid[slot]), TMA_TILE, smem, s>>>(p, n, int(ntiles), d_err.p, omega_ptr());
     CK(cudaGetLastError());
   }
 
@@ -477,7 +476,7 @@ struct Engine final : EngineBase {
     const bool wide = sizeof(S) >= 4;
     const bool pair = std::is_same<A, float>::value && nx % 2 == 0 && !has_uniform_force();
     if (omega_on && !omega_kind_ok(kind))
-      throw Error(LBMB_ERR_UNSUPPORTED, "the pair and tile sweeps do not take a relaxation field");
+      throw Error(LBMB_ERR_UNSUPPORTED, "with a relaxation field the sweep runs on direct, bulk or window kernels");
     if (kind == LBMB_SWEEP_ASYNC && !wide)
       throw Error(LBMB_ERR_UNSUPPORTED, "the cp.async sweep needs 4- or 8-byte population storage");
     if ((kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE) && !pair)
@@ -565,7 +564,7 @@ struct Engine final : EngineBase {
 
   // Whether the two-cells-per-thread kernel covers this sweep.
   bool pair_ok(const HydroParams<A>& p, int) const {
-    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0 && !p.omega_field;
+    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0 && !omega_on;
   }
 
   // Tile list and window offsets of the tile-pipelined sweep.
@@ -619,7 +618,8 @@ struct Engine final : EngineBase {
         window_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(n_tiles_active, slots)));
       }
       if (n_tiles_active == 0) return;
-      kern<<<unsigned(window_grid[slot]), TILE_CELLS, smem, s>>>(p, tile_list.p, n_tiles_active, tile_dirs[ODD]);
+      kern<<<unsigned(window_grid[slot]), TILE_CELLS, smem, s>>>(p, tile_list.p, n_tiles_active, tile_dirs[ODD],
+                                                                 omega_ptr());
       CK(cudaGetLastError());
     }
   }
@@ -680,14 +680,15 @@ struct Engine final : EngineBase {
         const int bx = nx >= 128 ? 128 : int(ceil_div(nx, 32) * 32);
         dim3 block(bx), grid(unsigned(ceil_div(nx, bx)), unsigned(ny), unsigned(nz));
         if (p.uniform_force)
-          hydro_aa_kernel<Q, S, COLL, ODD, true><<<grid, block, 0, s>>>(p);
+          hydro_aa_kernel<Q, S, COLL, ODD, true><<<grid, block, 0, s>>>(p, omega_ptr());
         else
-          hydro_aa_kernel<Q, S, COLL, ODD, false><<<grid, block, 0, s>>>(p);
+          hydro_aa_kernel<Q, S, COLL, ODD, false><<<grid, block, 0, s>>>(p, omega_ptr());
         CK(cudaGetLastError());
       }
     }
     if (cells && !p.uniform_force && nslots > 0) {
-      hydro_cells_kernel<Q, S, COLL, ODD><<<unsigned(ceil_div(nslots, 128)), 128, 0, s>>>(p, slot_cell.p, nslots);
+      hydro_cells_kernel<Q, S, COLL, ODD><<<unsigned(ceil_div(nslots, 128)), 128, 0, s>>>(p, slot_cell.p, nslots,
+                                                                                          omega_ptr());
       CK(cudaGetLastError());
     }
   }
@@ -872,6 +873,12 @@ struct Engine final : EngineBase {
     if (lean_ok(coll))
       for (int ev = 10; ev >= 6; --ev)
         for (int od = 9; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
+    if (omega_on) {
+      std::vector<Cand> keep;
+      for (const Cand& cd : cands)
+        if (omega_kind_ok(cd.kind)) keep.push_back(cd);
+      cands.swap(keep);
+    }
     const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
     const int ae0 = async_minb[0], ao0 = async_minb[1];
     const int we0 = window_minb[0], wo0 = window_minb[1];
@@ -1167,21 +1174,21 @@ struct Engine final : EngineBase {
   // ---- per-cell relaxation field and WALE (les.rs) -------------------------
   DevBuf<A> omega_dev;
   bool omega_on = false;
+  const A* omega_ptr() const { return omega_on ? omega_dev.p : nullptr; }
 
-  // Kinds without the field: the two-cells-per-thread pair and tile kernels.
-  bool omega_kind_ok(int kind) const { return !(kind == LBMB_SWEEP_PAIR || kind == LBMB_SWEEP_TILE); }
+  // Kinds that take the field: direct loads, bulk copies and the window
+  // kernel (the tuned cp.async, lean, pair and tile kernels keep their
+  // uniform-rate code; a per-cell rate cost the cp.async central-moment
+  // kernel 14% on B200 even when unused).
+  bool omega_kind_ok(int kind) const {
+    return kind == LBMB_SWEEP_DIRECT || kind == LBMB_SWEEP_BULK || kind == LBMB_SWEEP_WINDOW;
+  }
   void omega_install() {
     if (cfg.smagorinsky_cs > 0.0)
       throw Error(LBMB_ERR_UNSUPPORTED, "a relaxation field and the Smagorinsky option cannot be combined");
     omega_on = true;
-    if (!omega_kind_ok(kernel_mode)) kernel_mode = lean_ok(coll) ? LBMB_SWEEP_LEAN : default_kernel();
+    if (!omega_kind_ok(kernel_mode)) kernel_mode = window_ok() ? LBMB_SWEEP_WINDOW : LBMB_SWEEP_DIRECT;
     invalidate_graphs();
-  }
-  int default_kernel() const {
-    if (lean_ok(coll)) return LBMB_SWEEP_LEAN;
-    if (sizeof(S) >= 4 && !has_uniform_force()) return LBMB_SWEEP_ASYNC;
-    if (sizeof(S) < 4 && window_ok()) return LBMB_SWEEP_WINDOW;
-    return LBMB_SWEEP_DIRECT;
   }
 
   void set_omega_field(const double* omega) override {

@@ -55,10 +55,6 @@ struct HydroParams {
   A les_c;  // 18 sqrt(2) Cs^2 (0: no LES)
   A tau0;   // 3 nu + 1/2
   A magic;  // TRT magic parameter (<= 0: BGK, omega_m = omega_p)
-  // Per-cell relaxation field (Solver::set_omega_field; null when off): TRT
-  // takes omega+ = field, c+ = 1 - omega+/2 with omega- unchanged
-  // (kernels.rs:151-156), the central moment its shear rate (kernels.rs:481).
-  const A* omega_field;
 };
 
 // Smagorinsky LES on the shear rate (no reference counterpart; off unless
@@ -123,16 +119,22 @@ __device__ __forceinline__ A les_tau(const A (&f)[Q], A rho, A ux, A uy, A uz, A
 
 // Relaxation rates of one cell: the configured ones, or the LES-adjusted
 // ones (TRT keeps the magic parameter, BGK keeps omega_m = omega_p).
-template <int Q, class A, bool FAST = false>
+// omega: the per-cell relaxation field (Solver::set_omega_field; null when
+// off): TRT takes omega+ = field, c+ = 1 - omega+/2 with omega- unchanged
+// (kernels.rs:151-156), the central moment its shear rate (kernels.rs:481).
+// It travels beside HydroParams rather than in it: the tuned sweep kernels
+// are sensitive to the layout of their parameter block (a changed layout
+// cost the cp.async central-moment kernel 8-14% on B200).
+template <int Q, class A, bool FAST = false, bool FIELD = true>
 __device__ __forceinline__ void cell_rates(const HydroParams<A>& p, const A (&f)[Q], A rho, A ux, A uy, A uz, A& op,
-                                           A& om, A& cp, A& cm, A& os, int64_t cell) {
+                                           A& om, A& cp, A& cm, A& os, int64_t cell, const A* omega = nullptr) {
   op = p.omega_p;
   om = p.omega_m;
   cp = p.cp;
   cm = p.cm;
   os = p.omega_shear;
-  if (p.omega_field) {
-    op = p.omega_field[cell];
+  if (FIELD && omega) {
+    op = omega[cell];
     cp = A(1) - op / A(2);
     os = op;
     return;
@@ -351,10 +353,13 @@ __device__ __forceinline__ void collide_cm(A (&f)[Q], A rho, A ux, A uy, A uz, A
 
 // One cell. GENERIC: solid-neighbour mask, moving walls and periodic wrap;
 // otherwise the interior fast path. FORCED: Guo source from the uniform
-// force and, on F_FORCED cells, the force slots.
-template <int Q, class S, int COLL, bool ODD, bool GENERIC, bool FORCED>
+// force and, on F_FORCED cells, the force slots. FIELD: the per-cell
+// relaxation field is read when set (kernels that never run with a field
+// compile it out).
+template <int Q, class S, int COLL, bool ODD, bool GENERIC, bool FORCED, bool FIELD = false>
 __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::A>& p, int x, int y, int z,
-                                           uint32_t cell, uint8_t fl) {
+                                           uint32_t cell, uint8_t fl,
+                                           const typename Codec<S>::A* omega = nullptr) {
   using A = typename Codec<S>::A;
   using L = Lat<Q>;
   using CD = Codec<S>;
@@ -436,7 +441,7 @@ __device__ __forceinline__ void hydro_cell(const HydroParams<typename Codec<S>::
   const A uy = (m1 + half * Fpy) * inv;
   const A uz = (m2 + half * Fpz) * inv;
   A op, om, cp, cm, os;
-  cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell);
+  cell_rates<Q, A, false, FIELD>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell, omega);
   if constexpr (COLL == COLL_CM)
     collide_cm<Q, FORCED, A>(f, rho, ux, uy, uz, Fcx, Fcy, Fcz, os);
   else
@@ -471,6 +476,13 @@ __device__ __noinline__ void hydro_cell_generic(const HydroParams<typename Codec
                                                 uint32_t cell, uint8_t fl) {
   hydro_cell<Q, S, COLL, ODD, true, FORCED>(p, x, y, z, cell, fl);
 }
+// The same with the per-cell relaxation field (kernels that take it).
+template <int Q, class S, int COLL, bool ODD, bool FORCED>
+__device__ __noinline__ void hydro_cell_generic_field(const HydroParams<typename Codec<S>::A> p, int x, int y, int z,
+                                                      uint32_t cell, uint8_t fl,
+                                                      const typename Codec<S>::A* omega) {
+  hydro_cell<Q, S, COLL, ODD, true, FORCED, true>(p, x, y, z, cell, fl, omega);
+}
 
 template <class A>
 struct HydroOccupancy {
@@ -482,7 +494,7 @@ struct HydroOccupancy {
 // the IBM force update); FORCED = true (uniform body force) forces every cell.
 template <int Q, class S, int COLL, bool ODD, bool FORCED>
 __global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
-    hydro_aa_kernel(HydroParams<typename Codec<S>::A> p) {
+    hydro_aa_kernel(HydroParams<typename Codec<S>::A> p, const typename Codec<S>::A* omega) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= p.nx) return;
   const int y = blockIdx.y, z = blockIdx.z;
@@ -491,14 +503,15 @@ __global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN
   if (fl & F_SOLID) return;
   if (!FORCED && (fl & F_FORCED)) return;
   if (fl & (F_BOUNDARY | F_WRAP))
-    hydro_cell_generic<Q, S, COLL, ODD, FORCED>(p, x, y, z, cell, fl);
+    hydro_cell_generic_field<Q, S, COLL, ODD, FORCED>(p, x, y, z, cell, fl, omega);
   else
-    hydro_cell<Q, S, COLL, ODD, false, FORCED>(p, x, y, z, cell, fl);
+    hydro_cell<Q, S, COLL, ODD, false, FORCED, true>(p, x, y, z, cell, fl, omega);
 }
 
 // Cell-list sweep over the forced cells (after the IBM force update).
 template <int Q, class S, int COLL, bool ODD>
-__device__ __forceinline__ void forced_cell(const HydroParams<typename Codec<S>::A>& p, uint32_t cell) {
+__device__ __forceinline__ void forced_cell(const HydroParams<typename Codec<S>::A>& p, uint32_t cell,
+                                            const typename Codec<S>::A* omega = nullptr) {
   const uint32_t nxy = uint32_t(p.nxy);
   const int z = int(cell / nxy);
   const uint32_t r = cell - uint32_t(z) * nxy;
@@ -506,15 +519,16 @@ __device__ __forceinline__ void forced_cell(const HydroParams<typename Codec<S>:
   const int x = int(r - uint32_t(y) * uint32_t(p.nx));
   const uint8_t fl = p.flags[cell];
   if (fl & F_SOLID) return;
-  hydro_cell<Q, S, COLL, ODD, true, true>(p, x, y, z, cell, fl);
+  hydro_cell<Q, S, COLL, ODD, true, true, true>(p, x, y, z, cell, fl, omega);
 }
 
 template <int Q, class S, int COLL, bool ODD>
 __global__ void __launch_bounds__(128, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
-    hydro_cells_kernel(HydroParams<typename Codec<S>::A> p, const int64_t* cells, int64_t ncells) {
+    hydro_cells_kernel(HydroParams<typename Codec<S>::A> p, const int64_t* cells, int64_t ncells,
+                       const typename Codec<S>::A* omega) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= ncells) return;
-  forced_cell<Q, S, COLL, ODD>(p, uint32_t(cells[i]));
+  forced_cell<Q, S, COLL, ODD>(p, uint32_t(cells[i]), omega);
 }
 
 }  // namespace lbmb

@@ -281,8 +281,7 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
         }
       const float rho = 1.f + dr;
       const float inv = fast_rcp(rho);
-      collide_cm_x2(FP, F1, rho, m0 * inv, m1 * inv, m2 * inv, p.omega_field ? p.omega_field[cell] : p.omega_shear,
-                    p.les_c, p.tau0);
+      collide_cm_x2(FP, F1, rho, m0 * inv, m1 * inv, m2 * inv, p.omega_shear, p.les_c, p.tau0);
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int jj = L::cy(q) + 1, kk = L::cz(q) + 1;
@@ -332,15 +331,15 @@ __global__ void __launch_bounds__(ASYNC_TILE, MINB)
     if constexpr (COLL == COLL_CM) {
       // subgrid rate from the transformed moments (fp32), else les_tau
       constexpr bool LK = std::is_same<A, float>::value;
-      A os = p.omega_field ? p.omega_field[cell] : p.omega_shear;
+      A os = p.omega_shear;
       if constexpr (!LK) {
         A op, om, cp, cm;
-        cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell);
+        cell_rates<Q, A, false, false>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell);
       }
       collide_cm<Q, false, A, LK>(f, rho, ux, uy, uz, z0, z0, z0, os, p.les_c, p.tau0);
     } else {
       A op, om, cp, cm, os;
-      cell_rates<Q, A, true>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell);
+      cell_rates<Q, A, true, false>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, cell);
       collide_trt<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, op, om, cp, cm);
     }
     const uint32_t mask = smk[stage * ASYNC_TILE + j];

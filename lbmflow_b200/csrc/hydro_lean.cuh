@@ -16,8 +16,11 @@ namespace lbmb {
 
 constexpr int LEAN_BLOCK = 128;
 
-template <int Q>
-__device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroParams<float>& p, int64_t cell) {
+// FIELD: take omega+ from the per-cell relaxation field when one is set
+// (the window kernel); the lean kernel is never launched with a field.
+template <int Q, bool FIELD = false>
+__device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroParams<float>& p, int64_t cell,
+                                                  const float* omega = nullptr) {
   using L = Lat<Q>;
   constexpr int NP = (Q - 1) / 2;
   static_assert(pair_heads_positive<Q>(), "pair head convention");
@@ -39,7 +42,7 @@ __device__ __forceinline__ float trt_lean_collide(float (&f)[Q], const HydroPara
   const float inv = rcp_fast(rho);
   const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
   const float usq = ux * ux + uy * uy + uz * uz;
-  float op = p.omega_field ? p.omega_field[cell] : p.omega_p, om = p.omega_m;
+  float op = (FIELD && omega) ? omega[cell] : p.omega_p, om = p.omega_m;
   if (p.les_c > 0.f) {
     float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll

@@ -85,7 +85,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 template <int Q, class S, int COLL, bool ODD, bool ROWS_ALIGNED>
 __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
-    hydro_tma_kernel(HydroParams<typename Codec<S>::A> p, int64_t ncells, int ntiles, int* err) {
+    hydro_tma_kernel(HydroParams<typename Codec<S>::A> p, int64_t ncells, int ntiles, int* err,
+                     const typename Codec<S>::A* omega) {
   using A = typename Codec<S>::A;
   using L = Lat<Q>;
   using CD = Codec<S>;
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
           const int64_t r = cell - int64_t(z) * nxy;
           const int y = int(r / nx);
           const int x = int(r - int64_t(y) * nx);
-          hydro_cell_generic<Q, S, COLL, ODD, false>(p, x, y, z, uint32_t(cell), fl);
+          hydro_cell_generic_field<Q, S, COLL, ODD, false>(p, x, y, z, uint32_t(cell), fl, omega);
         } else {
           const S* w = sm + s * Q * W::WIN;
           const uint32_t mask = (fl & F_BOUNDARY) ? p.nbr[cell] : 0u;
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
           const A ux = m0 * inv, uy = m1 * inv, uz = m2 * inv;
           const A z0 = A(0);
           A op, om, cp, cm, os;
-          cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, int64_t(cell));
+          cell_rates<Q, A>(p, f, rho, ux, uy, uz, op, om, cp, cm, os, int64_t(cell), omega);
           if constexpr (COLL == COLL_CM)
             collide_cm<Q, false, A>(f, rho, ux, uy, uz, z0, z0, z0, os);
           else

@@ -40,7 +40,7 @@ constexpr int window_stages() {
 // allocation is sized for (2 = 128 registers, 3 = 85 -> 80, 4 = 64).
 template <int Q, class S, bool ODD, int STAGES, int COLL, int MINB>
 __global__ void __launch_bounds__(TILE_CELLS, MINB)
-    hydro_window_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, TileDirs dirs) {
+    hydro_window_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, TileDirs dirs, const float* omega) {
   using L = Lat<Q>;
   using W = TileWin<S>;
   using CD = Codec<S>;
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(TILE_CELLS, MINB)
       const int z = int(c / uint32_t(nxy));
       const int r = int(c - uint32_t(z) * uint32_t(nxy));
       const int y = r / nx;
-      hydro_cell_generic<Q, S, COLL, ODD, false>(p, r - y * nx, y, z, c, uint8_t(fl));
+      hydro_cell_generic_field<Q, S, COLL, ODD, false>(p, r - y * nx, y, z, c, uint8_t(fl), omega);
       continue;
     }
     const uint32_t mk = (fl & F_BOUNDARY) ? p.nbr[c] : 0u;
@@ -114,10 +114,10 @@ __global__ void __launch_bounds__(TILE_CELLS, MINB)
       rho = 1.f + dr;
       const float inv = fast_rcp(rho);
       collide_cm<Q, false, float, true>(f, rho, m0 * inv, m1 * inv, m2 * inv, 0.f, 0.f, 0.f,
-                                        p.omega_field ? p.omega_field[c] : p.omega_shear, p.les_c,
+                                        omega ? omega[c] : p.omega_shear, p.les_c,
                                         p.tau0);
     } else {
-      rho = trt_lean_collide<Q>(f, p, int64_t(c));
+      rho = trt_lean_collide<Q, true>(f, p, int64_t(c), omega);
     }
     if (fl & F_MOVING) {
 #pragma unroll

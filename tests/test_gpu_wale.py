@@ -18,7 +18,7 @@ from cases import TOL, cavity
 
 pytestmark = pytest.mark.gpu
 
-FIELD_KINDS = ["direct", "bulk", "async", "lean", "window"]
+FIELD_KINDS = ["direct", "bulk", "window"]
 
 
 def oracle(dims, prec, **kw):
@@ -35,11 +35,12 @@ def periodic_state(n=12, nu=0.02, u0=0.04):
     return (n, n, n), np.ones(n ** 3), u, nu
 
 
-@pytest.mark.parametrize("kind", ["direct", "async", "lean"])
+@pytest.mark.parametrize("kind", ["direct", "window"])
 def test_uniform_field_equals_field_off(kind):
     dims, rho, u, nu = periodic_state()
-    off = lb.Solver(dims, storage="f64" if kind != "lean" else "f32", nu=nu, periodic=(True, True, True))
-    on = lb.Solver(dims, storage="f64" if kind != "lean" else "f32", nu=nu, periodic=(True, True, True))
+    st = "f64" if kind == "direct" else "f32"
+    off = lb.Solver(dims, storage=st, nu=nu, periodic=(True, True, True))
+    on = lb.Solver(dims, storage=st, nu=nu, periodic=(True, True, True))
     for g in (off, on):
         g.set_sweep_kernel(kind)
         g.init_with(rho, u)
@@ -47,7 +48,7 @@ def test_uniform_field_equals_field_off(kind):
     assert on.sweep_kernel == kind
     off.run(7)
     on.run(7)
-    eps = np.finfo(np.float64 if kind != "lean" else np.float32).eps
+    eps = np.finfo(np.float64 if st == "f64" else np.float32).eps
     a, b = off.stage_out(), on.stage_out()
     assert np.abs(a - b).max() <= 5 * eps * max(np.abs(a).max(), 1.0)
 
@@ -56,9 +57,7 @@ def test_uniform_field_equals_field_off(kind):
 @pytest.mark.parametrize("q,coll", [(19, "trt"), (27, "cm")])
 def test_nonuniform_field_matches_oracle(kind, q, coll):
     dims, solid, wall_u, nu = cavity(14, u_lid=0.06, re=40.0)
-    if kind == "lean" and coll == "cm":
-        pytest.skip("TRT-only kernel")
-    prec = "f64" if kind in ("direct", "bulk", "async") else "f32"
+    prec = "f64" if kind in ("direct", "bulk") else "f32"
     os_ = 1.0 / (3.0 * nu + 0.5)
     g = lb.Solver(dims, lattice=q, collision=coll, storage=prec, nu=nu, omega_shear=os_, solid=solid, wall_u=wall_u)
     c = oracle(dims, prec, q=q, collision=coll, nu=nu, omega_shear=os_, solid=solid, wall_u=wall_u)
@@ -120,9 +119,11 @@ def test_field_refusals_and_removal():
     g = lb.Solver(dims, storage="f32", nu=nu, solid=solid, wall_u=wall_u)
     g.set_sweep_kernel("pair")
     g.set_omega_field(np.full(g.n, 1.5))
-    assert g.sweep_kernel not in ("pair", "tile")
-    with pytest.raises(lb.UnsupportedError):
-        g.set_sweep_kernel("tile")
+    assert g.sweep_kernel == "window"
+    for kind in ("tile", "pair", "lean", "async"):
+        with pytest.raises(lb.UnsupportedError):
+            g.set_sweep_kernel(kind)
+    assert {t[0] for t in g.autotune_sweep(4)["trials"]} <= {"direct", "bulk", "window"}
     g.set_omega_field(None)
     g.set_sweep_kernel("pair")
     s = lb.Solver(dims, storage="f32", nu=nu, solid=solid, wall_u=wall_u, smagorinsky_cs=0.1)
