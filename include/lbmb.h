@@ -36,7 +36,11 @@ enum lbmb_status {
   LBMB_ERR_UNSUPPORTED = -3, /* UnsupportedReason::NotImplemented */
   LBMB_ERR_DIVERGED = -4,    /* non-finite mass detected (Diverged) */
   LBMB_ERR_STATE = -5,       /* call out of order (e.g. scalar not enabled) */
-  LBMB_ERR_NOMEM = -6        /* device allocation failed */
+  LBMB_ERR_NOMEM = -6,       /* device allocation failed */
+  LBMB_ERR_CHECKPOINT = -7   /* CheckpointError: lbmb_last_error() reads
+                              * "<code>: <message>" with the reference's
+                              * stable code (CKPT_IO, CKPT_BAD_MAGIC,
+                              * CKPT_VERSION_MISMATCH, ...) */
 };
 
 enum lbmb_collision { LBMB_BGK = 0, LBMB_TRT = 1, LBMB_CENTRAL_MOMENT = 2 };
@@ -508,6 +512,94 @@ int lbmb_adjoint_torque(lbmb_solver* h, const lbmb_ibm_config* cfg, const lbmb_a
 
 /* Synchronize the solver stream. */
 int lbmb_sync(lbmb_solver* h);
+
+/* ---- Checkpoint/restart (the reference's v3 file format) -----------------
+ * A checkpoint is a directory: manifest.json and rank_0000_part_0000.bin
+ * (crates/lbm-core/src/solver.rs:29-44, 84-118, 4536-4724). Populations are
+ * written over the reference's halo-padded box (halo cells zero) in the
+ * run's dtype: "f64" for F64 storage, "f32" for F32 / F16 / BF16 storage
+ * (16-bit values widen exactly). The stale stash is written as zero planes.
+ * Restoring validates the manifest and the rank file (kind, format version,
+ * dtype, lattice, extents, scenario hash, decomposition hash, rank count,
+ * part geometry, mask hash, payload hash, section lengths, solid mask) and
+ * installs nothing on any failure. */
+
+/* Solver::time (solver.rs:4642): hydro steps taken since creation or
+ * installed by a restore. */
+int lbmb_get_time(const lbmb_solver* h, uint64_t* step);
+
+/* Name of a scalar distribution as the checkpoint records it (the
+ * reference's enable_scalar_distribution name, solver.rs:2856); default
+ * "scalar<k>". At most 63 bytes. */
+int lbmb_set_scalar_name(lbmb_solver* h, int32_t k, const char* name);
+
+/* QoiCheckpointState carried opaque (a JSON object) through save/restore
+ * (Solver::set_qoi_checkpoint_state / qoi_checkpoint_state; section
+ * QOI_ACCUMULATORS, solver.rs:4583-4585). json = NULL clears. get: len
+ * receives the byte length (-1 when none is set); at most cap bytes are
+ * copied. */
+int lbmb_set_qoi_checkpoint_state(lbmb_solver* h, const char* json, int64_t len);
+int lbmb_get_qoi_checkpoint_state(lbmb_solver* h, char* buf, int64_t cap, int64_t* len);
+
+/* Solver::save (solver.rs:4715-4724). */
+int lbmb_checkpoint_save(lbmb_solver* h, const char* dir);
+
+/* Solver::restore (solver.rs:4739-4742, load_into 4759-5060) into this
+ * solver, whose configuration and masks are the authority the checkpoint is
+ * checked against. The scalar distributions of the file replace the
+ * solver's: an enabled scalar is overwritten when its lattice matches,
+ * further ones are enabled; a solver with more scalars than the file, or
+ * with a different scalar lattice, is refused (CKPT_SCENARIO_MISMATCH). The
+ * body-force field of the file becomes the solver's field, both the one the
+ * next collision applies and the one inside the cached moments; solid-cell
+ * moments are installed as carried values. The relaxation field is not part
+ * of the format and is left as it is. */
+int lbmb_checkpoint_restore(lbmb_solver* h, const char* dir);
+
+/* The format on caller-owned compact host arrays, no device involved (the
+ * reference's write_part_checkpoint / read_rank_file on one part). */
+typedef struct {
+  int32_t lattice;    /* 19 | 27 */
+  int32_t collision;  /* lbmb_collision */
+  int32_t dtype_bits; /* 32 | 64: the run's arithmetic type */
+  int32_t dims[3];
+  int32_t periodic[3];
+  double nu, magic, omega_shear;
+  double force[3];
+} lbmb_checkpoint_spec;
+
+typedef struct {
+  char name[64];
+  double diffusivity;
+  int32_t q;          /* 7 or the hydro lattice */
+  double* h;          /* q x ncells, ordinary form, logical post-stream */
+  int64_t h_capacity; /* elements of h (read) */
+  double* conc;       /* ncells */
+} lbmb_checkpoint_scalar;
+
+typedef struct {
+  uint64_t step;
+  double* f;           /* Q x ncells, deviation form */
+  double* moments;     /* 4 x ncells: rho, ux, uy, uz */
+  int32_t has_force_field;
+  double* force_field; /* ncells x 3 */
+  int32_t n_scalars;
+  int32_t scalar_capacity; /* entries of scalars (read) */
+  lbmb_checkpoint_scalar* scalars;
+  int32_t has_qoi;
+  char* qoi_json;
+  int64_t qoi_len;
+  int64_t qoi_capacity; /* bytes of qoi_json (read) */
+} lbmb_checkpoint_data;
+
+int lbmb_checkpoint_write_host(const char* dir, const lbmb_checkpoint_spec* spec, const uint8_t* solid,
+                               const double* wall_u, const lbmb_checkpoint_data* data);
+int lbmb_checkpoint_read_host(const char* dir, const lbmb_checkpoint_spec* spec, const uint8_t* solid,
+                              const double* wall_u, lbmb_checkpoint_data* data);
+
+/* FNV-1a 64 of a byte buffer (the checkpoint payload hash, solver.rs:
+ * 831-835). */
+uint64_t lbmb_fnv1a64(const void* data, uint64_t len);
 
 #ifdef __cplusplus
 }

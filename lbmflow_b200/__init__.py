@@ -23,6 +23,7 @@ _i32p = C.POINTER(C.c_int32)
 _i64p = C.POINTER(C.c_int64)
 
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6
+ERR_CHECKPOINT = -7
 COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
 SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5, "window": 6}
@@ -43,7 +44,9 @@ EXPORTS = (
     "lbmb_batch_create", "lbmb_batch_autotune", "lbmb_batch_run", "lbmb_batch_destroy", "lbmb_adjoint_torque",
     "lbmb_gather_strain_rate", "lbmb_stress_field", "lbmb_stress_summary", "lbmb_wall_shear_proxy",
     "lbmb_scalar_interfacial_flux", "lbmb_scalar_oxygen_uptake", "lbmb_set_omega_field",
-    "lbmb_gather_velocity_gradient", "lbmb_wale_update",
+    "lbmb_gather_velocity_gradient", "lbmb_wale_update", "lbmb_get_time", "lbmb_set_scalar_name",
+    "lbmb_set_qoi_checkpoint_state", "lbmb_get_qoi_checkpoint_state", "lbmb_checkpoint_save",
+    "lbmb_checkpoint_restore", "lbmb_checkpoint_write_host", "lbmb_checkpoint_read_host", "lbmb_fnv1a64",
 )
 
 
@@ -63,12 +66,43 @@ class UnsupportedError(LbmbError):
     """UnsupportedReason::NotImplemented."""
 
 
+class CheckpointError(LbmbError):
+    """CheckpointError (solver.rs:46-82): .code is the reference's stable
+    code ("CKPT_IO", "CKPT_BAD_MAGIC", ...), .message its text, .status the
+    lbmb_status (-7)."""
+
+    def __init__(self, status, msg):
+        code, _, message = msg.partition(": ")
+        super().__init__(status, msg)
+        self.status = status
+        self.code = code
+        self.message = message
+
+
 class Diverged(LbmbError):
     """Non-finite mass detected by run_guarded; .completed steps ran."""
 
     def __init__(self, code, msg, completed):
         super().__init__(code, msg)
         self.completed = completed
+
+
+class _CkptSpec(C.Structure):
+    _fields_ = [("lattice", C.c_int32), ("collision", C.c_int32), ("dtype_bits", C.c_int32),
+                ("dims", C.c_int32 * 3), ("periodic", C.c_int32 * 3), ("nu", C.c_double), ("magic", C.c_double),
+                ("omega_shear", C.c_double), ("force", C.c_double * 3)]
+
+
+class _CkptScalar(C.Structure):
+    _fields_ = [("name", C.c_char * 64), ("diffusivity", C.c_double), ("q", C.c_int32), ("h", _dp),
+                ("h_capacity", C.c_int64), ("conc", _dp)]
+
+
+class _CkptData(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("f", _dp), ("moments", _dp), ("has_force_field", C.c_int32),
+                ("force_field", _dp), ("n_scalars", C.c_int32), ("scalar_capacity", C.c_int32),
+                ("scalars", C.POINTER(_CkptScalar)), ("has_qoi", C.c_int32), ("qoi_json", C.POINTER(C.c_char)),
+                ("qoi_len", C.c_int64), ("qoi_capacity", C.c_int64)]
 
 
 class _Config(C.Structure):
@@ -227,6 +261,16 @@ def lib():
                                           C.POINTER(_AdjointResult), _dp, _dp]
         L.lbmb_reduce_populations_noalloc.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64, vp, _dp,
                                                       _dp, vp]
+        L.lbmb_get_time.argtypes = [vp, C.POINTER(C.c_uint64)]
+        L.lbmb_set_scalar_name.argtypes = [vp, C.c_int32, C.c_char_p]
+        L.lbmb_set_qoi_checkpoint_state.argtypes = [vp, C.c_char_p, C.c_int64]
+        L.lbmb_get_qoi_checkpoint_state.argtypes = [vp, C.c_char_p, C.c_int64, _i64p]
+        L.lbmb_checkpoint_save.argtypes = [vp, C.c_char_p]
+        L.lbmb_checkpoint_restore.argtypes = [vp, C.c_char_p]
+        L.lbmb_checkpoint_write_host.argtypes = [C.c_char_p, C.POINTER(_CkptSpec), _u8p, _dp, C.POINTER(_CkptData)]
+        L.lbmb_checkpoint_read_host.argtypes = [C.c_char_p, C.POINTER(_CkptSpec), _u8p, _dp, C.POINTER(_CkptData)]
+        L.lbmb_fnv1a64.argtypes = [C.c_char_p, C.c_uint64]
+        L.lbmb_fnv1a64.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -241,6 +285,8 @@ def _check(rc, completed=None):
         raise UnsupportedError(rc, msg)
     if rc == ERR_DIVERGED:
         raise Diverged(rc, msg, completed)
+    if rc == ERR_CHECKPOINT:
+        raise CheckpointError(rc, msg)
     raise LbmbError(rc, msg)
 
 
@@ -585,11 +631,60 @@ class Solver:
                 "dJ_domega_minus": r.dJ_domega_minus, "dJ_dpos": dpos[:3 * nm].reshape(nm, 3), "torque": tq,
                 "forward_ms": r.forward_ms, "adjoint_ms": r.adjoint_ms}
 
+    # --- checkpoint/restart ---------------------------------------------------
+    @property
+    def time(self):
+        """Solver::time: hydro steps taken since creation (or restored)."""
+        t = C.c_uint64()
+        _check(lib().lbmb_get_time(self.h, C.byref(t)))
+        return t.value
+
+    def save(self, directory):
+        """Solver::save (solver.rs:4715-4724): manifest.json plus
+        rank_0000_part_0000.bin in the reference's v3 format."""
+        _check(lib().lbmb_checkpoint_save(self.h, os.fsencode(directory)))
+
+    def restore(self, directory):
+        """Solver::restore (solver.rs:4739-4742): CheckpointError with the
+        reference's code on any mismatch, before anything is installed."""
+        _check(lib().lbmb_checkpoint_restore(self.h, os.fsencode(directory)))
+
+    @classmethod
+    def load(cls, directory, dims, **kw):
+        """Solver::load (solver.rs:4726-4737): build from the spec, restore."""
+        s = cls(dims, **kw)
+        s.restore(directory)
+        return s
+
+    def set_scalar_name(self, k, name):
+        _check(lib().lbmb_set_scalar_name(self.h, int(k), name.encode()))
+
+    @property
+    def qoi_checkpoint_state(self):
+        """QoiCheckpointState carried through checkpoints (JSON text or None)."""
+        n = C.c_int64()
+        _check(lib().lbmb_get_qoi_checkpoint_state(self.h, None, 0, C.byref(n)))
+        if n.value < 0:
+            return None
+        buf = C.create_string_buffer(n.value + 1)
+        _check(lib().lbmb_get_qoi_checkpoint_state(self.h, buf, n.value, C.byref(n)))
+        return buf.raw[:n.value].decode()
+
+    @qoi_checkpoint_state.setter
+    def qoi_checkpoint_state(self, text):
+        if text is None:
+            _check(lib().lbmb_set_qoi_checkpoint_state(self.h, None, 0))
+        else:
+            b = text.encode()
+            _check(lib().lbmb_set_qoi_checkpoint_state(self.h, b, len(b)))
+
     # --- passive scalar -----------------------------------------------------
-    def enable_scalar_distribution(self, diffusivity, q=None):
+    def enable_scalar_distribution(self, diffusivity, q=None, name=None):
         k = C.c_int32()
         _check(lib().lbmb_enable_scalar(self.h, int(self.q if q is None else q), float(diffusivity),
                                         C.byref(k)))
+        if name is not None:
+            self.set_scalar_name(k.value, name)
         return k.value
 
     def set_scalar_concentration(self, k, values):
@@ -726,3 +821,96 @@ def build_stirred_tank(spec: TankSpec):
                                      _d(wv), _d(pos), _d(w), m.value, C.byref(m), _d(center), _d(omega)))
     return {"solid": solid, "baffle": baffle, "wall_velocity": wv.reshape(n, 3),
             "marker_pos": pos.reshape(-1, 3), "marker_w": w, "center": center, "omega": omega}
+
+
+# ---------------------------------------------------------------------------
+# Checkpoint format on host arrays (no device): the reference's
+# write_part_checkpoint / read_rank_file for one part.
+# ---------------------------------------------------------------------------
+def _ckpt_spec(spec):
+    dims = tuple(int(d) for d in spec["dims"])
+    nu = float(spec.get("nu", 1.0 / 6.0))
+    om = spec.get("omega_shear")
+    return _CkptSpec(int(spec.get("lattice", 19)), COLLISION[spec.get("collision", "trt")],
+                     64 if spec.get("dtype", "f64") == "f64" else 32, (C.c_int32 * 3)(*dims),
+                     (C.c_int32 * 3)(*[int(bool(p)) for p in spec.get("periodic", (False, False, False))]), nu,
+                     float(spec.get("magic", MAGIC_STD)), float(1.0 / (3.0 * nu + 0.5) if om is None else om),
+                     (C.c_double * 3)(*[float(f) for f in spec.get("force", (0.0, 0.0, 0.0))])), dims
+
+
+def _masks(n, solid, wall_u):
+    s = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8).ravel()
+    w = None if wall_u is None else _f64(wall_u, 3 * n)
+    return s, w
+
+
+def checkpoint_write_host(directory, spec, state, solid=None, wall_u=None):
+    """Write a checkpoint from host arrays. spec: dims, lattice, collision,
+    dtype ("f32" | "f64"), nu, magic, omega_shear, periodic, force. state:
+    step, f (Q x n), moments (4 x n), force_field (n x 3 or None), scalars
+    (list of dicts name, diffusivity, q, h (q x n), conc), qoi (JSON text or
+    None)."""
+    cs, dims = _ckpt_spec(spec)
+    n = dims[0] * dims[1] * dims[2]
+    q = cs.lattice
+    f = _f64(state["f"], q * n)
+    mo = _f64(state["moments"], 4 * n)
+    ff = state.get("force_field")
+    ff = None if ff is None else _f64(ff, 3 * n)
+    scal = state.get("scalars") or []
+    keep = []
+    arr = (_CkptScalar * max(len(scal), 1))()
+    for i, x in enumerate(scal):
+        h = _f64(x["h"], int(x["q"]) * n)
+        c = _f64(x["conc"], n)
+        keep += [h, c]
+        arr[i].name = x["name"].encode()
+        arr[i].diffusivity = float(x["diffusivity"])
+        arr[i].q = int(x["q"])
+        arr[i].h = _d(h)
+        arr[i].h_capacity = h.size
+        arr[i].conc = _d(c)
+    qoi = state.get("qoi")
+    qb = None if qoi is None else C.create_string_buffer(qoi.encode(), len(qoi.encode()))
+    data = _CkptData(int(state.get("step", 0)), _d(f), _d(mo), int(ff is not None), _d(ff), len(scal), len(scal),
+                     arr, int(qoi is not None), None if qb is None else C.cast(qb, C.POINTER(C.c_char)),
+                     0 if qoi is None else len(qoi.encode()), 0 if qoi is None else len(qoi.encode()))
+    s, w = _masks(n, solid, wall_u)
+    _check(lib().lbmb_checkpoint_write_host(os.fsencode(directory), C.byref(cs),
+                                            None if s is None else s.ctypes.data_as(_u8p), _d(w), C.byref(data)))
+
+
+def checkpoint_read_host(directory, spec, solid=None, wall_u=None, max_scalars=8, max_qoi_bytes=1 << 20):
+    """Read and validate a checkpoint against spec and masks; returns the
+    state dict of checkpoint_write_host. CheckpointError on any mismatch."""
+    cs, dims = _ckpt_spec(spec)
+    n = dims[0] * dims[1] * dims[2]
+    q = cs.lattice
+    f = np.zeros(q * n)
+    mo = np.zeros(4 * n)
+    ff = np.zeros(3 * n)
+    hs = [np.zeros(27 * n) for _ in range(max_scalars)]
+    cs_ = [np.zeros(n) for _ in range(max_scalars)]
+    arr = (_CkptScalar * max_scalars)()
+    for i in range(max_scalars):
+        arr[i].h = _d(hs[i])
+        arr[i].h_capacity = hs[i].size
+        arr[i].conc = _d(cs_[i])
+    qb = C.create_string_buffer(max_qoi_bytes)
+    data = _CkptData(0, _d(f), _d(mo), 0, _d(ff), 0, max_scalars, arr, 0, C.cast(qb, C.POINTER(C.c_char)), 0,
+                     max_qoi_bytes)
+    s, w = _masks(n, solid, wall_u)
+    _check(lib().lbmb_checkpoint_read_host(os.fsencode(directory), C.byref(cs),
+                                           None if s is None else s.ctypes.data_as(_u8p), _d(w), C.byref(data)))
+    return {"step": data.step, "f": f.reshape(q, n), "moments": mo.reshape(4, n),
+            "force_field": ff.reshape(n, 3) if data.has_force_field else None,
+            "scalars": [{"name": arr[i].name.decode(), "diffusivity": arr[i].diffusivity, "q": arr[i].q,
+                         "h": hs[i][:arr[i].q * n].reshape(arr[i].q, n).copy(), "conc": cs_[i].copy()}
+                        for i in range(data.n_scalars)],
+            "qoi": qb.raw[:data.qoi_len].decode() if data.has_qoi else None}
+
+
+def fnv1a64(data):
+    """FNV-1a 64 of bytes (the checkpoint payload hash)."""
+    b = bytes(data)
+    return int(lib().lbmb_fnv1a64(b, len(b)))

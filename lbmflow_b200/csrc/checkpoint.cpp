@@ -1,0 +1,1030 @@
+// Checkpoint/restart files in the reference's v3 format: writer, reader,
+// hashes and the host-only C ABI entries (lbmb_checkpoint_write_host,
+// lbmb_checkpoint_read_host, lbmb_fnv1a64).
+//
+// Reference: crates/lbm-core/src/solver.rs:29-44 (format constants),
+// 84-118 (manifest, rank entry, section table, rank header), 831-1058
+// (hashes, names, real codec), 1108-1215 (rank file reader), 1217-1287
+// (scalar section), 4536-4724 (writer, manifest, save), 4739-5066 (restore).
+#include "checkpoint.hpp"
+
+#include <cctype>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iterator>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <sys/stat.h>
+#include <sys/types.h>
+
+#include "../../include/lbmb.h"
+
+namespace lbmb {
+extern thread_local std::string g_last_error;
+
+namespace ckpt {
+namespace {
+
+constexpr uint32_t FORMAT_VERSION = 3;
+constexpr char MAGIC[8] = {'L', 'B', 'M', 'K', 'P', 'T', 0, 0};
+constexpr uint32_t SEC_F_PRIMARY = 1, SEC_STALE_STASH = 2, SEC_MOMENTS = 3, SEC_SOLID = 4, SEC_FORCE_FIELD = 5,
+                   SEC_SCALAR_FIELDS = 6, SEC_PHASE_FIELD = 7, SEC_QOI_ACCUMULATORS = 10;
+const char* RANK_FILE = "rank_0000_part_0000.bin";
+
+[[noreturn]] void fail(const std::string& code, const std::string& msg) { throw Failure(code, msg); }
+
+// ---- little-endian byte codec (solver.rs:1062-1109) ----------------------
+void put(std::string& out, uint64_t v, int bytes) {
+  for (int i = 0; i < bytes; ++i) out.push_back(char((v >> (8 * i)) & 0xff));
+}
+void put_f64(std::string& out, double v) {
+  uint64_t b;
+  std::memcpy(&b, &v, 8);
+  put(out, b, 8);
+}
+// push_real_bytes (solver.rs:1011-1021): f32 runs store each value as f32.
+void put_real(std::string& out, double v, bool f64) {
+  if (f64) {
+    put_f64(out, v);
+  } else {
+    const float x = float(v);
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    put(out, b, 4);
+  }
+}
+
+struct Reader {
+  const std::string& b;
+  size_t pos = 0;
+  const char* what;
+  Reader(const std::string& bytes, const char* w) : b(bytes), what(w) {}
+  // take (solver.rs:1074-1085)
+  const char* take(size_t n) {
+    if (pos > b.size() || b.size() - pos < n) fail("CKPT_TRUNCATED", what);
+    const char* p = b.data() + pos;
+    pos += n;
+    return p;
+  }
+  uint64_t uint(int bytes) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(take(size_t(bytes)));
+    uint64_t v = 0;
+    for (int i = 0; i < bytes; ++i) v |= uint64_t(p[i]) << (8 * i);
+    return v;
+  }
+  double f64() {
+    const uint64_t u = uint(8);
+    double v;
+    std::memcpy(&v, &u, 8);
+    return v;
+  }
+};
+
+// read_real_bytes (solver.rs:1023-1048)
+std::vector<double> read_reals(const char* p, size_t len, size_t expected, bool f64) {
+  const size_t w = f64 ? 8 : 4;
+  if (len != expected * w)
+    fail("CKPT_GEOM_MISMATCH", "section length " + std::to_string(len) + " does not match expected " +
+                                   std::to_string(expected) + " values of " + std::to_string(w) + " bytes");
+  std::vector<double> out(expected);
+  for (size_t i = 0; i < expected; ++i) {
+    const unsigned char* q = reinterpret_cast<const unsigned char*>(p) + i * w;
+    uint64_t u = 0;
+    for (size_t k = 0; k < w; ++k) u |= uint64_t(q[k]) << (8 * k);
+    if (f64) {
+      std::memcpy(&out[i], &u, 8);
+    } else {
+      const uint32_t u32 = uint32_t(u);
+      float x;
+      std::memcpy(&x, &u32, 4);
+      out[i] = double(x);
+    }
+  }
+  return out;
+}
+
+// ---- FNV-1a 64 streams (solver.rs:831-859) --------------------------------
+struct Hasher {
+  uint64_t h = 0xcbf29ce484222325ull;
+  void bytes(const void* d, size_t n) { h = fnv1a64(d, n, h); }
+  void u64(uint64_t v) {
+    unsigned char b[8];
+    for (int i = 0; i < 8; ++i) b[i] = (v >> (8 * i)) & 0xff;
+    bytes(b, 8);
+  }
+  void f64(double v) {
+    uint64_t u;
+    std::memcpy(&u, &v, 8);
+    u64(u);
+  }
+  // hash_real: f32 runs hash the f32 bits (4 bytes), f64 runs the f64 bits.
+  void real(double v, bool is64) {
+    if (is64) {
+      f64(v);
+    } else {
+      const float x = float(v);
+      uint32_t u;
+      std::memcpy(&u, &x, 4);
+      unsigned char b[4];
+      for (int i = 0; i < 4; ++i) b[i] = (u >> (8 * i)) & 0xff;
+      bytes(b, 4);
+    }
+  }
+};
+
+// ---- halo-padded geometry (fields.rs:99-150; halo 1 on every axis) --------
+struct Pad {
+  int64_t nx, ny, nz, px, py, pz;
+  explicit Pad(const Spec& s)
+      : nx(s.dims[0]), ny(s.dims[1]), nz(s.dims[2]), px(nx + 2), py(ny + 2), pz(nz + 2) {}
+  int64_t np() const { return px * py * pz; }
+  int64_t nc() const { return nx * ny * nz; }
+  int64_t pidx(int64_t x, int64_t y, int64_t z) const { return ((z + 1) * py + (y + 1)) * px + (x + 1); }
+};
+
+// Compact cell whose value the padded mask cell holds after the reference's
+// mask exchange (halo.rs:457-492 over a monolithic part, subdomain.rs:31-44):
+// periodic axes wrap (corners forwarded through the x, y, z phases); a halo
+// cell behind a non-periodic face keeps the default (-1 here).
+int64_t mask_source(const Spec& s, const Pad& g, int64_t x, int64_t y, int64_t z) {
+  int64_t c[3] = {x, y, z};
+  const int64_t n[3] = {g.nx, g.ny, g.nz};
+  for (int a = 0; a < 3; ++a) {
+    if (c[a] >= 0 && c[a] < n[a]) continue;
+    if (!s.periodic[a]) return -1;
+    c[a] = (c[a] + n[a]) % n[a];
+  }
+  return (c[2] * g.ny + c[1]) * g.nx + c[0];
+}
+
+void padded_masks(const Spec& s, const uint8_t* solid, const double* wall_u, std::vector<uint8_t>& ps,
+                  std::vector<double>& pw) {
+  const Pad g(s);
+  ps.assign(size_t(g.np()), 0);
+  pw.assign(size_t(3 * g.np()), 0.0);
+  for (int64_t z = -1; z <= g.nz; ++z)
+    for (int64_t y = -1; y <= g.ny; ++y)
+      for (int64_t x = -1; x <= g.nx; ++x) {
+        const int64_t src = mask_source(s, g, x, y, z);
+        if (src < 0) continue;
+        const int64_t p = g.pidx(x, y, z);
+        ps[size_t(p)] = solid && solid[src] ? 1 : 0;
+        if (wall_u)
+          for (int k = 0; k < 3; ++k) pw[size_t(3 * p + k)] = wall_u[3 * src + k];
+      }
+}
+
+const char* lattice_name(int q) { return q == 19 ? "D3Q19" : q == 27 ? "D3Q27" : "unknown"; }
+int lattice_id(int q) { return q == 19 ? 319 : q == 27 ? 327 : 0; }
+const char* dtype_name(bool f64) { return f64 ? "f64" : "f32"; }
+
+// Q planes of a compact field into padded planes (halo zero), one padded
+// row per append. The byte image is the host's: the format is little-endian
+// and so are the hosts this library builds for.
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "checkpoint writer assumes a little-endian host");
+template <class T>
+void put_padded_t(std::string& out, const Pad& g, const double* v, int planes) {
+  std::vector<T> row(size_t(g.px), T(0));
+  const std::vector<T> zero(size_t(g.px), T(0));
+  const size_t rb = size_t(g.px) * sizeof(T);
+  for (int q = 0; q < planes; ++q)
+    for (int64_t pz = 0; pz < g.pz; ++pz)
+      for (int64_t py = 0; py < g.py; ++py) {
+        const bool core_row = v && pz >= 1 && pz <= g.nz && py >= 1 && py <= g.ny;
+        if (!core_row) {
+          out.append(reinterpret_cast<const char*>(zero.data()), rb);
+          continue;
+        }
+        const double* src = v + size_t(q) * size_t(g.nc()) + size_t(((pz - 1) * g.ny + (py - 1)) * g.nx);
+        for (int64_t x = 0; x < g.nx; ++x) row[size_t(x + 1)] = T(src[x]);
+        out.append(reinterpret_cast<const char*>(row.data()), rb);
+      }
+}
+void put_padded(std::string& out, const Spec& s, const double* v, int planes, bool f64) {
+  const Pad g(s);
+  if (f64) put_padded_t<double>(out, g, v, planes);
+  else put_padded_t<float>(out, g, v, planes);
+}
+
+std::vector<double> core_of(const std::vector<double>& padded, const Spec& s, int planes) {
+  const Pad g(s);
+  std::vector<double> out(size_t(planes) * size_t(g.nc()));
+  for (int q = 0; q < planes; ++q)
+    for (int64_t z = 0; z < g.nz; ++z)
+      for (int64_t y = 0; y < g.ny; ++y)
+        for (int64_t x = 0; x < g.nx; ++x)
+          out[size_t(q) * size_t(g.nc()) + size_t((z * g.ny + y) * g.nx + x)] =
+              padded[size_t(q) * size_t(g.np()) + size_t(g.pidx(x, y, z))];
+  return out;
+}
+
+// ---- JSON (serde_json::to_string_pretty layout; minimal reader) ------------
+struct JVal {
+  enum Kind { NUL, BOOL, NUM, STR, ARR, OBJ } kind = NUL;
+  bool b = false;
+  std::string text;  // number text or string value
+  std::vector<JVal> arr;
+  std::vector<std::pair<std::string, JVal>> obj;
+  const JVal* get(const std::string& k) const {
+    for (auto& kv : obj)
+      if (kv.first == k) return &kv.second;
+    return nullptr;
+  }
+};
+
+struct JParser {
+  const std::string& s;
+  size_t i = 0;
+  explicit JParser(const std::string& t) : s(t) {}
+  [[noreturn]] void bad(const std::string& m) {
+    fail("CKPT_MANIFEST_INVALID", m + " at byte " + std::to_string(i));
+  }
+  void ws() {
+    while (i < s.size() && (s[i] == ' ' || s[i] == '\n' || s[i] == '\r' || s[i] == '\t')) ++i;
+  }
+  bool lit(const char* w) {
+    const size_t n = std::strlen(w);
+    if (s.compare(i, n, w) == 0) {
+      i += n;
+      return true;
+    }
+    return false;
+  }
+  std::string str() {
+    if (s[i] != '"') bad("expected string");
+    ++i;
+    std::string out;
+    while (true) {
+      if (i >= s.size()) bad("unterminated string");
+      const char c = s[i++];
+      if (c == '"') break;
+      if (c != '\\') {
+        out.push_back(c);
+        continue;
+      }
+      if (i >= s.size()) bad("unterminated escape");
+      const char e = s[i++];
+      switch (e) {
+        case '"': out.push_back('"'); break;
+        case '\\': out.push_back('\\'); break;
+        case '/': out.push_back('/'); break;
+        case 'b': out.push_back('\b'); break;
+        case 'f': out.push_back('\f'); break;
+        case 'n': out.push_back('\n'); break;
+        case 'r': out.push_back('\r'); break;
+        case 't': out.push_back('\t'); break;
+        case 'u': {
+          if (i + 4 > s.size()) bad("short unicode escape");
+          const unsigned cp = unsigned(std::stoul(s.substr(i, 4), nullptr, 16));
+          i += 4;
+          if (cp < 0x80) {
+            out.push_back(char(cp));
+          } else if (cp < 0x800) {
+            out.push_back(char(0xc0 | (cp >> 6)));
+            out.push_back(char(0x80 | (cp & 0x3f)));
+          } else {
+            out.push_back(char(0xe0 | (cp >> 12)));
+            out.push_back(char(0x80 | ((cp >> 6) & 0x3f)));
+            out.push_back(char(0x80 | (cp & 0x3f)));
+          }
+          break;
+        }
+        default: bad("bad escape");
+      }
+    }
+    return out;
+  }
+  JVal value(int depth = 0) {
+    if (depth > 64) bad("nesting too deep");
+    ws();
+    if (i >= s.size()) bad("unexpected end");
+    JVal v;
+    const char c = s[i];
+    if (c == '{') {
+      v.kind = JVal::OBJ;
+      ++i;
+      ws();
+      if (s[i] == '}') {
+        ++i;
+        return v;
+      }
+      while (true) {
+        ws();
+        std::string k = str();
+        ws();
+        if (i >= s.size() || s[i] != ':') bad("expected ':'");
+        ++i;
+        v.obj.emplace_back(std::move(k), value(depth + 1));
+        ws();
+        if (i < s.size() && s[i] == ',') {
+          ++i;
+          continue;
+        }
+        if (i < s.size() && s[i] == '}') {
+          ++i;
+          break;
+        }
+        bad("expected ',' or '}'");
+      }
+    } else if (c == '[') {
+      v.kind = JVal::ARR;
+      ++i;
+      ws();
+      if (s[i] == ']') {
+        ++i;
+        return v;
+      }
+      while (true) {
+        v.arr.push_back(value(depth + 1));
+        ws();
+        if (i < s.size() && s[i] == ',') {
+          ++i;
+          continue;
+        }
+        if (i < s.size() && s[i] == ']') {
+          ++i;
+          break;
+        }
+        bad("expected ',' or ']'");
+      }
+    } else if (c == '"') {
+      v.kind = JVal::STR;
+      v.text = str();
+    } else if (lit("true")) {
+      v.kind = JVal::BOOL;
+      v.b = true;
+    } else if (lit("false")) {
+      v.kind = JVal::BOOL;
+    } else if (lit("null")) {
+      v.kind = JVal::NUL;
+    } else {
+      const size_t st = i;
+      while (i < s.size() && (std::isdigit(static_cast<unsigned char>(s[i])) || s[i] == '-' || s[i] == '+' ||
+                              s[i] == '.' || s[i] == 'e' || s[i] == 'E'))
+        ++i;
+      if (i == st) bad("unexpected character");
+      v.kind = JVal::NUM;
+      v.text = s.substr(st, i - st);
+    }
+    return v;
+  }
+};
+
+// serde field access: a missing field or a value of the wrong type is a
+// manifest error (the reference's From<serde_json::Error>, solver.rs:77-81).
+const JVal& field(const JVal& o, const char* k) {
+  const JVal* v = o.get(k);
+  if (!v) fail("CKPT_MANIFEST_INVALID", std::string("missing field `") + k + "`");
+  return *v;
+}
+uint64_t as_u64(const JVal& v, const char* k) {
+  if (v.kind != JVal::NUM || v.text.empty() || v.text.find_first_not_of("0123456789") != std::string::npos)
+    fail("CKPT_MANIFEST_INVALID", std::string("invalid type for `") + k + "`: expected an unsigned integer");
+  errno = 0;
+  const unsigned long long x = std::strtoull(v.text.c_str(), nullptr, 10);
+  if (errno == ERANGE) fail("CKPT_MANIFEST_INVALID", std::string("integer out of range for `") + k + "`");
+  return uint64_t(x);
+}
+const std::string& as_str(const JVal& v, const char* k) {
+  if (v.kind != JVal::STR) fail("CKPT_MANIFEST_INVALID", std::string("invalid type for `") + k + "`: expected a string");
+  return v.text;
+}
+std::vector<uint64_t> as_u64x3(const JVal& v, const char* k) {
+  if (v.kind != JVal::ARR || v.arr.size() != 3)
+    fail("CKPT_MANIFEST_INVALID", std::string("invalid type for `") + k + "`: expected an array of 3");
+  return {as_u64(v.arr[0], k), as_u64(v.arr[1], k), as_u64(v.arr[2], k)};
+}
+
+// serde_json's f64 text for the manifest's `time` (an integer-valued f64
+// prints with a trailing ".0").
+std::string f64_text(double v) {
+  char buf[64];
+  if (v == std::floor(v) && std::fabs(v) < 1e16) {
+    std::snprintf(buf, sizeof buf, "%.1f", v);
+    return buf;
+  }
+  std::snprintf(buf, sizeof buf, "%.17g", v);
+  return buf;
+}
+
+std::string json_escape(const std::string& t) {
+  std::string o = "\"";
+  for (char c : t) {
+    const unsigned char u = static_cast<unsigned char>(c);
+    if (c == '"') o += "\\\"";
+    else if (c == '\\') o += "\\\\";
+    else if (c == '\n') o += "\\n";
+    else if (c == '\r') o += "\\r";
+    else if (c == '\t') o += "\\t";
+    else if (u < 0x20) {
+      char b[8];
+      std::snprintf(b, sizeof b, "\\u%04x", u);
+      o += b;
+    } else o.push_back(c);
+  }
+  return o + "\"";
+}
+
+std::string arr3(uint64_t a, uint64_t b, uint64_t c, const std::string& ind) {
+  return "[\n" + ind + "  " + std::to_string(a) + ",\n" + ind + "  " + std::to_string(b) + ",\n" + ind + "  " +
+         std::to_string(c) + "\n" + ind + "]";
+}
+
+// checkpoint_manifest + write_checkpoint_manifest (solver.rs:4632-4670).
+std::string manifest_text(const Spec& s, uint64_t step, uint64_t bytes, uint64_t payload_hash, uint64_t mhash,
+                          bool stats) {
+  std::string j = "{\n";
+  j += "  \"kind\": \"lbmflow-checkpoint\",\n";
+  j += "  \"format_version\": " + std::to_string(FORMAT_VERSION) + ",\n";
+  j += "  \"step\": " + std::to_string(step) + ",\n";
+  j += "  \"time\": " + f64_text(double(step)) + ",\n";
+  j += "  \"dtype\": \"" + std::string(dtype_name(s.f64)) + "\",\n";
+  j += "  \"lattice\": \"" + std::string(lattice_name(s.q)) + "\",\n";
+  j += "  \"global\": " + arr3(uint64_t(s.dims[0]), uint64_t(s.dims[1]), uint64_t(s.dims[2]), "  ") + ",\n";
+  j += "  \"scenario_hash\": \"" + hash_string(spec_hash(s)) + "\",\n";
+  j += "  \"decomp_hash\": \"" + hash_string(decomp_hash(s)) + "\",\n";
+  j += "  \"nranks\": 1,\n";
+  j += "  \"ranks\": [\n";
+  j += "    {\n";
+  j += "      \"rank\": 0,\n";
+  j += "      \"part\": 0,\n";
+  j += "      \"file\": \"" + std::string(RANK_FILE) + "\",\n";
+  j += "      \"origin\": " + arr3(0, 0, 0, "      ") + ",\n";
+  j += "      \"core\": " + arr3(uint64_t(s.dims[0]), uint64_t(s.dims[1]), uint64_t(s.dims[2]), "      ") + ",\n";
+  j += "      \"bytes\": " + std::to_string(bytes) + ",\n";
+  j += "      \"payload_hash\": \"" + hash_string(payload_hash) + "\",\n";
+  j += "      \"mask_hash\": \"" + hash_string(mhash) + "\"\n";
+  j += "    }\n";
+  j += "  ],\n";
+  j += "  \"reserved\": {\n";
+  j += "    \"particles\": false,\n";
+  j += "    \"rng\": false,\n";
+  j += std::string("    \"stats\": ") + (stats ? "true" : "false") + "\n";
+  j += "  }\n";
+  j += "}";
+  return j;
+}
+
+std::string read_file(const std::string& path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) fail("CKPT_IO", "No such file or directory (os error 2): " + path);
+  std::string b((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  if (in.bad()) fail("CKPT_IO", "read failed: " + path);
+  return b;
+}
+
+void write_file(const std::string& path, const std::string& bytes) {
+  std::ofstream out(path, std::ios::binary | std::ios::trunc);
+  if (!out) fail("CKPT_IO", "cannot create " + path);
+  out.write(bytes.data(), std::streamsize(bytes.size()));
+  out.flush();
+  if (!out) fail("CKPT_IO", "write failed: " + path);
+}
+
+// std::fs::create_dir_all
+void make_dirs(const std::string& dir) {
+  std::string cur;
+  std::stringstream ss(dir);
+  std::string part;
+  if (!dir.empty() && dir[0] == '/') cur = "/";
+  while (std::getline(ss, part, '/')) {
+    if (part.empty()) continue;
+    cur += part;
+    if (::mkdir(cur.c_str(), 0777) != 0 && errno != EEXIST) fail("CKPT_IO", "cannot create directory " + cur);
+    struct stat sb;
+    if (::stat(cur.c_str(), &sb) != 0 || !S_ISDIR(sb.st_mode)) fail("CKPT_IO", "not a directory: " + cur);
+    cur += "/";
+  }
+}
+
+std::string join(const std::string& dir, const std::string& f) {
+  return dir.empty() ? f : (dir.back() == '/' ? dir + f : dir + "/" + f);
+}
+
+// scalar_checkpoint_bytes (solver.rs:1200-1217): the ping-pong partner is
+// written as zero planes like the hydro stash.
+std::string scalar_bytes(const Spec& s, const std::vector<Scalar>& sc) {
+  const Pad g(s);
+  std::string out;
+  put(out, sc.size(), 4);
+  for (const Scalar& x : sc) {
+    put(out, x.name.size(), 4);
+    out += x.name;
+    put_f64(out, x.diffusivity);
+    const uint64_t hl = uint64_t(x.q) * uint64_t(g.np());
+    put(out, hl, 8);
+    put_padded(out, s, x.h.data(), x.q, s.f64);
+    put(out, hl, 8);
+    put_padded(out, s, nullptr, x.q, s.f64);
+    put(out, uint64_t(g.nc()), 8);
+    for (int64_t c = 0; c < g.nc(); ++c) put_real(out, x.conc[size_t(c)], s.f64);
+  }
+  return out;
+}
+
+// restore_scalar_checkpoint (solver.rs:1219-1287). The reference's scalars
+// live on the hydro lattice; a D3Q7 scalar (7 planes) is read too.
+std::vector<Scalar> parse_scalars(const std::string& bytes, const Spec& s) {
+  const Pad g(s);
+  Reader r(bytes, "rank file ended before the declared header/table/payload");
+  const size_t w = s.f64 ? 8 : 4;
+  const uint64_t count = r.uint(4);
+  std::vector<Scalar> out;
+  for (uint64_t k = 0; k < count; ++k) {
+    Scalar x;
+    const uint64_t nl = r.uint(4);
+    x.name.assign(r.take(size_t(nl)), size_t(nl));
+    x.diffusivity = r.f64();
+    const uint64_t hl = r.uint(8);
+    if (hl > bytes.size()) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+    const char* hp = r.take(size_t(hl) * w);
+    const uint64_t tl = r.uint(8);
+    if (tl > bytes.size()) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+    r.take(size_t(tl) * w);
+    const uint64_t cl = r.uint(8);
+    if (cl > bytes.size()) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+    const char* cp = r.take(size_t(cl) * w);
+    const uint64_t np = uint64_t(g.np());
+    const bool q_ok = hl % np == 0 && (hl / np == 7 || hl / np == uint64_t(s.q));
+    if (!q_ok || tl != hl || cl != uint64_t(g.nc()))
+      fail("CKPT_GEOM_MISMATCH", "scalar checkpoint section length differs from current geometry");
+    x.q = int(hl / np);
+    x.h = core_of(read_reals(hp, size_t(hl) * w, size_t(hl), s.f64), s, x.q);
+    x.conc = read_reals(cp, size_t(cl) * w, size_t(cl), s.f64);
+    out.push_back(std::move(x));
+  }
+  if (r.pos != bytes.size()) fail("CKPT_PAYLOAD_CORRUPT", "scalar checkpoint section has trailing bytes");
+  return out;
+}
+
+}  // namespace
+
+bool json_object(const std::string& text) {
+  try {
+    JParser q(text);
+    const JVal v = q.value();
+    q.ws();
+    return q.i == text.size() && v.kind == JVal::OBJ;
+  } catch (const Failure&) {
+    return false;
+  }
+}
+
+uint64_t fnv1a64(const void* data, size_t len, uint64_t h) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < len; ++i) {
+    h ^= p[i];
+    h *= 0x100000001b3ull;
+  }
+  return h;
+}
+
+std::string hash_string(uint64_t h) {
+  char buf[40];
+  std::snprintf(buf, sizeof buf, "fnv1a64:%016llx", static_cast<unsigned long long>(h));
+  return buf;
+}
+
+// spec_hash (solver.rs:881-945) with every face closed and no sources or
+// face patches.
+uint64_t spec_hash(const Spec& s) {
+  Hasher h;
+  h.u64(3);
+  h.u64(uint64_t(s.q));
+  for (int a = 0; a < 3; ++a) h.u64(uint64_t(s.dims[a]));
+  h.f64(s.nu);
+  if (s.collision == LBMB_BGK) {
+    h.u64(1);
+  } else if (s.collision == LBMB_TRT) {
+    h.u64(2);
+    h.f64(s.magic);
+  } else {
+    h.u64(3);
+    h.f64(s.omega_shear);
+  }
+  for (int a = 0; a < 3; ++a) h.u64(s.periodic[a] ? 1 : 0);
+  for (int f = 0; f < 6; ++f) h.u64(0);  // FaceBC::Closed
+  for (int a = 0; a < 3; ++a) h.real(s.force[a], s.f64);
+  return h.h;
+}
+
+// decomp_hash (solver.rs:947-965) of the monolithic part: neighbours are
+// Some(0) behind periodic faces (hashed 0 + 1) and None (0) elsewhere.
+uint64_t decomp_hash(const Spec& s) {
+  Hasher h;
+  h.u64(1);
+  for (int a = 0; a < 3; ++a) h.u64(s.periodic[a] ? 1 : 0);
+  for (int a = 0; a < 3; ++a) h.u64(0);
+  for (int a = 0; a < 3; ++a) h.u64(uint64_t(s.dims[a]));
+  for (int f = 0; f < 6; ++f) h.u64(s.periodic[f / 2] ? 1 : 0);
+  return h.h;
+}
+
+// part_mask_hash (solver.rs:967-979) over the padded masks.
+uint64_t mask_hash(const Spec& s, const uint8_t* solid, const double* wall_u) {
+  std::vector<uint8_t> ps;
+  std::vector<double> pw;
+  padded_masks(s, solid, wall_u, ps, pw);
+  Hasher h;
+  h.u64(ps.size());
+  for (uint8_t v : ps) h.u64(v);
+  for (double v : pw) h.real(v, s.f64);
+  return h.h;
+}
+
+void save(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u, const State& st) {
+  if (s.q != 19 && s.q != 27) fail("CKPT_LATTICE_MISMATCH", "checkpoint lattice must be D3Q19 or D3Q27");
+  const Pad g(s);
+  const int64_t nc = g.nc(), np = g.np();
+  if (int64_t(st.f.size()) != s.q * nc || int64_t(st.moments.size()) != 4 * nc ||
+      (st.has_force_field && int64_t(st.force_field.size()) != 3 * nc))
+    fail("CKPT_GEOM_MISMATCH", "state arrays differ from the checkpoint geometry");
+  for (const Scalar& x : st.scalars)
+    if ((x.q != 7 && x.q != s.q) || int64_t(x.h.size()) != x.q * nc || int64_t(x.conc.size()) != nc)
+      fail("CKPT_GEOM_MISMATCH", "scalar arrays differ from the checkpoint geometry");
+  // write_part_checkpoint (solver.rs:4536-4630)
+  std::vector<std::pair<uint32_t, std::string>> sec;
+  {
+    std::string b;
+    b.reserve(size_t(s.q) * size_t(np) * (s.f64 ? 8 : 4));
+    put_padded(b, s, st.f.data(), s.q, s.f64);
+    sec.emplace_back(SEC_F_PRIMARY, std::move(b));
+  }
+  {
+    std::string b;
+    b.reserve(size_t(s.q) * size_t(np) * (s.f64 ? 8 : 4));
+    put_padded(b, s, nullptr, s.q, s.f64);
+    sec.emplace_back(SEC_STALE_STASH, std::move(b));
+  }
+  {
+    std::string b;
+    for (double v : st.moments) put_real(b, v, s.f64);
+    sec.emplace_back(SEC_MOMENTS, std::move(b));
+  }
+  std::vector<uint8_t> ps;
+  std::vector<double> pw;
+  padded_masks(s, solid, wall_u, ps, pw);
+  sec.emplace_back(SEC_SOLID, std::string(ps.begin(), ps.end()));
+  if (st.has_force_field) {
+    std::string b;
+    for (double v : st.force_field) put_real(b, v, s.f64);
+    sec.emplace_back(SEC_FORCE_FIELD, std::move(b));
+  }
+  if (!st.scalars.empty()) sec.emplace_back(SEC_SCALAR_FIELDS, scalar_bytes(s, st.scalars));
+  if (st.has_qoi) sec.emplace_back(SEC_QOI_ACCUMULATORS, st.qoi_json);
+
+  std::string head;
+  head.append(MAGIC, 8);
+  put(head, FORMAT_VERSION, 4);
+  head.push_back(0);
+  head.push_back(s.f64 ? 1 : 0);
+  put(head, uint64_t(lattice_id(s.q)), 2);
+  put(head, uint64_t(s.q), 2);
+  put(head, 3, 2);
+  put(head, uint64_t(np), 8);
+  put(head, uint64_t(nc), 8);
+  put(head, sec.size(), 4);
+  uint64_t off = 0;
+  for (auto& e : sec) {
+    put(head, e.first, 4);
+    put(head, off, 8);
+    put(head, e.second.size(), 8);
+    off += e.second.size();
+  }
+  uint64_t ph = 0xcbf29ce484222325ull;
+  for (auto& e : sec) ph = fnv1a64(e.second.data(), e.second.size(), ph);
+  std::string trailer;
+  put(trailer, ph, 8);
+  const uint64_t total = head.size() + off + trailer.size();
+
+  make_dirs(dir);
+  {
+    const std::string path = join(dir, RANK_FILE);
+    std::ofstream out(path, std::ios::binary | std::ios::trunc);
+    if (!out) fail("CKPT_IO", "cannot create " + path);
+    out.write(head.data(), std::streamsize(head.size()));
+    for (auto& e : sec) out.write(e.second.data(), std::streamsize(e.second.size()));
+    out.write(trailer.data(), std::streamsize(trailer.size()));
+    out.flush();
+    if (!out) fail("CKPT_IO", "write failed: " + path);
+  }
+  write_file(join(dir, "manifest.json"), manifest_text(s, st.step, total, ph, mask_hash(s, solid, wall_u), st.has_qoi));
+}
+
+State load(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u) {
+  const Pad g(s);
+  const int64_t nc = g.nc(), np = g.np();
+  // load_into (solver.rs:4759-4824)
+  const std::string text = read_file(join(dir, "manifest.json"));
+  JParser jp(text);
+  const JVal m = jp.value();
+  jp.ws();
+  if (jp.i != text.size()) jp.bad("trailing characters");
+  if (m.kind != JVal::OBJ) fail("CKPT_MANIFEST_INVALID", "invalid type: expected struct CheckpointManifest");
+  const std::string& kind = as_str(field(m, "kind"), "kind");
+  const uint64_t fver = as_u64(field(m, "format_version"), "format_version");
+  const uint64_t step = as_u64(field(m, "step"), "step");
+  const JVal& tm = field(m, "time");
+  if (tm.kind != JVal::NUM) fail("CKPT_MANIFEST_INVALID", "invalid type for `time`: expected f64");
+  const std::string& dtype = as_str(field(m, "dtype"), "dtype");
+  const std::string& lattice = as_str(field(m, "lattice"), "lattice");
+  const std::vector<uint64_t> global = as_u64x3(field(m, "global"), "global");
+  const std::string& scen = as_str(field(m, "scenario_hash"), "scenario_hash");
+  const std::string& dech = as_str(field(m, "decomp_hash"), "decomp_hash");
+  const uint64_t nranks = as_u64(field(m, "nranks"), "nranks");
+  const JVal& ranks = field(m, "ranks");
+  if (ranks.kind != JVal::ARR) fail("CKPT_MANIFEST_INVALID", "invalid type for `ranks`: expected a sequence");
+  struct Entry {
+    uint64_t rank, part;
+    std::string file;
+    std::vector<uint64_t> origin, core;
+    uint64_t bytes;
+    std::string payload_hash, mask_hash;
+  };
+  std::vector<Entry> entries;
+  for (const JVal& r : ranks.arr) {
+    if (r.kind != JVal::OBJ) fail("CKPT_MANIFEST_INVALID", "invalid type: expected struct CheckpointRank");
+    entries.push_back({as_u64(field(r, "rank"), "rank"), as_u64(field(r, "part"), "part"),
+                       as_str(field(r, "file"), "file"), as_u64x3(field(r, "origin"), "origin"),
+                       as_u64x3(field(r, "core"), "core"), as_u64(field(r, "bytes"), "bytes"),
+                       as_str(field(r, "payload_hash"), "payload_hash"), as_str(field(r, "mask_hash"), "mask_hash")});
+  }
+  const JVal& reserved = field(m, "reserved");
+  if (reserved.kind != JVal::OBJ) fail("CKPT_MANIFEST_INVALID", "invalid type for `reserved`: expected a map");
+  for (auto& kv : reserved.obj)
+    if (kv.second.kind != JVal::BOOL) fail("CKPT_MANIFEST_INVALID", "invalid type for `reserved`: expected bool");
+
+  if (kind != "lbmflow-checkpoint") fail("CKPT_BAD_MAGIC", "manifest kind is " + kind);
+  if (fver != FORMAT_VERSION)
+    fail("CKPT_VERSION_MISMATCH",
+         "checkpoint format_version " + std::to_string(fver) + " differs from supported " +
+             std::to_string(FORMAT_VERSION) +
+             "; rerun from the original scenario or migrate with a checkpoint upgrader before restart");
+  if (dtype != dtype_name(s.f64))
+    fail("CKPT_DTYPE_MISMATCH", "checkpoint dtype " + dtype + " differs from run dtype " + dtype_name(s.f64));
+  if (lattice != lattice_name(s.q))
+    fail("CKPT_LATTICE_MISMATCH",
+         "checkpoint lattice " + lattice + " differs from run lattice " + lattice_name(s.q));
+  auto dims_text = [](uint64_t a, uint64_t b, uint64_t c) {
+    return "[" + std::to_string(a) + ", " + std::to_string(b) + ", " + std::to_string(c) + "]";
+  };
+  if (global[0] != uint64_t(s.dims[0]) || global[1] != uint64_t(s.dims[1]) || global[2] != uint64_t(s.dims[2]))
+    fail("CKPT_GEOM_MISMATCH", "checkpoint global " + dims_text(global[0], global[1], global[2]) +
+                                   " differs from run " + dims_text(uint64_t(s.dims[0]), uint64_t(s.dims[1]),
+                                                                    uint64_t(s.dims[2])));
+  const std::string expected = hash_string(spec_hash(s));
+  if (scen != expected)
+    fail("CKPT_SCENARIO_MISMATCH", "scenario_hash differed: checkpoint=" + scen + " current=" + expected);
+  // load_into_with_layout (solver.rs:4895-5060)
+  const std::string cur_dec = hash_string(decomp_hash(s));
+  if (dech != cur_dec) fail("CKPT_DECOMP_MISMATCH", "decomp_hash differed: checkpoint=" + dech + " current=" + cur_dec);
+  if (nranks != 1)
+    fail("CKPT_RANK_MISMATCH", "checkpoint rank count " + std::to_string(nranks) + " differs from current 1");
+  std::vector<const Entry*> mine;
+  for (auto& e : entries)
+    if (e.rank == 0) mine.push_back(&e);
+  if (mine.size() != 1)
+    fail("CKPT_DECOMP_MISMATCH", "checkpoint has " + std::to_string(mine.size()) +
+                                     " payload parts for rank 0, current owner has 1");
+  const Entry& e = *mine[0];
+  if (e.origin[0] || e.origin[1] || e.origin[2] || e.core[0] != uint64_t(s.dims[0]) ||
+      e.core[1] != uint64_t(s.dims[1]) || e.core[2] != uint64_t(s.dims[2]))
+    fail("CKPT_GEOM_MISMATCH", "part geometry differed: checkpoint rank=0 part=" + std::to_string(e.part) +
+                                   " origin=" + dims_text(e.origin[0], e.origin[1], e.origin[2]) + " core=" +
+                                   dims_text(e.core[0], e.core[1], e.core[2]) + ", current origin=[0, 0, 0] core=" +
+                                   dims_text(uint64_t(s.dims[0]), uint64_t(s.dims[1]), uint64_t(s.dims[2])));
+  const std::string cur_mask = hash_string(mask_hash(s, solid, wall_u));
+  if (e.mask_hash != cur_mask)
+    fail("CKPT_MASK_MISMATCH", "mask_hash differed for rank=0 part=" + std::to_string(e.part) +
+                                   ": checkpoint=" + e.mask_hash + " current=" + cur_mask);
+
+  // read_rank_file (solver.rs:1108-1198)
+  if (e.file.find('/') != std::string::npos || e.file == ".." || e.file.empty())
+    fail("CKPT_MANIFEST_INVALID", "rank file name must be a plain file name: " + e.file);
+  const std::string bytes = read_file(join(dir, e.file));
+  Reader r(bytes, "rank file ended before the declared header/table/payload");
+  if (std::memcmp(r.take(8), MAGIC, 8) != 0) fail("CKPT_BAD_MAGIC", "rank file magic is not LBMKPT");
+  const uint64_t rv = r.uint(4);
+  if (rv != FORMAT_VERSION)
+    fail("CKPT_VERSION_MISMATCH",
+         "rank file format_version " + std::to_string(rv) + " differs from supported " +
+             std::to_string(FORMAT_VERSION) +
+             "; rerun from the original scenario or migrate with a checkpoint upgrader before restart");
+  if (r.uint(1) != 0) fail("CKPT_BAD_MAGIC", "cross-endian checkpoints are not supported by this checkpoint format");
+  const uint64_t hdtype = r.uint(1), hlat = r.uint(2), hq = r.uint(2), hd = r.uint(2);
+  const uint64_t hnp = r.uint(8), hnc = r.uint(8);
+  const uint64_t nsec = r.uint(4);
+  struct Sec {
+    uint64_t id, off, len;
+  };
+  std::vector<Sec> table;
+  for (uint64_t k = 0; k < nsec; ++k) {
+    Sec t;
+    t.id = r.uint(4);
+    t.off = r.uint(8);
+    t.len = r.uint(8);
+    table.push_back(t);
+  }
+  if (bytes.size() - r.pos < 8) fail("CKPT_TRUNCATED", "rank file is missing payload hash trailer");
+  const size_t pend = bytes.size() - 8;
+  Reader tr(bytes, "");
+  tr.pos = pend;
+  const uint64_t phash = tr.uint(8);
+  const char* payload = bytes.data() + r.pos;
+  const size_t plen = pend - r.pos;
+  if (fnv1a64(payload, plen) != phash)
+    fail("CKPT_PAYLOAD_CORRUPT", "rank file payload hash does not match its contents");
+  std::map<uint32_t, std::pair<size_t, size_t>> sections;  // id -> (offset, length); later entries win
+  for (const Sec& t : table) {
+    if (t.off > plen || t.len > plen - t.off)
+      fail("CKPT_TRUNCATED", "section " + std::to_string(t.id) + " range " + std::to_string(t.off) + ".." +
+                                 std::to_string(t.off + t.len) + " exceeds payload length " + std::to_string(plen));
+    sections[uint32_t(t.id)] = {size_t(t.off), size_t(t.len)};
+  }
+  if (hdtype != (s.f64 ? 1u : 0u)) fail("CKPT_DTYPE_MISMATCH", "rank file dtype differs from requested run precision");
+  if (hlat != uint64_t(lattice_id(s.q)) || hq != uint64_t(s.q) || hd != 3)
+    fail("CKPT_LATTICE_MISMATCH", "rank file lattice metadata differs from requested lattice");
+  if (hnp != uint64_t(np) || hnc != uint64_t(nc))
+    fail("CKPT_GEOM_MISMATCH", "rank file np/n_core " + std::to_string(hnp) + "/" + std::to_string(hnc) +
+                                   " differs from current " + std::to_string(np) + "/" + std::to_string(nc));
+  if (hash_string(phash) != e.payload_hash)
+    fail("CKPT_PAYLOAD_CORRUPT",
+         "rank payload hash " + hash_string(phash) + " differs from manifest " + e.payload_hash);
+  auto section = [&](uint32_t id) -> const std::pair<size_t, size_t>* {
+    auto it = sections.find(id);
+    return it == sections.end() ? nullptr : &it->second;
+  };
+  auto required = [&](uint32_t id, const char* name) {
+    const auto* p = section(id);
+    if (!p) fail("CKPT_TRUNCATED", std::string("checkpoint is missing required section ") + name);
+    return *p;
+  };
+  State st;
+  st.step = step;
+  {
+    const auto p = required(SEC_F_PRIMARY, "F_PRIMARY");
+    st.f = core_of(read_reals(payload + p.first, p.second, size_t(s.q) * size_t(np), s.f64), s, s.q);
+    const auto t = required(SEC_STALE_STASH, "STALE_STASH");
+    read_reals(payload + t.first, t.second, size_t(s.q) * size_t(np), s.f64);
+    const auto mo = required(SEC_MOMENTS, "MOMENTS");
+    st.moments = read_reals(payload + mo.first, mo.second, size_t(4 * nc), s.f64);
+  }
+  if (const auto* p = section(SEC_SOLID)) {
+    if (p->second != size_t(np))
+      fail("CKPT_GEOM_MISMATCH", "solid section length differs from current padded geometry");
+    std::vector<uint8_t> ps;
+    std::vector<double> pw;
+    padded_masks(s, solid, wall_u, ps, pw);
+    for (size_t i = 0; i < size_t(np); ++i)
+      if ((payload[p->first + i] != 0) != (ps[i] != 0))
+        fail("CKPT_MASK_MISMATCH", "serialized solid mask differs from rebuilt mask");
+  }
+  if (const auto* p = section(SEC_FORCE_FIELD)) {
+    st.has_force_field = true;
+    st.force_field = read_reals(payload + p->first, p->second, size_t(3 * nc), s.f64);
+  }
+  if (const auto* p = section(SEC_SCALAR_FIELDS)) st.scalars = parse_scalars(std::string(payload + p->first, p->second), s);
+  if (section(SEC_PHASE_FIELD))
+    fail("CKPT_UNSUPPORTED", "the checkpoint carries a phase-field distribution; this solver is single-phase");
+  if (const auto* p = section(SEC_QOI_ACCUMULATORS)) {
+    st.has_qoi = true;
+    st.qoi_json.assign(payload + p->first, p->second);
+    if (!json_object(st.qoi_json)) fail("CKPT_MANIFEST_INVALID", "QOI accumulator section is not a JSON object");
+  }
+  return st;
+}
+
+}  // namespace ckpt
+}  // namespace lbmb
+
+// ---------------------------------------------------------------------------
+// Host-only C ABI: the format on caller-owned compact arrays (no device).
+// ---------------------------------------------------------------------------
+namespace {
+
+lbmb::ckpt::Spec to_spec(const lbmb_checkpoint_spec& c) {
+  if (c.lattice != 19 && c.lattice != 27) throw lbmb::ckpt::Failure("CKPT_LATTICE_MISMATCH", "lattice must be 19 or 27");
+  if (c.dtype_bits != 32 && c.dtype_bits != 64)
+    throw lbmb::ckpt::Failure("CKPT_DTYPE_MISMATCH", "dtype_bits must be 32 or 64");
+  for (int a = 0; a < 3; ++a)
+    if (c.dims[a] < 1) throw lbmb::ckpt::Failure("CKPT_GEOM_MISMATCH", "dims must be positive");
+  lbmb::ckpt::Spec s;
+  s.q = c.lattice;
+  s.collision = c.collision;
+  s.f64 = c.dtype_bits == 64;
+  for (int a = 0; a < 3; ++a) {
+    s.dims[a] = c.dims[a];
+    s.periodic[a] = c.periodic[a] != 0;
+    s.force[a] = c.force[a];
+  }
+  s.nu = c.nu;
+  s.magic = c.magic;
+  s.omega_shear = c.omega_shear;
+  return s;
+}
+
+template <class F>
+int host_guarded(F&& fn) {
+  try {
+    fn();
+    lbmb::g_last_error.clear();
+    return LBMB_OK;
+  } catch (const lbmb::ckpt::Failure& e) {
+    lbmb::g_last_error = e.what();
+    return LBMB_ERR_CHECKPOINT;
+  } catch (const std::bad_alloc&) {
+    lbmb::g_last_error = "host allocation failed";
+    return LBMB_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    lbmb::g_last_error = e.what();
+    return LBMB_ERR_INVALID;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t lbmb_fnv1a64(const void* data, uint64_t len) { return lbmb::ckpt::fnv1a64(data, size_t(len)); }
+
+int lbmb_checkpoint_write_host(const char* dir, const lbmb_checkpoint_spec* spec, const uint8_t* solid,
+                               const double* wall_u, const lbmb_checkpoint_data* data) {
+  return host_guarded([&] {
+    if (!dir || !spec || !data || !data->f || !data->moments)
+      throw std::invalid_argument("null argument");
+    const lbmb::ckpt::Spec s = to_spec(*spec);
+    const size_t n = size_t(s.dims[0]) * size_t(s.dims[1]) * size_t(s.dims[2]);
+    lbmb::ckpt::State st;
+    st.step = data->step;
+    st.f.assign(data->f, data->f + size_t(s.q) * n);
+    st.moments.assign(data->moments, data->moments + 4 * n);
+    st.has_force_field = data->has_force_field != 0;
+    if (st.has_force_field) {
+      if (!data->force_field) throw std::invalid_argument("null force field");
+      st.force_field.assign(data->force_field, data->force_field + 3 * n);
+    }
+    if (data->n_scalars < 0 || (data->n_scalars > 0 && !data->scalars)) throw std::invalid_argument("bad scalar list");
+    for (int32_t k = 0; k < data->n_scalars; ++k) {
+      const lbmb_checkpoint_scalar& c = data->scalars[k];
+      if (!c.h || !c.conc) throw std::invalid_argument("null scalar array");
+      lbmb::ckpt::Scalar x;
+      x.name.assign(c.name, strnlen(c.name, sizeof c.name));
+      x.diffusivity = c.diffusivity;
+      x.q = c.q;
+      x.h.assign(c.h, c.h + size_t(c.q) * n);
+      x.conc.assign(c.conc, c.conc + n);
+      st.scalars.push_back(std::move(x));
+    }
+    st.has_qoi = data->has_qoi != 0;
+    if (st.has_qoi) {
+      if (!data->qoi_json || data->qoi_len < 0) throw std::invalid_argument("bad QOI JSON");
+      st.qoi_json.assign(data->qoi_json, size_t(data->qoi_len));
+    }
+    lbmb::ckpt::save(dir, s, solid, wall_u, st);
+  });
+}
+
+int lbmb_checkpoint_read_host(const char* dir, const lbmb_checkpoint_spec* spec, const uint8_t* solid,
+                              const double* wall_u, lbmb_checkpoint_data* data) {
+  return host_guarded([&] {
+    if (!dir || !spec || !data || !data->f || !data->moments) throw std::invalid_argument("null argument");
+    const lbmb::ckpt::Spec s = to_spec(*spec);
+    const size_t n = size_t(s.dims[0]) * size_t(s.dims[1]) * size_t(s.dims[2]);
+    const lbmb::ckpt::State st = lbmb::ckpt::load(dir, s, solid, wall_u);
+    if (int64_t(st.scalars.size()) > int64_t(data->scalar_capacity))
+      throw lbmb::ckpt::Failure("CKPT_GEOM_MISMATCH", "more scalar distributions than the caller's capacity");
+    for (size_t k = 0; k < st.scalars.size(); ++k) {
+      const lbmb_checkpoint_scalar& c = data->scalars[k];
+      if (!c.h || !c.conc || c.h_capacity < int64_t(st.scalars[k].h.size()) ||
+          st.scalars[k].name.size() >= sizeof c.name)
+        throw lbmb::ckpt::Failure("CKPT_GEOM_MISMATCH", "scalar buffers smaller than the checkpoint's");
+    }
+    if (st.has_qoi && (!data->qoi_json || data->qoi_capacity < int64_t(st.qoi_json.size())))
+      throw lbmb::ckpt::Failure("CKPT_GEOM_MISMATCH", "QOI buffer smaller than the checkpoint's");
+    if (st.has_force_field && !data->force_field) throw std::invalid_argument("null force field");
+    data->step = st.step;
+    std::memcpy(data->f, st.f.data(), size_t(s.q) * n * sizeof(double));
+    std::memcpy(data->moments, st.moments.data(), 4 * n * sizeof(double));
+    data->has_force_field = st.has_force_field ? 1 : 0;
+    if (st.has_force_field) std::memcpy(data->force_field, st.force_field.data(), 3 * n * sizeof(double));
+    data->n_scalars = int32_t(st.scalars.size());
+    for (size_t k = 0; k < st.scalars.size(); ++k) {
+      lbmb_checkpoint_scalar& c = data->scalars[k];
+      std::memset(c.name, 0, sizeof c.name);
+      std::memcpy(c.name, st.scalars[k].name.data(), st.scalars[k].name.size());
+      c.diffusivity = st.scalars[k].diffusivity;
+      c.q = st.scalars[k].q;
+      std::memcpy(c.h, st.scalars[k].h.data(), st.scalars[k].h.size() * sizeof(double));
+      std::memcpy(c.conc, st.scalars[k].conc.data(), n * sizeof(double));
+    }
+    data->has_qoi = st.has_qoi ? 1 : 0;
+    data->qoi_len = int64_t(st.qoi_json.size());
+    if (st.has_qoi) std::memcpy(data->qoi_json, st.qoi_json.data(), st.qoi_json.size());
+  });
+}
+
+}  // extern "C"

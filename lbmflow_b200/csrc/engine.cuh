@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/lbmb.h"
+#include "checkpoint.hpp"
 #include "aux.cuh"
 #include "hydro.cuh"
 #include "hydro_tma.cuh"
@@ -95,6 +96,7 @@ struct BodyState {
 
 template <class A>
 struct ScalarStateT {
+  std::string name;
   int q = 7;
   double diffusivity = 0.0;
   int parity = 0;
@@ -155,6 +157,18 @@ struct EngineBase {
                           int64_t* count) = 0;
   virtual int q() const = 0;
   virtual const std::vector<uint8_t>& solid() const = 0;
+  // Checkpoint/restart (checkpoint.hpp): the state a checkpoint carries,
+  // the fit of a loaded state (checked before anything is installed) and
+  // its installation.
+  virtual void checkpoint_gather(ckpt::State& s) = 0;
+  virtual void checkpoint_check(const ckpt::State& s) const = 0;
+  virtual void checkpoint_install(const ckpt::State& s) = 0;
+  virtual void set_scalar_name(int k, const std::string& name) = 0;
+  virtual const lbmb_config& config() const = 0;
+  uint64_t time = 0;              // Solver::time: hydro steps taken
+  std::vector<double> wall_u_in;  // creation wall velocities (n x 3; empty: zero)
+  bool has_qoi = false;           // QoiCheckpointState carried opaque
+  std::string qoi_json;
   double last_total_ms = 0.0, last_hydro_ms = 0.0;
   int64_t last_hydro_launches = 0;
 };
@@ -256,6 +270,7 @@ struct Engine final : EngineBase {
     solid_h.assign(size_t(n), 0);
     if (solid)
       for (int64_t i = 0; i < n; ++i) solid_h[i] = solid[i] ? 1 : 0;
+    if (wu) wall_u_in.assign(wu, wu + 3 * n);
     build_flags(wu);
     // Guard margin: shifted TMA windows of the odd step reach up to
     // nx*ny + nx + 1 cells (+ alignment slack and one tile) beyond a plane.
@@ -394,6 +409,51 @@ struct Engine final : EngineBase {
     grow(s_spread, size_t(3 * slot_cap), size_t(3 * cap));
     slot_cap = cap;
     invalidate_graphs();
+  }
+
+  // Force slots of the given cells, appending a slot (and the F_FORCED
+  // flag) for each cell that has none yet; returns the slot of every entry.
+  std::vector<int32_t> ensure_slots(const std::vector<int64_t>& cells) {
+    std::vector<int32_t> out(cells.size());
+    int64_t need = nslots;
+    for (int64_t c : cells)
+      if (fslot_h[c] < 0) {
+        fslot_h[c] = -2;  // mark new
+        ++need;
+      }
+    grow_slots(need);
+    std::vector<int64_t> new_cells;
+    for (size_t k = 0; k < cells.size(); ++k) {
+      const int64_t c = cells[k];
+      if (fslot_h[c] == -2) {
+        fslot_h[c] = int32_t(nslots + int64_t(new_cells.size()));
+        new_cells.push_back(c);
+      }
+      out[k] = fslot_h[c];
+    }
+    if (!new_cells.empty()) {
+      for (size_t i = 0; i < new_cells.size(); ++i) {
+        slot_cell_h.push_back(new_cells[i]);
+        flags_h[new_cells[i]] |= F_FORCED;
+      }
+      CK(cudaMemcpyAsync(slot_cell.p + nslots, new_cells.data(), new_cells.size() * sizeof(int64_t),
+                         cudaMemcpyHostToDevice, st));
+      nslots += int64_t(new_cells.size());
+      if (new_cells.size() > 4096) {
+        // many cells: upload the whole slot map and flag array
+        CK(cudaMemcpyAsync(fslot.p, fslot_h.data(), size_t(n) * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(flags.p, flags_h.data(), size_t(n), cudaMemcpyHostToDevice, st));
+      } else {
+        for (size_t i = 0; i < new_cells.size(); ++i) {
+          CK(cudaMemcpyAsync(fslot.p + new_cells[i], &fslot_h[new_cells[i]], sizeof(int32_t),
+                             cudaMemcpyHostToDevice, st));
+          CK(cudaMemcpyAsync(flags.p + new_cells[i], &flags_h[new_cells[i]], 1, cudaMemcpyHostToDevice, st));
+        }
+      }
+      CK(cudaStreamSynchronize(st));
+      invalidate_graphs();
+    }
+    return out;
   }
 
   HydroParams<A> hydro_params() {
@@ -807,6 +867,7 @@ struct Engine final : EngineBase {
     // so its steps are checked at once.
     pending_launches = launches;
     timing_pending = true;
+    time += uint64_t(steps);
     if (kernel_mode == LBMB_SWEEP_BULK) {
       CK(cudaEventSynchronize(ev1));
       check_device_error();
@@ -1533,41 +1594,7 @@ struct Engine final : EngineBase {
       st_off[m + 1] = int32_t(st_cell.size());
     }
     // global slots for the cells (appended, never removed)
-    std::vector<int32_t> st_slot(st_cell.size());
-    int64_t need = nslots;
-    for (int64_t c : st_cell)
-      if (fslot_h[c] < 0) {
-        fslot_h[c] = -2;  // mark new
-        ++need;
-      }
-    grow_slots(need);
-    std::vector<int64_t> new_cells;
-    for (size_t k = 0; k < st_cell.size(); ++k) {
-      const int64_t c = st_cell[k];
-      if (fslot_h[c] == -2) {
-        fslot_h[c] = int32_t(nslots + int64_t(new_cells.size()));
-        new_cells.push_back(c);
-      }
-      st_slot[k] = fslot_h[c];
-    }
-    if (!new_cells.empty()) {
-      std::vector<int32_t> ids(new_cells.size());
-      for (size_t i = 0; i < new_cells.size(); ++i) {
-        ids[i] = int32_t(nslots + int64_t(i));
-        slot_cell_h.push_back(new_cells[i]);
-        flags_h[new_cells[i]] |= F_FORCED;
-      }
-      CK(cudaMemcpyAsync(slot_cell.p + nslots, new_cells.data(), new_cells.size() * sizeof(int64_t),
-                         cudaMemcpyHostToDevice, st));
-      nslots += int64_t(new_cells.size());
-      // scatter new slot ids and flags
-      for (size_t i = 0; i < new_cells.size(); ++i) {
-        CK(cudaMemcpyAsync(fslot.p + new_cells[i], &fslot_h[new_cells[i]], sizeof(int32_t), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(flags.p + new_cells[i], &flags_h[new_cells[i]], 1, cudaMemcpyHostToDevice, st));
-      }
-      CK(cudaStreamSynchronize(st));
-      invalidate_graphs();
-    }
+    const std::vector<int32_t> st_slot = ensure_slots(st_cell);
     // body slots and reverse CSR in marker order
     std::vector<int32_t> local(size_t(nslots), -1);
     std::vector<int32_t> bslot;
@@ -1763,6 +1790,7 @@ struct Engine final : EngineBase {
     if (!(std::isfinite(d) && d > 0.0)) invalid("scalar diffusivity must be finite > 0");
     if (q != 7 && q != Q) invalid("scalar lattice must be D3Q7 or the hydro lattice");
     auto sc = std::make_unique<ScalarStateT<A>>();
+    sc->name = "scalar" + std::to_string(scalars.size());
     sc->q = q;
     sc->diffusivity = d;
     sc->hplane = plane;
@@ -1804,6 +1832,128 @@ struct Engine final : EngineBase {
     CK(cudaMemcpyAsync(c, dc.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
   }
+  // ---- checkpoint/restart (Solver::save / restore, solver.rs:4536-5066) ----
+  const lbmb_config& config() const override { return cfg; }
+  void set_scalar_name(int k, const std::string& name) override {
+    if (name.empty() || name.size() > 63) invalid("scalar name must have 1 to 63 bytes");
+    scalar(k).name = name;
+  }
+  // Logical scalar populations (q x n, f64) of the current scalar state.
+  void scalar_populations(ScalarStateT<A>& sc, double* out) {
+    DevBuf<double> d;
+    d.alloc(size_t(sc.q) * size_t(n));
+    const unsigned g = unsigned(ceil_div(n, 128));
+    if (sc.q == 7)
+      scalar_stage_out_kernel<7, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, d.p,
+                                                       n);
+    else
+      scalar_stage_out_kernel<Q, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, d.p,
+                                                       n);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d.p, size_t(sc.q) * size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  void checkpoint_gather(ckpt::State& s) override {
+    s.step = time;
+    s.f.resize(size_t(Q) * size_t(n));
+    stage_out(s.f.data());
+    s.moments.resize(size_t(4) * size_t(n));
+    read_moments(s.moments.data(), s.moments.data() + n, s.moments.data() + 2 * n, s.moments.data() + 3 * n);
+    s.has_force_field = field_present;
+    s.force_field.clear();
+    if (field_present) {
+      s.force_field.resize(size_t(3) * size_t(n));
+      get_force_field(s.force_field.data());
+    }
+    s.scalars.clear();
+    for (size_t k = 0; k < scalars.size(); ++k) {
+      ScalarStateT<A>& sc = *scalars[k];
+      ckpt::Scalar x;
+      x.name = sc.name;
+      x.diffusivity = sc.diffusivity;
+      x.q = sc.q;
+      x.h.resize(size_t(sc.q) * size_t(n));
+      scalar_populations(sc, x.h.data());
+      x.conc.resize(size_t(n));
+      get_scalar(int(k), x.conc.data());
+      s.scalars.push_back(std::move(x));
+    }
+    s.has_qoi = has_qoi;
+    s.qoi_json = qoi_json;
+  }
+  void checkpoint_check(const ckpt::State& s) const override {
+    if (scalars.size() > s.scalars.size())
+      throw ckpt::Failure("CKPT_SCENARIO_MISMATCH",
+                          "solver has " + std::to_string(scalars.size()) + " scalar distributions, checkpoint has " +
+                              std::to_string(s.scalars.size()));
+    for (size_t k = 0; k < s.scalars.size(); ++k) {
+      const int q = s.scalars[k].q;
+      if (q != 7 && q != Q) throw ckpt::Failure("CKPT_GEOM_MISMATCH", "scalar lattice must be D3Q7 or the hydro lattice");
+      if (k < scalars.size() && scalars[k]->q != q)
+        throw ckpt::Failure("CKPT_SCENARIO_MISMATCH", "scalar " + std::to_string(k) + " lattice differs: checkpoint D3Q" +
+                                                          std::to_string(q) + ", solver D3Q" +
+                                                          std::to_string(scalars[k]->q));
+      if (!(std::isfinite(s.scalars[k].diffusivity) && s.scalars[k].diffusivity > 0.0))
+        throw ckpt::Failure("CKPT_PAYLOAD_CORRUPT", "scalar diffusivity must be finite > 0");
+    }
+  }
+  // Body-force field of a checkpoint: slots for the fluid cells with a
+  // nonzero force, the values in both the applied field and the field inside
+  // the cached moments (null: no field).
+  void install_force_field(const double* ff) {
+    if (ff) {
+      std::vector<int64_t> cells;
+      for (int64_t c = 0; c < n; ++c)
+        if (!solid_h[c] && fslot_h[c] < 0 && (ff[3 * c] != 0.0 || ff[3 * c + 1] != 0.0 || ff[3 * c + 2] != 0.0))
+          cells.push_back(c);
+      ensure_slots(cells);
+    }
+    if (nslots) {
+      std::vector<Vec4<A>> hv(size_t(nslots), Vec4<A>{A(0), A(0), A(0), A(0)});
+      if (ff)
+        for (int64_t k = 0; k < nslots; ++k) {
+          const int64_t c = slot_cell_h[size_t(k)];
+          hv[size_t(k)] = Vec4<A>{A(ff[3 * c]), A(ff[3 * c + 1]), A(ff[3 * c + 2]), A(0)};
+        }
+      CK(cudaMemcpyAsync(fcur.p, hv.data(), hv.size() * sizeof(Vec4<A>), cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(fprev.p, hv.data(), hv.size() * sizeof(Vec4<A>), cudaMemcpyHostToDevice, st));
+      CK(cudaStreamSynchronize(st));
+    }
+    field_present = ff != nullptr;
+    fprev_stale = false;
+    invalidate_graphs();
+  }
+  void checkpoint_install(const ckpt::State& s) override {
+    checkpoint_check(s);
+    sync();
+    stage_in(s.f.data());
+    install_force_field(s.has_force_field ? s.force_field.data() : nullptr);
+    // carried solid-cell moments (moments are never updated on solids)
+    for (int64_t c = 0; c < n; ++c)
+      if (solid_h[c]) {
+        init_rho_h[c] = s.moments[size_t(c)];
+        for (int k = 0; k < 3; ++k) init_u_h[size_t(3 * c + k)] = s.moments[size_t((k + 1) * n + c)];
+      }
+    d_init_u_ok = false;
+    for (size_t k = 0; k < s.scalars.size(); ++k) {
+      const ckpt::Scalar& x = s.scalars[k];
+      if (k >= scalars.size()) enable_scalar(x.q, x.diffusivity);
+      ScalarStateT<A>& sc = *scalars[k];
+      sc.diffusivity = x.diffusivity;
+      sc.name = x.name;
+      DevBuf<double> d;
+      d.upload(x.h.data(), x.h.size(), st);
+      scalar_stage_in_kernel<A><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(sc.h.p, sc.hplane, d.p, sc.q, n);
+      CK(cudaGetLastError());
+      sc.parity = 0;
+      CK(cudaStreamSynchronize(st));
+    }
+    time = s.step;
+    has_qoi = s.has_qoi;
+    qoi_json = s.qoi_json;
+    invalidate_graphs();
+  }
+
   // Oxygen transfer / uptake on scalar k (the gather -> host source ->
   // set composition of the reference, on the device). a's arrays are host
   // pointers (n values each, or null); *sum = the source integral.
@@ -1971,6 +2121,7 @@ struct Engine final : EngineBase {
     if (ffo) CK(cudaMemcpy(ffo, d_ff.p, size_t(3 * steps) * sizeof(double), cudaMemcpyDeviceToHost));
     if (iters) CK(cudaMemcpy(iters, d_it.p, size_t(steps) * sizeof(int32_t), cudaMemcpyDeviceToHost));
     if (cv && k >= 0) CK(cudaMemcpy(cv, d_cv.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
+    time += uint64_t(steps);
   }
 
   BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,
@@ -2343,6 +2494,7 @@ struct Engine final : EngineBase {
     field_present = true;
     fprev_stale = false;
     invalidate_graphs();
+    time += uint64_t(N);
     // d omega / d nu (params.rs:205-217): omega+ = 1/(3 nu + 1/2),
     // omega- = 1/(magic/(3 nu) + 1/2) for TRT, = omega+ for BGK
     const double nu = cfg.nu;
@@ -2565,6 +2717,7 @@ struct Batch final : BatchBase {
       e->field_present = true;
       e->fprev_stale = false;
       e->invalidate_graphs();
+      e->time += uint64_t(steps);
     }
   }
 

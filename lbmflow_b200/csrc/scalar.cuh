@@ -155,6 +155,40 @@ __global__ void scalar_gather_kernel(const A* hb, int64_t hpl, const uint8_t* fl
   out[cell] = double(scalar_conc<SQ, A>(hb, hpl, cell, x, y, z, nx, ny, nz, mask, sparity));
 }
 
+// Logical post-stream scalar populations -> f64 q-major (checkpoint gather),
+// the read of scalar_step_kernel; solid cells report their raw own slots.
+template <int SQ, class A>
+__global__ void scalar_stage_out_kernel(const A* hb, int64_t hpl, const uint8_t* flags, const uint32_t* nbr, int nx,
+                                        int ny, int nz, int sparity, double* out, int64_t n) {
+  using L = Lat<SQ>;
+  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (cell >= n) return;
+  const uint8_t fl = flags[cell];
+  if (sparity == 0 || (fl & F_SOLID)) {
+#pragma unroll
+    for (int q = 0; q < SQ; ++q) out[q * n + cell] = double(hb[q * hpl + cell]);
+    return;
+  }
+  int x, y, z;
+  cell_xyz(cell, nx, ny, x, y, z);
+  const uint32_t mask = (fl & F_BOUNDARY) ? nbr[cell] : 0u;
+  const Nbr nb(x, y, z, nx, ny, nz);
+#pragma unroll
+  for (int q = 0; q < SQ; ++q) {
+    const int o = opp(q);
+    const A v = ((mask >> o) & 1u) ? hb[q * hpl + cell] : hb[o * hpl + nb.at(-L::cx(q), -L::cy(q), -L::cz(q))];
+    out[q * n + cell] = double(v);
+  }
+}
+
+// f64 q-major scalar populations -> normal (parity 0) layout.
+template <class A>
+__global__ void scalar_stage_in_kernel(A* hb, int64_t hpl, const double* in, int sq, int64_t n) {
+  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (cell >= n) return;
+  for (int q = 0; q < sq; ++q) hb[q * hpl + cell] = A(in[q * n + cell]);
+}
+
 // h = h_eq(C, u) at every cell with u of the current hydro state (solids:
 // u from the host-side initial values), normal layout (set_scalar_
 // concentration, solver.rs:2910-2966).

@@ -103,6 +103,9 @@ static int guarded(F&& fn) {
   } catch (const Error& e) {
     lbmb::g_last_error = e.what();
     return e.code;
+  } catch (const lbmb::ckpt::Failure& e) {
+    lbmb::g_last_error = e.what();
+    return LBMB_ERR_CHECKPOINT;
   } catch (const std::bad_alloc&) {
     lbmb::g_last_error = "host allocation failed";
     return LBMB_ERR_NOMEM;
@@ -559,6 +562,91 @@ int lbmb_sync(lbmb_solver* h) {
   return guarded([&] {
     NEED(h);
     h->e->sync();
+  });
+}
+
+// ---- checkpoint/restart ------------------------------------------------------
+
+static lbmb::ckpt::Spec checkpoint_spec(const lbmb_config& c) {
+  lbmb::ckpt::Spec s;
+  s.q = c.lattice;
+  s.collision = c.collision;
+  s.f64 = c.storage == LBMB_STORE_F64;
+  for (int a = 0; a < 3; ++a) {
+    s.dims[a] = c.dims[a];
+    s.periodic[a] = c.periodic[a] != 0;
+    s.force[a] = c.force[a];
+  }
+  s.nu = c.nu;
+  s.magic = c.magic;
+  s.omega_shear = c.omega_shear;
+  return s;
+}
+
+int lbmb_get_time(const lbmb_solver* h, uint64_t* step) {
+  return guarded([&] {
+    if (!h || !h->e || !step) throw Error(LBMB_ERR_INVALID, "null argument");
+    *step = h->e->time;
+  });
+}
+
+int lbmb_set_scalar_name(lbmb_solver* h, int32_t k, const char* name) {
+  return guarded([&] {
+    NEED(h);
+    if (!name) throw Error(LBMB_ERR_INVALID, "null argument");
+    h->e->set_scalar_name(k, std::string(name));
+  });
+}
+
+int lbmb_set_qoi_checkpoint_state(lbmb_solver* h, const char* json, int64_t len) {
+  return guarded([&] {
+    NEED(h);
+    if (!json) {
+      h->e->has_qoi = false;
+      h->e->qoi_json.clear();
+      return;
+    }
+    if (len < 0) throw Error(LBMB_ERR_INVALID, "negative length");
+    std::string t(json, size_t(len));
+    if (!lbmb::ckpt::json_object(t)) throw Error(LBMB_ERR_INVALID, "QOI checkpoint state must be a JSON object");
+    h->e->has_qoi = true;
+    h->e->qoi_json = std::move(t);
+  });
+}
+
+int lbmb_get_qoi_checkpoint_state(lbmb_solver* h, char* buf, int64_t cap, int64_t* len) {
+  return guarded([&] {
+    NEED(h);
+    if (!len) throw Error(LBMB_ERR_INVALID, "null argument");
+    if (!h->e->has_qoi) {
+      *len = -1;
+      return;
+    }
+    *len = int64_t(h->e->qoi_json.size());
+    if (buf && cap > 0) std::memcpy(buf, h->e->qoi_json.data(), size_t(std::min<int64_t>(cap, *len)));
+  });
+}
+
+int lbmb_checkpoint_save(lbmb_solver* h, const char* dir) {
+  return guarded([&] {
+    NEED(h);
+    if (!dir) throw Error(LBMB_ERR_INVALID, "null argument");
+    lbmb::ckpt::State st;
+    h->e->checkpoint_gather(st);
+    const auto& wu = h->e->wall_u_in;
+    lbmb::ckpt::save(dir, checkpoint_spec(h->e->config()), h->e->solid().data(), wu.empty() ? nullptr : wu.data(),
+                     st);
+  });
+}
+
+int lbmb_checkpoint_restore(lbmb_solver* h, const char* dir) {
+  return guarded([&] {
+    NEED(h);
+    if (!dir) throw Error(LBMB_ERR_INVALID, "null argument");
+    const auto& wu = h->e->wall_u_in;
+    const lbmb::ckpt::State st = lbmb::ckpt::load(dir, checkpoint_spec(h->e->config()), h->e->solid().data(),
+                                                  wu.empty() ? nullptr : wu.data());
+    h->e->checkpoint_install(st);
   });
 }
 

@@ -98,6 +98,12 @@ def lib():
         L.lbmo_oxygen_uptake.argtypes = [_dp, _dp, C.c_long, C.c_double, C.c_int, _dp, _dp, _dp, _dp]
         L.lbmo_henry_equilibrium.restype = C.c_double
         L.lbmo_henry_equilibrium.argtypes = [C.c_double, C.c_double]
+        L.lbmo_state_get.argtypes = [C.c_void_p, _dp, _dp, _dp, _ip, _dp, C.POINTER(C.c_uint64)]
+        L.lbmo_state_set.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, _dp, C.c_uint64]
+        L.lbmo_scalar_count.restype = C.c_int
+        L.lbmo_scalar_count.argtypes = [C.c_void_p]
+        L.lbmo_scalar_raw_get.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp, _dp]
+        L.lbmo_scalar_raw_set.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp, _dp]
         L.lbmo_interfacial_area_density.restype = C.c_double
         L.lbmo_interfacial_area_density.argtypes = [C.c_double, _dp, C.c_double]
         _lib = L
@@ -135,6 +141,7 @@ class OracleSolver:
         self.dims = tuple(int(d) for d in dims)
         self.n = self.dims[0] * self.dims[1] * self.dims[2]
         self.q = q
+        self.real_bits = real_bits
         dims_a = (C.c_int * 3)(*self.dims)
         per_a = (C.c_int * 3)(*[int(bool(p)) for p in periodic])
         force_a = np.asarray(force, dtype=np.float64)
@@ -250,6 +257,38 @@ class OracleSolver:
         out = np.zeros(self.n)
         lib().lbmo_scalar_get(self.h, k, _d(out))
         return out
+
+    def state(self):
+        """Raw state: f and ftmp (Q x n, deviation form), moments (4 x n),
+        force field (n x 3 or None), time, and per scalar its lattice,
+        diffusivity, h and htmp (q x n) and concentration."""
+        f, ft, mo, ff = (np.zeros(self.q * self.n), np.zeros(self.q * self.n), np.zeros(4 * self.n),
+                         np.zeros(3 * self.n))
+        has, t = C.c_int(), C.c_uint64()
+        lib().lbmo_state_get(self.h, _d(f), _d(ft), _d(mo), C.byref(has), _d(ff), C.byref(t))
+        scal = []
+        for k in range(lib().lbmo_scalar_count(self.h)):
+            q, d = C.c_int(), C.c_double()
+            lib().lbmo_scalar_raw_get(self.h, k, C.byref(q), C.byref(d), None, None, None)
+            h, ht, c = np.zeros(q.value * self.n), np.zeros(q.value * self.n), np.zeros(self.n)
+            lib().lbmo_scalar_raw_get(self.h, k, C.byref(q), C.byref(d), _d(h), _d(ht), _d(c))
+            scal.append({"q": q.value, "diffusivity": d.value, "h": h.reshape(q.value, self.n),
+                         "htmp": ht.reshape(q.value, self.n), "conc": c})
+        return {"step": t.value, "f": f.reshape(self.q, self.n), "ftmp": ft.reshape(self.q, self.n),
+                "moments": mo.reshape(4, self.n), "force_field": ff.reshape(self.n, 3) if has.value else None,
+                "scalars": scal}
+
+    def set_state(self, st):
+        """Install a raw state as the reference's load_into does (no moment
+        recomputation); scalars k < len(st["scalars"]) must be enabled."""
+        ff = st.get("force_field")
+        lib().lbmo_state_set(self.h, _d(_as_d(st["f"], self.q * self.n)), _d(_as_d(st["ftmp"], self.q * self.n)),
+                             _d(_as_d(st["moments"], 4 * self.n)), int(ff is not None),
+                             _d(_as_d(np.zeros(3 * self.n) if ff is None else ff, 3 * self.n)), int(st["step"]))
+        for k, x in enumerate(st.get("scalars", [])):
+            q = int(x["q"])
+            lib().lbmo_scalar_raw_set(self.h, k, float(x["diffusivity"]), _d(_as_d(x["h"], q * self.n)),
+                                      _d(_as_d(x["htmp"], q * self.n)), _d(_as_d(x["conc"], self.n)))
 
     def run_tank(self, pos, w, center, omega, steps, probe_every=1, scalar=-1,
                  max_iterations=3, slip_tolerance=1e-2, kernel_radius=1, relaxation=1.0):

@@ -32,6 +32,14 @@ struct AnySolver {
   virtual void set_omega_field(const double* v) = 0;
   virtual void velocity_gradient(double* g9) const = 0;
   virtual void wale(bool has_max, double tau_max, double* nu_t, double* diag) = 0;
+  // Raw solver state for the checkpoint restatement (fields.rs SoaFields:
+  // f, ftmp, rho/ux/uy/uz, force_field, scalars; Solver::time).
+  virtual void state_get(double* f, double* ftmp, double* mom, int* has_ff, double* ff, uint64_t* time) const = 0;
+  virtual void state_set(const double* f, const double* ftmp, const double* mom, int has_ff, const double* ff,
+                         uint64_t time) = 0;
+  virtual int scalar_count() const = 0;
+  virtual void scalar_raw_get(int k, int* q, double* d, double* h, double* htmp, double* conc) const = 0;
+  virtual void scalar_raw_set(int k, double d, const double* h, const double* htmp, const double* conc) = 0;
 };
 
 template <class L, class T>
@@ -89,6 +97,58 @@ struct Impl final : AnySolver {
     s.wale_update(has_max, tau_max, v, diag);
     if (nu_t)
       for (size_t c = 0; c < s.n; ++c) nu_t[c] = double(v[c]);
+  }
+  void state_get(double* f, double* ftmp, double* mom, int* has_ff, double* ff, uint64_t* time) const override {
+    for (size_t i = 0; i < s.f.size(); ++i) {
+      f[i] = double(s.f[i]);
+      ftmp[i] = double(s.ftmp[i]);
+    }
+    for (size_t c = 0; c < s.n; ++c) {
+      mom[c] = double(s.rho[c]);
+      mom[s.n + c] = double(s.ux[c]);
+      mom[2 * s.n + c] = double(s.uy[c]);
+      mom[3 * s.n + c] = double(s.uz[c]);
+    }
+    *has_ff = s.has_force_field ? 1 : 0;
+    for (size_t i = 0; i < 3 * s.n; ++i) ff[i] = s.has_force_field ? double(s.force_field[i]) : 0.0;
+    *time = s.time;
+  }
+  void state_set(const double* f, const double* ftmp, const double* mom, int has_ff, const double* ff,
+                 uint64_t time) override {
+    for (size_t i = 0; i < s.f.size(); ++i) {
+      s.f[i] = T(f[i]);
+      s.ftmp[i] = T(ftmp[i]);
+    }
+    for (size_t c = 0; c < s.n; ++c) {
+      s.rho[c] = T(mom[c]);
+      s.ux[c] = T(mom[s.n + c]);
+      s.uy[c] = T(mom[2 * s.n + c]);
+      s.uz[c] = T(mom[3 * s.n + c]);
+    }
+    s.has_force_field = has_ff != 0;
+    s.force_field.assign(has_ff ? 3 * s.n : 0, T(0));
+    if (has_ff)
+      for (size_t i = 0; i < 3 * s.n; ++i) s.force_field[i] = T(ff[i]);
+    s.time = time;
+  }
+  int scalar_count() const override { return int(s.scalars.size()); }
+  void scalar_raw_get(int k, int* q, double* d, double* h, double* htmp, double* conc) const override {
+    const auto& sc = s.scalars.at(size_t(k));
+    *q = sc.q;
+    *d = sc.diffusivity;
+    if (h)
+      for (size_t i = 0; i < sc.h.size(); ++i) h[i] = double(sc.h[i]);
+    if (htmp)
+      for (size_t i = 0; i < sc.htmp.size(); ++i) htmp[i] = double(sc.htmp[i]);
+    if (conc)
+      for (size_t c = 0; c < sc.conc.size(); ++c) conc[c] = double(sc.conc[c]);
+  }
+  void scalar_raw_set(int k, double d, const double* h, const double* htmp, const double* conc) override {
+    auto& sc = s.scalars.at(size_t(k));
+    sc.diffusivity = d;
+    for (size_t i = 0; i < sc.h.size(); ++i) sc.h[i] = T(h[i]);
+    for (size_t i = 0; i < sc.htmp.size(); ++i) sc.htmp[i] = T(htmp[i]);
+    for (size_t c = 0; c < sc.conc.size(); ++c) sc.conc[c] = T(conc[c]);
   }
   void strain_rate(double* s6, double* gamma) const override {
     for (size_t c = 0; c < s.n; ++c) {
@@ -347,6 +407,20 @@ long lbmo_run_tank(void* h, const double* pos, const double* w, long nm, const d
 // row-major g[i][j] = du_i/dx_j) and WaleLes::update (tau_eff_max NaN for
 // no bound; diag: 5 values).
 void lbmo_set_omega_field(void* h, const double* v) { static_cast<AnySolver*>(h)->set_omega_field(v); }
+void lbmo_state_get(void* h, double* f, double* ftmp, double* mom, int* has_ff, double* ff, uint64_t* time) {
+  static_cast<AnySolver*>(h)->state_get(f, ftmp, mom, has_ff, ff, time);
+}
+void lbmo_state_set(void* h, const double* f, const double* ftmp, const double* mom, int has_ff, const double* ff,
+                    uint64_t time) {
+  static_cast<AnySolver*>(h)->state_set(f, ftmp, mom, has_ff, ff, time);
+}
+int lbmo_scalar_count(void* h) { return static_cast<AnySolver*>(h)->scalar_count(); }
+void lbmo_scalar_raw_get(void* h, int k, int* q, double* d, double* hh, double* htmp, double* conc) {
+  static_cast<AnySolver*>(h)->scalar_raw_get(k, q, d, hh, htmp, conc);
+}
+void lbmo_scalar_raw_set(void* h, int k, double d, const double* hh, const double* htmp, const double* conc) {
+  static_cast<AnySolver*>(h)->scalar_raw_set(k, d, hh, htmp, conc);
+}
 void lbmo_gather_velocity_gradient(void* h, double* g9) { static_cast<AnySolver*>(h)->velocity_gradient(g9); }
 void lbmo_wale_update(void* h, double tau_eff_max, double* nu_t, double* diag) {
   static_cast<AnySolver*>(h)->wale(std::isfinite(tau_eff_max), tau_eff_max, nu_t, diag);
