@@ -228,6 +228,45 @@ def oxygen_study(g, dims, solid, T):
             abs(led_c["source_integral_mol_s"])}
 
 
+def checkpoint_study(g):
+    """Solver::save / restore (the reference's v3 checkpoint files,
+    solver.rs:4536-5066) of the final headline state: populations, moments,
+    the IBM force field and the D3Q7 scalar, through the C ABI into a
+    temporary directory; then a full-size resume check: 2 steps from the
+    saved state, restore, the same 2 steps again, moments bit for bit."""
+    import shutil
+    import tempfile
+    d = tempfile.mkdtemp(prefix="lbmb_ckpt_")
+    try:
+        g.sync()
+        t0 = time.perf_counter()
+        g.save(d)
+        save_ms = (time.perf_counter() - t0) * 1e3
+        nbytes = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+        t0 = time.perf_counter()
+        g.stage_out()
+        gather_ms = (time.perf_counter() - t0) * 1e3
+        step0 = g.time
+        g.run(2)
+        a = g.read_moments()
+        t0 = time.perf_counter()
+        g.restore(d)
+        restore_ms = (time.perf_counter() - t0) * 1e3
+        restored_step = g.time
+        g.run(2)
+        b = g.read_moments()
+        exact = all(np.array_equal(x, y) for x, y in zip(a, b))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return {"what": "checkpoint save + restore of the final state (manifest.json + rank_0000_part_0000.bin, "
+                    "reference v3 format: padded f32/f64 planes, zero stash, FNV-1a 64 payload hash)",
+            "bytes": nbytes, "save_ms": save_ms, "restore_ms": restore_ms,
+            "save_GBps": nbytes / save_ms / 1e6, "restore_GBps": nbytes / restore_ms / 1e6,
+            "state_gather_ms": gather_ms, "state_gather_note": "device -> host of the logical populations (f64)",
+            "step": step0, "restored_step": restored_step, "resume_bit_exact_2_steps": bool(exact),
+            "directory": "tempfile.mkdtemp() on the bench host"}
+
+
 # ---------------------------------------------------------------------------
 # Distributed plumbing (replicas: one independent tank per GPU)
 # ---------------------------------------------------------------------------
@@ -592,6 +631,8 @@ def run_b200(args, rank, world, local):
     if world == 1 and args.shear:
         extra["shear_qoi"] = shear_study(g, dims, solid, nu, args.tank_T, q, storage)
         extra["oxygen_transfer"] = oxygen_study(g, dims, solid, args.tank_T)
+    if world == 1 and args.ckpt:
+        extra["checkpoint"] = checkpoint_study(g)
     g.close()
     if args.sweep_steps > 0:
         sw = sweep_study(args, rank, world, local)
@@ -691,6 +732,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--shear", type=int, default=1, help="stress QOI study on the final state (0: skip)")
+    ap.add_argument("--ckpt", type=int, default=1, help="checkpoint save/restore study on the final state (0: skip)")
     ap.add_argument("--variants", type=int, default=1)
     ap.add_argument("--les-cs", type=float, default=0.1, help="Smagorinsky constant (0: reference operators)")
     ap.add_argument("--big-T", type=int, default=256, help="tank diameter of the throughput study")

@@ -574,11 +574,38 @@ bool json_object(const std::string& text) {
   }
 }
 
+// FNV-1a 64: h = (h ^ byte) * P per byte, mod 2^64. A zero byte leaves
+// h ^ 0 = h, so a run of k zero bytes multiplies h by P^k; 64-byte blocks
+// that are all zero (the stash planes, halo rows) take one multiply by P^64
+// instead of 64 dependent steps. The result is the byte-serial hash.
+namespace {
+constexpr uint64_t FNV_PRIME = 0x100000001b3ull;
+constexpr uint64_t prime_pow(int k) {
+  uint64_t r = 1;
+  for (int i = 0; i < k; ++i) r *= FNV_PRIME;
+  return r;
+}
+constexpr uint64_t FNV_PRIME_64 = prime_pow(64);
+}  // namespace
+
 uint64_t fnv1a64(const void* data, size_t len, uint64_t h) {
   const unsigned char* p = static_cast<const unsigned char*>(data);
-  for (size_t i = 0; i < len; ++i) {
+  size_t i = 0;
+  for (; i + 64 <= len; i += 64) {
+    uint64_t w[8];
+    std::memcpy(w, p + i, 64);
+    if ((w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) == 0) {
+      h *= FNV_PRIME_64;
+      continue;
+    }
+    for (int k = 0; k < 64; ++k) {
+      h ^= p[i + size_t(k)];
+      h *= FNV_PRIME;
+    }
+  }
+  for (; i < len; ++i) {
     h ^= p[i];
-    h *= 0x100000001b3ull;
+    h *= FNV_PRIME;
   }
   return h;
 }
