@@ -49,6 +49,55 @@ __global__ void stage_in_kernel(S* fb, int64_t pl, const double* in, int64_t n) 
   for (int q = 0; q < Q; ++q) Codec<S>::st(fb + q * pl + cell, typename Codec<S>::A(in[q * n + cell]));
 }
 
+// Checkpoint image of the populations (solver.rs:4550-4552 over
+// fields.rs:3-15): Q planes over the halo-padded box, padded index
+// ((z + 1) (ny + 2) + y + 1) (nx + 2) + x + 1, halo cells zero, core cells
+// the logical post-stream values in the file's type T (solid cells: their
+// raw own slots, as stage_out). One thread per padded cell.
+template <int Q, class S, class T>
+__global__ void pack_padded_kernel(const S* fb, int64_t pl, const uint8_t* flags, const uint32_t* nbr, int nx,
+                                   int ny, int nz, int parity, T* out, int64_t np) {
+  using A = typename Codec<S>::A;
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int64_t px = nx + 2, pxy = px * (ny + 2);
+  const int zz = int(p / pxy);
+  const int64_t r = p - zz * pxy;
+  const int yy = int(r / px);
+  const int x = int(r - yy * px) - 1, y = yy - 1, z = zz - 1;
+  if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) out[q * np + p] = T(0);
+    return;
+  }
+  const int64_t cell = (int64_t(z) * ny + y) * nx + x;
+  const uint8_t fl = flags[cell];
+  A f[Q];
+  if (fl & F_SOLID) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) f[q] = Codec<S>::ld(fb + q * pl + cell);
+  } else {
+    const uint32_t mask = (fl & F_BOUNDARY) ? nbr[cell] : 0u;
+    load_post_stream<Q, S>(fb, pl, cell, x, y, z, nx, ny, nz, mask, parity, f);
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) out[q * np + p] = T(f[q]);
+}
+
+// Checkpoint image -> normal (parity 0) storage layout. One thread per cell.
+template <int Q, class S, class T>
+__global__ void unpack_padded_kernel(S* fb, int64_t pl, const T* img, int nx, int ny, int nz, int64_t n) {
+  using A = typename Codec<S>::A;
+  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (cell >= n) return;
+  int x, y, z;
+  cell_xyz(cell, nx, ny, x, y, z);
+  const int64_t np = int64_t(nx + 2) * (ny + 2) * (nz + 2);
+  const int64_t p = (int64_t(z + 1) * (ny + 2) + (y + 1)) * (nx + 2) + (x + 1);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) Codec<S>::st(fb + q * pl + cell, A(img[q * np + p]));
+}
+
 // Moments of the current state (kernels.rs:627-668) with the force field
 // that is inside the cached moments (fprev). Solid cells are skipped.
 template <int Q, class S>

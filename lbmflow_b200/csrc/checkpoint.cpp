@@ -18,6 +18,9 @@
 #include <map>
 #include <memory>
 #include <sstream>
+#include <atomic>
+#include <functional>
+#include <thread>
 #include <sys/stat.h>
 #include <sys/types.h>
 
@@ -31,8 +34,6 @@ namespace {
 
 constexpr uint32_t FORMAT_VERSION = 3;
 constexpr char MAGIC[8] = {'L', 'B', 'M', 'K', 'P', 'T', 0, 0};
-constexpr uint32_t SEC_F_PRIMARY = 1, SEC_STALE_STASH = 2, SEC_MOMENTS = 3, SEC_SOLID = 4, SEC_FORCE_FIELD = 5,
-                   SEC_SCALAR_FIELDS = 6, SEC_PHASE_FIELD = 7, SEC_QOI_ACCUMULATORS = 10;
 const char* RANK_FILE = "rank_0000_part_0000.bin";
 
 [[noreturn]] void fail(const std::string& code, const std::string& msg) { throw Failure(code, msg); }
@@ -46,67 +47,6 @@ void put_f64(std::string& out, double v) {
   std::memcpy(&b, &v, 8);
   put(out, b, 8);
 }
-// push_real_bytes (solver.rs:1011-1021): f32 runs store each value as f32.
-void put_real(std::string& out, double v, bool f64) {
-  if (f64) {
-    put_f64(out, v);
-  } else {
-    const float x = float(v);
-    uint32_t b;
-    std::memcpy(&b, &x, 4);
-    put(out, b, 4);
-  }
-}
-
-struct Reader {
-  const std::string& b;
-  size_t pos = 0;
-  const char* what;
-  Reader(const std::string& bytes, const char* w) : b(bytes), what(w) {}
-  // take (solver.rs:1074-1085)
-  const char* take(size_t n) {
-    if (pos > b.size() || b.size() - pos < n) fail("CKPT_TRUNCATED", what);
-    const char* p = b.data() + pos;
-    pos += n;
-    return p;
-  }
-  uint64_t uint(int bytes) {
-    const unsigned char* p = reinterpret_cast<const unsigned char*>(take(size_t(bytes)));
-    uint64_t v = 0;
-    for (int i = 0; i < bytes; ++i) v |= uint64_t(p[i]) << (8 * i);
-    return v;
-  }
-  double f64() {
-    const uint64_t u = uint(8);
-    double v;
-    std::memcpy(&v, &u, 8);
-    return v;
-  }
-};
-
-// read_real_bytes (solver.rs:1023-1048)
-std::vector<double> read_reals(const char* p, size_t len, size_t expected, bool f64) {
-  const size_t w = f64 ? 8 : 4;
-  if (len != expected * w)
-    fail("CKPT_GEOM_MISMATCH", "section length " + std::to_string(len) + " does not match expected " +
-                                   std::to_string(expected) + " values of " + std::to_string(w) + " bytes");
-  std::vector<double> out(expected);
-  for (size_t i = 0; i < expected; ++i) {
-    const unsigned char* q = reinterpret_cast<const unsigned char*>(p) + i * w;
-    uint64_t u = 0;
-    for (size_t k = 0; k < w; ++k) u |= uint64_t(q[k]) << (8 * k);
-    if (f64) {
-      std::memcpy(&out[i], &u, 8);
-    } else {
-      const uint32_t u32 = uint32_t(u);
-      float x;
-      std::memcpy(&x, &u32, 4);
-      out[i] = double(x);
-    }
-  }
-  return out;
-}
-
 // ---- FNV-1a 64 streams (solver.rs:831-859) --------------------------------
 struct Hasher {
   uint64_t h = 0xcbf29ce484222325ull;
@@ -208,18 +148,6 @@ void put_padded(std::string& out, const Spec& s, const double* v, int planes, bo
   const Pad g(s);
   if (f64) put_padded_t<double>(out, g, v, planes);
   else put_padded_t<float>(out, g, v, planes);
-}
-
-std::vector<double> core_of(const std::vector<double>& padded, const Spec& s, int planes) {
-  const Pad g(s);
-  std::vector<double> out(size_t(planes) * size_t(g.nc()));
-  for (int q = 0; q < planes; ++q)
-    for (int64_t z = 0; z < g.nz; ++z)
-      for (int64_t y = 0; y < g.ny; ++y)
-        for (int64_t x = 0; x < g.nx; ++x)
-          out[size_t(q) * size_t(g.nc()) + size_t((z * g.ny + y) * g.nx + x)] =
-              padded[size_t(q) * size_t(g.np()) + size_t(g.pidx(x, y, z))];
-  return out;
 }
 
 // ---- JSON (serde_json::to_string_pretty layout; minimal reader) ------------
@@ -411,24 +339,6 @@ std::string f64_text(double v) {
   return buf;
 }
 
-std::string json_escape(const std::string& t) {
-  std::string o = "\"";
-  for (char c : t) {
-    const unsigned char u = static_cast<unsigned char>(c);
-    if (c == '"') o += "\\\"";
-    else if (c == '\\') o += "\\\\";
-    else if (c == '\n') o += "\\n";
-    else if (c == '\r') o += "\\r";
-    else if (c == '\t') o += "\\t";
-    else if (u < 0x20) {
-      char b[8];
-      std::snprintf(b, sizeof b, "\\u%04x", u);
-      o += b;
-    } else o.push_back(c);
-  }
-  return o + "\"";
-}
-
 std::string arr3(uint64_t a, uint64_t b, uint64_t c, const std::string& ind) {
   return "[\n" + ind + "  " + std::to_string(a) + ",\n" + ind + "  " + std::to_string(b) + ",\n" + ind + "  " +
          std::to_string(c) + "\n" + ind + "]";
@@ -503,62 +413,6 @@ void make_dirs(const std::string& dir) {
 
 std::string join(const std::string& dir, const std::string& f) {
   return dir.empty() ? f : (dir.back() == '/' ? dir + f : dir + "/" + f);
-}
-
-// scalar_checkpoint_bytes (solver.rs:1200-1217): the ping-pong partner is
-// written as zero planes like the hydro stash.
-std::string scalar_bytes(const Spec& s, const std::vector<Scalar>& sc) {
-  const Pad g(s);
-  std::string out;
-  put(out, sc.size(), 4);
-  for (const Scalar& x : sc) {
-    put(out, x.name.size(), 4);
-    out += x.name;
-    put_f64(out, x.diffusivity);
-    const uint64_t hl = uint64_t(x.q) * uint64_t(g.np());
-    put(out, hl, 8);
-    put_padded(out, s, x.h.data(), x.q, s.f64);
-    put(out, hl, 8);
-    put_padded(out, s, nullptr, x.q, s.f64);
-    put(out, uint64_t(g.nc()), 8);
-    for (int64_t c = 0; c < g.nc(); ++c) put_real(out, x.conc[size_t(c)], s.f64);
-  }
-  return out;
-}
-
-// restore_scalar_checkpoint (solver.rs:1219-1287). The reference's scalars
-// live on the hydro lattice; a D3Q7 scalar (7 planes) is read too.
-std::vector<Scalar> parse_scalars(const std::string& bytes, const Spec& s) {
-  const Pad g(s);
-  Reader r(bytes, "rank file ended before the declared header/table/payload");
-  const size_t w = s.f64 ? 8 : 4;
-  const uint64_t count = r.uint(4);
-  std::vector<Scalar> out;
-  for (uint64_t k = 0; k < count; ++k) {
-    Scalar x;
-    const uint64_t nl = r.uint(4);
-    x.name.assign(r.take(size_t(nl)), size_t(nl));
-    x.diffusivity = r.f64();
-    const uint64_t hl = r.uint(8);
-    if (hl > bytes.size()) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
-    const char* hp = r.take(size_t(hl) * w);
-    const uint64_t tl = r.uint(8);
-    if (tl > bytes.size()) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
-    r.take(size_t(tl) * w);
-    const uint64_t cl = r.uint(8);
-    if (cl > bytes.size()) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
-    const char* cp = r.take(size_t(cl) * w);
-    const uint64_t np = uint64_t(g.np());
-    const bool q_ok = hl % np == 0 && (hl / np == 7 || hl / np == uint64_t(s.q));
-    if (!q_ok || tl != hl || cl != uint64_t(g.nc()))
-      fail("CKPT_GEOM_MISMATCH", "scalar checkpoint section length differs from current geometry");
-    x.q = int(hl / np);
-    x.h = core_of(read_reals(hp, size_t(hl) * w, size_t(hl), s.f64), s, x.q);
-    x.conc = read_reals(cp, size_t(cl) * w, size_t(cl), s.f64);
-    out.push_back(std::move(x));
-  }
-  if (r.pos != bytes.size()) fail("CKPT_PAYLOAD_CORRUPT", "scalar checkpoint section has trailing bytes");
-  return out;
 }
 
 }  // namespace
@@ -663,6 +517,125 @@ uint64_t mask_hash(const Spec& s, const uint8_t* solid, const double* wall_u) {
   return h.h;
 }
 
+uint64_t padded_cells(const Spec& s) { return uint64_t(Pad(s).np()); }
+
+std::string solid_section(const Spec& s, const uint8_t* solid) {
+  std::vector<uint8_t> ps;
+  std::vector<double> pw;
+  padded_masks(s, solid, nullptr, ps, pw);
+  return std::string(ps.begin(), ps.end());
+}
+
+uint64_t fnv1a64_zeros(uint64_t len, uint64_t h) {
+  // k zero bytes multiply h by P^k (binary powering, mod 2^64)
+  uint64_t r = 1, b = FNV_PRIME;
+  for (uint64_t k = len; k; k >>= 1) {
+    if (k & 1) r *= b;
+    b *= b;
+  }
+  return h * r;
+}
+
+void append_reals(std::string& out, const double* v, size_t count, bool f64) {
+  const size_t w = f64 ? 8 : 4;
+  const size_t at = out.size();
+  out.resize(at + count * w);
+  char* d = &out[at];
+  if (f64) {
+    std::memcpy(d, v, count * 8);
+  } else {
+    for (size_t i = 0; i < count; ++i) {
+      const float x = float(v[i]);
+      std::memcpy(d + 4 * i, &x, 4);
+    }
+  }
+}
+
+void reals_to_double(const char* p, size_t count, bool f64, double* out) {
+  if (f64) {
+    std::memcpy(out, p, count * 8);
+    return;
+  }
+  for (size_t i = 0; i < count; ++i) {
+    float x;
+    std::memcpy(&x, p + 4 * i, 4);
+    out[i] = double(x);
+  }
+}
+
+void unpad_to_double(const char* img, const Spec& s, int planes, double* out) {
+  const Pad g(s);
+  const size_t w = s.f64 ? 8 : 4;
+  for (int q = 0; q < planes; ++q)
+    for (int64_t z = 0; z < g.nz; ++z)
+      for (int64_t y = 0; y < g.ny; ++y)
+        reals_to_double(img + (size_t(q) * size_t(g.np()) + size_t(g.pidx(0, y, z))) * w, size_t(g.nx), s.f64,
+                        out + size_t(q) * size_t(g.nc()) + size_t((z * g.ny + y) * g.nx));
+}
+
+// write_part_checkpoint + write_checkpoint_manifest (solver.rs:4536-4670)
+// with the payload given as pieces. The rank file is written on a second
+// thread while this one hashes the same pieces; zero pieces are written from
+// a zero block and hashed as one multiply.
+void write(const std::string& dir, const Spec& s, uint64_t step, const std::vector<SectionOut>& secs,
+           const uint8_t* solid, const double* wall_u, bool stats) {
+  if (s.q != 19 && s.q != 27) fail("CKPT_LATTICE_MISMATCH", "checkpoint lattice must be D3Q19 or D3Q27");
+  const Pad g(s);
+  std::string head;
+  head.append(MAGIC, 8);
+  put(head, FORMAT_VERSION, 4);
+  head.push_back(0);
+  head.push_back(s.f64 ? 1 : 0);
+  put(head, uint64_t(lattice_id(s.q)), 2);
+  put(head, uint64_t(s.q), 2);
+  put(head, 3, 2);
+  put(head, uint64_t(g.np()), 8);
+  put(head, uint64_t(g.nc()), 8);
+  put(head, secs.size(), 4);
+  uint64_t off = 0;
+  for (const SectionOut& e : secs) {
+    uint64_t len = 0;
+    for (const Piece& p : e.pieces) len += p.len;
+    put(head, e.id, 4);
+    put(head, off, 8);
+    put(head, len, 8);
+    off += len;
+  }
+  const uint64_t total = head.size() + off + 8;
+  make_dirs(dir);
+  const std::string path = join(dir, RANK_FILE);
+  std::FILE* fh = std::fopen(path.c_str(), "wb");
+  if (!fh) fail("CKPT_IO", "cannot create " + path);
+  bool write_ok = true;
+  std::thread writer([&] {
+    static const std::vector<char> zeros(size_t(1) << 20, 0);
+    write_ok = std::fwrite(head.data(), 1, head.size(), fh) == head.size();
+    for (const SectionOut& e : secs)
+      for (const Piece& p : e.pieces) {
+        if (!write_ok) return;
+        if (p.data) {
+          write_ok = std::fwrite(p.data, 1, size_t(p.len), fh) == size_t(p.len);
+        } else {
+          for (uint64_t left = p.len; left && write_ok;) {
+            const size_t k = size_t(std::min<uint64_t>(left, zeros.size()));
+            write_ok = std::fwrite(zeros.data(), 1, k, fh) == k;
+            left -= k;
+          }
+        }
+      }
+  });
+  uint64_t ph = 0xcbf29ce484222325ull;
+  for (const SectionOut& e : secs)
+    for (const Piece& p : e.pieces) ph = p.data ? fnv1a64(p.data, size_t(p.len), ph) : fnv1a64_zeros(p.len, ph);
+  writer.join();
+  std::string trailer;
+  put(trailer, ph, 8);
+  if (write_ok) write_ok = std::fwrite(trailer.data(), 1, 8, fh) == 8;
+  if (std::fclose(fh) != 0) write_ok = false;
+  if (!write_ok) fail("CKPT_IO", "write failed: " + path);
+  write_file(join(dir, "manifest.json"), manifest_text(s, step, total, ph, mask_hash(s, solid, wall_u), stats));
+}
+
 void save(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u, const State& st) {
   if (s.q != 19 && s.q != 27) fail("CKPT_LATTICE_MISMATCH", "checkpoint lattice must be D3Q19 or D3Q27");
   const Pad g(s);
@@ -673,76 +646,76 @@ void save(const std::string& dir, const Spec& s, const uint8_t* solid, const dou
   for (const Scalar& x : st.scalars)
     if ((x.q != 7 && x.q != s.q) || int64_t(x.h.size()) != x.q * nc || int64_t(x.conc.size()) != nc)
       fail("CKPT_GEOM_MISMATCH", "scalar arrays differ from the checkpoint geometry");
-  // write_part_checkpoint (solver.rs:4536-4630)
-  std::vector<std::pair<uint32_t, std::string>> sec;
+  const uint64_t w = s.f64 ? 8 : 4;
+  std::vector<std::string> keep;  // storage of the pieces
+  keep.reserve(16 + 4 * st.scalars.size());
+  auto piece = [&](std::string b) {
+    keep.push_back(std::move(b));
+    return Piece{keep.back().data(), keep.back().size()};
+  };
+  std::vector<SectionOut> secs;
   {
     std::string b;
-    b.reserve(size_t(s.q) * size_t(np) * (s.f64 ? 8 : 4));
     put_padded(b, s, st.f.data(), s.q, s.f64);
-    sec.emplace_back(SEC_F_PRIMARY, std::move(b));
+    secs.push_back({SEC_F_PRIMARY, {piece(std::move(b))}});
   }
+  secs.push_back({SEC_STALE_STASH, {Piece{nullptr, uint64_t(s.q) * uint64_t(np) * w}}});
   {
     std::string b;
-    b.reserve(size_t(s.q) * size_t(np) * (s.f64 ? 8 : 4));
-    put_padded(b, s, nullptr, s.q, s.f64);
-    sec.emplace_back(SEC_STALE_STASH, std::move(b));
+    append_reals(b, st.moments.data(), st.moments.size(), s.f64);
+    secs.push_back({SEC_MOMENTS, {piece(std::move(b))}});
   }
-  {
-    std::string b;
-    for (double v : st.moments) put_real(b, v, s.f64);
-    sec.emplace_back(SEC_MOMENTS, std::move(b));
-  }
-  std::vector<uint8_t> ps;
-  std::vector<double> pw;
-  padded_masks(s, solid, wall_u, ps, pw);
-  sec.emplace_back(SEC_SOLID, std::string(ps.begin(), ps.end()));
+  secs.push_back({SEC_SOLID, {piece(solid_section(s, solid))}});
   if (st.has_force_field) {
     std::string b;
-    for (double v : st.force_field) put_real(b, v, s.f64);
-    sec.emplace_back(SEC_FORCE_FIELD, std::move(b));
+    append_reals(b, st.force_field.data(), st.force_field.size(), s.f64);
+    secs.push_back({SEC_FORCE_FIELD, {piece(std::move(b))}});
   }
-  if (!st.scalars.empty()) sec.emplace_back(SEC_SCALAR_FIELDS, scalar_bytes(s, st.scalars));
-  if (st.has_qoi) sec.emplace_back(SEC_QOI_ACCUMULATORS, st.qoi_json);
-
-  std::string head;
-  head.append(MAGIC, 8);
-  put(head, FORMAT_VERSION, 4);
-  head.push_back(0);
-  head.push_back(s.f64 ? 1 : 0);
-  put(head, uint64_t(lattice_id(s.q)), 2);
-  put(head, uint64_t(s.q), 2);
-  put(head, 3, 2);
-  put(head, uint64_t(np), 8);
-  put(head, uint64_t(nc), 8);
-  put(head, sec.size(), 4);
-  uint64_t off = 0;
-  for (auto& e : sec) {
-    put(head, e.first, 4);
-    put(head, off, 8);
-    put(head, e.second.size(), 8);
-    off += e.second.size();
+  if (!st.scalars.empty()) {
+    SectionOut sec{SEC_SCALAR_FIELDS, {}};
+    std::string count;
+    put(count, st.scalars.size(), 4);
+    sec.pieces.push_back(piece(std::move(count)));
+    for (const Scalar& x : st.scalars) {
+      std::string b;
+      put_padded(b, s, x.h.data(), x.q, s.f64);
+      sec.pieces.push_back(piece(scalar_head(x.name, x.diffusivity, uint64_t(x.q) * uint64_t(np))));
+      sec.pieces.push_back(piece(std::move(b)));
+      for (const Piece& p : scalar_tail(x.q, np, nc, w)) sec.pieces.push_back(p.data ? piece(std::string(p.data, p.len)) : p);
+      std::string c;
+      append_reals(c, x.conc.data(), x.conc.size(), s.f64);
+      sec.pieces.push_back(piece(std::move(c)));
+    }
+    secs.push_back(std::move(sec));
   }
-  uint64_t ph = 0xcbf29ce484222325ull;
-  for (auto& e : sec) ph = fnv1a64(e.second.data(), e.second.size(), ph);
-  std::string trailer;
-  put(trailer, ph, 8);
-  const uint64_t total = head.size() + off + trailer.size();
-
-  make_dirs(dir);
-  {
-    const std::string path = join(dir, RANK_FILE);
-    std::ofstream out(path, std::ios::binary | std::ios::trunc);
-    if (!out) fail("CKPT_IO", "cannot create " + path);
-    out.write(head.data(), std::streamsize(head.size()));
-    for (auto& e : sec) out.write(e.second.data(), std::streamsize(e.second.size()));
-    out.write(trailer.data(), std::streamsize(trailer.size()));
-    out.flush();
-    if (!out) fail("CKPT_IO", "write failed: " + path);
-  }
-  write_file(join(dir, "manifest.json"), manifest_text(s, st.step, total, ph, mask_hash(s, solid, wall_u), st.has_qoi));
+  if (st.has_qoi) secs.push_back({SEC_QOI_ACCUMULATORS, {piece(st.qoi_json)}});
+  write(dir, s, st.step, secs, solid, wall_u, st.has_qoi);
 }
 
-State load(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u) {
+// Scalar entry of the SCALAR_FIELDS section (solver.rs:1200-1217): name,
+// diffusivity and the h length before the h planes ...
+std::string scalar_head(const std::string& name, double diffusivity, uint64_t h_len) {
+  std::string b;
+  put(b, name.size(), 4);
+  b += name;
+  put_f64(b, diffusivity);
+  put(b, h_len, 8);
+  return b;
+}
+// ... then the ping-pong partner (zero planes) and the concentration
+// length; the concentration values follow.
+std::vector<Piece> scalar_tail(int q, int64_t np, int64_t nc, uint64_t w) {
+  static thread_local std::string len_h, len_c;
+  len_h.clear();
+  put(len_h, uint64_t(q) * uint64_t(np), 8);
+  len_c.clear();
+  put(len_c, uint64_t(nc), 8);
+  return {Piece{len_h.data(), 8}, Piece{nullptr, uint64_t(q) * uint64_t(np) * w}, Piece{len_c.data(), 8}};
+}
+
+// read_rank_file + load_into (solver.rs:1108-1198, 4759-5060).
+View read(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u,
+          const std::function<char*(size_t)>& alloc) {
   const Pad g(s);
   const int64_t nc = g.nc(), np = g.np();
   // load_into (solver.rs:4759-4824)
@@ -829,42 +802,103 @@ State load(const std::string& dir, const Spec& s, const uint8_t* solid, const do
     fail("CKPT_MASK_MISMATCH", "mask_hash differed for rank=0 part=" + std::to_string(e.part) +
                                    ": checkpoint=" + e.mask_hash + " current=" + cur_mask);
 
-  // read_rank_file (solver.rs:1108-1198)
+  // read_rank_file (solver.rs:1108-1198): the file is read on a second
+  // thread in blocks while this one hashes the payload behind it.
   if (e.file.find('/') != std::string::npos || e.file == ".." || e.file.empty())
     fail("CKPT_MANIFEST_INVALID", "rank file name must be a plain file name: " + e.file);
-  const std::string bytes = read_file(join(dir, e.file));
-  Reader r(bytes, "rank file ended before the declared header/table/payload");
-  if (std::memcmp(r.take(8), MAGIC, 8) != 0) fail("CKPT_BAD_MAGIC", "rank file magic is not LBMKPT");
-  const uint64_t rv = r.uint(4);
+  const std::string path = join(dir, e.file);
+  struct stat sb;
+  if (::stat(path.c_str(), &sb) != 0) fail("CKPT_IO", "No such file or directory (os error 2): " + path);
+  const size_t fsize = size_t(sb.st_size);
+  std::FILE* fh = std::fopen(path.c_str(), "rb");
+  if (!fh) fail("CKPT_IO", "cannot open " + path);
+  char* buf = alloc(std::max<size_t>(fsize, 1));
+  std::atomic<size_t> avail{0};
+  std::atomic<bool> read_failed{false};
+  std::thread reader([&] {
+    constexpr size_t BLOCK = size_t(16) << 20;
+    size_t done = 0;
+    while (done < fsize) {
+      const size_t k = std::fread(buf + done, 1, std::min(BLOCK, fsize - done), fh);
+      if (k == 0) {
+        read_failed = true;
+        break;
+      }
+      done += k;
+      avail.store(done, std::memory_order_release);
+    }
+  });
+  struct Joiner {
+    std::thread& t;
+    std::FILE* f;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+      std::fclose(f);
+    }
+  } joiner{reader, fh};
+  auto wait_for = [&](size_t upto) {
+    while (avail.load(std::memory_order_acquire) < upto) {
+      if (read_failed) fail("CKPT_IO", "read failed: " + path);
+      std::this_thread::yield();
+    }
+  };
+  // header and section table
+  size_t pos = 0;
+  auto take = [&](size_t k) -> const char* {
+    if (fsize - pos < k || pos > fsize)
+      fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+    wait_for(pos + k);
+    const char* p = buf + pos;
+    pos += k;
+    return p;
+  };
+  auto uint = [&](int bytes) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(take(size_t(bytes)));
+    uint64_t v = 0;
+    for (int i = 0; i < bytes; ++i) v |= uint64_t(p[i]) << (8 * i);
+    return v;
+  };
+  if (std::memcmp(take(8), MAGIC, 8) != 0) fail("CKPT_BAD_MAGIC", "rank file magic is not LBMKPT");
+  const uint64_t rv = uint(4);
   if (rv != FORMAT_VERSION)
     fail("CKPT_VERSION_MISMATCH",
          "rank file format_version " + std::to_string(rv) + " differs from supported " +
              std::to_string(FORMAT_VERSION) +
              "; rerun from the original scenario or migrate with a checkpoint upgrader before restart");
-  if (r.uint(1) != 0) fail("CKPT_BAD_MAGIC", "cross-endian checkpoints are not supported by this checkpoint format");
-  const uint64_t hdtype = r.uint(1), hlat = r.uint(2), hq = r.uint(2), hd = r.uint(2);
-  const uint64_t hnp = r.uint(8), hnc = r.uint(8);
-  const uint64_t nsec = r.uint(4);
+  if (uint(1) != 0) fail("CKPT_BAD_MAGIC", "cross-endian checkpoints are not supported by this checkpoint format");
+  const uint64_t hdtype = uint(1), hlat = uint(2), hq = uint(2), hd = uint(2);
+  const uint64_t hnp = uint(8), hnc = uint(8);
+  const uint64_t nsec = uint(4);
   struct Sec {
     uint64_t id, off, len;
   };
   std::vector<Sec> table;
   for (uint64_t k = 0; k < nsec; ++k) {
     Sec t;
-    t.id = r.uint(4);
-    t.off = r.uint(8);
-    t.len = r.uint(8);
+    t.id = uint(4);
+    t.off = uint(8);
+    t.len = uint(8);
     table.push_back(t);
   }
-  if (bytes.size() - r.pos < 8) fail("CKPT_TRUNCATED", "rank file is missing payload hash trailer");
-  const size_t pend = bytes.size() - 8;
-  Reader tr(bytes, "");
-  tr.pos = pend;
-  const uint64_t phash = tr.uint(8);
-  const char* payload = bytes.data() + r.pos;
-  const size_t plen = pend - r.pos;
-  if (fnv1a64(payload, plen) != phash)
-    fail("CKPT_PAYLOAD_CORRUPT", "rank file payload hash does not match its contents");
+  if (fsize - pos < 8) fail("CKPT_TRUNCATED", "rank file is missing payload hash trailer");
+  const size_t pend = fsize - 8;
+  const char* payload = buf + pos;
+  const size_t plen = pend - pos;
+  uint64_t ph_calc = 0xcbf29ce484222325ull;
+  {
+    constexpr size_t STEP = size_t(4) << 20;
+    for (size_t at = pos; at < pend;) {
+      const size_t k = std::min(STEP, pend - at);
+      wait_for(at + k);
+      ph_calc = fnv1a64(buf + at, k, ph_calc);
+      at += k;
+    }
+  }
+  wait_for(fsize);
+  reader.join();
+  uint64_t phash = 0;
+  for (int i = 0; i < 8; ++i) phash |= uint64_t(static_cast<unsigned char>(buf[pend + size_t(i)])) << (8 * i);
+  if (ph_calc != phash) fail("CKPT_PAYLOAD_CORRUPT", "rank file payload hash does not match its contents");
   std::map<uint32_t, std::pair<size_t, size_t>> sections;  // id -> (offset, length); later entries win
   for (const Sec& t : table) {
     if (t.off > plen || t.len > plen - t.off)
@@ -890,15 +924,23 @@ State load(const std::string& dir, const Spec& s, const uint8_t* solid, const do
     if (!p) fail("CKPT_TRUNCATED", std::string("checkpoint is missing required section ") + name);
     return *p;
   };
-  State st;
-  st.step = step;
+  const size_t w = s.f64 ? 8 : 4;
+  auto check_len = [&](size_t len, size_t expected) {
+    if (len != expected * w)
+      fail("CKPT_GEOM_MISMATCH", "section length " + std::to_string(len) + " does not match expected " +
+                                     std::to_string(expected) + " values of " + std::to_string(w) + " bytes");
+  };
+  View v;
+  v.step = step;
   {
     const auto p = required(SEC_F_PRIMARY, "F_PRIMARY");
-    st.f = core_of(read_reals(payload + p.first, p.second, size_t(s.q) * size_t(np), s.f64), s, s.q);
+    check_len(p.second, size_t(s.q) * size_t(np));
+    v.f = payload + p.first;
     const auto t = required(SEC_STALE_STASH, "STALE_STASH");
-    read_reals(payload + t.first, t.second, size_t(s.q) * size_t(np), s.f64);
+    check_len(t.second, size_t(s.q) * size_t(np));
     const auto mo = required(SEC_MOMENTS, "MOMENTS");
-    st.moments = read_reals(payload + mo.first, mo.second, size_t(4 * nc), s.f64);
+    check_len(mo.second, size_t(4 * nc));
+    v.moments = payload + mo.first;
   }
   if (const auto* p = section(SEC_SOLID)) {
     if (p->second != size_t(np))
@@ -911,18 +953,110 @@ State load(const std::string& dir, const Spec& s, const uint8_t* solid, const do
         fail("CKPT_MASK_MISMATCH", "serialized solid mask differs from rebuilt mask");
   }
   if (const auto* p = section(SEC_FORCE_FIELD)) {
-    st.has_force_field = true;
-    st.force_field = read_reals(payload + p->first, p->second, size_t(3 * nc), s.f64);
+    check_len(p->second, size_t(3 * nc));
+    v.force_field = payload + p->first;
   }
-  if (const auto* p = section(SEC_SCALAR_FIELDS)) st.scalars = parse_scalars(std::string(payload + p->first, p->second), s);
+  if (const auto* p = section(SEC_SCALAR_FIELDS)) {
+    // restore_scalar_checkpoint (solver.rs:1219-1287). The reference's
+    // scalars live on the hydro lattice; a D3Q7 scalar (7 planes) is read too.
+    const char* base = payload + p->first;
+    const size_t blen = p->second;
+    size_t at = 0;
+    auto stake = [&](size_t k) -> const char* {
+      if (at > blen || blen - at < k) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+      const char* r = base + at;
+      at += k;
+      return r;
+    };
+    auto suint = [&](int bytes) {
+      const unsigned char* q = reinterpret_cast<const unsigned char*>(stake(size_t(bytes)));
+      uint64_t x = 0;
+      for (int i = 0; i < bytes; ++i) x |= uint64_t(q[i]) << (8 * i);
+      return x;
+    };
+    const uint64_t count = suint(4);
+    for (uint64_t k = 0; k < count; ++k) {
+      ScalarView x;
+      const uint64_t nl = suint(4);
+      x.name.assign(stake(size_t(nl)), size_t(nl));
+      const uint64_t db = suint(8);
+      std::memcpy(&x.diffusivity, &db, 8);
+      const uint64_t hl = suint(8);
+      if (hl > blen) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+      x.h = stake(size_t(hl) * w);
+      const uint64_t tl = suint(8);
+      if (tl > blen) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+      stake(size_t(tl) * w);
+      const uint64_t cl = suint(8);
+      if (cl > blen) fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
+      x.conc = stake(size_t(cl) * w);
+      const bool q_ok = hl % uint64_t(np) == 0 && (hl / uint64_t(np) == 7 || hl / uint64_t(np) == uint64_t(s.q));
+      if (!q_ok || tl != hl || cl != uint64_t(nc))
+        fail("CKPT_GEOM_MISMATCH", "scalar checkpoint section length differs from current geometry");
+      x.q = int(hl / uint64_t(np));
+      v.scalars.push_back(std::move(x));
+    }
+    if (at != blen) fail("CKPT_PAYLOAD_CORRUPT", "scalar checkpoint section has trailing bytes");
+  }
   if (section(SEC_PHASE_FIELD))
     fail("CKPT_UNSUPPORTED", "the checkpoint carries a phase-field distribution; this solver is single-phase");
   if (const auto* p = section(SEC_QOI_ACCUMULATORS)) {
-    st.has_qoi = true;
-    st.qoi_json.assign(payload + p->first, p->second);
-    if (!json_object(st.qoi_json)) fail("CKPT_MANIFEST_INVALID", "QOI accumulator section is not a JSON object");
+    v.has_qoi = true;
+    v.qoi_json.assign(payload + p->first, p->second);
+    if (!json_object(v.qoi_json)) fail("CKPT_MANIFEST_INVALID", "QOI accumulator section is not a JSON object");
   }
+  return v;
+}
+
+State load(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u) {
+  const Pad g(s);
+  const size_t nc = size_t(g.nc());
+  std::string storage;
+  const View v = read(dir, s, solid, wall_u, [&](size_t b) {
+    storage.resize(b);
+    return &storage[0];
+  });
+  State st;
+  st.step = v.step;
+  st.f.resize(size_t(s.q) * nc);
+  unpad_to_double(v.f, s, s.q, st.f.data());
+  st.moments.resize(4 * nc);
+  reals_to_double(v.moments, 4 * nc, s.f64, st.moments.data());
+  if (v.force_field) {
+    st.has_force_field = true;
+    st.force_field.resize(3 * nc);
+    reals_to_double(v.force_field, 3 * nc, s.f64, st.force_field.data());
+  }
+  for (const ScalarView& x : v.scalars) {
+    Scalar y;
+    y.name = x.name;
+    y.diffusivity = x.diffusivity;
+    y.q = x.q;
+    y.h.resize(size_t(x.q) * nc);
+    unpad_to_double(x.h, s, x.q, y.h.data());
+    y.conc.resize(nc);
+    reals_to_double(x.conc, nc, s.f64, y.conc.data());
+    st.scalars.push_back(std::move(y));
+  }
+  st.has_qoi = v.has_qoi;
+  st.qoi_json = v.qoi_json;
   return st;
+}
+
+Spec spec_of(const lbmb_config& c) {
+  Spec s;
+  s.q = c.lattice;
+  s.collision = c.collision;
+  s.f64 = c.storage == LBMB_STORE_F64;
+  for (int a = 0; a < 3; ++a) {
+    s.dims[a] = c.dims[a];
+    s.periodic[a] = c.periodic[a] != 0;
+    s.force[a] = c.force[a];
+  }
+  s.nu = c.nu;
+  s.magic = c.magic;
+  s.omega_shear = c.omega_shear;
+  return s;
 }
 
 }  // namespace ckpt

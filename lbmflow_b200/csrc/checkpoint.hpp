@@ -22,9 +22,12 @@
 // carries state into the next step.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
+
+#include "../../include/lbmb.h"
 
 namespace lbmb {
 namespace ckpt {
@@ -74,6 +77,62 @@ uint64_t decomp_hash(const Spec& s);
 uint64_t mask_hash(const Spec& s, const uint8_t* solid, const double* wall_u);
 std::string hash_string(uint64_t h);
 
+// A run of payload bytes: data, or (data == nullptr) len zero bytes.
+struct Piece {
+  const char* data;
+  uint64_t len;
+};
+struct SectionOut {
+  uint32_t id;
+  std::vector<Piece> pieces;
+};
+// Section ids (solver.rs:31-44).
+constexpr uint32_t SEC_F_PRIMARY = 1, SEC_STALE_STASH = 2, SEC_MOMENTS = 3, SEC_SOLID = 4, SEC_FORCE_FIELD = 5,
+                   SEC_SCALAR_FIELDS = 6, SEC_PHASE_FIELD = 7, SEC_QOI_ACCUMULATORS = 10;
+
+// A scalar entry as read: h points at q padded planes, conc at n values,
+// both in the file's dtype.
+struct ScalarView {
+  std::string name;
+  double diffusivity = 0.0;
+  int q = 0;
+  const char* h = nullptr;
+  const char* conc = nullptr;
+};
+// A validated checkpoint in memory: pointers into the rank file image.
+struct View {
+  uint64_t step = 0;
+  const char* f = nullptr;            // Q padded planes, file dtype
+  const char* moments = nullptr;      // 4 x n, file dtype
+  const char* force_field = nullptr;  // n x 3, file dtype, or null
+  std::vector<ScalarView> scalars;
+  bool has_qoi = false;
+  std::string qoi_json;
+};
+
+uint64_t padded_cells(const Spec& s);
+// The SOLID section: the padded mask after the mask exchange, one byte per
+// padded cell.
+std::string solid_section(const Spec& s, const uint8_t* solid);
+// hash of `len` zero bytes continuing h
+uint64_t fnv1a64_zeros(uint64_t len, uint64_t h);
+void append_reals(std::string& out, const double* v, size_t count, bool f64);
+void reals_to_double(const char* p, size_t count, bool f64, double* out);
+void unpad_to_double(const char* img, const Spec& s, int planes, double* out);
+std::string scalar_head(const std::string& name, double diffusivity, uint64_t h_len);
+std::vector<Piece> scalar_tail(int q, int64_t np, int64_t nc, uint64_t w);
+
+// The rank file (header, section table, payload pieces, hash trailer) and
+// the manifest; the payload is hashed while a second thread writes it.
+void write(const std::string& dir, const Spec& s, uint64_t step, const std::vector<SectionOut>& secs,
+           const uint8_t* solid, const double* wall_u, bool stats);
+
+// Every check of the reference's restore, in its order and with its codes;
+// the rank file image lands in memory from alloc(bytes) and is hashed while
+// it is read.
+View read(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u,
+          const std::function<char*(size_t)>& alloc);
+
 // Whether the text is one JSON object (the QOI accumulator section).
 bool json_object(const std::string& text);
 
@@ -84,6 +143,10 @@ void save(const std::string& dir, const Spec& s, const uint8_t* solid, const dou
 // Solver::restore / load_into (solver.rs:4739-5066): every check runs before
 // anything is returned, in the reference's order and with its codes.
 State load(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u);
+
+// The checkpoint Spec of a solver configuration: dtype "f64" for F64
+// storage, "f32" for F32 / F16 / BF16 storage.
+Spec spec_of(const lbmb_config& c);
 
 }  // namespace ckpt
 }  // namespace lbmb

@@ -157,12 +157,10 @@ struct EngineBase {
                           int64_t* count) = 0;
   virtual int q() const = 0;
   virtual const std::vector<uint8_t>& solid() const = 0;
-  // Checkpoint/restart (checkpoint.hpp): the state a checkpoint carries,
-  // the fit of a loaded state (checked before anything is installed) and
-  // its installation.
-  virtual void checkpoint_gather(ckpt::State& s) = 0;
-  virtual void checkpoint_check(const ckpt::State& s) const = 0;
-  virtual void checkpoint_install(const ckpt::State& s) = 0;
+  // Checkpoint/restart in the reference's v3 format (checkpoint.hpp):
+  // Solver::save and Solver::restore.
+  virtual void checkpoint_save(const std::string& dir) = 0;
+  virtual void checkpoint_restore(const std::string& dir) = 0;
   virtual void set_scalar_name(int k, const std::string& name) = 0;
   virtual const lbmb_config& config() const = 0;
   uint64_t time = 0;              // Solver::time: hydro steps taken
@@ -1838,65 +1836,192 @@ struct Engine final : EngineBase {
     if (name.empty() || name.size() > 63) invalid("scalar name must have 1 to 63 bytes");
     scalar(k).name = name;
   }
-  // Logical scalar populations (q x n, f64) of the current scalar state.
-  void scalar_populations(ScalarStateT<A>& sc, double* out) {
-    DevBuf<double> d;
-    d.alloc(size_t(sc.q) * size_t(n));
-    const unsigned g = unsigned(ceil_div(n, 128));
-    if (sc.q == 7)
-      scalar_stage_out_kernel<7, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, d.p,
-                                                       n);
-    else
-      scalar_stage_out_kernel<Q, A><<<g, 128, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz, sc.parity, d.p,
-                                                       n);
+  // Pinned host staging of checkpoint images (kept between calls).
+  struct PinBuf {
+    char* p = nullptr;
+    size_t n = 0;
+    PinBuf() = default;
+    PinBuf(const PinBuf&) = delete;
+    PinBuf& operator=(const PinBuf&) = delete;
+    ~PinBuf() {
+      if (p) cudaFreeHost(p);
+    }
+    char* ensure(size_t b) {
+      if (b > n) {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&p), b, cudaHostAllocDefault));
+        n = b;
+      }
+      return p;
+    }
+  };
+  PinBuf ckpt_pin;
+  // file dtype of the populations: f64 storage writes "f64", the rest "f32"
+  using FileT = typename std::conditional<std::is_same<S, double>::value, double, float>::type;
+
+  // Solver::save (solver.rs:4536-4724): the device packs the padded
+  // population and scalar planes in the file's type, one copy brings them to
+  // pinned memory, and the writer hashes them while a second thread writes
+  // the rank file.
+  void checkpoint_save(const std::string& dir) override {
+    const ckpt::Spec sp = ckpt::spec_of(cfg);
+    const size_t w = sizeof(FileT);
+    const int64_t np = int64_t(ckpt::padded_cells(sp));
+    size_t total = size_t(Q) * size_t(np) * w;
+    for (auto& sc : scalars) total += size_t(sc->q) * size_t(np) * w;
+    DevBuf<char> img;
+    img.alloc(total);
+    char* pin = ckpt_pin.ensure(total);
+    const unsigned g = unsigned(ceil_div(np, 256));
+    pack_padded_kernel<Q, S, FileT><<<g, 256, 0, st>>>(fp, plane, flags.p, nbr.p, nx, ny, nz, parity,
+                                                      reinterpret_cast<FileT*>(img.p), np);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, d.p, size_t(sc.q) * size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-  }
-  void checkpoint_gather(ckpt::State& s) override {
-    s.step = time;
-    s.f.resize(size_t(Q) * size_t(n));
-    stage_out(s.f.data());
-    s.moments.resize(size_t(4) * size_t(n));
-    read_moments(s.moments.data(), s.moments.data() + n, s.moments.data() + 2 * n, s.moments.data() + 3 * n);
-    s.has_force_field = field_present;
-    s.force_field.clear();
+    size_t off = size_t(Q) * size_t(np) * w;
+    std::vector<size_t> soff;
+    for (auto& scp : scalars) {
+      ScalarStateT<A>& sc = *scp;
+      FileT* out = reinterpret_cast<FileT*>(img.p + off);
+      if (sc.q == 7)
+        scalar_pack_padded_kernel<7, A, FileT><<<g, 256, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz,
+                                                                   sc.parity, out, np);
+      else
+        scalar_pack_padded_kernel<Q, A, FileT><<<g, 256, 0, st>>>(sc.h.p, sc.hplane, flags.p, nbr.p, nx, ny, nz,
+                                                                   sc.parity, out, np);
+      CK(cudaGetLastError());
+      soff.push_back(off);
+      off += size_t(sc.q) * size_t(np) * w;
+    }
+    CK(cudaMemcpyAsync(pin, img.p, total, cudaMemcpyDeviceToHost, st));
+    // moments (solid cells carried), force field, concentrations
+    std::vector<double> mom(size_t(4) * size_t(n));
+    read_moments(mom.data(), mom.data() + n, mom.data() + 2 * n, mom.data() + 3 * n);
+    std::vector<double> ff;
     if (field_present) {
-      s.force_field.resize(size_t(3) * size_t(n));
-      get_force_field(s.force_field.data());
+      ff.resize(size_t(3) * size_t(n));
+      get_force_field(ff.data());
     }
-    s.scalars.clear();
+    std::vector<std::vector<double>> conc(scalars.size());
     for (size_t k = 0; k < scalars.size(); ++k) {
-      ScalarStateT<A>& sc = *scalars[k];
-      ckpt::Scalar x;
-      x.name = sc.name;
-      x.diffusivity = sc.diffusivity;
-      x.q = sc.q;
-      x.h.resize(size_t(sc.q) * size_t(n));
-      scalar_populations(sc, x.h.data());
-      x.conc.resize(size_t(n));
-      get_scalar(int(k), x.conc.data());
-      s.scalars.push_back(std::move(x));
+      conc[k].resize(size_t(n));
+      get_scalar(int(k), conc[k].data());
     }
-    s.has_qoi = has_qoi;
-    s.qoi_json = qoi_json;
+    CK(cudaStreamSynchronize(st));
+    std::vector<std::string> keep;
+    keep.reserve(8 + 4 * scalars.size());
+    auto piece = [&](std::string b) {
+      keep.push_back(std::move(b));
+      return ckpt::Piece{keep.back().data(), keep.back().size()};
+    };
+    auto reals = [&](const std::vector<double>& v) {
+      std::string b;
+      ckpt::append_reals(b, v.data(), v.size(), sp.f64);
+      return piece(std::move(b));
+    };
+    std::vector<ckpt::SectionOut> secs;
+    secs.push_back({ckpt::SEC_F_PRIMARY, {ckpt::Piece{pin, uint64_t(Q) * uint64_t(np) * w}}});
+    secs.push_back({ckpt::SEC_STALE_STASH, {ckpt::Piece{nullptr, uint64_t(Q) * uint64_t(np) * w}}});
+    secs.push_back({ckpt::SEC_MOMENTS, {reals(mom)}});
+    secs.push_back({ckpt::SEC_SOLID, {piece(ckpt::solid_section(sp, solid_h.data()))}});
+    if (field_present) secs.push_back({ckpt::SEC_FORCE_FIELD, {reals(ff)}});
+    if (!scalars.empty()) {
+      ckpt::SectionOut sec{ckpt::SEC_SCALAR_FIELDS, {}};
+      std::string count;
+      const uint32_t cnt = uint32_t(scalars.size());
+      count.append(reinterpret_cast<const char*>(&cnt), 4);
+      sec.pieces.push_back(piece(std::move(count)));
+      for (size_t k = 0; k < scalars.size(); ++k) {
+        const ScalarStateT<A>& sc = *scalars[k];
+        const uint64_t hl = uint64_t(sc.q) * uint64_t(np);
+        sec.pieces.push_back(piece(ckpt::scalar_head(sc.name, sc.diffusivity, hl)));
+        sec.pieces.push_back(ckpt::Piece{pin + soff[k], hl * w});
+        for (const ckpt::Piece& p : ckpt::scalar_tail(sc.q, np, n, w))
+          sec.pieces.push_back(p.data ? piece(std::string(p.data, size_t(p.len))) : p);
+        sec.pieces.push_back(reals(conc[k]));
+      }
+      secs.push_back(std::move(sec));
+    }
+    if (has_qoi) secs.push_back({ckpt::SEC_QOI_ACCUMULATORS, {piece(qoi_json)}});
+    ckpt::write(dir, sp, time, secs, solid_h.data(), wall_u_in.empty() ? nullptr : wall_u_in.data(), has_qoi);
   }
-  void checkpoint_check(const ckpt::State& s) const override {
-    if (scalars.size() > s.scalars.size())
+
+  // Solver::restore (solver.rs:4739-5060): the rank file is read into pinned
+  // memory and hashed as it arrives; after every check the padded planes go
+  // to the device in one copy and are unpacked into the parity-0 layout.
+  void checkpoint_restore(const std::string& dir) override {
+    const ckpt::Spec sp = ckpt::spec_of(cfg);
+    const size_t w = sizeof(FileT);
+    const int64_t np = int64_t(ckpt::padded_cells(sp));
+    const ckpt::View v = ckpt::read(dir, sp, solid_h.data(), wall_u_in.empty() ? nullptr : wall_u_in.data(),
+                                    [&](size_t b) { return ckpt_pin.ensure(b); });
+    // the scalars of the file replace the solver's: checked before anything
+    // is installed
+    if (scalars.size() > v.scalars.size())
       throw ckpt::Failure("CKPT_SCENARIO_MISMATCH",
                           "solver has " + std::to_string(scalars.size()) + " scalar distributions, checkpoint has " +
-                              std::to_string(s.scalars.size()));
-    for (size_t k = 0; k < s.scalars.size(); ++k) {
-      const int q = s.scalars[k].q;
-      if (q != 7 && q != Q) throw ckpt::Failure("CKPT_GEOM_MISMATCH", "scalar lattice must be D3Q7 or the hydro lattice");
+                              std::to_string(v.scalars.size()));
+    for (size_t k = 0; k < v.scalars.size(); ++k) {
+      const int q = v.scalars[k].q;
       if (k < scalars.size() && scalars[k]->q != q)
         throw ckpt::Failure("CKPT_SCENARIO_MISMATCH", "scalar " + std::to_string(k) + " lattice differs: checkpoint D3Q" +
                                                           std::to_string(q) + ", solver D3Q" +
                                                           std::to_string(scalars[k]->q));
-      if (!(std::isfinite(s.scalars[k].diffusivity) && s.scalars[k].diffusivity > 0.0))
+      if (!(std::isfinite(v.scalars[k].diffusivity) && v.scalars[k].diffusivity > 0.0))
         throw ckpt::Failure("CKPT_PAYLOAD_CORRUPT", "scalar diffusivity must be finite > 0");
+      if (v.scalars[k].name.empty() || v.scalars[k].name.size() > 63)
+        throw ckpt::Failure("CKPT_PAYLOAD_CORRUPT", "scalar name must have 1 to 63 bytes");
     }
+    std::vector<double> mom(size_t(4) * size_t(n));
+    ckpt::reals_to_double(v.moments, mom.size(), sp.f64, mom.data());
+    std::vector<double> ff;
+    if (v.force_field) {
+      ff.resize(size_t(3) * size_t(n));
+      ckpt::reals_to_double(v.force_field, ff.size(), sp.f64, ff.data());
+    }
+    size_t total = size_t(Q) * size_t(np) * w;
+    for (const auto& x : v.scalars) total += size_t(x.q) * size_t(np) * w;
+    DevBuf<char> img;
+    img.alloc(total);
+    sync();
+    CK(cudaMemcpyAsync(img.p, v.f, size_t(Q) * size_t(np) * w, cudaMemcpyHostToDevice, st));
+    size_t off = size_t(Q) * size_t(np) * w;
+    std::vector<size_t> soff;
+    for (const auto& x : v.scalars) {
+      CK(cudaMemcpyAsync(img.p + off, x.h, size_t(x.q) * size_t(np) * w, cudaMemcpyHostToDevice, st));
+      soff.push_back(off);
+      off += size_t(x.q) * size_t(np) * w;
+    }
+    const unsigned g = unsigned(ceil_div(n, 256));
+    unpack_padded_kernel<Q, S, FileT><<<g, 256, 0, st>>>(fp, plane, reinterpret_cast<const FileT*>(img.p), nx, ny,
+                                                        nz, n);
+    CK(cudaGetLastError());
+    parity = 0;
+    install_force_field(v.force_field ? ff.data() : nullptr);
+    for (int64_t c = 0; c < n; ++c)
+      if (solid_h[c]) {
+        init_rho_h[c] = mom[size_t(c)];
+        for (int k = 0; k < 3; ++k) init_u_h[size_t(3 * c + k)] = mom[size_t((k + 1) * n + c)];
+      }
+    d_init_u_ok = false;
+    for (size_t k = 0; k < v.scalars.size(); ++k) {
+      const ckpt::ScalarView& x = v.scalars[k];
+      if (k >= scalars.size()) enable_scalar(x.q, x.diffusivity);
+      ScalarStateT<A>& sc = *scalars[k];
+      sc.diffusivity = x.diffusivity;
+      sc.name = x.name;
+      scalar_unpack_padded_kernel<A, FileT><<<g, 256, 0, st>>>(
+          sc.h.p, sc.hplane, reinterpret_cast<const FileT*>(img.p + soff[k]), sc.q, nx, ny, nz, n);
+      CK(cudaGetLastError());
+      sc.parity = 0;
+    }
+    CK(cudaStreamSynchronize(st));
+    time = v.step;
+    has_qoi = v.has_qoi;
+    qoi_json = v.qoi_json;
+    invalidate_graphs();
   }
+
   // Body-force field of a checkpoint: slots for the fluid cells with a
   // nonzero force, the values in both the applied field and the field inside
   // the cached moments (null: no field).
@@ -1923,37 +2048,6 @@ struct Engine final : EngineBase {
     fprev_stale = false;
     invalidate_graphs();
   }
-  void checkpoint_install(const ckpt::State& s) override {
-    checkpoint_check(s);
-    sync();
-    stage_in(s.f.data());
-    install_force_field(s.has_force_field ? s.force_field.data() : nullptr);
-    // carried solid-cell moments (moments are never updated on solids)
-    for (int64_t c = 0; c < n; ++c)
-      if (solid_h[c]) {
-        init_rho_h[c] = s.moments[size_t(c)];
-        for (int k = 0; k < 3; ++k) init_u_h[size_t(3 * c + k)] = s.moments[size_t((k + 1) * n + c)];
-      }
-    d_init_u_ok = false;
-    for (size_t k = 0; k < s.scalars.size(); ++k) {
-      const ckpt::Scalar& x = s.scalars[k];
-      if (k >= scalars.size()) enable_scalar(x.q, x.diffusivity);
-      ScalarStateT<A>& sc = *scalars[k];
-      sc.diffusivity = x.diffusivity;
-      sc.name = x.name;
-      DevBuf<double> d;
-      d.upload(x.h.data(), x.h.size(), st);
-      scalar_stage_in_kernel<A><<<unsigned(ceil_div(n, 128)), 128, 0, st>>>(sc.h.p, sc.hplane, d.p, sc.q, n);
-      CK(cudaGetLastError());
-      sc.parity = 0;
-      CK(cudaStreamSynchronize(st));
-    }
-    time = s.step;
-    has_qoi = s.has_qoi;
-    qoi_json = s.qoi_json;
-    invalidate_graphs();
-  }
-
   // Oxygen transfer / uptake on scalar k (the gather -> host source ->
   // set composition of the reference, on the device). a's arrays are host
   // pointers (n values each, or null); *sum = the source integral.

@@ -155,38 +155,54 @@ __global__ void scalar_gather_kernel(const A* hb, int64_t hpl, const uint8_t* fl
   out[cell] = double(scalar_conc<SQ, A>(hb, hpl, cell, x, y, z, nx, ny, nz, mask, sparity));
 }
 
-// Logical post-stream scalar populations -> f64 q-major (checkpoint gather),
-// the read of scalar_step_kernel; solid cells report their raw own slots.
-template <int SQ, class A>
-__global__ void scalar_stage_out_kernel(const A* hb, int64_t hpl, const uint8_t* flags, const uint32_t* nbr, int nx,
-                                        int ny, int nz, int sparity, double* out, int64_t n) {
+// Checkpoint image of a scalar's populations (the SCALAR_FIELDS h planes,
+// solver.rs:1200-1217): SQ planes over the halo-padded box, halo zero, the
+// logical post-stream values (the read of scalar_step_kernel) in the file's
+// type T; solid cells report their raw own slots. One thread per padded cell.
+template <int SQ, class A, class T>
+__global__ void scalar_pack_padded_kernel(const A* hb, int64_t hpl, const uint8_t* flags, const uint32_t* nbr, int nx,
+                                          int ny, int nz, int sparity, T* out, int64_t np) {
   using L = Lat<SQ>;
-  const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (cell >= n) return;
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int64_t px = nx + 2, pxy = px * (ny + 2);
+  const int zz = int(p / pxy);
+  const int64_t r = p - zz * pxy;
+  const int yy = int(r / px);
+  const int x = int(r - yy * px) - 1, y = yy - 1, z = zz - 1;
+  if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) {
+#pragma unroll
+    for (int q = 0; q < SQ; ++q) out[q * np + p] = T(0);
+    return;
+  }
+  const int64_t cell = (int64_t(z) * ny + y) * nx + x;
   const uint8_t fl = flags[cell];
   if (sparity == 0 || (fl & F_SOLID)) {
 #pragma unroll
-    for (int q = 0; q < SQ; ++q) out[q * n + cell] = double(hb[q * hpl + cell]);
+    for (int q = 0; q < SQ; ++q) out[q * np + p] = T(hb[q * hpl + cell]);
     return;
   }
-  int x, y, z;
-  cell_xyz(cell, nx, ny, x, y, z);
   const uint32_t mask = (fl & F_BOUNDARY) ? nbr[cell] : 0u;
   const Nbr nb(x, y, z, nx, ny, nz);
 #pragma unroll
   for (int q = 0; q < SQ; ++q) {
     const int o = opp(q);
     const A v = ((mask >> o) & 1u) ? hb[q * hpl + cell] : hb[o * hpl + nb.at(-L::cx(q), -L::cy(q), -L::cz(q))];
-    out[q * n + cell] = double(v);
+    out[q * np + p] = T(v);
   }
 }
 
-// f64 q-major scalar populations -> normal (parity 0) layout.
-template <class A>
-__global__ void scalar_stage_in_kernel(A* hb, int64_t hpl, const double* in, int sq, int64_t n) {
+// Checkpoint image of a scalar -> normal (parity 0) layout.
+template <class A, class T>
+__global__ void scalar_unpack_padded_kernel(A* hb, int64_t hpl, const T* img, int sq, int nx, int ny, int nz,
+                                            int64_t n) {
   const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (cell >= n) return;
-  for (int q = 0; q < sq; ++q) hb[q * hpl + cell] = A(in[q * n + cell]);
+  int x, y, z;
+  cell_xyz(cell, nx, ny, x, y, z);
+  const int64_t np = int64_t(nx + 2) * (ny + 2) * (nz + 2);
+  const int64_t p = (int64_t(z + 1) * (ny + 2) + (y + 1)) * (nx + 2) + (x + 1);
+  for (int q = 0; q < sq; ++q) hb[q * hpl + cell] = A(img[q * np + p]);
 }
 
 // h = h_eq(C, u) at every cell with u of the current hydro state (solids:

@@ -567,22 +567,6 @@ int lbmb_sync(lbmb_solver* h) {
 
 // ---- checkpoint/restart ------------------------------------------------------
 
-static lbmb::ckpt::Spec checkpoint_spec(const lbmb_config& c) {
-  lbmb::ckpt::Spec s;
-  s.q = c.lattice;
-  s.collision = c.collision;
-  s.f64 = c.storage == LBMB_STORE_F64;
-  for (int a = 0; a < 3; ++a) {
-    s.dims[a] = c.dims[a];
-    s.periodic[a] = c.periodic[a] != 0;
-    s.force[a] = c.force[a];
-  }
-  s.nu = c.nu;
-  s.magic = c.magic;
-  s.omega_shear = c.omega_shear;
-  return s;
-}
-
 int lbmb_get_time(const lbmb_solver* h, uint64_t* step) {
   return guarded([&] {
     if (!h || !h->e || !step) throw Error(LBMB_ERR_INVALID, "null argument");
@@ -631,11 +615,7 @@ int lbmb_checkpoint_save(lbmb_solver* h, const char* dir) {
   return guarded([&] {
     NEED(h);
     if (!dir) throw Error(LBMB_ERR_INVALID, "null argument");
-    lbmb::ckpt::State st;
-    h->e->checkpoint_gather(st);
-    const auto& wu = h->e->wall_u_in;
-    lbmb::ckpt::save(dir, checkpoint_spec(h->e->config()), h->e->solid().data(), wu.empty() ? nullptr : wu.data(),
-                     st);
+    h->e->checkpoint_save(dir);
   });
 }
 
@@ -643,10 +623,7 @@ int lbmb_checkpoint_restore(lbmb_solver* h, const char* dir) {
   return guarded([&] {
     NEED(h);
     if (!dir) throw Error(LBMB_ERR_INVALID, "null argument");
-    const auto& wu = h->e->wall_u_in;
-    const lbmb::ckpt::State st = lbmb::ckpt::load(dir, checkpoint_spec(h->e->config()), h->e->solid().data(),
-                                                  wu.empty() ? nullptr : wu.data());
-    h->e->checkpoint_install(st);
+    h->e->checkpoint_restore(dir);
   });
 }
 

@@ -251,3 +251,23 @@ def test_qoi_state_and_time_round_trip(tmp_path):
     assert h.time == 4 and h.qoi_checkpoint_state == '{"accumulators": []}'
     with pytest.raises(lb.SpecError):
         h.qoi_checkpoint_state = "[1, 2]"
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16"])
+def test_device_writer_equals_host_writer(tmp_path, prec):
+    """The device-packed checkpoint (padded planes packed on the device,
+    pinned copy, overlapped hash) is byte-identical to the host writer of
+    the same state gathered through the ABI, which the CPU tests pin to the
+    oracle's writer."""
+    dims, solid, body = small_tank()
+    om = 1.0 / 0.56
+    g = lb.Solver(dims, lattice=27, collision="cm", storage=prec, nu=0.02, omega_shear=om, solid=solid)
+    g.run_impeller(body, 5)
+    g.save(str(tmp_path / "d"))
+    spec = {"dims": dims, "lattice": 27, "collision": "cm", "nu": 0.02, "magic": lb.MAGIC_STD, "omega_shear": om,
+            "periodic": (False,) * 3, "force": (0.0, 0.0, 0.0), "dtype": "f64" if prec == "f64" else "f32"}
+    state = {"step": g.time, "f": g.stage_out(), "moments": np.stack(g.read_moments()),
+             "force_field": g.force_field(), "scalars": [], "qoi": None}
+    lb.checkpoint_write_host(str(tmp_path / "h"), spec, state, solid=solid)
+    for fn in ("manifest.json", ock.RANK_FILE):
+        assert (tmp_path / "d" / fn).read_bytes() == (tmp_path / "h" / fn).read_bytes(), fn
