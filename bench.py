@@ -239,13 +239,12 @@ def checkpoint_study(g):
     d = tempfile.mkdtemp(prefix="lbmb_ckpt_")
     try:
         g.sync()
-        t0 = time.perf_counter()
-        g.save(d)
-        save_ms = (time.perf_counter() - t0) * 1e3
+        save_ms = []
+        for _ in range(2):  # the first call also allocates the pinned staging buffer
+            t0 = time.perf_counter()
+            g.save(d)
+            save_ms.append((time.perf_counter() - t0) * 1e3)
         nbytes = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
-        t0 = time.perf_counter()
-        g.stage_out()
-        gather_ms = (time.perf_counter() - t0) * 1e3
         step0 = g.time
         g.run(2)
         a = g.read_moments()
@@ -260,9 +259,11 @@ def checkpoint_study(g):
         shutil.rmtree(d, ignore_errors=True)
     return {"what": "checkpoint save + restore of the final state (manifest.json + rank_0000_part_0000.bin, "
                     "reference v3 format: padded f32/f64 planes, zero stash, FNV-1a 64 payload hash)",
-            "bytes": nbytes, "save_ms": save_ms, "restore_ms": restore_ms,
-            "save_GBps": nbytes / save_ms / 1e6, "restore_GBps": nbytes / restore_ms / 1e6,
-            "state_gather_ms": gather_ms, "state_gather_note": "device -> host of the logical populations (f64)",
+            "bytes": nbytes, "save_ms": save_ms[1], "first_save_ms": save_ms[0], "restore_ms": restore_ms,
+            "save_GBps": nbytes / save_ms[1] / 1e6, "restore_GBps": nbytes / restore_ms / 1e6,
+            "path": "device packs the padded planes in the file type, one pinned copy each way; the host "
+                    "hashes (FNV-1a 64, byte-serial; all-zero 64-byte blocks as one multiply) while a second "
+                    "thread writes / reads the rank file",
             "step": step0, "restored_step": restored_step, "resume_bit_exact_2_steps": bool(exact),
             "directory": "tempfile.mkdtemp() on the bench host"}
 
