@@ -302,7 +302,7 @@ struct Engine final : EngineBase {
 
   ~Engine() override {
     if (step_graph) cudaGraphExecDestroy(step_graph);
-    if (apply_graph) cudaGraphExecDestroy(apply_graph);
+    for (auto& e : apply_cache) cudaGraphExecDestroy(e.exec);
     if (st) cudaStreamSynchronize(st);
     bodies.clear();
     scalars.clear();
@@ -374,10 +374,8 @@ struct Engine final : EngineBase {
       CK(cudaGraphExecDestroy(step_graph));
       step_graph = nullptr;
     }
-    if (apply_graph) {
-      CK(cudaGraphExecDestroy(apply_graph));
-      apply_graph = nullptr;
-    }
+    for (auto& e : apply_cache) CK(cudaGraphExecDestroy(e.exec));
+    apply_cache.clear();
   }
 
   // Grow the force-slot arrays, keeping content.
@@ -1734,8 +1732,15 @@ struct Engine final : EngineBase {
     int64_t parity, field_at_call, sweeps;
     double force[3];
   };
-  cudaGraphExec_t apply_graph = nullptr;
-  ApplyKey apply_key;
+  // Instantiated IBM graphs by key. A runner alternates between the two AA
+  // parities (and a caller may alternate bodies), so a single cached graph
+  // would be captured and instantiated again on every call.
+  struct ApplyEntry {
+    ApplyKey key;
+    cudaGraphExec_t exec;
+  };
+  std::vector<ApplyEntry> apply_cache;
+  static constexpr size_t APPLY_CACHE = 8;
 
   void ibm_apply(int b, const lbmb_ibm_config& c, lbmb_ibm_diag* out) override {
     BodyState& B = body_for(b, c);
@@ -1749,20 +1754,23 @@ struct Engine final : EngineBase {
     k.field_at_call = field_present ? 1 : 0;
     k.sweeps = c.max_iterations;
     for (int i = 0; i < 3; ++i) k.force[i] = cfg.force[i];
-    if (!apply_graph || std::memcmp(&k, &apply_key, sizeof(k)) != 0) {
-      if (apply_graph) {
-        CK(cudaGraphExecDestroy(apply_graph));
-        apply_graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    for (auto& e : apply_cache)
+      if (std::memcmp(&k, &e.key, sizeof(k)) == 0) exec = e.exec;
+    if (!exec) {
+      if (apply_cache.size() >= APPLY_CACHE) {
+        CK(cudaGraphExecDestroy(apply_cache.front().exec));
+        apply_cache.erase(apply_cache.begin());
       }
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       enqueue_ibm(B, c, nullptr, nullptr, nullptr, nullptr, field_present);
       CK(cudaStreamEndCapture(st, &g));
-      CK(cudaGraphInstantiate(&apply_graph, g, 0));
+      CK(cudaGraphInstantiate(&exec, g, 0));
       CK(cudaGraphDestroy(g));
-      apply_key = k;
+      apply_cache.push_back({k, exec});
     }
-    CK(cudaGraphLaunch(apply_graph, st));
+    CK(cudaGraphLaunch(exec, st));
     field_present = true;
     fprev_stale = true;
     IbmDiagDev d;
