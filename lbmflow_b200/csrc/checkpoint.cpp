@@ -18,11 +18,12 @@
 #include <map>
 #include <memory>
 #include <sstream>
-#include <atomic>
-#include <functional>
 #include <thread>
+#include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <sys/types.h>
+#include <unistd.h>
 
 #include "../../include/lbmb.h"
 
@@ -519,6 +520,10 @@ uint64_t mask_hash(const Spec& s, const uint8_t* solid, const double* wall_u) {
 
 uint64_t padded_cells(const Spec& s) { return uint64_t(Pad(s).np()); }
 
+Mapping::~Mapping() {
+  if (p) ::munmap(const_cast<char*>(p), n);
+}
+
 std::string solid_section(const Spec& s, const uint8_t* solid) {
   std::vector<uint8_t> ps;
   std::vector<double> pw;
@@ -714,8 +719,7 @@ std::vector<Piece> scalar_tail(int q, int64_t np, int64_t nc, uint64_t w) {
 }
 
 // read_rank_file + load_into (solver.rs:1108-1198, 4759-5060).
-View read(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u,
-          const std::function<char*(size_t)>& alloc) {
+View read(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u) {
   const Pad g(s);
   const int64_t nc = g.nc(), np = g.np();
   // load_into (solver.rs:4759-4824)
@@ -802,52 +806,41 @@ View read(const std::string& dir, const Spec& s, const uint8_t* solid, const dou
     fail("CKPT_MASK_MISMATCH", "mask_hash differed for rank=0 part=" + std::to_string(e.part) +
                                    ": checkpoint=" + e.mask_hash + " current=" + cur_mask);
 
-  // read_rank_file (solver.rs:1108-1198): the file is read on a second
-  // thread in blocks while this one hashes the payload behind it.
+  // read_rank_file (solver.rs:1108-1198): the file is mapped (no copy; a
+  // checkpoint just written is served from the page cache) and the payload
+  // hashed in place.
   if (e.file.find('/') != std::string::npos || e.file == ".." || e.file.empty())
     fail("CKPT_MANIFEST_INVALID", "rank file name must be a plain file name: " + e.file);
   const std::string path = join(dir, e.file);
-  struct stat sb;
-  if (::stat(path.c_str(), &sb) != 0) fail("CKPT_IO", "No such file or directory (os error 2): " + path);
-  const size_t fsize = size_t(sb.st_size);
-  std::FILE* fh = std::fopen(path.c_str(), "rb");
-  if (!fh) fail("CKPT_IO", "cannot open " + path);
-  char* buf = alloc(std::max<size_t>(fsize, 1));
-  std::atomic<size_t> avail{0};
-  std::atomic<bool> read_failed{false};
-  std::thread reader([&] {
-    constexpr size_t BLOCK = size_t(16) << 20;
-    size_t done = 0;
-    while (done < fsize) {
-      const size_t k = std::fread(buf + done, 1, std::min(BLOCK, fsize - done), fh);
-      if (k == 0) {
-        read_failed = true;
-        break;
+  auto map = std::make_shared<Mapping>();
+  {
+    const int fd = ::open(path.c_str(), O_RDONLY);
+    if (fd < 0) fail("CKPT_IO", "No such file or directory (os error 2): " + path);
+    struct stat sb;
+    if (::fstat(fd, &sb) != 0) {
+      ::close(fd);
+      fail("CKPT_IO", "cannot stat " + path);
+    }
+    map->n = size_t(sb.st_size);
+    if (map->n > 0) {
+      void* p = ::mmap(nullptr, map->n, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (p == MAP_FAILED) {
+        ::close(fd);
+        fail("CKPT_IO", "cannot map " + path);
       }
-      done += k;
-      avail.store(done, std::memory_order_release);
+      map->p = static_cast<const char*>(p);
+      ::madvise(p, map->n, MADV_SEQUENTIAL);
+      ::madvise(p, map->n, MADV_WILLNEED);
     }
-  });
-  struct Joiner {
-    std::thread& t;
-    std::FILE* f;
-    ~Joiner() {
-      if (t.joinable()) t.join();
-      std::fclose(f);
-    }
-  } joiner{reader, fh};
-  auto wait_for = [&](size_t upto) {
-    while (avail.load(std::memory_order_acquire) < upto) {
-      if (read_failed) fail("CKPT_IO", "read failed: " + path);
-      std::this_thread::yield();
-    }
-  };
+    ::close(fd);
+  }
+  const char* buf = map->p;
+  const size_t fsize = map->n;
   // header and section table
   size_t pos = 0;
   auto take = [&](size_t k) -> const char* {
-    if (fsize - pos < k || pos > fsize)
+    if (pos > fsize || fsize - pos < k)
       fail("CKPT_TRUNCATED", "rank file ended before the declared header/table/payload");
-    wait_for(pos + k);
     const char* p = buf + pos;
     pos += k;
     return p;
@@ -884,18 +877,7 @@ View read(const std::string& dir, const Spec& s, const uint8_t* solid, const dou
   const size_t pend = fsize - 8;
   const char* payload = buf + pos;
   const size_t plen = pend - pos;
-  uint64_t ph_calc = 0xcbf29ce484222325ull;
-  {
-    constexpr size_t STEP = size_t(4) << 20;
-    for (size_t at = pos; at < pend;) {
-      const size_t k = std::min(STEP, pend - at);
-      wait_for(at + k);
-      ph_calc = fnv1a64(buf + at, k, ph_calc);
-      at += k;
-    }
-  }
-  wait_for(fsize);
-  reader.join();
+  const uint64_t ph_calc = fnv1a64(payload, plen);
   uint64_t phash = 0;
   for (int i = 0; i < 8; ++i) phash |= uint64_t(static_cast<unsigned char>(buf[pend + size_t(i)])) << (8 * i);
   if (ph_calc != phash) fail("CKPT_PAYLOAD_CORRUPT", "rank file payload hash does not match its contents");
@@ -931,6 +913,7 @@ View read(const std::string& dir, const Spec& s, const uint8_t* solid, const dou
                                      std::to_string(expected) + " values of " + std::to_string(w) + " bytes");
   };
   View v;
+  v.hold = map;
   v.step = step;
   {
     const auto p = required(SEC_F_PRIMARY, "F_PRIMARY");
@@ -1011,11 +994,7 @@ View read(const std::string& dir, const Spec& s, const uint8_t* solid, const dou
 State load(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u) {
   const Pad g(s);
   const size_t nc = size_t(g.nc());
-  std::string storage;
-  const View v = read(dir, s, solid, wall_u, [&](size_t b) {
-    storage.resize(b);
-    return &storage[0];
-  });
+  const View v = read(dir, s, solid, wall_u);
   State st;
   st.step = v.step;
   st.f.resize(size_t(s.q) * nc);

@@ -22,7 +22,7 @@
 // carries state into the next step.
 #pragma once
 #include <cstdint>
-#include <functional>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -99,8 +99,19 @@ struct ScalarView {
   const char* h = nullptr;
   const char* conc = nullptr;
 };
-// A validated checkpoint in memory: pointers into the rank file image.
+// A read-only mapping of a rank file.
+struct Mapping {
+  const char* p = nullptr;
+  size_t n = 0;
+  Mapping() = default;
+  Mapping(const Mapping&) = delete;
+  Mapping& operator=(const Mapping&) = delete;
+  ~Mapping();
+};
+// A validated checkpoint in memory: pointers into the mapped rank file,
+// which `hold` keeps mapped.
 struct View {
+  std::shared_ptr<const Mapping> hold;
   uint64_t step = 0;
   const char* f = nullptr;            // Q padded planes, file dtype
   const char* moments = nullptr;      // 4 x n, file dtype
@@ -127,11 +138,9 @@ std::vector<Piece> scalar_tail(int q, int64_t np, int64_t nc, uint64_t w);
 void write(const std::string& dir, const Spec& s, uint64_t step, const std::vector<SectionOut>& secs,
            const uint8_t* solid, const double* wall_u, bool stats);
 
-// Every check of the reference's restore, in its order and with its codes;
-// the rank file image lands in memory from alloc(bytes) and is hashed while
-// it is read.
-View read(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u,
-          const std::function<char*(size_t)>& alloc);
+// Every check of the reference's restore, in its order and with its codes,
+// on the mapped rank file.
+View read(const std::string& dir, const Spec& s, const uint8_t* solid, const double* wall_u);
 
 // Whether the text is one JSON object (the QOI accumulator section).
 bool json_object(const std::string& text);

@@ -778,7 +778,18 @@ struct Engine final : EngineBase {
   // One full step on the stream: hydro, the cached-moment field refresh,
   // then the scalars (which read the moments of the new state).
   void enqueue_step() {
-    launch_hydro(parity);
+    if (nslots > 0 && !has_uniform_force()) {
+      // forced cells on the side stream beside the full-grid sweep of the
+      // others (disjoint AA slots), as in the runner step
+      CK(cudaEventRecord(ev_fork, st));
+      CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+      launch_hydro(parity, st2, false, true);
+      launch_hydro(parity, st, true, false);
+      CK(cudaEventRecord(ev_join, st2));
+      CK(cudaStreamWaitEvent(st, ev_join, 0));
+    } else {
+      launch_hydro(parity);
+    }
     parity ^= 1;
     if (fprev_stale) {
       CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
@@ -1954,15 +1965,14 @@ struct Engine final : EngineBase {
     ckpt::write(dir, sp, time, secs, solid_h.data(), wall_u_in.empty() ? nullptr : wall_u_in.data(), has_qoi);
   }
 
-  // Solver::restore (solver.rs:4739-5060): the rank file is read into pinned
-  // memory and hashed as it arrives; after every check the padded planes go
-  // to the device in one copy and are unpacked into the parity-0 layout.
+  // Solver::restore (solver.rs:4739-5060): the rank file is mapped and
+  // hashed in place; after every check the padded planes go to the device in
+  // one copy each and are unpacked into the parity-0 layout.
   void checkpoint_restore(const std::string& dir) override {
     const ckpt::Spec sp = ckpt::spec_of(cfg);
     const size_t w = sizeof(FileT);
     const int64_t np = int64_t(ckpt::padded_cells(sp));
-    const ckpt::View v = ckpt::read(dir, sp, solid_h.data(), wall_u_in.empty() ? nullptr : wall_u_in.data(),
-                                    [&](size_t b) { return ckpt_pin.ensure(b); });
+    const ckpt::View v = ckpt::read(dir, sp, solid_h.data(), wall_u_in.empty() ? nullptr : wall_u_in.data());
     // the scalars of the file replace the solver's: checked before anything
     // is installed
     if (scalars.size() > v.scalars.size())
