@@ -613,19 +613,19 @@ void write(const std::string& dir, const Spec& s, uint64_t step, const std::vect
   if (!fh) fail("CKPT_IO", "cannot create " + path);
   bool write_ok = true;
   std::thread writer([&] {
-    static const std::vector<char> zeros(size_t(1) << 20, 0);
+    static const std::vector<char> zeros(size_t(1) << 20, 0);  // zero runs shorter than 1 MB
     write_ok = std::fwrite(head.data(), 1, head.size(), fh) == head.size();
     for (const SectionOut& e : secs)
       for (const Piece& p : e.pieces) {
         if (!write_ok) return;
         if (p.data) {
           write_ok = std::fwrite(p.data, 1, size_t(p.len), fh) == size_t(p.len);
+        } else if (p.len >= (uint64_t(1) << 20)) {
+          // a long zero run is left as a hole (it reads back as zeros); the
+          // trailer written after it sets the file's length
+          write_ok = ::fseeko(fh, off_t(p.len), SEEK_CUR) == 0;
         } else {
-          for (uint64_t left = p.len; left && write_ok;) {
-            const size_t k = size_t(std::min<uint64_t>(left, zeros.size()));
-            write_ok = std::fwrite(zeros.data(), 1, k, fh) == k;
-            left -= k;
-          }
+          write_ok = std::fwrite(zeros.data(), 1, size_t(p.len), fh) == size_t(p.len);
         }
       }
   });
