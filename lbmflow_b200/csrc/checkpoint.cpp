@@ -208,7 +208,14 @@ struct JParser {
         case 't': out.push_back('\t'); break;
         case 'u': {
           if (i + 4 > s.size()) bad("short unicode escape");
-          const unsigned cp = unsigned(std::stoul(s.substr(i, 4), nullptr, 16));
+          unsigned cp = 0;
+          for (int k = 0; k < 4; ++k) {
+            const char h = s[i + size_t(k)];
+            const int d = h >= '0' && h <= '9' ? h - '0' : h >= 'a' && h <= 'f' ? h - 'a' + 10
+                          : h >= 'A' && h <= 'F' ? h - 'A' + 10 : -1;
+            if (d < 0) bad("bad unicode escape");
+            cp = cp * 16 + unsigned(d);
+          }
           i += 4;
           if (cp < 0x80) {
             out.push_back(char(cp));
