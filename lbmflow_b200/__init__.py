@@ -880,16 +880,17 @@ def checkpoint_write_host(directory, spec, state, solid=None, wall_u=None):
                                             None if s is None else s.ctypes.data_as(_u8p), _d(w), C.byref(data)))
 
 
-def checkpoint_read_host(directory, spec, solid=None, wall_u=None, max_scalars=8, max_qoi_bytes=1 << 20):
+def checkpoint_read_host(directory, spec, solid=None, wall_u=None, max_scalars=2, max_qoi_bytes=1 << 20):
     """Read and validate a checkpoint against spec and masks; returns the
-    state dict of checkpoint_write_host. CheckpointError on any mismatch."""
+    state dict of checkpoint_write_host. CheckpointError on any mismatch
+    (including more scalar distributions than max_scalars)."""
     cs, dims = _ckpt_spec(spec)
     n = dims[0] * dims[1] * dims[2]
     q = cs.lattice
     f = np.zeros(q * n)
     mo = np.zeros(4 * n)
     ff = np.zeros(3 * n)
-    hs = [np.zeros(27 * n) for _ in range(max_scalars)]
+    hs = [np.zeros(max(q, 7) * n) for _ in range(max_scalars)]
     cs_ = [np.zeros(n) for _ in range(max_scalars)]
     arr = (_CkptScalar * max_scalars)()
     for i in range(max_scalars):

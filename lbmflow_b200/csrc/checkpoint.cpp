@@ -619,6 +619,12 @@ void write(const std::string& dir, const Spec& s, uint64_t step, const std::vect
   std::FILE* fh = std::fopen(path.c_str(), "wb");
   if (!fh) fail("CKPT_IO", "cannot create " + path);
   bool write_ok = true;
+  struct Closer {  // closes the file if anything below throws
+    std::FILE*& f;
+    ~Closer() {
+      if (f) std::fclose(f);
+    }
+  } closer{fh};
   std::thread writer([&] {
     static const std::vector<char> zeros(size_t(1) << 20, 0);  // zero runs shorter than 1 MB
     write_ok = std::fwrite(head.data(), 1, head.size(), fh) == head.size();
@@ -644,6 +650,7 @@ void write(const std::string& dir, const Spec& s, uint64_t step, const std::vect
   put(trailer, ph, 8);
   if (write_ok) write_ok = std::fwrite(trailer.data(), 1, 8, fh) == 8;
   if (std::fclose(fh) != 0) write_ok = false;
+  fh = nullptr;
   if (!write_ok) fail("CKPT_IO", "write failed: " + path);
   write_file(join(dir, "manifest.json"), manifest_text(s, step, total, ph, mask_hash(s, solid, wall_u), stats));
 }
