@@ -1704,21 +1704,22 @@ struct Engine final : EngineBase {
     IbmArgs a = ibm_args(B, c);
     const unsigned gs = unsigned(std::max<int64_t>(1, ceil_div(B.ns, IBM_BLOCK)));
     const unsigned gm = unsigned(std::max<int64_t>(1, ceil_div(B.nm, IBM_BLOCK)));
-    ibm_prep_kernel<Q, S><<<gs, IBM_BLOCK, 0, sx>>>(a, fp, plane, slot_cell.p, flags.p, nbr.p, nx, ny, nz,
-                                                    parity, fcur.p, field_at_call ? 1 : 0,
-                                                    double(A(cfg.force[0])), double(A(cfg.force[1])),
-                                                    double(A(cfg.force[2])));
-    CK(cudaGetLastError());
+    const uint8_t* fl = flags.p;
+    const uint32_t* nb = nbr.p;
+    const Vec4<A>* fc = fcur.p;
+    launch_pdl(ibm_prep_kernel<Q, S>, gs, sx, a, static_cast<const S*>(fp), plane,
+               static_cast<const int64_t*>(slot_cell.p), fl, nb, nx, ny, nz, parity, fc, field_at_call ? 1 : 0,
+               double(A(cfg.force[0])), double(A(cfg.force[1])), double(A(cfg.force[2])));
     for (int s = 0; s < c.max_iterations; ++s) {
       if (sv && nslots)
         CK(cudaMemcpyAsync(sv->du + size_t(s) * sv->ns3 * 3, s_du.p, size_t(nslots) * 3 * sizeof(double),
                            cudaMemcpyDeviceToDevice, sx));
-      ibm_interp_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s);
+      launch_pdl(ibm_interp_kernel, gm, sx, a, s);
       if (sv && B.nm)
         CK(cudaMemcpyAsync(sv->imp + size_t(s) * sv->nm * 3, B.imp.p, size_t(B.nm) * 3 * sizeof(double),
                            cudaMemcpyDeviceToDevice, sx));
-      ibm_spread_kernel<<<gs, IBM_BLOCK, 0, sx>>>(a);
-      ibm_diag_kernel<<<gm, IBM_BLOCK, 0, sx>>>(a, s, int(gs));
+      launch_pdl(ibm_spread_kernel, gs, sx, a);
+      launch_pdl(ibm_diag_kernel, gm, sx, a, s, int(gs));
     }
     if (sv) {
       if (nslots) {
@@ -1728,8 +1729,24 @@ struct Engine final : EngineBase {
       if (B.nm) CK(cudaMemcpyAsync(sv->mob, B.mob.p, size_t(B.nm) * sizeof(double), cudaMemcpyDeviceToDevice, sx));
     }
     CK(cudaGetLastError());
-    ibm_commit_kernel<A><<<gs, IBM_BLOCK, 0, sx>>>(a, fcur.p, s_torque, s_ff, s_it, counter);
-    CK(cudaGetLastError());
+    launch_pdl(ibm_commit_kernel<A>, gs, sx, a, fcur.p, s_torque, s_ff, s_it, counter);
+  }
+
+  // One IBM-chain kernel of IBM_BLOCK threads with programmatic stream
+  // serialization (the kernel waits for its predecessor with pdl_wait).
+  template <class... KArgs, class... Args>
+  void launch_pdl(void (*kernel)(KArgs...), unsigned grid, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(IBM_BLOCK);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&lc, kernel, static_cast<KArgs>(args)...));
   }
 
   // The IBM launch sequence of apply_rotating_ibm, captured once and

@@ -25,6 +25,12 @@ namespace lbmb {
 
 constexpr int IBM_BLOCK = 128;
 
+// The chain's kernels are launched with programmatic stream serialization:
+// a kernel may be scheduled while its predecessor finishes, and waits here,
+// before touching any memory, until the predecessor grid has completed and
+// its writes are visible.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 struct IbmDiagDev {
   double slip_max, slip_rms, slip_max_rel, slip_rms_rel;
   double torque[3], fluid_force[3], marker_force[3];
@@ -166,6 +172,7 @@ __global__ void ibm_prep_kernel(IbmArgs a, const S* fb, int64_t pl, const int64_
                                 const uint8_t* flags, const uint32_t* nbr, int nx, int ny, int nz,
                                 int parity, const Vec4<typename Codec<S>::A>* fcur, int field_present,
                                 double gx, double gy, double gz) {
+  pdl_wait();
   ibm_prep_body<Q, S>(a, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, fb, pl, slot_cell, flags, nbr, nx, ny, nz,
                       parity, fcur, field_present, gx, gy, gz);
 }
@@ -215,6 +222,7 @@ __device__ __forceinline__ void ibm_interp_body(const IbmArgs& a, int64_t m, int
 }
 
 static __global__ void ibm_interp_kernel(IbmArgs a, int sweep) {
+  pdl_wait();
   ibm_interp_body(a, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, sweep);
 }
 
@@ -271,7 +279,10 @@ __device__ __forceinline__ void ibm_spread_body(const IbmArgs& a, int64_t bid) {
     for (int c = 0; c < 3; ++c) a.part_spread[3 * bid + c] = ff[c];
 }
 
-static __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) { ibm_spread_body(a, blockIdx.x); }
+static __global__ void __launch_bounds__(IBM_BLOCK) ibm_spread_kernel(IbmArgs a) {
+  pdl_wait();
+  ibm_spread_body(a, blockIdx.x);
+}
 
 // Slip statistics and the sweep's global reduction (solver.rs:3211-3253).
 // bid / nblk: block index and block count of this body's diag grid.
@@ -370,6 +381,7 @@ __device__ __forceinline__ void ibm_diag_body(const IbmArgs& a, int sweep, int n
 }
 
 static __global__ void __launch_bounds__(IBM_BLOCK) ibm_diag_kernel(IbmArgs a, int sweep, int nblk_spread) {
+  pdl_wait();
   ibm_diag_body(a, sweep, nblk_spread, blockIdx.x, gridDim.x);
 }
 
@@ -399,6 +411,7 @@ __device__ __forceinline__ void ibm_commit_body(const IbmArgs& a, int64_t i, Vec
 template <class A>
 __global__ void ibm_commit_kernel(IbmArgs a, Vec4<A>* fcur, double* series_torque, double* series_ff,
                                   int32_t* series_iters, int64_t* step_counter) {
+  pdl_wait();
   ibm_commit_body<A>(a, int64_t(blockIdx.x) * blockDim.x + threadIdx.x, fcur, series_torque, series_ff,
                      series_iters, step_counter);
 }
