@@ -785,6 +785,12 @@ struct Engine final : EngineBase {
       CK(cudaStreamWaitEvent(st2, ev_fork, 0));
       launch_hydro(parity, st2, false, true);
       launch_hydro(parity, st, true, false);
+      // the cached-moment field refresh follows the forced cells on the side
+      // stream (the full-grid sweep reads neither field)
+      if (fprev_stale) {
+        CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st2));
+        fprev_stale = false;
+      }
       CK(cudaEventRecord(ev_join, st2));
       CK(cudaStreamWaitEvent(st, ev_join, 0));
     } else {
@@ -2196,13 +2202,13 @@ struct Engine final : EngineBase {
       fprev_stale = true;
       launch_hydro(parity, st2, false, true);
       launch_hydro(parity, st, true, false);
+      // cached-moment field refresh on the side stream behind the forced
+      // cells, hidden by the full-grid sweep
+      if (nslots) CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st2));
+      fprev_stale = false;
       CK(cudaEventRecord(ev_join, st2));
       CK(cudaStreamWaitEvent(st, ev_join, 0));
       parity ^= 1;
-      if (fprev_stale) {
-        CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st));
-        fprev_stale = false;
-      }
       for (auto& sc : scalars) scalar_step(*sc);
       ++launches;
       if (k >= 0 && ((step_index + 1) % probe_every == 0 || step_index + 1 == steps))
