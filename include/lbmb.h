@@ -343,10 +343,35 @@ int lbmb_scalar_cv(lbmb_solver* h, int32_t k, double* cv);
  * torque_lu = -diag.torque[2] (runner.rs:1396-1425), the fluid force
  * (steps x 3) and the IBM iteration count; and, if scalar >= 0, the scalar
  * CV every probe_every steps (NaN elsewhere). Any output may be NULL.
- * The loop is captured in CUDA graphs; nothing syncs to the host inside. */
+ * As the reference runner (runner.rs:1125-1128), the f64 total mass is
+ * checked after every 1000th step of the call; a non-finite value stops the
+ * run there (status "diverged"): the call returns LBMB_ERR_DIVERGED, the
+ * outputs hold the executed steps (NaN, iterations 0, after them) and
+ * lbmb_run_impeller_status reports the executed step count. Between checks
+ * the loop replays a CUDA graph of 16 steps, captured on the first call and
+ * kept by the handle (with its series buffers) while the body, the IBM
+ * configuration, the sweep kernel and the scalar set are unchanged; the
+ * device time of lbmb_last_timing covers the steps only. */
 int lbmb_run_impeller(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg, int64_t steps,
                       int32_t scalar, int64_t probe_every, double* torque_lu, double* fluid_force,
                       double* cv, int32_t* ibm_iterations);
+
+/* Outcome of the last lbmb_run_impeller call on this handle (the runner's
+ * `executed` and `status`, runner.rs:1077-1129): *executed = steps taken,
+ * *diverged = 1 when the run stopped on a non-finite total mass. Either
+ * pointer may be NULL. */
+int lbmb_run_impeller_status(lbmb_solver* h, int64_t* executed, int32_t* diverged);
+
+/* No counterpart in the reference (failure detection of the device path).
+ * Bound on every mbarrier wait of the bulk-copy sweep kernels
+ * (LBMB_SWEEP_BULK, LBMB_SWEEP_STAGED), in SM clock cycles; 0 restores the
+ * default (2^31, about a second). A wait that runs out sets a device error
+ * flag, waits (bounded) for the kernel's own copies and returns; the call
+ * that launched the step then fails with LBMB_ERR_CUDA ("device wait timed
+ * out") and the context stays usable. A negative value is a self-test: the
+ * next such sweep waits -cycles on a barrier nothing arrives at, reports the
+ * timeout and leaves the populations untouched. */
+int lbmb_set_wait_limit(lbmb_solver* h, int64_t cycles);
 
 /* Device time of the last lbmb_step / lbmb_run_impeller call in ms (CUDA
  * events on the solver stream), and the hydro kernel's share of it. */
@@ -382,10 +407,11 @@ int lbmb_build_stirred_tank(const lbmb_tank_spec* spec, uint8_t* solid, uint8_t*
  *   force:  host, uniform body force for the F/2 momentum term, or NULL.
  *   out:    host, {fluid cells, sum f_dev, momentum x, y, z}.
  *   stream: cudaStream_t to run on (NULL: the legacy default stream).
- * ncells above 33,554,432 (2^25) is rejected with LBMB_ERR_INVALID. The
- * first call on a device looks up the array's device address (make it
- * before any stream capture). Calls share the array: calls that overlap on
- * the GPU race and must be serialized by the caller. */
+ * ncells above 33,554,432 (2^25) is rejected with LBMB_ERR_INVALID. Each
+ * call looks up the array's address in the current device context (a
+ * lookup, not an allocation); the first call on a device loads the array's
+ * module, so make it before any stream capture. Calls share the array:
+ * calls that overlap on the GPU race and must be serialized by the caller. */
 int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, int64_t ncells, int64_t plane,
                                     const uint8_t* solid, const double force[3], double out[5], void* stream);
 
@@ -407,7 +433,13 @@ int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, i
  *   LBMB_SWEEP_WINDOW  one cell per thread, tiles of 256 cells staged in
  *                      shared memory by 16-byte cp.async windows several
  *                      tiles ahead (TRT/BGK or central moment, fp32/fp16/
- *                      bf16 storage, no uniform body force).
+ *                      bf16 storage, no uniform body force);
+ *   LBMB_SWEEP_STAGED  two x-adjacent cells per thread with the packed fp32x2
+ *                      collision, fed from a shared-memory ring of 448-cell
+ *                      tiles that one producer warp fills with bulk copies
+ *                      (mbarrier completion, bounded waits) (TRT/BGK,
+ *                      fp32/fp16/bf16 storage, even nx, no uniform body force,
+ *                      no relaxation field).
  * A kind that cannot run the solver's configuration returns
  * LBMB_ERR_UNSUPPORTED and leaves the current kind in place. */
 typedef enum {
@@ -417,7 +449,8 @@ typedef enum {
   LBMB_SWEEP_PAIR = 3,
   LBMB_SWEEP_TILE = 4,
   LBMB_SWEEP_LEAN = 5,
-  LBMB_SWEEP_WINDOW = 6
+  LBMB_SWEEP_WINDOW = 6,
+  LBMB_SWEEP_STAGED = 7
 } lbmb_sweep_kind;
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
@@ -432,7 +465,9 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
  * step, where the IBM kernels run concurrently on a side stream. Window
  * kernel: resident 256-thread blocks per SM per parity, 2 (128 registers),
  * 3 (80) or 4 (64), with a tile ring of 3 where shared memory allows, else
- * 2; default 2 for the central moment, 3 for TRT/BGK. */
+ * 2; default 2 for the central moment, 3 for TRT/BGK. Staged kernel:
+ * resident 256-thread blocks per SM per parity, 1 (up to 255 registers),
+ * 2 (128, the default) or 3 (80). */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind
@@ -600,6 +635,128 @@ int lbmb_checkpoint_read_host(const char* dir, const lbmb_checkpoint_spec* spec,
 /* FNV-1a 64 of a byte buffer (the checkpoint payload hash, solver.rs:
  * 831-835). */
 uint64_t lbmb_fnv1a64(const void* data, uint64_t len);
+
+
+/* ---- Runner QOIs, unit report, scalar pulse, capabilities -------------- */
+
+/* qoi::PowerQoiResult (crates/lbm-core/src/qoi.rs:455-468), nq omitted
+ * (the reference runner skips it: no discharge surface). */
+typedef struct {
+  double torque_n_m;
+  double power_w;
+  double rotational_speed_hz;
+  double np;            /* P / (rho N^3 D^5) */
+  double p_over_v_w_m3; /* P / V */
+} lbmb_power_result;
+
+/* qoi::power_qois (crates/lbm-core/src/qoi.rs:477-505): P = omega Tq,
+ * N = omega / 2 pi. LBMB_ERR_INVALID for non-finite or non-positive
+ * dimensional inputs, or N <= 0 (the reference's Err). */
+int lbmb_power_qois(double torque_n_m, double omega_rad_s, double rho_kg_m3, double impeller_diameter_m,
+                    double working_volume_m3, lbmb_power_result* out);
+
+/* torque_record_from_ibm + write_power_qois (crates/lbm-cli/src/runner.rs:
+ * 1396-1425, 1514-1543) over the per-step lattice torque series that
+ * lbmb_run_impeller writes (entry s - 1 = step s): the runner records steps
+ * with s % probe_every == 0 or s == run_steps, converts each to N m with
+ * rho dx^5 / dt^2, averages the records with s >= run_steps / 2 (all
+ * records when none is that late) and applies power_qois with the
+ * impeller's SI angular speed. executed = steps the run took (a diverged
+ * run stops early); *records_used (may be NULL) = records averaged. */
+int lbmb_power_from_torque_series(const double* torque_lu, int64_t executed, int64_t run_steps, int64_t probe_every,
+                                  double rho_kg_m3, double dx_m, double dt_s, double omega_rad_s,
+                                  double impeller_diameter_m, double working_volume_m3, lbmb_power_result* out,
+                                  int64_t* records_used);
+
+/* Inputs of bioprocess_unit_report for a single-phase stirred tank
+ * (crates/lbm-scenario/src/units.rs:116-208). */
+typedef struct {
+  double vessel_diameter_m;
+  double liquid_height_m;
+  double impeller_diameter_m;
+  double rotational_speed_rpm;
+  double liquid_density_kg_m3;
+  double liquid_viscosity_pa_s;
+  double dt_s;
+  int32_t grid[3];
+  double scalar_diffusivity_m2_s; /* passive scalar diffusivity; <= 0: no scalar model */
+} lbmb_unit_input;
+
+/* Feasibility codes of the unit report (units.rs:8-31, 210-305), as bits. */
+enum lbmb_unit_issue {
+  LBMB_UNIT_MA_LATTICE_HIGH = 1,            /* warning: Ma > 0.10 */
+  LBMB_UNIT_MA_LATTICE_TOO_HIGH = 2,        /* rejection: Ma > 0.30 */
+  LBMB_UNIT_TAU_NEAR_HALF = 4,              /* warning: 0.5 < tau <= 0.55 */
+  LBMB_UNIT_TAU_NON_POSITIVE_VISCOSITY = 8, /* rejection: tau <= 0.5 */
+  LBMB_UNIT_GRID_REYNOLDS_HIGH = 16,        /* warning: u_lu / nu_lu > 15 */
+  LBMB_UNIT_SCALAR_DIFFUSION_UNSTABLE = 32  /* warning: nu_lu / D_lu > 25 */
+};
+
+/* UnitReport's lattice mapping and single-phase groups (units.rs:33-95). */
+typedef struct {
+  double dx_m;    /* vessel diameter / nx */
+  double dt_s;
+  double u_ref_lu; /* N D dt / dx */
+  double nu_lu;    /* (mu / rho) dt / dx^2 */
+  double tau_lu;   /* 3 nu_lu + 1/2 */
+  double cs2_lu;   /* 1/3 */
+  double reynolds; /* rho N D^2 / mu */
+  double froude;   /* N^2 D / g */
+  double mach_lattice;
+  double schmidt;  /* NaN without a scalar */
+  double peclet;   /* u_ref T / D; NaN without a scalar */
+  double scalar_diffusivity_lu; /* D dt / dx^2; NaN without a scalar */
+  double grid_reynolds;         /* u_ref_lu / nu_lu */
+  uint32_t warnings;            /* lbmb_unit_issue bits */
+  uint32_t rejections;          /* lbmb_unit_issue bits */
+} lbmb_unit_mapping;
+
+/* bioprocess_unit_report (units.rs:96-325), single-phase subset: fills
+ * *out; LBMB_ERR_INVALID for a non-positive input (require_positive),
+ * LBMB_ERR_UNSUPPORTED with *out filled when a rejection fired (the
+ * checked report's OutOfValidityRange). */
+int lbmb_unit_report(const lbmb_unit_input* in, lbmb_unit_mapping* out);
+
+/* scalar_initial_condition, pulse branch (crates/lbm-cli/src/runner.rs:
+ * 1317-1377): values[cell] = concentration on fluid cells whose centre
+ * ((x + 0.5) dx, ...) lies within radius_m of center_m, else 0 (solid may
+ * be NULL: no solids). */
+int lbmb_scalar_top_hat_pulse(const int32_t dims[3], const uint8_t* solid, double dx_m, const double center_m[3],
+                              double radius_m, double concentration, double* values);
+
+/* The pulse's lattice diffusivity D dt / dx^2 (runner.rs:1371-1375), the
+ * value lbmb_enable_scalar takes. */
+int lbmb_scalar_diffusivity_lu(double diffusivity_m2_s, double dt_s, double dx_m, double* d_lu);
+
+/* Reasons a distribution family is unsupported (UnsupportedReason,
+ * crates/lbm-core/src/solver.rs:174). */
+enum lbmb_unsupported_reason { LBMB_SUPPORTED = 0, LBMB_UNSUPPORTED_NOT_IMPLEMENTED = 1 };
+
+/* The Backend trait's capability hooks (crates/lbm-core/src/backend.rs:
+ * 162-199, 343-345) for this device backend, plus what the handle's
+ * configuration enables here. */
+typedef struct {
+  int32_t handles_single_part_periodic_halo; /* 1: periodic axes wrap inside the sweep */
+  int32_t supports_localized_features;       /* 0: no volume sources or masked face patches */
+  int32_t supports_d3q27_open_faces;         /* 0: no open faces */
+  int32_t supports_two_pass;                 /* 0: the collide-stream is one fused sweep */
+  int32_t supports_gravity_body_force;       /* 0: uniform and IBM force fields only */
+  int32_t distribution_hydro;                /* lbmb_unsupported_reason */
+  int32_t distribution_phase;
+  int32_t distribution_scalar;
+  int64_t run_chunk_size;                    /* steps one call takes without a host sync (INT64_MAX: any) */
+  uint32_t lattices;                         /* bit 0: D3Q19, bit 1: D3Q27, bit 2: D3Q7 scalars */
+  uint32_t storages;                         /* bit k: lbmb_storage k */
+  uint32_t collisions;                       /* bit k: lbmb_collision k */
+  int32_t adjoint;                           /* the handle's configuration allows lbmb_adjoint_torque */
+  int32_t batch;                             /* ... lbmb_batch_create */
+  int32_t checkpoint;                        /* ... lbmb_checkpoint_save / restore */
+} lbmb_backend_caps;
+
+/* Capability query (Backend::distribution_support and supports_* hooks,
+ * backend.rs:162-199). h may be NULL: the backend's general answers, with
+ * adjoint / batch / checkpoint reporting what some configuration allows. */
+int lbmb_capabilities(lbmb_solver* h, lbmb_backend_caps* out);
 
 #ifdef __cplusplus
 }

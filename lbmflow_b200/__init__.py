@@ -26,7 +26,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, ERR_NOMEM =
 ERR_CHECKPOINT = -7
 COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
-SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5, "window": 6}
+SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5, "window": 6, "staged": 7}
 IMPELLER = {"rushton": 0, "pitched": 1, "flat_blade": 2}
 MAGIC_STD = 3.0 / 16.0
 RED_FLUID_CELLS, RED_MASS_DEV, RED_MOMENTUM = 0, 1, 2
@@ -47,6 +47,8 @@ EXPORTS = (
     "lbmb_gather_velocity_gradient", "lbmb_wale_update", "lbmb_get_time", "lbmb_set_scalar_name",
     "lbmb_set_qoi_checkpoint_state", "lbmb_get_qoi_checkpoint_state", "lbmb_checkpoint_save",
     "lbmb_checkpoint_restore", "lbmb_checkpoint_write_host", "lbmb_checkpoint_read_host", "lbmb_fnv1a64",
+    "lbmb_run_impeller_status", "lbmb_power_qois", "lbmb_power_from_torque_series", "lbmb_unit_report",
+    "lbmb_scalar_top_hat_pulse", "lbmb_scalar_diffusivity_lu", "lbmb_capabilities", "lbmb_set_wait_limit",
 )
 
 
@@ -197,6 +199,42 @@ class _TankSpec(C.Structure):
                 ("marker_spacing_cells", C.c_double), ("min_cells", C.c_double)]
 
 
+class _PowerResult(C.Structure):
+    _fields_ = [("torque_n_m", C.c_double), ("power_w", C.c_double), ("rotational_speed_hz", C.c_double),
+                ("np", C.c_double), ("p_over_v_w_m3", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class _UnitInput(C.Structure):
+    _fields_ = [("vessel_diameter_m", C.c_double), ("liquid_height_m", C.c_double),
+                ("impeller_diameter_m", C.c_double), ("rotational_speed_rpm", C.c_double),
+                ("liquid_density_kg_m3", C.c_double), ("liquid_viscosity_pa_s", C.c_double), ("dt_s", C.c_double),
+                ("grid", C.c_int32 * 3), ("scalar_diffusivity_m2_s", C.c_double)]
+
+
+class _UnitMapping(C.Structure):
+    _fields_ = [("dx_m", C.c_double), ("dt_s", C.c_double), ("u_ref_lu", C.c_double), ("nu_lu", C.c_double),
+                ("tau_lu", C.c_double), ("cs2_lu", C.c_double), ("reynolds", C.c_double), ("froude", C.c_double),
+                ("mach_lattice", C.c_double), ("schmidt", C.c_double), ("peclet", C.c_double),
+                ("scalar_diffusivity_lu", C.c_double), ("grid_reynolds", C.c_double), ("warnings", C.c_uint32),
+                ("rejections", C.c_uint32)]
+
+
+class _BackendCaps(C.Structure):
+    _fields_ = [("handles_single_part_periodic_halo", C.c_int32), ("supports_localized_features", C.c_int32),
+                ("supports_d3q27_open_faces", C.c_int32), ("supports_two_pass", C.c_int32),
+                ("supports_gravity_body_force", C.c_int32), ("distribution_hydro", C.c_int32),
+                ("distribution_phase", C.c_int32), ("distribution_scalar", C.c_int32),
+                ("run_chunk_size", C.c_int64), ("lattices", C.c_uint32), ("storages", C.c_uint32),
+                ("collisions", C.c_uint32), ("adjoint", C.c_int32), ("batch", C.c_int32), ("checkpoint", C.c_int32)]
+
+
+# Feasibility codes of the unit report (crates/lbm-scenario/src/units.rs), by bit.
+UNIT_ISSUES = {1: "MA_LATTICE_HIGH", 2: "MA_LATTICE_TOO_HIGH", 4: "TAU_NEAR_HALF", 8: "TAU_NON_POSITIVE_VISCOSITY",
+               16: "GRID_REYNOLDS_HIGH", 32: "SCALAR_DIFFUSION_UNSTABLE"}
+
 _lib = None
 
 
@@ -231,6 +269,7 @@ def lib():
         L.lbmb_scalar_cv.argtypes = [vp, C.c_int32, _dp]
         L.lbmb_run_impeller.argtypes = [vp, C.c_int32, C.POINTER(_IbmConfig), C.c_int64, C.c_int32,
                                         C.c_int64, _dp, _dp, _dp, _i32p]
+        L.lbmb_run_impeller_status.argtypes = [vp, _i64p, _i32p]
         L.lbmb_last_timing.argtypes = [vp, _dp, _dp, _i64p]
         L.lbmb_build_wall_rims.argtypes = [_i32p, _i32p, _dp, _u8p, _dp]
         L.lbmb_build_stirred_tank.argtypes = [C.POINTER(_TankSpec), _u8p, _u8p, _dp, _dp, _dp, C.c_int64,
@@ -271,6 +310,14 @@ def lib():
         L.lbmb_checkpoint_read_host.argtypes = [C.c_char_p, C.POINTER(_CkptSpec), _u8p, _dp, C.POINTER(_CkptData)]
         L.lbmb_fnv1a64.argtypes = [C.c_char_p, C.c_uint64]
         L.lbmb_fnv1a64.restype = C.c_uint64
+        L.lbmb_power_qois.argtypes = [C.c_double] * 5 + [C.POINTER(_PowerResult)]
+        L.lbmb_power_from_torque_series.argtypes = [_dp, C.c_int64, C.c_int64, C.c_int64] + [C.c_double] * 6 + [
+            C.POINTER(_PowerResult), _i64p]
+        L.lbmb_unit_report.argtypes = [C.POINTER(_UnitInput), C.POINTER(_UnitMapping)]
+        L.lbmb_scalar_top_hat_pulse.argtypes = [_i32p, _u8p, C.c_double, _dp, C.c_double, C.c_double, _dp]
+        L.lbmb_scalar_diffusivity_lu.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
+        L.lbmb_capabilities.argtypes = [vp, C.POINTER(_BackendCaps)]
+        L.lbmb_set_wait_limit.argtypes = [vp, C.c_int64]
         _lib = L
     return _lib
 
@@ -411,6 +458,11 @@ class Solver:
 
     def sync(self):
         _check(lib().lbmb_sync(self.h))
+
+    def set_wait_limit(self, cycles):
+        """Bound (SM cycles) on the bulk-copy sweeps' mbarrier waits; 0 = the
+        default, negative = the timeout self-test on the next such sweep."""
+        _check(lib().lbmb_set_wait_limit(self.h, int(cycles)))
 
     def set_sweep_kernel(self, kind):
         """Pick the collide-stream kernel ("direct", "bulk", "async", "pair", "tile", "lean", "window");
@@ -601,16 +653,24 @@ class Solver:
 
     def run_impeller(self, body: RotatingBody, steps, cfg: DirectForcingConfig = None, scalar=-1,
                      probe_every=1):
-        """Runner hot loop (runner.rs:1079-1129) on the device."""
+        """Runner hot loop (runner.rs:1079-1129) on the device. The f64 total
+        mass is checked after every 1000th step; a non-finite value stops the
+        run with status "diverged" (runner.rs:1125-1128), and the series
+        after the executed steps read NaN."""
         cfg = cfg or DirectForcingConfig()
         torque = np.empty(steps)
         ff = np.empty(3 * steps)
         iters = np.empty(steps, dtype=np.int32)
         cv = np.full(steps, np.nan) if scalar >= 0 else None
-        _check(lib().lbmb_run_impeller(self.h, self._slot_for(body), C.byref(cfg._c()), int(steps), int(scalar),
-                                       int(probe_every), _d(torque), _d(ff), _d(cv),
-                                       iters.ctypes.data_as(_i32p)))
-        return {"torque_lu": torque, "fluid_force": ff.reshape(steps, 3), "ibm_iterations": iters, "cv": cv}
+        rc = lib().lbmb_run_impeller(self.h, self._slot_for(body), C.byref(cfg._c()), int(steps), int(scalar),
+                                     int(probe_every), _d(torque), _d(ff), _d(cv), iters.ctypes.data_as(_i32p))
+        if rc != ERR_DIVERGED:
+            _check(rc)
+        executed = C.c_int64()
+        diverged = C.c_int32()
+        _check(lib().lbmb_run_impeller_status(self.h, C.byref(executed), C.byref(diverged)))
+        return {"torque_lu": torque, "fluid_force": ff.reshape(steps, 3), "ibm_iterations": iters, "cv": cv,
+                "executed": executed.value, "status": "diverged" if diverged.value else "completed"}
 
     def adjoint_torque(self, body: RotatingBody, steps, window_begin=None, checkpoint_every=100,
                        cfg: DirectForcingConfig = None):
@@ -755,6 +815,80 @@ def mixing_time_from_cv(times, cv):
     hit99 = fin & (cv <= 0.01 * cv0)
     return {"cv0": cv0, "t95": float(times[np.argmax(hit95)]) if hit95.any() else None,
             "t99": float(times[np.argmax(hit99)]) if hit99.any() else None}
+
+
+def power_qois(torque_n_m, omega_rad_s, rho_kg_m3, impeller_diameter_m, working_volume_m3):
+    """qoi::power_qois (crates/lbm-core/src/qoi.rs:477-505)."""
+    r = _PowerResult()
+    _check(lib().lbmb_power_qois(float(torque_n_m), float(omega_rad_s), float(rho_kg_m3),
+                                 float(impeller_diameter_m), float(working_volume_m3), C.byref(r)))
+    return r.as_dict()
+
+
+def power_from_torque_series(torque_lu, run_steps, probe_every, rho_kg_m3, dx_m, dt_s, omega_rad_s,
+                             impeller_diameter_m, working_volume_m3, executed=None):
+    """The runner's power QOIs (crates/lbm-cli/src/runner.rs:1396-1425,
+    1514-1543) from the per-step lattice torque series of run_impeller:
+    records at probe steps, SI torque, mean over the last half of the run."""
+    t = _f64(torque_lu)
+    executed = t.size if executed is None else int(executed)
+    r = _PowerResult()
+    used = C.c_int64()
+    _check(lib().lbmb_power_from_torque_series(_d(t), executed, int(run_steps), int(probe_every), float(rho_kg_m3),
+                                               float(dx_m), float(dt_s), float(omega_rad_s),
+                                               float(impeller_diameter_m), float(working_volume_m3), C.byref(r),
+                                               C.byref(used)))
+    out = r.as_dict()
+    out["records_used"] = used.value
+    return out
+
+
+def unit_report(vessel_diameter_m, liquid_height_m, impeller_diameter_m, rotational_speed_rpm, liquid_density_kg_m3,
+                liquid_viscosity_pa_s, dt_s, grid, scalar_diffusivity_m2_s=None, checked=True):
+    """bioprocess_unit_report (crates/lbm-scenario/src/units.rs:96-325),
+    single-phase subset. checked=True raises UnsupportedError when a
+    rejection fires (compute_unit_report); False returns the report with its
+    rejections (unit_report_with_diagnostics)."""
+    i = _UnitInput(float(vessel_diameter_m), float(liquid_height_m), float(impeller_diameter_m),
+                   float(rotational_speed_rpm), float(liquid_density_kg_m3), float(liquid_viscosity_pa_s), float(dt_s),
+                   (C.c_int32 * 3)(*[int(g) for g in grid]),
+                   float(scalar_diffusivity_m2_s) if scalar_diffusivity_m2_s else 0.0)
+    m = _UnitMapping()
+    rc = lib().lbmb_unit_report(C.byref(i), C.byref(m))
+    if rc != ERR_UNSUPPORTED or checked:
+        _check(rc)
+    out = {k: getattr(m, k) for k, _ in _UnitMapping._fields_ if k not in ("warnings", "rejections")}
+    out["warnings"] = [v for b, v in UNIT_ISSUES.items() if m.warnings & b]
+    out["rejections"] = [v for b, v in UNIT_ISSUES.items() if m.rejections & b]
+    return out
+
+
+def scalar_top_hat_pulse(dims, solid, dx_m, center_m, radius_m, concentration=1.0):
+    """scalar_initial_condition, pulse branch (crates/lbm-cli/src/runner.rs:
+    1317-1377): `concentration` on fluid cells within radius_m of center_m."""
+    dims = [int(d) for d in dims]
+    n = dims[0] * dims[1] * dims[2]
+    so = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8).ravel()
+    out = np.empty(n)
+    _check(lib().lbmb_scalar_top_hat_pulse((C.c_int32 * 3)(*dims), None if so is None else so.ctypes.data_as(_u8p),
+                                           float(dx_m), _d(_f64(center_m, 3)), float(radius_m), float(concentration),
+                                           _d(out)))
+    return out
+
+
+def scalar_diffusivity_lu(diffusivity_m2_s, dt_s, dx_m):
+    """D dt / dx^2 (crates/lbm-cli/src/runner.rs:1371-1375)."""
+    v = C.c_double()
+    _check(lib().lbmb_scalar_diffusivity_lu(float(diffusivity_m2_s), float(dt_s), float(dx_m), C.byref(v)))
+    return v.value
+
+
+def capabilities(solver=None):
+    """The Backend trait's capability hooks (crates/lbm-core/src/backend.rs:
+    162-199, 343-345) for this backend (and a solver's configuration)."""
+    c = _BackendCaps()
+    _check(lib().lbmb_capabilities(None if solver is None else solver.h, C.byref(c)))
+    return {k: getattr(c, k) for k, _ in _BackendCaps._fields_}
 
 
 def gaussian_pulse(dims, solid, center, sigma):

@@ -46,7 +46,7 @@ __global__ void stage_in_kernel(S* fb, int64_t pl, const double* in, int64_t n) 
   const int64_t cell = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (cell >= n) return;
 #pragma unroll
-  for (int q = 0; q < Q; ++q) Codec<S>::st(fb + q * pl + cell, typename Codec<S>::A(in[q * n + cell]));
+  for (int q = 0; q < Q; ++q) Codec<S>::stage(fb + q * pl + cell, typename Codec<S>::A(in[q * n + cell]));
 }
 
 // Checkpoint image of the populations (solver.rs:4550-4552 over
@@ -95,7 +95,7 @@ __global__ void unpack_padded_kernel(S* fb, int64_t pl, const T* img, int nx, in
   const int64_t np = int64_t(nx + 2) * (ny + 2) * (nz + 2);
   const int64_t p = (int64_t(z + 1) * (ny + 2) + (y + 1)) * (nx + 2) + (x + 1);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) Codec<S>::st(fb + q * pl + cell, A(img[q * np + p]));
+  for (int q = 0; q < Q; ++q) Codec<S>::stage(fb + q * pl + cell, A(img[q * np + p]));
 }
 
 // Moments of the current state (kernels.rs:627-668) with the force field

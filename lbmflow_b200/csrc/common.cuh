@@ -25,7 +25,8 @@ enum : uint8_t {
 // x + (cx, cy, 0) when that cell is fluid, and bounces back otherwise.
 constexpr uint32_t NBR_SLIP = 1u << 31;
 
-// Storage codecs: populations are stored as S and computed in A.
+// Storage codecs: populations are stored as S and computed in A. st() is
+// the store of a fused step; stage() converts a value staged from the host.
 template <class S>
 struct Codec;
 
@@ -34,6 +35,7 @@ struct Codec<float> {
   using A = float;
   __device__ __forceinline__ static float ld(const float* p) { return *p; }
   __device__ __forceinline__ static void st(float* p, float v) { *p = v; }
+  __device__ __forceinline__ static void stage(float* p, float v) { *p = v; }
 };
 
 template <>
@@ -41,13 +43,40 @@ struct Codec<double> {
   using A = double;
   __device__ __forceinline__ static double ld(const double* p) { return *p; }
   __device__ __forceinline__ static void st(double* p, double v) { *p = v; }
+  __device__ __forceinline__ static void stage(double* p, double v) { *p = v; }
 };
+
+// The reference's host binary16 encoder (crates/lbm-core/src/gpu/
+// backend.rs:160-186), used where populations are staged from the host:
+// nearest with ties away from zero (the first dropped mantissa bit decides),
+// magnitudes below 2^-25 flush to a signed zero, exponents >= 31 (NaN
+// included) saturate to infinity. The fused steps store with the device's
+// nearest-even conversion.
+__device__ __forceinline__ uint16_t f16_bits_ref(float v) {
+  const uint32_t x = __float_as_uint(v);
+  const uint16_t sign = uint16_t((x >> 16) & 0x8000u);
+  const int32_t e = int32_t((x >> 23) & 0xffu) - 127 + 15;
+  const uint32_t mant = x & 0x7fffffu;
+  if (e <= 0) {
+    if (e < -10) return sign;
+    const uint32_t m = mant | 0x800000u;
+    const uint32_t shift = uint32_t(14 - e);
+    uint16_t h = uint16_t(m >> shift);
+    if ((m >> (shift - 1)) & 1u) h = uint16_t(h + 1);
+    return uint16_t(sign | h);
+  }
+  if (e >= 31) return uint16_t(sign | 0x7c00u);
+  uint16_t h = uint16_t(sign | (uint16_t(e) << 10) | uint16_t(mant >> 13));
+  if (mant & 0x1000u) h = uint16_t(h + 1);
+  return h;
+}
 
 template <>
 struct Codec<__half> {
   using A = float;
   __device__ __forceinline__ static float ld(const __half* p) { return __half2float(*p); }
   __device__ __forceinline__ static void st(__half* p, float v) { *p = __float2half_rn(v); }
+  __device__ __forceinline__ static void stage(__half* p, float v) { *p = __ushort_as_half(f16_bits_ref(v)); }
 };
 
 template <>
@@ -55,6 +84,7 @@ struct Codec<__nv_bfloat16> {
   using A = float;
   __device__ __forceinline__ static float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
   __device__ __forceinline__ static void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+  __device__ __forceinline__ static void stage(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
 // Force slot / wall velocity records (x, y, z, pad) in the arithmetic type.

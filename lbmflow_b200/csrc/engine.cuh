@@ -29,6 +29,7 @@
 #include "hydro_tile.cuh"
 #include "hydro_lean.cuh"
 #include "hydro_window.cuh"
+#include "hydro_staged.cuh"
 #include "batch.cuh"
 #include "adjoint.cuh"
 #include "ibm.cuh"
@@ -131,6 +132,11 @@ struct EngineBase {
   virtual void get_scalar(int k, double* c) = 0;
   virtual void run_impeller(int b, const lbmb_ibm_config& cfg, int64_t steps, int k, int64_t probe_every,
                             double* torque, double* ff, double* cv, int32_t* iters) = 0;
+  virtual void run_status(int64_t* executed, int32_t* diverged) = 0;
+  virtual void set_wait_limit(long long cycles) = 0;
+  // What this handle's current configuration allows: the adjoint and the
+  // batched runner (the checks lbmb_adjoint_torque / lbmb_batch_create make).
+  virtual void allows(int32_t* adjoint, int32_t* batch) const = 0;
   virtual void sync() = 0;
   virtual void timing(double* total_ms, double* hydro_ms, int64_t* launches) = 0;
   virtual void set_sweep_kernel(int kind) = 0;
@@ -211,6 +217,13 @@ struct Engine final : EngineBase {
   // tile-pipelined sweep: tiles holding a non-solid cell, window offsets
   DevBuf<int32_t> tile_list;
   int n_tiles_active = 0;
+  // staged sweep: tiles of STG_CELLS cells holding a non-solid cell
+  DevBuf<int32_t> stg_list;
+  int n_stg_active = 0;
+  int stg_grid[4] = {0, 0, 0, 0};
+  // nx and nx * ny are multiples of 16 bytes of elements (staged windows'
+  // read offsets known at compile time)
+  bool stg_rows_aligned = false;
   TileDirs tile_dirs[2];
   int tile_grid[2] = {0, 0};
   // persistent window-kernel grid per (parity, concurrent with the IBM chain)
@@ -272,7 +285,7 @@ struct Engine final : EngineBase {
     build_flags(wu);
     // Guard margin: shifted TMA windows of the odd step reach up to
     // nx*ny + nx + 1 cells (+ alignment slack and one tile) beyond a plane.
-    margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 128, 64) * 64;
+    margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 2 * STG_CELLS + 128, 64) * 64;
     f_alloc.alloc(size_t(Q) * plane + 2 * size_t(margin));
     CK(cudaMemsetAsync(f_alloc.p, 0, (size_t(Q) * plane + 2 * size_t(margin)) * sizeof(S), st));
     fp = f_alloc.p + margin;
@@ -287,6 +300,7 @@ struct Engine final : EngineBase {
     CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c.device));
     ntiles = ceil_div(n, TMA_TILE);
     rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
+    stg_rows_aligned = (nx % (16 / int(sizeof(S))) == 0) && ((int64_t(nx) * ny) % (16 / int(sizeof(S))) == 0);
     // default sweep: the lean kernel where it applies (TRT/BGK, fp32/16-bit
     // storage, no uniform force), else cp.async (4/8-byte storage), the
     // window kernel (16-bit storage) or direct loads (uniform force)
@@ -303,6 +317,8 @@ struct Engine final : EngineBase {
   ~Engine() override {
     if (step_graph) cudaGraphExecDestroy(step_graph);
     for (auto& e : apply_cache) cudaGraphExecDestroy(e.exec);
+    for (auto& g : run_graphs)
+      if (g) cudaGraphExecDestroy(g);
     if (st) cudaStreamSynchronize(st);
     bodies.clear();
     scalars.clear();
@@ -362,7 +378,12 @@ struct Engine final : EngineBase {
           flags_h[c] = fl;
           nb[c] = m;
         }
-    flags.upload(flags_h, st);
+    // padded to whole staged tiles (and one more) with solid bytes: the
+    // staged sweep copies a tile's flags as one block
+    const size_t nflags = size_t(ceil_div(n, STG_CELLS) + 1) * STG_CELLS;
+    if (flags.n < nflags) flags.alloc(nflags);
+    CK(cudaMemsetAsync(flags.p, F_SOLID, nflags, st));
+    CK(cudaMemcpyAsync(flags.p, flags_h.data(), size_t(n), cudaMemcpyHostToDevice, st));
     nbr.upload(nb, st);
     wall_u.upload(w, st);
     CK(cudaStreamSynchronize(st));
@@ -376,6 +397,7 @@ struct Engine final : EngineBase {
     }
     for (auto& e : apply_cache) CK(cudaGraphExecDestroy(e.exec));
     apply_cache.clear();
+    drop_run_graphs();
   }
 
   // Grow the force-slot arrays, keeping content.
@@ -494,7 +516,7 @@ struct Engine final : EngineBase {
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TMA_TILE, smem));
       tma_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sm_count) * std::max(per_sm, 1))));
     }
-    kern<<<unsigned(tma_grid[slot]), TMA_TILE, smem, s>>>(p, n, int(ntiles), d_err.p, omega_ptr());
+    kern<<<unsigned(tma_grid[slot]), TMA_TILE, smem, s>>>(p, n, int(ntiles), d_err.p, omega_ptr(), wait_limit);
     CK(cudaGetLastError());
   }
 
@@ -542,6 +564,10 @@ struct Engine final : EngineBase {
       throw Error(LBMB_ERR_UNSUPPORTED, "the window sweep needs fp32/fp16/bf16 storage and no uniform body force");
     if (kind == LBMB_SWEEP_LEAN && !lean_ok(coll))
       throw Error(LBMB_ERR_UNSUPPORTED, "the lean sweep needs TRT/BGK, fp32/fp16/bf16 storage and no uniform body force");
+    if (kind == LBMB_SWEEP_STAGED && !staged_ok())
+      throw Error(LBMB_ERR_UNSUPPORTED,
+                  "the staged sweep needs TRT/BGK, fp32/fp16/bf16 storage, even nx, no uniform body force and no "
+                  "relaxation field");
     kernel_mode = kind;
     invalidate_graphs();
   }
@@ -567,6 +593,16 @@ struct Engine final : EngineBase {
       async_minb[0] = even;
       async_minb[1] = odd;
       for (int& g : async_grid) g = 0;
+      invalidate_graphs();
+      return;
+    }
+    if (kernel_mode == LBMB_SWEEP_STAGED) {
+      auto ok = [](int v) { return v >= 1 && v <= 3; };
+      if (!ok(even) || !ok(odd))
+        throw Error(LBMB_ERR_INVALID, "sweep variant: staged resident blocks per SM must be 1, 2 or 3");
+      staged_minb[0] = even;
+      staged_minb[1] = odd;
+      for (int& g : stg_grid) g = 0;
       invalidate_graphs();
       return;
     }
@@ -637,6 +673,20 @@ struct Engine final : EngineBase {
     tile_list.alloc(list.size());
     if (!list.empty())
       CK(cudaMemcpyAsync(tile_list.p, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    {
+      const int64_t ns = ceil_div(n, STG_CELLS);
+      std::vector<int32_t> sl;
+      for (int64_t t = 0; t < ns; ++t) {
+        bool any = false;
+        for (int64_t c = t * STG_CELLS; c < std::min<int64_t>(n, (t + 1) * STG_CELLS) && !any; ++c)
+          any = !(flags_h[size_t(c)] & F_SOLID);
+        if (any) sl.push_back(int32_t(t));
+      }
+      n_stg_active = int(sl.size());
+      stg_list.alloc(sl.size());
+      if (!sl.empty())
+        CK(cudaMemcpyAsync(stg_list.p, sl.data(), sl.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    }
     using L = Lat<Q>;
     const int64_t E = 16 / int64_t(sizeof(S));
     for (int q = 0; q < Q; ++q) {
@@ -707,6 +757,51 @@ struct Engine final : EngineBase {
     }
   }
 
+  // Resident 288-thread blocks per SM of the staged sweep, per parity.
+  int staged_minb[2] = {2, 2};
+  bool staged_ok() const {
+    return std::is_same<A, float>::value && coll == COLL_TRT && nx % 2 == 0 && !has_uniform_force() && !omega_on;
+  }
+
+  template <bool ODD, int MINB>
+  void launch_staged_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    if constexpr (std::is_same<A, float>::value) {
+      if (stg_rows_aligned) launch_staged_ra<ODD, MINB, true>(p, s, concurrent);
+      else launch_staged_ra<ODD, MINB, false>(p, s, concurrent);
+    }
+  }
+  template <bool ODD, int MINB, bool RA>
+  void launch_staged_ra(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    if constexpr (std::is_same<A, float>::value) {
+      constexpr int STAGES = sizeof(S) == 2 ? 4 : 2;
+      auto kern = hydro_staged_kernel<Q, S, ODD, STAGES, MINB, RA>;
+      const size_t smem = staged_smem_bytes<Q, S, STAGES>();
+      const int slot = (ODD ? 1 : 0) + (concurrent ? 2 : 0);
+      if (stg_grid[slot] == 0) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, STG_THREADS, smem));
+        // in a runner step leave block slots free for the IBM chain on the
+        // side stream, as the cp.async grid does
+        const int64_t reserve = concurrent ? int64_t(async_reserve) / 2 : 0;
+        const int64_t slots = int64_t(sm_count) * std::max(per_sm, 1) - reserve;
+        stg_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(n_stg_active, slots)));
+      }
+      if (n_stg_active == 0) return;
+      kern<<<unsigned(stg_grid[slot]), STG_THREADS, smem, s>>>(p, stg_list.p, n_stg_active, tile_dirs[ODD], d_err.p,
+                                                               wait_limit);
+      CK(cudaGetLastError());
+    }
+  }
+  template <bool ODD>
+  void launch_staged(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
+    switch (staged_minb[ODD]) {
+      case 1: launch_staged_mb<ODD, 1>(p, s, concurrent); break;
+      case 3: launch_staged_mb<ODD, 3>(p, s, concurrent); break;
+      default: launch_staged_mb<ODD, 2>(p, s, concurrent); break;
+    }
+  }
+
   template <bool ODD, int COLL>
   void launch_pair(const HydroParams<A>& p, cudaStream_t s) {
     if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
@@ -727,6 +822,8 @@ struct Engine final : EngineBase {
         launch_tile<ODD, COLL>(p, s);
       } else if (kernel_mode == LBMB_SWEEP_LEAN && lean_ok(COLL) && !p.uniform_force) {
         launch_lean<ODD>(p, s);
+      } else if (kernel_mode == LBMB_SWEEP_STAGED && COLL == COLL_TRT && staged_ok()) {
+        launch_staged<ODD>(p, s, !cells);
       } else if (!p.uniform_force && kernel_mode == 1) {
         if (rows_aligned) launch_tma<COLL, ODD, true>(p, s);
         else launch_tma<COLL, ODD, false>(p, s);
@@ -748,6 +845,11 @@ struct Engine final : EngineBase {
       CK(cudaGetLastError());
     }
   }
+
+  // Bound on every mbarrier wait of the bulk-copy sweeps, in SM cycles
+  // (lbmb_set_wait_limit); a negative value runs the timeout self-test.
+  long long wait_limit = WAIT_LIMIT_DEFAULT;
+  void set_wait_limit(long long cycles) override { wait_limit = cycles == 0 ? WAIT_LIMIT_DEFAULT : cycles; }
 
   // Raise (and clear) a device-side error reported by a bounded wait.
   void check_device_error() {
@@ -876,12 +978,12 @@ struct Engine final : EngineBase {
     // Asynchronous: the call returns once the work is queued (every other
     // entry point runs on the same stream, and the ones that return data
     // synchronize). The device time is resolved when it is asked for. The
-    // bulk-copy kernel is the only one that can raise a device error flag,
-    // so its steps are checked at once.
+    // bulk-copy kernels are the only ones that can raise a device error
+    // flag, so their steps are checked at once.
     pending_launches = launches;
     timing_pending = true;
     time += uint64_t(steps);
-    if (kernel_mode == LBMB_SWEEP_BULK) {
+    if (kernel_mode == LBMB_SWEEP_BULK || kernel_mode == LBMB_SWEEP_STAGED) {
       CK(cudaEventSynchronize(ev1));
       check_device_error();
     }
@@ -947,6 +1049,9 @@ struct Engine final : EngineBase {
     if (lean_ok(coll))
       for (int ev = 10; ev >= 6; --ev)
         for (int od = 9; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
+    if (staged_ok())
+      for (int ev = 1; ev <= 3; ++ev)
+        for (int od = 1; od <= 3; ++od) cands.push_back({LBMB_SWEEP_STAGED, ev, od});
     if (omega_on) {
       std::vector<Cand> keep;
       for (const Cand& cd : cands)
@@ -956,6 +1061,7 @@ struct Engine final : EngineBase {
     const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
     const int ae0 = async_minb[0], ao0 = async_minb[1];
     const int we0 = window_minb[0], wo0 = window_minb[1];
+    const int se0 = staged_minb[0], so0 = staged_minb[1];
     const int par0 = parity;
     const size_t fbytes = f_alloc.n * sizeof(S);
     DevBuf<S> save;
@@ -978,6 +1084,11 @@ struct Engine final : EngineBase {
         window_minb[1] = cd.od;
         for (int& g : window_grid) g = 0;
       }
+      if (cd.kind == LBMB_SWEEP_STAGED) {
+        staged_minb[0] = cd.ev;
+        staged_minb[1] = cd.od;
+        for (int& g : stg_grid) g = 0;
+      }
       for (int i = 0; i < 2; ++i) launch_hydro(i);  // warm-up (first launches set up grids)
       CK(cudaEventRecord(ev0, st));
       for (int i = 0; i < steps; ++i) launch_hydro(i & 1);
@@ -990,6 +1101,7 @@ struct Engine final : EngineBase {
     };
     const double t_default = trial(kind0 == LBMB_SWEEP_ASYNC    ? Cand{kind0, ae0, ao0}
                                    : kind0 == LBMB_SWEEP_WINDOW ? Cand{kind0, we0, wo0}
+                                   : kind0 == LBMB_SWEEP_STAGED ? Cand{kind0, se0, so0}
                                                                 : Cand{kind0, ev0_, od0});
     int best = -1;
     double best_ms = 0.0;
@@ -1030,8 +1142,16 @@ struct Engine final : EngineBase {
       window_minb[0] = we0;
       window_minb[1] = wo0;
     }
+    if (kernel_mode == LBMB_SWEEP_STAGED) {
+      staged_minb[0] = cands[best].ev;
+      staged_minb[1] = cands[best].od;
+    } else {
+      staged_minb[0] = se0;
+      staged_minb[1] = so0;
+    }
     for (int& g : async_grid) g = 0;
     for (int& g : window_grid) g = 0;
+    for (int& g : stg_grid) g = 0;
     CK(cudaMemcpyAsync(f_alloc.p, save.p, fbytes, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
     parity = par0;
@@ -1040,6 +1160,7 @@ struct Engine final : EngineBase {
       out->kind = kernel_mode;
       const int* mb = kernel_mode == LBMB_SWEEP_ASYNC    ? async_minb
                       : kernel_mode == LBMB_SWEEP_WINDOW ? window_minb
+                      : kernel_mode == LBMB_SWEEP_STAGED ? staged_minb
                                                          : lean_minb;
       out->even_blocks_per_sm = mb[0];
       out->odd_blocks_per_sm = mb[1];
@@ -2168,24 +2289,71 @@ struct Engine final : EngineBase {
   }
 
   // ---- runner loop ------------------------------------------------------
+  // Series buffers of the runner (torque, fluid force, IBM iterations, CV,
+  // step counter), kept on the handle and grown only when a longer run needs
+  // them: the captured runner graph writes into them, so it stays valid from
+  // one call to the next.
+  DevBuf<double> run_torque, run_ff, run_cv;
+  DevBuf<int32_t> run_it;
+  DevBuf<int64_t> run_counter;
+  int64_t run_cap = 0;
+  // The instantiated runner graph (RUN_G steps from parity 0) and what it
+  // was captured with: the IBM launch arguments, the body, the probed scalar
+  // and the parity of every scalar at the graph's first step. Sweep kernel,
+  // geometry, slots and scalar set changes destroy it (invalidate_graphs).
+  static constexpr int64_t RUN_G = 16;
+  struct RunKey {
+    ApplyKey apply;
+    int32_t body;
+    int32_t nscal;
+    const void* sc_h[8];
+    int32_t sc_par[8];
+  };
+  RunKey run_key;
+  // graphs of 16, 8, 4 and 2 steps (index 0..3) for the same key, so that a
+  // span that is not a multiple of 16 replays graphs down to one step
+  static constexpr int RUN_NG = 4;
+  cudaGraphExec_t run_graphs[RUN_NG] = {nullptr, nullptr, nullptr, nullptr};
+  bool run_graph = false;
+  // Outcome of the last run_impeller call (runner.rs:1077-1129): steps
+  // executed and whether the run stopped on a non-finite total mass.
+  int64_t run_executed = 0;
+  bool run_diverged = false;
+  // The runner checks the f64 total mass after every DIVERGE_EVERY-th step
+  // of a run and stops at the first non-finite value (runner.rs:1125-1128).
+  static constexpr int64_t DIVERGE_EVERY = 1000;
+
+  void drop_run_graphs() {
+    for (auto& g : run_graphs)
+      if (g) {
+        CK(cudaGraphExecDestroy(g));
+        g = nullptr;
+      }
+    run_graph = false;
+  }
+
+  void run_reserve(int64_t steps) {
+    if (steps <= run_cap && run_counter.p) return;
+    const int64_t cap = std::max<int64_t>({steps, 2 * run_cap, int64_t(1024)});
+    run_torque.alloc(size_t(cap));
+    run_ff.alloc(size_t(3 * cap));
+    run_it.alloc(size_t(cap));
+    run_cv.alloc(size_t(cap));
+    run_counter.alloc(1);
+    run_cap = cap;
+    drop_run_graphs();
+  }
+
   void run_impeller(int b, const lbmb_ibm_config& c, int64_t steps, int k, int64_t probe_every, double* torque,
                     double* ffo, double* cv, int32_t* iters) override {
     BodyState& B = body_for(b, c);
     if (k >= 0) scalar(k);
     if (probe_every <= 0) probe_every = 1;
-    DevBuf<double> d_torque, d_ff, d_cv;
-    DevBuf<int32_t> d_it;
-    DevBuf<int64_t> d_counter;
-    d_torque.alloc(size_t(steps));
-    d_ff.alloc(size_t(3 * steps));
-    d_it.alloc(size_t(steps));
-    d_counter.alloc(1);
-    CK(cudaMemsetAsync(d_counter.p, 0, sizeof(int64_t), st));
-    if (k >= 0) {
-      d_cv.alloc(size_t(steps));
-      fill_nan(d_cv.p, steps);
-    }
-    CK(cudaEventRecord(ev0, st));
+    run_reserve(steps);
+    run_executed = 0;
+    run_diverged = false;
+    CK(cudaMemsetAsync(run_counter.p, 0, sizeof(int64_t), st));
+    if (k >= 0) fill_nan(run_cv.p, steps);
     int64_t launches = 0;
     auto one_step = [&](int64_t step_index) {
       // Fork: the IBM chain (clear -> direct forcing -> forced-cell hydro)
@@ -2197,7 +2365,7 @@ struct Engine final : EngineBase {
       // Solver::clear_body_force_field: the IBM field is non-uniform, so the
       // cached moments keep it (F_prev) while the new field starts at zero.
       if (nslots) CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st2));
-      enqueue_ibm(B, c, d_torque.p, d_ff.p, d_it.p, d_counter.p, false, st2);
+      enqueue_ibm(B, c, run_torque.p, run_ff.p, run_it.p, run_counter.p, false, st2);
       field_present = true;
       fprev_stale = true;
       launch_hydro(parity, st2, false, true);
@@ -2212,37 +2380,91 @@ struct Engine final : EngineBase {
       for (auto& sc : scalars) scalar_step(*sc);
       ++launches;
       if (k >= 0 && ((step_index + 1) % probe_every == 0 || step_index + 1 == steps))
-        enqueue_cv(*scalars[k], d_cv.p + step_index, double(n - solid_count()));
+        enqueue_cv(*scalars[k], run_cv.p + step_index, double(n - solid_count()));
     };
-    // Graph capture of a block of G steps (parity-aligned), replayed.
-    const int64_t G = 16;
-    int64_t done = 0;
-    if (parity != 0 && steps > 0) {
-      one_step(done);
-      ++done;
-    }
-    const bool probes_every_step = (k >= 0);
-    if (!probes_every_step) {
-      cudaGraphExec_t exec = nullptr;
-      while (steps - done >= G) {
-        if (!exec) {
-          cudaGraph_t g;
-          const int par0 = parity;
-          CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-          for (int64_t i = 0; i < G; ++i) one_step(0);
-          CK(cudaStreamEndCapture(st, &g));
-          CK(cudaGraphInstantiate(&exec, g, 0));
-          CK(cudaGraphDestroy(g));
-          parity = par0;
-          launches -= G;
-        }
-        CK(cudaGraphLaunch(exec, st));
-        done += G;
-        launches += G;
+    // Graph replay of blocks of 16, 8, 4 or 2 steps (parity-aligned) when
+    // no scalar is probed. The graphs are captured, instantiated and
+    // uploaded before the timed region and kept for the next call while
+    // their key holds.
+    const bool use_graph = (k < 0) && steps - (parity ? 1 : 0) >= 2 && scalars.size() <= 8;
+    if (use_graph) {
+      RunKey key;
+      std::memset(&key, 0, sizeof(key));
+      key.apply.a = ibm_args(B, c);
+      key.apply.f = fp;
+      key.apply.slots = slot_cell.p;
+      key.apply.field = fcur.p;
+      key.apply.sweeps = c.max_iterations;
+      for (int i = 0; i < 3; ++i) key.apply.force[i] = cfg.force[i];
+      key.body = b;
+      key.nscal = int32_t(scalars.size());
+      // scalar parities at the graph's first step (hydro parity 0)
+      for (size_t i = 0; i < scalars.size(); ++i) {
+        key.sc_h[i] = scalars[i]->h.p;
+        key.sc_par[i] = scalars[i]->parity ^ parity;
       }
-      if (exec) CK(cudaGraphExecDestroy(exec));
+      if (run_graph && std::memcmp(&key, &run_key, sizeof(key)) != 0) drop_run_graphs();
+      if (!run_graph) {
+        // capture from parity 0 with the scalar parities the graph will
+        // start from, then put the host state back
+        const int par0 = parity;
+        std::vector<int> spar(scalars.size());
+        for (size_t i = 0; i < scalars.size(); ++i) {
+          spar[i] = scalars[i]->parity;
+          scalars[i]->parity = key.sc_par[i];
+        }
+        const bool fpres = field_present, fstale = fprev_stale;
+        for (int gi = 0; gi < RUN_NG; ++gi) {
+          parity = 0;
+          cudaGraph_t g;
+          CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+          for (int64_t i = 0; i < (RUN_G >> gi); ++i) one_step(0);
+          CK(cudaStreamEndCapture(st, &g));
+          CK(cudaGraphInstantiate(&run_graphs[gi], g, 0));
+          CK(cudaGraphDestroy(g));
+          // upload now, so that the first replay inside a timed span does
+          // not carry it
+          CK(cudaGraphUpload(run_graphs[gi], st));
+        }
+        run_graph = true;
+        parity = par0;
+        for (size_t i = 0; i < scalars.size(); ++i) scalars[i]->parity = spar[i];
+        field_present = fpres;
+        fprev_stale = fstale;
+        launches = 0;
+        run_key = key;
+      }
     }
-    for (; done < steps; ++done) one_step(done);
+    CK(cudaEventRecord(ev0, st));
+    int64_t done = 0;
+    while (done < steps) {
+      // next divergence check after step number `check` (1-based)
+      const int64_t check = (done / DIVERGE_EVERY + 1) * DIVERGE_EVERY;
+      const int64_t stop = std::min(steps, check);
+      while (done < stop) {
+        int gi = 0;
+        while (gi < RUN_NG && stop - done < (RUN_G >> gi)) ++gi;
+        if (use_graph && parity == 0 && gi < RUN_NG) {
+          CK(cudaGraphLaunch(run_graphs[gi], st));
+          done += RUN_G >> gi;
+          launches += RUN_G >> gi;
+          field_present = true;
+          fprev_stale = false;
+        } else {
+          one_step(done);
+          ++done;
+        }
+      }
+      if (done == check) {
+        double r[5];
+        reduce_all(r);  // synchronizes the stream
+        if (!std::isfinite(r[0] + r[1])) {
+          run_diverged = true;
+          break;
+        }
+      }
+    }
+    run_executed = done;
     CK(cudaEventRecord(ev1, st));
     CK(cudaEventSynchronize(ev1));
     check_device_error();
@@ -2252,11 +2474,41 @@ struct Engine final : EngineBase {
     last_hydro_ms = ms;
     last_hydro_launches = launches;
     timing_pending = false;
-    if (torque) CK(cudaMemcpy(torque, d_torque.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
-    if (ffo) CK(cudaMemcpy(ffo, d_ff.p, size_t(3 * steps) * sizeof(double), cudaMemcpyDeviceToHost));
-    if (iters) CK(cudaMemcpy(iters, d_it.p, size_t(steps) * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    if (cv && k >= 0) CK(cudaMemcpy(cv, d_cv.p, size_t(steps) * sizeof(double), cudaMemcpyDeviceToHost));
-    time += uint64_t(steps);
+    // series of the executed steps; the steps a diverged run did not take
+    // read NaN (iterations 0)
+    const size_t ex = size_t(done), rest = size_t(steps - done);
+    const double qnan = std::nan("");
+    if (torque) {
+      if (ex) CK(cudaMemcpy(torque, run_torque.p, ex * sizeof(double), cudaMemcpyDeviceToHost));
+      std::fill(torque + ex, torque + ex + rest, qnan);
+    }
+    if (ffo) {
+      if (ex) CK(cudaMemcpy(ffo, run_ff.p, 3 * ex * sizeof(double), cudaMemcpyDeviceToHost));
+      std::fill(ffo + 3 * ex, ffo + 3 * (ex + rest), qnan);
+    }
+    if (iters) {
+      if (ex) CK(cudaMemcpy(iters, run_it.p, ex * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      std::fill(iters + ex, iters + ex + rest, 0);
+    }
+    if (cv && k >= 0) {
+      if (ex) CK(cudaMemcpy(cv, run_cv.p, ex * sizeof(double), cudaMemcpyDeviceToHost));
+      std::fill(cv + ex, cv + ex + rest, qnan);
+    }
+    time += uint64_t(done);
+    if (run_diverged)
+      throw Error(LBMB_ERR_DIVERGED, "runner: non-finite total mass after step " + std::to_string(done));
+  }
+
+  void allows(int32_t* adjoint, int32_t* batch) const override {
+    const bool f32 = std::is_same<A, float>::value;
+    const bool trt = coll == COLL_TRT;
+    *adjoint = (trt && !omega_on && !(cfg.smagorinsky_cs > 0.0) && !has_uniform_force() && scalars.empty()) ? 1 : 0;
+    *batch = (trt && f32 && !has_uniform_force() && scalars.empty() && !omega_on) ? 1 : 0;
+  }
+
+  void run_status(int64_t* executed, int32_t* diverged) override {
+    if (executed) *executed = run_executed;
+    if (diverged) *diverged = run_diverged ? 1 : 0;
   }
 
   BatchBase* make_batch(const std::vector<EngineBase*>& all, const int32_t* bodies,

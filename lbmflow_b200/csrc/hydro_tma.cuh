@@ -40,8 +40,12 @@ struct TmaWin {
 
 template <int Q, class S>
 constexpr size_t tma_smem_bytes() {
-  return size_t(2) * Q * TmaWin<S>::BYTES + 2 * sizeof(uint64_t);
+  return size_t(2) * Q * TmaWin<S>::BYTES + 3 * sizeof(uint64_t);
 }
+
+// Default bound on one mbarrier wait of the bulk-copy sweeps, in SM clock
+// cycles (about a second at 1.9 GHz).
+constexpr long long WAIT_LIMIT_DEFAULT = 1LL << 31;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -74,19 +78,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for phase `parity` of an mbarrier for at most ~2^31 clock cycles.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Wait for phase `parity` of an mbarrier for at most `limit` clock cycles.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  long long limit = WAIT_LIMIT_DEFAULT) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > (1LL << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
+}
+
+// Self-test of the timeout path (wait_limit < 0): thread 0 waits up to
+// -wait_limit cycles on an mbarrier that nothing arrives at, then reports
+// the timeout through the device error flag. Nothing is copied or written.
+__device__ __forceinline__ void wait_selftest(uint64_t* bar, long long wait_limit, int* err) {
+  if (!mbar_wait_bounded(bar, 0u, -wait_limit)) atomicOr(err, 1);
 }
 
 template <int Q, class S, int COLL, bool ODD, bool ROWS_ALIGNED>
 __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>::MIN_BLOCKS)
     hydro_tma_kernel(HydroParams<typename Codec<S>::A> p, int64_t ncells, int ntiles, int* err,
-                     const typename Codec<S>::A* omega) {
+                     const typename Codec<S>::A* omega, long long wait_limit) {
   using A = typename Codec<S>::A;
   using L = Lat<Q>;
   using CD = Codec<S>;
@@ -111,9 +123,14 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
     timed_out = 0;
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  if (wait_limit < 0) {
+    if (j == 0) wait_selftest(&bar[2], wait_limit, err);
+    return;
+  }
   auto issue = [&](int t, int s) {
     const int64_t c0 = int64_t(t) * TMA_TILE;
     const uint32_t bytes = ODD ? uint32_t(W::BYTES) : uint32_t(W::EVEN_BYTES);
@@ -134,12 +151,12 @@ __global__ void __launch_bounds__(TMA_TILE, HydroOccupancy<typename Codec<S>::A>
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       issue(tn, s ^ 1);
     }
-    if (!mbar_wait_bounded(&bar[s], uint32_t((it >> 1) & 1))) atomicOr(&timed_out, 1);
+    if (!mbar_wait_bounded(&bar[s], uint32_t((it >> 1) & 1), wait_limit)) atomicOr(&timed_out, 1);
     __syncthreads();
     if (timed_out) {
       if (j == 0) {
         atomicOr(err, 1);
-        if (tn < ntiles) mbar_wait_bounded(&bar[s ^ 1], uint32_t(((it + 1) >> 1) & 1));
+        if (tn < ntiles) mbar_wait_bounded(&bar[s ^ 1], uint32_t(((it + 1) >> 1) & 1), wait_limit);
       }
       return;
     }

@@ -16,7 +16,6 @@
 // different host threads on the same device) race on it and must be
 // serialized by the caller.
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/lbmb.h"
@@ -36,35 +35,26 @@ constexpr int64_t NOALLOC_MAX_BLOCKS = 16384;
 constexpr int64_t NOALLOC_MAX_CELLS = NOALLOC_MAX_BLOCKS * NOALLOC_CELLS_PER_BLOCK;  // 2^25
 constexpr int64_t NOALLOC_RESULT = NOALLOC_MAX_BLOCKS * 5;                       // result offset
 constexpr int64_t NOALLOC_DOUBLES = NOALLOC_RESULT + 8;
-constexpr int NOALLOC_MAX_DEVICES = 64;
+constexpr int NOALLOC_FINISH_THREADS = 256;
 
 __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
-
-std::mutex g_scratch_mu;
-double* g_scratch_ptr[NOALLOC_MAX_DEVICES] = {};
 
 struct NoAllocError {
   int code;
   std::string msg;
 };
 
-// Device address of the scratch array on the current device. In host code
-// g_noalloc_scratch only names a host-side shadow, so the address is looked
-// up once per device (with that device current) and cached.
+// Device address of the scratch array in the current device's context. In
+// host code g_noalloc_scratch only names a host-side shadow, so the address
+// is looked up with the device current. The lookup runs on every call (it
+// allocates nothing): a cached address would go stale when the context is
+// torn down and rebuilt (cudaDeviceReset) and the module loaded again.
 double* scratch_on_current_device() {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) throw NoAllocError{LBMB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e)};
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw NoAllocError{LBMB_ERR_UNSUPPORTED, "device ordinal beyond 63"};
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      throw NoAllocError{LBMB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
-    g_scratch_ptr[dev] = static_cast<double*>(p);
-  }
-  return g_scratch_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    throw NoAllocError{LBMB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)};
+  return static_cast<double*>(p);
 }
 
 // Block b reduces cells [b * 2048, (b + 1) * 2048) in a fixed order and
@@ -112,13 +102,27 @@ __global__ void __launch_bounds__(NOALLOC_THREADS)
     }
 }
 
-__global__ void reduce_linear_finish_kernel(const double* part, int64_t nblk, double* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int k = 0; k < 5; ++k) {
-    double s = 0.0;
-    for (int64_t b = 0; b < nblk; ++b) s += part[5 * b + k];
-    out[k] = s;
+// One block: thread t sums the partials of blocks t, t + 256, t + 512, ...
+// in that order, then a fixed shared-memory tree folds the 256 sums; the
+// result does not depend on timing.
+__global__ void __launch_bounds__(NOALLOC_FINISH_THREADS)
+    reduce_linear_finish_kernel(const double* part, int64_t nblk, double* out) {
+  __shared__ double sh[5][NOALLOC_FINISH_THREADS];
+  const int t = threadIdx.x;
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int64_t b = t; b < nblk; b += NOALLOC_FINISH_THREADS)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] += part[5 * b + k];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) sh[k][t] = v[k];
+  __syncthreads();
+  for (int w = NOALLOC_FINISH_THREADS / 2; w > 0; w >>= 1) {
+    if (t < w)
+#pragma unroll
+      for (int k = 0; k < 5; ++k) sh[k][t] += sh[k][t + w];
+    __syncthreads();
   }
+  if (t < 5) out[t] = sh[t][0];
 }
 
 template <int Q, class S>
@@ -166,7 +170,7 @@ extern "C" int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, i
       default:
         throw NoAllocError{LBMB_ERR_INVALID, "unknown storage precision"};
     }
-    reduce_linear_finish_kernel<<<1, 32, 0, st>>>(scratch, nblk, scratch + NOALLOC_RESULT);
+    reduce_linear_finish_kernel<<<1, NOALLOC_FINISH_THREADS, 0, st>>>(scratch, nblk, scratch + NOALLOC_RESULT);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(out, scratch + NOALLOC_RESULT, 5 * sizeof(double), cudaMemcpyDeviceToHost, st);

@@ -471,6 +471,13 @@ int lbmb_run_impeller(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg, 
   });
 }
 
+int lbmb_run_impeller_status(lbmb_solver* h, int64_t* executed, int32_t* diverged) {
+  return guarded([&] {
+    NEED(h);
+    h->e->run_status(executed, diverged);
+  });
+}
+
 int lbmb_last_timing(lbmb_solver* h, double* total_ms, double* hydro_ms, int64_t* hydro_launches) {
   return guarded([&] {
     if (!h || !h->e) throw Error(LBMB_ERR_INVALID, "null solver");
@@ -481,7 +488,7 @@ int lbmb_last_timing(lbmb_solver* h, double* total_ms, double* hydro_ms, int64_t
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind) {
   return guarded([&] {
     NEED(h);
-    if (kind < LBMB_SWEEP_DIRECT || kind > LBMB_SWEEP_WINDOW) lbmb::invalid("unknown sweep kernel kind");
+    if (kind < LBMB_SWEEP_DIRECT || kind > LBMB_SWEEP_STAGED) lbmb::invalid("unknown sweep kernel kind");
     h->e->set_sweep_kernel(kind);
   });
 }
@@ -555,6 +562,44 @@ int lbmb_adjoint_torque(lbmb_solver* h, const lbmb_ibm_config* cfg, const lbmb_a
     NEED(h);
     if (!cfg || !ac) lbmb::invalid("null argument");
     h->e->adjoint_torque(*cfg, *ac, out, dJ_dpos, torque);
+  });
+}
+
+int lbmb_set_wait_limit(lbmb_solver* h, int64_t cycles) {
+  return guarded([&] {
+    NEED(h);
+    h->e->set_wait_limit((long long)cycles);
+  });
+}
+
+int lbmb_capabilities(lbmb_solver* h, lbmb_backend_caps* out) {
+  return guarded([&] {
+    if (!out) lbmb::invalid("null output");
+    if (h && !h->e) lbmb::invalid("null solver");
+    std::memset(out, 0, sizeof(*out));
+    // backend.rs:162-199: periodic single-part axes wrap inside the sweep;
+    // localized sources, open faces, the two-pass split and gravity are not
+    // on this path; hydro and scalar distributions are stepped, phase-field
+    // distributions are not
+    out->handles_single_part_periodic_halo = 1;
+    out->supports_localized_features = 0;
+    out->supports_d3q27_open_faces = 0;
+    out->supports_two_pass = 0;
+    out->supports_gravity_body_force = 0;
+    out->distribution_hydro = LBMB_SUPPORTED;
+    out->distribution_phase = LBMB_UNSUPPORTED_NOT_IMPLEMENTED;
+    out->distribution_scalar = LBMB_SUPPORTED;
+    out->run_chunk_size = INT64_MAX;  // backend.rs:343-345: any span per call
+    out->lattices = 1u | 2u | 4u;
+    out->storages = (1u << LBMB_STORE_F32) | (1u << LBMB_STORE_F16) | (1u << LBMB_STORE_BF16) | (1u << LBMB_STORE_F64);
+    out->collisions = (1u << LBMB_BGK) | (1u << LBMB_TRT) | (1u << LBMB_CENTRAL_MOMENT);
+    out->checkpoint = 1;
+    if (h) {
+      h->e->allows(&out->adjoint, &out->batch);
+    } else {
+      out->adjoint = 1;
+      out->batch = 1;
+    }
   });
 }
 

@@ -144,7 +144,96 @@ struct StepParams {  // params.rs:302-320 (subset on the hot path)
   // cy, 0) when that cell is fluid (bounce-back otherwise). Not a reference
   // feature; restated here so the device path stays checkable with it on.
   bool free_slip_top = false;
+  // 16-bit population storage (0: off, 1: binary16, 2: bfloat16): every
+  // population the step writes is rounded to the 16-bit format (nearest,
+  // ties to even) in deviation form, as a device that stores f_i - w_i in 16
+  // bits and computes in fp32 (the reference's wgpu f16 design,
+  // crates/lbm-core/src/gpu/wgsl.rs:231-243, gpu/backend.rs:160-229).
+  int store16 = 0;
 };
+
+// ---------------------------------------------------------------------------
+// 16-bit storage codecs.
+// The reference's host codec (crates/lbm-core/src/gpu/backend.rs:160-213):
+// f32 -> binary16 keeps the top 10 mantissa bits and adds one when the
+// first dropped bit is set (nearest, ties away from zero), flushes
+// magnitudes below 2^-25 to a signed zero, builds subnormals by shifting the
+// implicit-bit mantissa, and saturates exponents >= 31 to infinity (NaN
+// included). Decoding is exact.
+// ---------------------------------------------------------------------------
+inline uint16_t f32_to_f16_bits(float value) {
+  uint32_t x;
+  std::memcpy(&x, &value, 4);
+  const uint16_t sign = uint16_t((x >> 16) & 0x8000u);
+  const int32_t exp = int32_t((x >> 23) & 0xffu) - 127 + 15;
+  const uint32_t mant = x & 0x7fffffu;
+  if (exp <= 0) {
+    if (exp < -10) return sign;
+    const uint32_t m = mant | 0x800000u;
+    const uint32_t shift = uint32_t(14 - exp);
+    uint16_t half = uint16_t(m >> shift);
+    if (((m >> (shift - 1)) & 1u) != 0) half = uint16_t(half + 1);
+    return uint16_t(sign | half);
+  }
+  if (exp >= 31) return uint16_t(sign | 0x7c00u);
+  uint16_t half = uint16_t(sign | (uint16_t(exp) << 10) | uint16_t(mant >> 13));
+  if ((mant & 0x1000u) != 0) half = uint16_t(half + 1);
+  return half;
+}
+
+inline float f16_bits_to_f32(uint16_t bits) {
+  const uint32_t sign = uint32_t(bits & 0x8000u) << 16;
+  const uint32_t exp = (bits >> 10) & 0x1fu;
+  const uint32_t mant = bits & 0x03ffu;
+  uint32_t out;
+  if (exp == 0) {
+    if (mant == 0) {
+      out = sign;
+    } else {
+      uint32_t m = mant;
+      int32_t e = -14;
+      while ((m & 0x400u) == 0) {
+        m <<= 1;
+        e -= 1;
+      }
+      m &= 0x3ffu;
+      out = sign | (uint32_t(e + 127) << 23) | (m << 13);
+    }
+  } else if (exp == 31) {
+    out = sign | 0x7f800000u | (mant << 13);
+  } else {
+    out = sign | ((exp - 15 + 127) << 23) | (mant << 13);
+  }
+  float f;
+  std::memcpy(&f, &out, 4);
+  return f;
+}
+
+// Round to the nearest binary16 value, ties to even (the device-side f16()
+// store of the fused step); finite inputs only on this path.
+inline float round_f16_rne(float v) { return float(_Float16(v)); }
+
+// Round to the nearest bfloat16 value, ties to even (top 16 bits of the
+// binary32 pattern after adding 0x7fff plus the lowest kept bit).
+inline float round_bf16_rne(float v) {
+  uint32_t x;
+  std::memcpy(&x, &v, 4);
+  if ((x & 0x7fffffffu) > 0x7f800000u) return v;  // NaN stays NaN
+  x += 0x7fffu + ((x >> 16) & 1u);
+  x &= 0xffff0000u;
+  float f;
+  std::memcpy(&f, &x, 4);
+  return f;
+}
+
+// The stored value of a population in the given 16-bit mode (1: binary16,
+// 2: bfloat16).
+inline float store16_round(int mode, float v) { return mode == 1 ? round_f16_rne(v) : round_bf16_rne(v); }
+// Host staging of a population into 16-bit storage: the reference's codec
+// for binary16, nearest-even for bfloat16 (no reference codec).
+inline float stage16(int mode, float v) {
+  return mode == 1 ? f16_bits_to_f32(f32_to_f16_bits(v)) : round_bf16_rne(v);
+}
 
 template <class L, class T>
 KParams<T> make_kparams(const StepParams& p) {  // KParams::new, params.rs:350-374
@@ -886,9 +975,22 @@ class Solver {
 
   // One Solver::step (solver.rs:2237-2280): run_span(1) = collide, stream,
   // swap, update_moments; then the scalar ADE.
+  // 16-bit storage: round every population of the fluid cells that the
+  // stream just wrote.
+  void round_stored(std::vector<T>& g) {
+    if (!params.store16) return;
+    const int mode = params.store16;
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < long(n); ++c) {
+      if (solid[c]) continue;
+      for (int q = 0; q < L::Q; ++q) g[q * n + c] = T(store16_round(mode, float(g[q * n + c])));
+    }
+  }
+
   void step() {
     collide();
     stream();
+    round_stored(ftmp);
     std::swap(f, ftmp);
     update_moments();
     ++time;
@@ -1471,6 +1573,192 @@ inline void stamp_impeller_wall_velocity(TankGeometry& g) {
   }
 }
 
+// Flat-blade (disc) turbine of the device library's tank builder
+// (lbmflow_b200/csrc/host_geometry.cpp, kind "flat_blade"; the reference has
+// no such generator). Restated here so that a tank built with it needs only
+// the oracle: markers on the analytic surfaces at a uniform spacing h cells
+// (disc of diameter 0.75 D as concentric rings on both faces, blades of
+// radial length D/4 and height D/5 at the rim on both faces of a plate of
+// thickness max(0.04 D, 1 cell)); weights are the face area per marker.
+// The target velocity of each marker, for the wall-velocity stamp, is
+// Omega_z x (p - c) in SI with c = (nx/2, ny/2, clearance) dx.
+inline void build_flat_blade_turbine(const int dims[3], double dx, double diameter_m, double clearance_m,
+                                     int blade_count, double spacing_cells, double omega_z, TankGeometry& out) {
+  const double h = spacing_cells;
+  const double D = diameter_m / dx, R = 0.5 * D;
+  const double cx = 0.5 * dims[0], cy = 0.5 * dims[1], cz = clearance_m / dx;
+  const double t = std::max(0.04 * D, 1.0);
+  const double blade_len = 0.25 * D, blade_h = 0.2 * D, r_in = R - blade_len;
+  const double r_disc = 0.375 * D;
+  const double cxs = 0.5 * dims[0] * dx, cys = 0.5 * dims[1] * dx;
+  out.marker_pos.clear();
+  out.marker_weight.clear();
+  out.marker_wall_velocity.clear();
+  auto add = [&](double x, double y, double z, double w) {
+    out.marker_pos.push_back(x);
+    out.marker_pos.push_back(y);
+    out.marker_pos.push_back(z);
+    out.marker_weight.push_back(w);
+    const double p[3] = {x * dx, y * dx, z * dx};
+    const double r[3] = {p[0] - cxs, p[1] - cys, p[2] - clearance_m};
+    out.marker_wall_velocity.push_back(0.0 * r[2] - omega_z * r[1]);
+    out.marker_wall_velocity.push_back(omega_z * r[0] - 0.0 * r[2]);
+    out.marker_wall_velocity.push_back(0.0 * r[1] - 0.0 * r[0]);
+  };
+  const int rings = int(std::ceil(r_disc / h));
+  std::vector<double> rr;
+  std::vector<int> rn;
+  int total = 0;
+  for (int k = 0; k <= rings; ++k) {
+    const double r = r_disc * double(k) / double(rings);
+    const int m = k == 0 ? 1 : std::max(1, int(std::lround(TAU * r / h)));
+    rr.push_back(r);
+    rn.push_back(m);
+    total += m;
+  }
+  const double w_disc = 3.14159265358979323846264338327950288 * r_disc * r_disc / double(total);
+  for (int face = 0; face < 2; ++face) {
+    const double z = cz + (face ? 0.5 : -0.5) * t;
+    for (size_t k = 0; k < rr.size(); ++k)
+      for (int j = 0; j < rn[k]; ++j) {
+        const double th = TAU * (double(j) + 0.5 * double(k & 1)) / double(rn[k]);
+        add(cx + rr[k] * std::cos(th), cy + rr[k] * std::sin(th), z, w_disc);
+      }
+  }
+  const int nr = std::max(1, int(std::ceil(blade_len / h)));
+  const int nzb = std::max(1, int(std::ceil(blade_h / h)));
+  const double w_blade = blade_len * blade_h / double((nr + 1) * (nzb + 1));
+  for (int b = 0; b < blade_count; ++b) {
+    const double th = TAU * double(b) / double(blade_count);
+    const double er[2] = {std::cos(th), std::sin(th)}, et[2] = {-std::sin(th), std::cos(th)};
+    for (int face = 0; face < 2; ++face) {
+      const double off = (face ? 0.5 : -0.5) * t;
+      for (int i = 0; i <= nr; ++i) {
+        const double r = r_in + blade_len * double(i) / double(nr);
+        for (int k = 0; k <= nzb; ++k) {
+          const double z = cz - 0.5 * blade_h + blade_h * double(k) / double(nzb);
+          add(cx + r * er[0] + off * et[0], cy + r * er[1] + off * et[1], z, w_blade);
+        }
+      }
+    }
+  }
+  out.center[0] = cxs / dx;
+  out.center[1] = cys / dx;
+  out.center[2] = clearance_m / dx;
+  out.omega[0] = 0.0;
+  out.omega[1] = 0.0;
+  out.omega[2] = omega_z;
+}
+
+// ---------------------------------------------------------------------------
+// Runner QOIs and set-up helpers (crates/lbm-cli/src/runner.rs,
+// crates/lbm-scenario/src/units.rs).
+// ---------------------------------------------------------------------------
+// f64::powi for the small exponents used here: binary exponentiation from
+// the low bits (x^3 = x * x^2, x^5 = x * x^4).
+inline double powi(double x, int k) {
+  double r = 1.0, sq = x;
+  bool first = true;
+  while (k) {
+    if (k & 1) {
+      r = first ? sq : r * sq;
+      first = false;
+    }
+    k >>= 1;
+    if (k) sq = sq * sq;
+  }
+  return r;
+}
+
+// torque_record_from_ibm (runner.rs:1396-1425): N m per lattice torque unit.
+inline double torque_scale(double rho, double dx, double dt) { return rho * powi(dx, 5) / powi(dt, 2); }
+
+// write_power_qois averaging (runner.rs:1514-1543) over the runner's
+// records: records at steps s (1-based) with s % probe_every == 0 or
+// s == run_steps among the executed steps; mean torque (N m) over records
+// with s >= run_steps / 2, or over all records when none is that late.
+// Returns NaN when there is no record.
+inline double runner_mean_torque(const double* torque_lu, long executed, long run_steps, long probe_every, double rho,
+                                 double dx, double dt, long* used) {
+  if (probe_every <= 0) probe_every = 1;
+  const double sc = torque_scale(rho, dx, dt);
+  std::vector<std::pair<long, double>> recs;
+  for (long s = 1; s <= executed; ++s)
+    if (s % probe_every == 0 || s == run_steps) recs.push_back({s, torque_lu[s - 1] * sc});
+  if (recs.empty()) return NAN;
+  const long start = run_steps / 2;
+  std::vector<double> win;
+  for (auto& r : recs)
+    if (r.first >= start) win.push_back(r.second);
+  if (win.empty())
+    for (auto& r : recs) win.push_back(r.second);
+  double sum = 0.0;
+  for (double v : win) sum += v;
+  if (used) *used = long(win.size());
+  return sum / double(win.size());
+}
+
+// bioprocess_unit_report_unchecked (units.rs:116-325), single-phase
+// stirred tank with an optional passive scalar (d_scalar <= 0: none).
+// out: dx, dt, u_ref_lu, nu_lu, tau_lu, cs2, Re, Fr, Ma, Sc, Pe, D_lu,
+// grid Re; warn/rej bits: 1 MA_LATTICE_HIGH, 2 MA_LATTICE_TOO_HIGH, 4
+// TAU_NEAR_HALF, 8 TAU_NON_POSITIVE_VISCOSITY, 16 GRID_REYNOLDS_HIGH, 32
+// SCALAR_DIFFUSION_UNSTABLE. Returns false for a non-positive input.
+inline bool unit_report(double vessel_d, double liquid_h, double imp_d, double rpm, double rho, double mu, double dt,
+                        const int grid[3], double d_scalar, double out[13], unsigned* warn, unsigned* rej) {
+  for (double v : {vessel_d, liquid_h, imp_d, rpm, rho, mu, dt})
+    if (!(std::isfinite(v) && v > 0.0)) return false;
+  if (grid[0] == 0 || grid[1] == 0 || grid[2] == 0) return false;
+  const double n_hz = rpm / 60.0;
+  const double u_ref_m_s = n_hz * imp_d;
+  const double nu_m2_s = mu / rho;
+  const double dx_m = vessel_d / double(grid[0]);
+  const double u_ref_lu = u_ref_m_s * dt / dx_m;
+  const double nu_lu = nu_m2_s * dt / (dx_m * dx_m);
+  const double tau_lu = 3.0 * nu_lu + 0.5;
+  const double cs2 = 1.0 / 3.0;
+  const double mach = u_ref_lu / std::sqrt(cs2);
+  const double re = rho * n_hz * powi(imp_d, 2) / mu;
+  const double fr = powi(n_hz, 2) * imp_d / 9.80665;
+  const bool has_d = d_scalar > 0.0;
+  const double sc = has_d ? nu_m2_s / d_scalar : NAN;
+  const double pe = has_d ? u_ref_m_s * vessel_d / d_scalar : NAN;
+  const double d_lu = has_d ? d_scalar * dt / (dx_m * dx_m) : NAN;
+  unsigned w = 0, r = 0;
+  if (mach > 0.30)
+    r |= 2;
+  else if (mach > 0.10)
+    w |= 1;
+  if (tau_lu <= 0.5)
+    r |= 8;
+  else if (tau_lu <= 0.55)
+    w |= 4;
+  const double grid_re = u_ref_lu / nu_lu;
+  if (grid_re > 15.0) w |= 16;
+  if (has_d && nu_lu / d_lu > 25.0) w |= 32;
+  const double vals[13] = {dx_m, dt, u_ref_lu, nu_lu, tau_lu, cs2, re, fr, mach, sc, pe, d_lu, grid_re};
+  for (int i = 0; i < 13; ++i) out[i] = vals[i];
+  *warn = w;
+  *rej = r;
+  return true;
+}
+
+// scalar_initial_condition, pulse branch (runner.rs:1317-1377): the pulse
+// concentration on fluid cells whose centre lies within the radius.
+inline void top_hat_pulse(const int dims[3], const uint8_t* solid, double dx, const double center[3], double radius,
+                          double conc, double* values) {
+  for (int z = 0; z < dims[2]; ++z)
+    for (int y = 0; y < dims[1]; ++y)
+      for (int x = 0; x < dims[0]; ++x) {
+        const size_t i = (size_t(z) * dims[1] + y) * dims[0] + x;
+        values[i] = 0.0;
+        if (solid && solid[i]) continue;
+        const double p[3] = {(double(x) + 0.5) * dx, (double(y) + 0.5) * dx, (double(z) + 0.5) * dx};
+        const double r = std::sqrt(powi(p[0] - center[0], 2) + powi(p[1] - center[1], 2) + powi(p[2] - center[2], 2));
+        if (r <= radius) values[i] = conc;
+      }
+}
+
 // ---------------------------------------------------------------------------
 // QOI formulas (crates/lbm-core/src/qoi.rs:477-556).
 // ---------------------------------------------------------------------------
@@ -1485,7 +1773,7 @@ inline PowerQoi power_qois(double torque, double omega, double rho, double d, do
   double n_hz = omega / TAU;
   if (!(n_hz > 0.0)) throw std::runtime_error("rotational speed must be positive for Np/Nq");
   double power = omega * torque;
-  double denom = rho * n_hz * n_hz * n_hz * std::pow(d, 5);
+  double denom = rho * powi(n_hz, 3) * powi(d, 5);
   return {torque, power, n_hz, power / denom, power / volume};
 }
 

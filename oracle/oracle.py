@@ -72,6 +72,20 @@ def lib():
                                       C.c_double, C.c_int, C.c_double, C.c_double, C.c_int,
                                       C.c_double, _u8p, _u8p, _dp, _dp, _dp, C.c_long, _dp, _dp,
                                       C.c_char_p, C.c_int]
+        L.lbmo_build_tank2.restype = C.c_long
+        L.lbmo_build_tank2.argtypes = [_ip, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, _u8p, _u8p, _dp,
+                                       _dp, _dp, C.c_long, _dp, _dp, C.c_char_p, C.c_int]
+        L.lbmo_set_store16.restype = C.c_int
+        L.lbmo_set_store16.argtypes = [C.c_void_p, C.c_int]
+        _fp = C.POINTER(C.c_float)
+        L.lbmo_codec16.argtypes = [C.c_int, _fp, _fp, C.c_long]
+        L.lbmo_f16_bits.argtypes = [_fp, C.POINTER(C.c_uint16), C.c_long]
+        L.lbmo_runner_power.restype = C.c_long
+        L.lbmo_runner_power.argtypes = [_dp, C.c_long, C.c_long, C.c_long] + [C.c_double] * 6 + [_dp]
+        L.lbmo_unit_report.restype = C.c_int
+        L.lbmo_unit_report.argtypes = [_dp, _ip, C.c_double, _dp, C.POINTER(C.c_uint)]
+        L.lbmo_top_hat_pulse.argtypes = [_ip, _u8p, C.c_double, _dp, C.c_double, C.c_double, _dp]
         L.lbmo_power_qois.restype = C.c_int
         L.lbmo_power_qois.argtypes = [C.c_double] * 5 + [_dp]
         L.lbmo_scalar_cv.restype = C.c_double
@@ -136,7 +150,7 @@ class OracleSolver:
 
     def __init__(self, dims, q=19, real_bits=64, collision="trt", nu=1.0 / 6.0, magic=MAGIC_STD,
                  omega_shear=0.0, periodic=(False, False, False), force=(0.0, 0.0, 0.0),
-                 solid=None, wall_u=None, smagorinsky_cs=0.0, free_slip_top=False):
+                 solid=None, wall_u=None, smagorinsky_cs=0.0, free_slip_top=False, store16=None):
         L = lib()
         self.dims = tuple(int(d) for d in dims)
         self.n = self.dims[0] * self.dims[1] * self.dims[2]
@@ -158,6 +172,10 @@ class OracleSolver:
             L.lbmo_set_smagorinsky(self.h, float(smagorinsky_cs))
         if free_slip_top:
             L.lbmo_set_free_slip_top(self.h, 1)
+        if store16:
+            # 16-bit population storage (fp32 arithmetic): "f16" or "bf16"
+            if L.lbmo_set_store16(self.h, {"f16": 1, "bf16": 2}[store16]) != 0:
+                raise ValueError("16-bit storage needs real_bits=32")
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -344,13 +362,16 @@ def wall_rims(dims, is_wall, wall_u, d=3):
 
 
 def build_tank(dims, dx, vessel_d, liquid_h, impeller_d, clearance, blades, omega_z,
-               baffle_w=0.0, baffle_t=0.0, kind=0):
+               baffle_w=0.0, baffle_t=0.0, kind=0, spacing=0.7):
+    """Tank voxels and one impeller's markers. kind 0 Rushton, 1 pitched
+    blade (the reference's generators), 2 the device library's flat-blade
+    turbine at `spacing` cells."""
     n = dims[0] * dims[1] * dims[2]
     err = C.create_string_buffer(256)
     dims_a = (C.c_int * 3)(*dims)
-    m = lib().lbmo_build_tank(dims_a, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind,
-                              impeller_d, clearance, blades, omega_z, None, None, None, None,
-                              None, 0, None, None, err, 256)
+    m = lib().lbmo_build_tank2(dims_a, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind,
+                               impeller_d, clearance, blades, omega_z, spacing, None, None, None, None,
+                               None, 0, None, None, err, 256)
     if m < 0:
         raise ValueError(err.value.decode())
     solid = np.zeros(n, dtype=np.uint8)
@@ -360,10 +381,10 @@ def build_tank(dims, dx, vessel_d, liquid_h, impeller_d, clearance, blades, omeg
     w = np.zeros(m)
     center = np.zeros(3)
     omega = np.zeros(3)
-    lib().lbmo_build_tank(dims_a, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind, impeller_d,
-                          clearance, blades, omega_z, solid.ctypes.data_as(_u8p),
-                          baffle.ctypes.data_as(_u8p), _d(wv), _d(pos), _d(w), m, _d(center),
-                          _d(omega), err, 256)
+    lib().lbmo_build_tank2(dims_a, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind, impeller_d,
+                           clearance, blades, omega_z, spacing, solid.ctypes.data_as(_u8p),
+                           baffle.ctypes.data_as(_u8p), _d(wv), _d(pos), _d(w), m, _d(center),
+                           _d(omega), err, 256)
     return {"solid": solid, "baffle": baffle, "wall_velocity": wv.reshape(n, 3),
             "marker_pos": pos.reshape(m, 3), "marker_w": w, "center": center, "omega": omega}
 
@@ -373,6 +394,66 @@ def power_qois(torque, omega, rho, d, volume):
     if lib().lbmo_power_qois(torque, omega, rho, d, volume, _d(out)) != 0:
         raise ValueError("invalid power QOI inputs")
     return dict(zip(("torque_n_m", "power_w", "rotational_speed_hz", "np", "p_over_v_w_m3"), out))
+
+
+def codec16(mode, values):
+    """16-bit storage rounding of float32 values: "ref_f16" the reference's
+    host binary16 codec (gpu/backend.rs:160-213, encode then decode),
+    "bf16" bfloat16 nearest-even, "f16" binary16 nearest-even."""
+    v = np.ascontiguousarray(values, dtype=np.float32).ravel()
+    out = np.empty_like(v)
+    fp = C.POINTER(C.c_float)
+    lib().lbmo_codec16({"ref_f16": 1, "bf16": 2, "f16": 3}[mode], v.ctypes.data_as(fp), out.ctypes.data_as(fp), v.size)
+    return out
+
+
+def f16_bits(values):
+    """The reference's f32_to_f16_bits (gpu/backend.rs:160-186)."""
+    v = np.ascontiguousarray(values, dtype=np.float32).ravel()
+    out = np.empty(v.size, dtype=np.uint16)
+    lib().lbmo_f16_bits(v.ctypes.data_as(C.POINTER(C.c_float)), out.ctypes.data_as(C.POINTER(C.c_uint16)), v.size)
+    return out
+
+
+def runner_power(torque_lu, run_steps, probe_every, rho, dx, dt, omega, d, volume, executed=None):
+    """write_power_qois over a per-step lattice torque series
+    (runner.rs:1396-1425, 1514-1543)."""
+    t = _as_d(torque_lu).ravel()
+    executed = t.size if executed is None else int(executed)
+    out = np.zeros(5)
+    used = lib().lbmo_runner_power(_d(t), executed, int(run_steps), int(probe_every), rho, dx, dt, omega, d, volume,
+                                   _d(out))
+    if used < 0:
+        raise ValueError("no torque records or invalid power QOI inputs")
+    r = dict(zip(("torque_n_m", "power_w", "rotational_speed_hz", "np", "p_over_v_w_m3"), out))
+    r["records_used"] = int(used)
+    return r
+
+
+UNIT_KEYS = ("dx_m", "dt_s", "u_ref_lu", "nu_lu", "tau_lu", "cs2_lu", "reynolds", "froude", "mach_lattice",
+             "schmidt", "peclet", "scalar_diffusivity_lu", "grid_reynolds")
+
+
+def unit_report(vessel_d, liquid_h, imp_d, rpm, rho, mu, dt, grid, d_scalar=0.0):
+    """bioprocess_unit_report_unchecked (units.rs:116-325), single phase."""
+    out = np.zeros(13)
+    bits = (C.c_uint * 2)()
+    if lib().lbmo_unit_report(_d(np.array([vessel_d, liquid_h, imp_d, rpm, rho, mu, dt], dtype=np.float64)),
+                              (C.c_int * 3)(*grid), float(d_scalar or 0.0), _d(out), bits) != 0:
+        raise ValueError("unit report inputs must be finite and positive")
+    r = dict(zip(UNIT_KEYS, out))
+    r["warnings"], r["rejections"] = int(bits[0]), int(bits[1])
+    return r
+
+
+def top_hat_pulse(dims, solid, dx, center, radius, conc=1.0):
+    """scalar_initial_condition, pulse branch (runner.rs:1317-1377)."""
+    n = dims[0] * dims[1] * dims[2]
+    out = np.zeros(n)
+    so = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8).ravel()
+    lib().lbmo_top_hat_pulse((C.c_int * 3)(*dims), None if so is None else so.ctypes.data_as(_u8p), float(dx),
+                             _d(_as_d(center)), float(radius), float(conc), _d(out))
+    return out
 
 
 def scalar_cv(values, include):

@@ -2,6 +2,7 @@
 // lbm_oracle.hpp). Loaded by tests/ through ctypes via oracle/oracle.py and
 // timed as the CPU baseline by bench.py. Never linked into the product.
 #include <memory>
+#include <type_traits>
 
 #include "lbm_oracle.hpp"
 
@@ -28,6 +29,7 @@ struct AnySolver {
   virtual int q() const = 0;
   virtual void set_smagorinsky(double cs) = 0;
   virtual void set_free_slip_top(bool on) = 0;
+  virtual bool set_store16(int mode) = 0;
   virtual void strain_rate(double* s6, double* gamma) const = 0;
   virtual void set_omega_field(const double* v) = 0;
   virtual void velocity_gradient(double* g9) const = 0;
@@ -50,14 +52,28 @@ struct Impl final : AnySolver {
   void step(int n) override { s.run(n); }
   void set_smagorinsky(double cs) override { s.params.smagorinsky_cs = cs; }
   void set_free_slip_top(bool on) override { s.params.free_slip_top = on; }
+  // 16-bit storage mode (fp32 arithmetic only).
+  bool set_store16(int mode) override {
+    if (mode != 0 && !std::is_same<T, float>::value) return false;
+    if (mode < 0 || mode > 2) return false;
+    s.params.store16 = mode;
+    return true;
+  }
   void stage_in(const double* f) override {
-    for (size_t i = 0; i < s.f.size(); ++i) s.f[i] = T(f[i]);
+    const int m = s.params.store16;
+    for (size_t i = 0; i < s.f.size(); ++i) s.f[i] = m ? T(stage16(m, float(f[i]))) : T(f[i]);
     s.update_moments();
   }
   void stage_out(double* f) const override {
     for (size_t i = 0; i < s.f.size(); ++i) f[i] = double(s.f[i]);
   }
-  void init_with(const double* r, const double* u) override { s.init_with(r, u); }
+  void init_with(const double* r, const double* u) override {
+    s.init_with(r, u);
+    if (const int m = s.params.store16) {  // staged into 16-bit storage
+      for (auto& v : s.f) v = T(stage16(m, float(v)));
+      s.update_moments();
+    }
+  }
   void read_moments(double* r, double* ux, double* uy, double* uz) const override {
     for (size_t c = 0; c < s.n; ++c) {
       if (r) r[c] = double(s.rho[c]);
@@ -306,11 +322,26 @@ void lbmo_wall_rims(int d, const int* dims, const int* is_wall, const double* u,
 // Stirred tank (cylinder + optional 4 baffles + one radial impeller, SI
 // inputs). Returns the marker count; when it exceeds max_markers only the
 // count is returned. kind: 0 Rushton, 1 pitched blade.
+long lbmo_build_tank2(const int* dims, double dx, double vessel_d, double liquid_h, double baffle_w, double baffle_t,
+                      int kind, double imp_d, double clearance, int blades, double omega_z, double spacing,
+                      uint8_t* solid, uint8_t* baffle, double* wall_velocity, double* marker_pos, double* marker_w,
+                      long max_markers, double* center, double* omega, char* err, int errlen);
+
 long lbmo_build_tank(const int* dims, double dx, double vessel_d, double liquid_h,
                      double baffle_w, double baffle_t, int kind, double imp_d, double clearance,
                      int blades, double omega_z, uint8_t* solid, uint8_t* baffle,
                      double* wall_velocity, double* marker_pos, double* marker_w, long max_markers,
                      double* center, double* omega, char* err, int errlen) {
+  return lbmo_build_tank2(dims, dx, vessel_d, liquid_h, baffle_w, baffle_t, kind, imp_d, clearance, blades, omega_z,
+                          0.7, solid, baffle, wall_velocity, marker_pos, marker_w, max_markers, center, omega, err,
+                          errlen);
+}
+
+// Kind 2: the device library's flat-blade turbine at `spacing` cells.
+long lbmo_build_tank2(const int* dims, double dx, double vessel_d, double liquid_h, double baffle_w, double baffle_t,
+                      int kind, double imp_d, double clearance, int blades, double omega_z, double spacing,
+                      uint8_t* solid, uint8_t* baffle, double* wall_velocity, double* marker_pos, double* marker_w,
+                      long max_markers, double* center, double* omega, char* err, int errlen) {
   try {
     TankGeometry g;
     for (int a = 0; a < 3; ++a) g.dims[a] = dims[a];
@@ -323,7 +354,10 @@ long lbmo_build_tank(const int* dims, double dx, double vessel_d, double liquid_
     if (baffle_w > 0.0)
       apply_baffle_mask(dims, dx, vessel_d, liquid_h, baffle_w, baffle_t, g.solid.data(),
                         g.baffle_mask.data());
-    build_radial_impeller(dims, dx, vessel_d, liquid_h, kind, imp_d, clearance, blades, omega_z, g);
+    if (kind == 2)
+      build_flat_blade_turbine(dims, dx, imp_d, clearance, blades, spacing, omega_z, g);
+    else
+      build_radial_impeller(dims, dx, vessel_d, liquid_h, kind, imp_d, clearance, blades, omega_z, g);
     stamp_impeller_wall_velocity(g);
     long m = long(g.marker_weight.size());
     if (solid) std::memcpy(solid, g.solid.data(), n);
@@ -342,6 +376,51 @@ long lbmo_build_tank(const int* dims, double dx, double vessel_d, double liquid_
     set_err(err, errlen, e.what());
     return -1;
   }
+}
+
+int lbmo_set_store16(void* h, int mode) { return static_cast<AnySolver*>(h)->set_store16(mode) ? 0 : -1; }
+
+// 16-bit codecs over n values: mode 1 the reference's host binary16 codec
+// (encode then decode), mode 2 bfloat16 nearest-even, mode 3 binary16
+// nearest-even (the device store).
+void lbmo_codec16(int mode, const float* in, float* out, long n) {
+  for (long i = 0; i < n; ++i)
+    out[i] = mode == 1 ? f16_bits_to_f32(f32_to_f16_bits(in[i])) : (mode == 2 ? round_bf16_rne(in[i]) : round_f16_rne(in[i]));
+}
+void lbmo_f16_bits(const float* in, uint16_t* out, long n) {
+  for (long i = 0; i < n; ++i) out[i] = f32_to_f16_bits(in[i]);
+}
+
+// Runner power QOIs from a per-step lattice torque series: out = power_qois
+// of the mean SI torque (runner_mean_torque); returns records used or -1.
+long lbmo_runner_power(const double* torque_lu, long executed, long run_steps, long probe_every, double rho, double dx,
+                       double dt, double omega, double d, double volume, double* out) {
+  long used = 0;
+  const double t = runner_mean_torque(torque_lu, executed, run_steps, probe_every, rho, dx, dt, &used);
+  if (!std::isfinite(t)) return -1;
+  try {
+    PowerQoi p = power_qois(t, omega, rho, d, volume);
+    out[0] = p.torque_n_m;
+    out[1] = p.power_w;
+    out[2] = p.rotational_speed_hz;
+    out[3] = p.np;
+    out[4] = p.p_over_v_w_m3;
+  } catch (...) {
+    return -1;
+  }
+  return used;
+}
+
+int lbmo_unit_report(const double* in7, const int* grid, double d_scalar, double* out13, unsigned* bits2) {
+  return unit_report(in7[0], in7[1], in7[2], in7[3], in7[4], in7[5], in7[6], grid, d_scalar, out13, &bits2[0],
+                     &bits2[1])
+             ? 0
+             : -1;
+}
+
+void lbmo_top_hat_pulse(const int* dims, const uint8_t* solid, double dx, const double* center, double radius,
+                        double conc, double* values) {
+  top_hat_pulse(dims, solid, dx, center, radius, conc, values);
 }
 
 int lbmo_power_qois(double torque, double omega, double rho, double d, double volume, double* out) {

@@ -39,13 +39,13 @@ def handle_reduce(s):
                     [s.reduce(lb.RED_MOMENTUM, a) for a in range(3)])
 
 
-@pytest.mark.parametrize("q,prec", [(19, "f32"), (27, "f64")])
+@pytest.mark.parametrize("q,prec", [(19, "f32"), (27, "f64"), (19, "f16"), (27, "bf16")])
 def test_noalloc_reduction_matches_handle_reduce(q, prec):
     import torch
     dims, solid, wall_u, nu = cavity(24, re=30.0)
     force = (1e-6, -2e-6, 5e-7)
     s = lb.Solver(dims, lattice=q, storage=prec, nu=nu, solid=solid, wall_u=wall_u, force=force)
-    dtype = torch.float32 if prec == "f32" else torch.float64
+    dtype = {"f32": torch.float32, "f64": torch.float64, "f16": torch.float16, "bf16": torch.bfloat16}[prec]
     solid_dev = torch.from_numpy(solid.astype(np.uint8)).cuda()
     for call in range(2):  # two calls in a row share the fixed scratch array
         s.run(17 + call)
@@ -53,9 +53,10 @@ def test_noalloc_reduction_matches_handle_reduce(q, prec):
         # stage_out is the exact f64 view of the stored values, so the cast
         # back to the storage type reproduces the device populations.
         f_dev = torch.from_numpy(s.stage_out()).to(dtype).cuda().contiguous()
-        # the solver keeps the uniform force in its storage precision
-        # (KParams::force is T), so pass the same rounded value
-        force_t = np.asarray(force, dtype=np.float32 if prec == "f32" else np.float64).astype(np.float64)
+        # the solver keeps the uniform force in its arithmetic precision
+        # (fp32 for fp32 and 16-bit storage, fp64 for fp64), so pass the same
+        # rounded value
+        force_t = np.asarray(force, dtype=np.float64 if prec == "f64" else np.float32).astype(np.float64)
         rc, out = noalloc_reduce(f_dev, prec, q, s.n, s.n, solid_dev, force_t)
         assert rc == lb.OK, lb.lib().lbmb_last_error()
         assert out[0] == ref[0]
