@@ -363,8 +363,8 @@ int lbmb_run_impeller(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg, 
 int lbmb_run_impeller_status(lbmb_solver* h, int64_t* executed, int32_t* diverged);
 
 /* No counterpart in the reference (failure detection of the device path).
- * Bound on every mbarrier wait of the bulk-copy sweep kernels
- * (LBMB_SWEEP_BULK, LBMB_SWEEP_STAGED), in SM clock cycles; 0 restores the
+ * Bound on every mbarrier wait of the bulk-copy sweep kernel
+ * (LBMB_SWEEP_BULK), in SM clock cycles; 0 restores the
  * default (2^31, about a second). A wait that runs out sets a device error
  * flag, waits (bounded) for the kernel's own copies and returns; the call
  * that launched the step then fails with LBMB_ERR_CUDA ("device wait timed
@@ -422,8 +422,10 @@ int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, i
  *   LBMB_SWEEP_BULK    bulk asynchronous copies staged in shared memory;
  *   LBMB_SWEEP_ASYNC   per-thread cp.async ring (4/8-byte storage);
  *   LBMB_SWEEP_PAIR    two x-adjacent cells per thread, 2-element accesses
- *                      and packed fp32x2 arithmetic (TRT/BGK, fp32/fp16/
- *                      bf16 storage, even nx, no uniform body force);
+ *                      (4 bytes and more for 16-bit storage) and packed
+ *                      fp32x2 arithmetic (TRT/BGK or central moment on
+ *                      D3Q27, fp32/fp16/bf16 storage, even nx, no uniform
+ *                      body force);
  *   LBMB_SWEEP_TILE    the pair update fed by 16-byte cp.async windows
  *                      staged in shared memory several tiles ahead (same
  *                      conditions as LBMB_SWEEP_PAIR);
@@ -433,13 +435,7 @@ int lbmb_reduce_populations_noalloc(const void* f, int32_t storage, int32_t q, i
  *   LBMB_SWEEP_WINDOW  one cell per thread, tiles of 256 cells staged in
  *                      shared memory by 16-byte cp.async windows several
  *                      tiles ahead (TRT/BGK or central moment, fp32/fp16/
- *                      bf16 storage, no uniform body force);
- *   LBMB_SWEEP_STAGED  two x-adjacent cells per thread with the packed fp32x2
- *                      collision, fed from a shared-memory ring of 448-cell
- *                      tiles that one producer warp fills with bulk copies
- *                      (mbarrier completion, bounded waits) (TRT/BGK,
- *                      fp32/fp16/bf16 storage, even nx, no uniform body force,
- *                      no relaxation field).
+ *                      bf16 storage, no uniform body force).
  * A kind that cannot run the solver's configuration returns
  * LBMB_ERR_UNSUPPORTED and leaves the current kind in place. */
 typedef enum {
@@ -449,8 +445,7 @@ typedef enum {
   LBMB_SWEEP_PAIR = 3,
   LBMB_SWEEP_TILE = 4,
   LBMB_SWEEP_LEAN = 5,
-  LBMB_SWEEP_WINDOW = 6,
-  LBMB_SWEEP_STAGED = 7
+  LBMB_SWEEP_WINDOW = 6
 } lbmb_sweep_kind;
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind);
 int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
@@ -465,9 +460,9 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
  * step, where the IBM kernels run concurrently on a side stream. Window
  * kernel: resident 256-thread blocks per SM per parity, 2 (128 registers),
  * 3 (80) or 4 (64), with a tile ring of 3 where shared memory allows, else
- * 2; default 2 for the central moment, 3 for TRT/BGK. Staged kernel:
- * resident 256-thread blocks per SM per parity, 1 (up to 255 registers),
- * 2 (128, the default) or 3 (80). */
+ * 2; default 2 for the central moment, 3 for TRT/BGK. Pair kernel (TRT/BGK):
+ * resident 128-thread blocks per SM per parity, 3 (168 registers), 4 (128,
+ * the default) or 5 (96). */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

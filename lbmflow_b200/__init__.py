@@ -26,7 +26,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DIVERGED, ERR_STATE, ERR_NOMEM =
 ERR_CHECKPOINT = -7
 COLLISION = {"bgk": 0, "trt": 1, "cm": 2, "central_moment": 2}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
-SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5, "window": 6, "staged": 7}
+SWEEP = {"direct": 0, "bulk": 1, "async": 2, "pair": 3, "tile": 4, "lean": 5, "window": 6}
 IMPELLER = {"rushton": 0, "pitched": 1, "flat_blade": 2}
 MAGIC_STD = 3.0 / 16.0
 RED_FLUID_CELLS, RED_MASS_DEV, RED_MOMENTUM = 0, 1, 2

@@ -29,7 +29,6 @@
 #include "hydro_tile.cuh"
 #include "hydro_lean.cuh"
 #include "hydro_window.cuh"
-#include "hydro_staged.cuh"
 #include "batch.cuh"
 #include "adjoint.cuh"
 #include "ibm.cuh"
@@ -217,13 +216,9 @@ struct Engine final : EngineBase {
   // tile-pipelined sweep: tiles holding a non-solid cell, window offsets
   DevBuf<int32_t> tile_list;
   int n_tiles_active = 0;
-  // staged sweep: tiles of STG_CELLS cells holding a non-solid cell
-  DevBuf<int32_t> stg_list;
-  int n_stg_active = 0;
-  int stg_grid[4] = {0, 0, 0, 0};
-  // nx and nx * ny are multiples of 16 bytes of elements (staged windows'
-  // read offsets known at compile time)
-  bool stg_rows_aligned = false;
+  // pair sweep: 64-cell tiles holding a non-solid cell
+  DevBuf<int32_t> pair_list;
+  int n_pair_tiles = 0;
   TileDirs tile_dirs[2];
   int tile_grid[2] = {0, 0};
   // persistent window-kernel grid per (parity, concurrent with the IBM chain)
@@ -285,7 +280,7 @@ struct Engine final : EngineBase {
     build_flags(wu);
     // Guard margin: shifted TMA windows of the odd step reach up to
     // nx*ny + nx + 1 cells (+ alignment slack and one tile) beyond a plane.
-    margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 2 * STG_CELLS + 128, 64) * 64;
+    margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 128, 64) * 64;
     f_alloc.alloc(size_t(Q) * plane + 2 * size_t(margin));
     CK(cudaMemsetAsync(f_alloc.p, 0, (size_t(Q) * plane + 2 * size_t(margin)) * sizeof(S), st));
     fp = f_alloc.p + margin;
@@ -300,7 +295,6 @@ struct Engine final : EngineBase {
     CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c.device));
     ntiles = ceil_div(n, TMA_TILE);
     rows_aligned = (nx % TmaWin<S>::PAD == 0) && ((int64_t(nx) * ny) % TmaWin<S>::PAD == 0);
-    stg_rows_aligned = (nx % (16 / int(sizeof(S))) == 0) && ((int64_t(nx) * ny) % (16 / int(sizeof(S))) == 0);
     // default sweep: the lean kernel where it applies (TRT/BGK, fp32/16-bit
     // storage, no uniform force), else cp.async (4/8-byte storage), the
     // window kernel (16-bit storage) or direct loads (uniform force)
@@ -378,12 +372,7 @@ struct Engine final : EngineBase {
           flags_h[c] = fl;
           nb[c] = m;
         }
-    // padded to whole staged tiles (and one more) with solid bytes: the
-    // staged sweep copies a tile's flags as one block
-    const size_t nflags = size_t(ceil_div(n, STG_CELLS) + 1) * STG_CELLS;
-    if (flags.n < nflags) flags.alloc(nflags);
-    CK(cudaMemsetAsync(flags.p, F_SOLID, nflags, st));
-    CK(cudaMemcpyAsync(flags.p, flags_h.data(), size_t(n), cudaMemcpyHostToDevice, st));
+    flags.upload(flags_h, st);
     nbr.upload(nb, st);
     wall_u.upload(w, st);
     CK(cudaStreamSynchronize(st));
@@ -564,10 +553,6 @@ struct Engine final : EngineBase {
       throw Error(LBMB_ERR_UNSUPPORTED, "the window sweep needs fp32/fp16/bf16 storage and no uniform body force");
     if (kind == LBMB_SWEEP_LEAN && !lean_ok(coll))
       throw Error(LBMB_ERR_UNSUPPORTED, "the lean sweep needs TRT/BGK, fp32/fp16/bf16 storage and no uniform body force");
-    if (kind == LBMB_SWEEP_STAGED && !staged_ok())
-      throw Error(LBMB_ERR_UNSUPPORTED,
-                  "the staged sweep needs TRT/BGK, fp32/fp16/bf16 storage, even nx, no uniform body force and no "
-                  "relaxation field");
     kernel_mode = kind;
     invalidate_graphs();
   }
@@ -596,13 +581,12 @@ struct Engine final : EngineBase {
       invalidate_graphs();
       return;
     }
-    if (kernel_mode == LBMB_SWEEP_STAGED) {
-      auto ok = [](int v) { return v >= 1 && v <= 3; };
+    if (kernel_mode == LBMB_SWEEP_PAIR) {
+      auto ok = [](int v) { return v >= 3 && v <= 5; };
       if (!ok(even) || !ok(odd))
-        throw Error(LBMB_ERR_INVALID, "sweep variant: staged resident blocks per SM must be 1, 2 or 3");
-      staged_minb[0] = even;
-      staged_minb[1] = odd;
-      for (int& g : stg_grid) g = 0;
+        throw Error(LBMB_ERR_INVALID, "sweep variant: pair resident blocks per SM must be 3, 4 or 5");
+      pair_minb[0] = even;
+      pair_minb[1] = odd;
       invalidate_graphs();
       return;
     }
@@ -669,24 +653,25 @@ struct Engine final : EngineBase {
         any = !(flags_h[size_t(c)] & F_SOLID);
       if (any) list.push_back(int32_t(t));
     }
+    {
+      // 64-cell warp tiles of the pair sweep holding a non-solid cell
+      const int64_t np = ceil_div(n, PAIR_TILE);
+      std::vector<int32_t> pl_;
+      for (int64_t t = 0; t < np; ++t) {
+        bool any = false;
+        for (int64_t c = t * PAIR_TILE; c < std::min<int64_t>(n, (t + 1) * PAIR_TILE) && !any; ++c)
+          any = !(flags_h[size_t(c)] & F_SOLID);
+        if (any) pl_.push_back(int32_t(t));
+      }
+      n_pair_tiles = int(pl_.size());
+      pair_list.alloc(pl_.size());
+      if (!pl_.empty())
+        CK(cudaMemcpyAsync(pair_list.p, pl_.data(), pl_.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    }
     n_tiles_active = int(list.size());
     tile_list.alloc(list.size());
     if (!list.empty())
       CK(cudaMemcpyAsync(tile_list.p, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    {
-      const int64_t ns = ceil_div(n, STG_CELLS);
-      std::vector<int32_t> sl;
-      for (int64_t t = 0; t < ns; ++t) {
-        bool any = false;
-        for (int64_t c = t * STG_CELLS; c < std::min<int64_t>(n, (t + 1) * STG_CELLS) && !any; ++c)
-          any = !(flags_h[size_t(c)] & F_SOLID);
-        if (any) sl.push_back(int32_t(t));
-      }
-      n_stg_active = int(sl.size());
-      stg_list.alloc(sl.size());
-      if (!sl.empty())
-        CK(cudaMemcpyAsync(stg_list.p, sl.data(), sl.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    }
     using L = Lat<Q>;
     const int64_t E = 16 / int64_t(sizeof(S));
     for (int q = 0; q < Q; ++q) {
@@ -757,57 +742,25 @@ struct Engine final : EngineBase {
     }
   }
 
-  // Resident 288-thread blocks per SM of the staged sweep, per parity.
-  int staged_minb[2] = {2, 2};
-  bool staged_ok() const {
-    return std::is_same<A, float>::value && coll == COLL_TRT && nx % 2 == 0 && !has_uniform_force() && !omega_on;
-  }
-
-  template <bool ODD, int MINB>
-  void launch_staged_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
-    if constexpr (std::is_same<A, float>::value) {
-      if (stg_rows_aligned) launch_staged_ra<ODD, MINB, true>(p, s, concurrent);
-      else launch_staged_ra<ODD, MINB, false>(p, s, concurrent);
-    }
-  }
-  template <bool ODD, int MINB, bool RA>
-  void launch_staged_ra(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
-    if constexpr (std::is_same<A, float>::value) {
-      constexpr int STAGES = sizeof(S) == 2 ? 4 : 2;
-      auto kern = hydro_staged_kernel<Q, S, ODD, STAGES, MINB, RA>;
-      const size_t smem = staged_smem_bytes<Q, S, STAGES>();
-      const int slot = (ODD ? 1 : 0) + (concurrent ? 2 : 0);
-      if (stg_grid[slot] == 0) {
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, STG_THREADS, smem));
-        // in a runner step leave block slots free for the IBM chain on the
-        // side stream, as the cp.async grid does
-        const int64_t reserve = concurrent ? int64_t(async_reserve) / 2 : 0;
-        const int64_t slots = int64_t(sm_count) * std::max(per_sm, 1) - reserve;
-        stg_grid[slot] = int(std::max<int64_t>(1, std::min<int64_t>(n_stg_active, slots)));
-      }
-      if (n_stg_active == 0) return;
-      kern<<<unsigned(stg_grid[slot]), STG_THREADS, smem, s>>>(p, stg_list.p, n_stg_active, tile_dirs[ODD], d_err.p,
-                                                               wait_limit);
+  // Resident 128-thread blocks per SM of the pair sweep, per parity
+  // (3 = 168 registers, 4 = 128, 5 = 96).
+  int pair_minb[2] = {4, 4};
+  template <bool ODD, int COLL, int MINB>
+  void launch_pair_mb(const HydroParams<A>& p, cudaStream_t s) {
+    if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
+      if (n_pair_tiles == 0) return;
+      const unsigned blocks = unsigned(ceil_div(n_pair_tiles, PAIR_BLOCK / 32));
+      hydro_pair_kernel<Q, S, ODD, MINB, COLL><<<blocks, PAIR_BLOCK, 0, s>>>(p, pair_list.p, n_pair_tiles,
+                                                                             uint32_t(n));
       CK(cudaGetLastError());
     }
   }
-  template <bool ODD>
-  void launch_staged(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
-    switch (staged_minb[ODD]) {
-      case 1: launch_staged_mb<ODD, 1>(p, s, concurrent); break;
-      case 3: launch_staged_mb<ODD, 3>(p, s, concurrent); break;
-      default: launch_staged_mb<ODD, 2>(p, s, concurrent); break;
-    }
-  }
-
   template <bool ODD, int COLL>
   void launch_pair(const HydroParams<A>& p, cudaStream_t s) {
-    if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
-      const uint32_t npairs = uint32_t(n / 2);
-      hydro_pair_kernel<Q, S, ODD, COLL><<<unsigned(ceil_div(npairs, PAIR_BLOCK)), PAIR_BLOCK, 0, s>>>(p, npairs);
-      CK(cudaGetLastError());
+    switch (pair_minb[ODD]) {
+      case 3: launch_pair_mb<ODD, COLL, 3>(p, s); return;
+      case 5: launch_pair_mb<ODD, COLL, 5>(p, s); return;
+      default: launch_pair_mb<ODD, COLL, 4>(p, s); return;
     }
   }
 
@@ -822,8 +775,7 @@ struct Engine final : EngineBase {
         launch_tile<ODD, COLL>(p, s);
       } else if (kernel_mode == LBMB_SWEEP_LEAN && lean_ok(COLL) && !p.uniform_force) {
         launch_lean<ODD>(p, s);
-      } else if (kernel_mode == LBMB_SWEEP_STAGED && COLL == COLL_TRT && staged_ok()) {
-        launch_staged<ODD>(p, s, !cells);
+
       } else if (!p.uniform_force && kernel_mode == 1) {
         if (rows_aligned) launch_tma<COLL, ODD, true>(p, s);
         else launch_tma<COLL, ODD, false>(p, s);
@@ -978,12 +930,12 @@ struct Engine final : EngineBase {
     // Asynchronous: the call returns once the work is queued (every other
     // entry point runs on the same stream, and the ones that return data
     // synchronize). The device time is resolved when it is asked for. The
-    // bulk-copy kernels are the only ones that can raise a device error
-    // flag, so their steps are checked at once.
+    // bulk-copy kernel is the only one that can raise a device error flag,
+    // so its steps are checked at once.
     pending_launches = launches;
     timing_pending = true;
     time += uint64_t(steps);
-    if (kernel_mode == LBMB_SWEEP_BULK || kernel_mode == LBMB_SWEEP_STAGED) {
+    if (kernel_mode == LBMB_SWEEP_BULK) {
       CK(cudaEventSynchronize(ev1));
       check_device_error();
     }
@@ -1038,7 +990,8 @@ struct Engine final : EngineBase {
     }
     if (!uf) cands.push_back({LBMB_SWEEP_BULK, 0, 0});
     if (is_f && nx % 2 == 0 && !uf && !omega_on) {
-      cands.push_back({LBMB_SWEEP_PAIR, 0, 0});
+      for (int ev = 3; ev <= 5; ++ev)
+        for (int od = 3; od <= 5; ++od) cands.push_back({LBMB_SWEEP_PAIR, ev, od});
       cands.push_back({LBMB_SWEEP_TILE, 0, 0});
     }
     if (window_ok()) {
@@ -1049,9 +1002,6 @@ struct Engine final : EngineBase {
     if (lean_ok(coll))
       for (int ev = 10; ev >= 6; --ev)
         for (int od = 9; od >= 6; --od) cands.push_back({LBMB_SWEEP_LEAN, ev, od});
-    if (staged_ok())
-      for (int ev = 1; ev <= 3; ++ev)
-        for (int od = 1; od <= 3; ++od) cands.push_back({LBMB_SWEEP_STAGED, ev, od});
     if (omega_on) {
       std::vector<Cand> keep;
       for (const Cand& cd : cands)
@@ -1061,7 +1011,7 @@ struct Engine final : EngineBase {
     const int kind0 = kernel_mode, ev0_ = lean_minb[0], od0 = lean_minb[1];
     const int ae0 = async_minb[0], ao0 = async_minb[1];
     const int we0 = window_minb[0], wo0 = window_minb[1];
-    const int se0 = staged_minb[0], so0 = staged_minb[1];
+    const int pe0 = pair_minb[0], po0 = pair_minb[1];
     const int par0 = parity;
     const size_t fbytes = f_alloc.n * sizeof(S);
     DevBuf<S> save;
@@ -1084,10 +1034,9 @@ struct Engine final : EngineBase {
         window_minb[1] = cd.od;
         for (int& g : window_grid) g = 0;
       }
-      if (cd.kind == LBMB_SWEEP_STAGED) {
-        staged_minb[0] = cd.ev;
-        staged_minb[1] = cd.od;
-        for (int& g : stg_grid) g = 0;
+      if (cd.kind == LBMB_SWEEP_PAIR) {
+        pair_minb[0] = cd.ev;
+        pair_minb[1] = cd.od;
       }
       for (int i = 0; i < 2; ++i) launch_hydro(i);  // warm-up (first launches set up grids)
       CK(cudaEventRecord(ev0, st));
@@ -1101,7 +1050,7 @@ struct Engine final : EngineBase {
     };
     const double t_default = trial(kind0 == LBMB_SWEEP_ASYNC    ? Cand{kind0, ae0, ao0}
                                    : kind0 == LBMB_SWEEP_WINDOW ? Cand{kind0, we0, wo0}
-                                   : kind0 == LBMB_SWEEP_STAGED ? Cand{kind0, se0, so0}
+                                   : kind0 == LBMB_SWEEP_PAIR   ? Cand{kind0, pe0, po0}
                                                                 : Cand{kind0, ev0_, od0});
     int best = -1;
     double best_ms = 0.0;
@@ -1142,16 +1091,15 @@ struct Engine final : EngineBase {
       window_minb[0] = we0;
       window_minb[1] = wo0;
     }
-    if (kernel_mode == LBMB_SWEEP_STAGED) {
-      staged_minb[0] = cands[best].ev;
-      staged_minb[1] = cands[best].od;
+    if (kernel_mode == LBMB_SWEEP_PAIR) {
+      pair_minb[0] = cands[best].ev;
+      pair_minb[1] = cands[best].od;
     } else {
-      staged_minb[0] = se0;
-      staged_minb[1] = so0;
+      pair_minb[0] = pe0;
+      pair_minb[1] = po0;
     }
     for (int& g : async_grid) g = 0;
     for (int& g : window_grid) g = 0;
-    for (int& g : stg_grid) g = 0;
     CK(cudaMemcpyAsync(f_alloc.p, save.p, fbytes, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
     parity = par0;
@@ -1160,7 +1108,7 @@ struct Engine final : EngineBase {
       out->kind = kernel_mode;
       const int* mb = kernel_mode == LBMB_SWEEP_ASYNC    ? async_minb
                       : kernel_mode == LBMB_SWEEP_WINDOW ? window_minb
-                      : kernel_mode == LBMB_SWEEP_STAGED ? staged_minb
+                      : kernel_mode == LBMB_SWEEP_PAIR   ? pair_minb
                                                          : lean_minb;
       out->even_blocks_per_sm = mb[0];
       out->odd_blocks_per_sm = mb[1];

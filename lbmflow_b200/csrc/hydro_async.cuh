@@ -20,11 +20,23 @@ namespace lbmb {
 // D3Q27 central-moment collision of one fp32 cell (no force) with the
 // x-opposite populations (-1, j, k) and (+1, j, k) of the 3 x 3 x 3 tensor
 // held together in a float2 (FP[j][k] = (f(-1, j-1, k-1), f(+1, j-1, k-1)),
-// F1[j][k] = f(0, j-1, k-1)): the equilibrium of both, the z and y passes of
-// the factorised transform and the final increment run as packed FFMA2 /
-// FADD2 / FMUL2 on the pairs, the x pass and the relaxation in scalar form.
-// Same operator as collide_cm<27, false, float, true> (the subgrid rate from
-// the transformed order-2 moments), with the packed operation order.
+// F1[j][k] = f(0, j-1, k-1)).
+//
+// The operator is the reference's (kernels.rs:406-533): with K = f - feq in
+// central moments about u, the post-collision moments keep order 0 and 1,
+// relax the order-2 deviatoric part at omega_s (1 - 0.16 |u|^2) capped at 2,
+// and relax the order-2 trace and every higher moment at 1, i.e. set them
+// to the equilibrium's. So f' = feq + T^-1 K' where K' holds only the five
+// deviatoric order-2 moments (1 - omega_s) (K_ab - tr K / 3 delta_ab); the
+// order-0/1 moments of f - feq are zero when u = j / rho (they are dropped
+// here: round-off), and the order-2 central moments of f - feq then equal
+// its raw ones, the non-equilibrium stress
+//   Pi_ab = sum_q c_a c_b f_q - rho u_a u_b - (rho - 1) / 3 delta_ab
+// (deviation form, second-order equilibrium). Only the backward transform
+// runs, on that sparse K': the x pass maps each of the six order-2 lines to
+// the three x velocities with fixed per-axis shape functions, then the y
+// and z passes of the factorised transform, packed on the x-opposite pairs
+// (FFMA2 / FADD2 / FMUL2). The subgrid rate comes from the same Pi.
 __device__ __forceinline__ void collide_cm_x2(float2 (&FP)[3][3], float (&F1)[3][3], float rho, float ux, float uy,
                                               float uz, float omega_shear, float les_c, float tau0) {
   using L = Lat<27>;
@@ -46,86 +58,107 @@ __device__ __forceinline__ void collide_cm_x2(float2 (&FP)[3][3], float (&F1)[3]
       }
     if (exact) return;
   }
+  // second moments of the populations
+  float sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float sp = FP[j][k].x + FP[j][k].y;  // c_x = +-1
+      const float dp = FP[j][k].y - FP[j][k].x;  // c_x f over the pair
+      const float s3 = sp + F1[j][k];
+      sxx += sp;
+      if (j != 1) syy += s3;
+      if (k != 1) szz += s3;
+      if (j == 2) sxy += dp;
+      if (j == 0) sxy -= dp;
+      if (k == 2) sxz += dp;
+      if (k == 0) sxz -= dp;
+      if (j != 1 && k != 1) syz = (j == k) ? syz + s3 : syz - s3;
+    }
+  const float d3 = drho * (1.f / 3.f);
+  const float pxx = (sxx - d3) - rho * ux * ux, pyy = (syy - d3) - rho * uy * uy, pzz = (szz - d3) - rho * uz * uz;
+  const float pxy = sxy - rho * ux * uy, pxz = sxz - rho * ux * uz, pyz = syz - rho * uy * uz;
   const float usq = (ux * ux + uy * uy) + uz * uz;
+  if (les_c > 0.f) {
+    const float pn = fast_sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz));
+    omega_shear = fast_rcp(0.5f * (tau0 + fast_sqrt(tau0 * tau0 + les_c * pn * fast_rcp(rho))));
+  }
+  const float os = fminf(omega_shear * (1.f + -0.16f * usq), 2.f);
+  const float keep = 1.f - os;
+  const float bulk = (pxx + pyy + pzz) * (1.f / 3.f);
+  const float k200 = keep * (pxx - bulk), k020 = keep * (pyy - bulk), k002 = keep * (pzz - bulk);
+  const float k110 = keep * pxy, k101 = keep * pxz, k011 = keep * pyz;
+  // x pass: per-axis shape functions of order 0, 1, 2 at c = (-1, +1) and 0
+  //   order 0: ((u^2 - u)/2, (u^2 + u)/2), 1 - u^2
+  //   order 1: (u - 1/2, u + 1/2), -2u
+  //   order 2: (1/2, 1/2), -1
+  const float ux2 = ux * ux;
+  const float2 s0 = make_float2(0.5f * (ux2 - ux), 0.5f * (ux2 + ux));
+  const float m0 = 1.f - ux2;
+  const float2 s1 = make_float2(ux - 0.5f, ux + 0.5f);
+  const float m1 = -2.f * ux;
+  // G[b][c]: the line (b, c) after the x pass, pair (c_x = -1, +1) and mid
+  // (c_x = 0); lines (1, 2), (2, 1), (2, 2) are zero
+  float2 GP[3][3];
+  float G1[3][3];
+  GP[0][0] = bc2(0.5f * k200);  G1[0][0] = -k200;            // (2, 0, 0)
+  GP[2][0] = mul2(s0, bc2(k020)); G1[2][0] = m0 * k020;      // (0, 2, 0)
+  GP[0][2] = mul2(s0, bc2(k002)); G1[0][2] = m0 * k002;      // (0, 0, 2)
+  GP[1][1] = mul2(s0, bc2(k011)); G1[1][1] = m0 * k011;      // (0, 1, 1)
+  GP[1][0] = mul2(s1, bc2(k110)); G1[1][0] = m1 * k110;      // (1, 1, 0)
+  GP[0][1] = mul2(s1, bc2(k101)); G1[0][1] = m1 * k101;      // (1, 0, 1)
+  const float2 uy2 = bc2(uy), uz2 = bc2(uz);
+  // y pass over b for each c: c = 0 full, c = 1 without order 2, c = 2 order 0 only
+  cm_bwd2(GP[0][0], GP[1][0], GP[2][0], uy2);
+  cm_bwd(G1[0][0], G1[1][0], G1[2][0], uy);
+  {
+    // (k0, k1, 0): m1 = k1 + u k0, m2 = u (u k0 + 2 k1)
+    const float2 k0 = GP[0][1], k1 = GP[1][1];
+    const float2 p1 = fma2(uy2, k0, k1);
+    const float2 p2 = mul2(uy2, fma2(uy2, k0, mul2(bc2(2.f), k1)));
+    GP[0][1] = mul2(bc2(0.5f), sub2(p2, p1));
+    GP[1][1] = sub2(k0, p2);
+    GP[2][1] = mul2(bc2(0.5f), add2(p2, p1));
+    const float q0 = G1[0][1], q1 = G1[1][1];
+    const float r1 = q1 + uy * q0;
+    const float r2 = uy * (uy * q0 + 2.f * q1);
+    G1[0][1] = 0.5f * (r2 - r1);
+    G1[1][1] = q0 - r2;
+    G1[2][1] = 0.5f * (r2 + r1);
+  }
+  {
+    const float uy_2 = uy * uy;
+    const float t0 = 0.5f * (uy_2 - uy), t1 = 1.f - uy_2, t2 = 0.5f * (uy_2 + uy);
+    const float2 k0 = GP[0][2];
+    const float q0 = G1[0][2];
+    GP[0][2] = mul2(bc2(t0), k0);
+    GP[1][2] = mul2(bc2(t1), k0);
+    GP[2][2] = mul2(bc2(t2), k0);
+    G1[0][2] = t0 * q0;
+    G1[1][2] = t1 * q0;
+    G1[2][2] = t2 * q0;
+  }
+  // z pass over c for each b
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    cm_bwd2(GP[j][0], GP[j][1], GP[j][2], uz2);
+    cm_bwd(G1[j][0], G1[j][1], G1[j][2], uz);
+  }
+  // f' = feq + the transformed increment
   const float2 uxpm = make_float2(-ux, ux);
   const float2 drho2 = bc2(drho), rho2 = bc2(rho), nusq2 = bc2(-1.5f * usq);
-  float2 KP[3][3];
-  float K1[3][3];
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const int nz = (j != 1) + (k != 1);
       const float v = float(j - 1) * uy + float(k - 1) * uz;
-      {
-        const float inner = (3.f * v + (4.5f * v) * v) - 1.5f * usq;
-        K1[j][k] = F1[j][k] - wgt(nz) * (drho + rho * inner);
-      }
+      const float inner1 = (3.f * v + (4.5f * v) * v) - 1.5f * usq;
+      F1[j][k] = wgt(nz) * (drho + rho * inner1) + G1[j][k];
       const float2 cu = add2(bc2(v), uxpm);
       const float2 inner = fma2(cu, fma2(bc2(4.5f), cu, bc2(3.f)), nusq2);
-      KP[j][k] = sub2(FP[j][k], mul2(bc2(wgt(nz + 1)), fma2(rho2, inner, drho2)));
-    }
-  // forward: z, y (packed pairs + the c_x = 0 plane), x (scalar)
-  const float2 uz2 = bc2(uz), uy2 = bc2(uy);
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    cm_fwd2(KP[j][0], KP[j][1], KP[j][2], uz2);
-    cm_fwd(K1[j][0], K1[j][1], K1[j][2], uz);
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    cm_fwd2(KP[0][k], KP[1][k], KP[2][k], uy2);
-    cm_fwd(K1[0][k], K1[1][k], K1[2][k], uy);
-  }
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cm_fwd(KP[j][k].x, K1[j][k], KP[j][k].y, ux);
-  // central moment (a, b, c): a = 0 -> KP[b][c].x, a = 1 -> K1[b][c], a = 2 -> KP[b][c].y
-  auto km = [&](int a, int b, int c) -> float& { return a == 0 ? KP[b][c].x : (a == 1 ? K1[b][c] : KP[b][c].y); };
-  if (les_c > 0.f) {
-    const float pxx = km(2, 0, 0), pyy = km(0, 2, 0), pzz = km(0, 0, 2);
-    const float pxy = km(1, 1, 0), pxz = km(1, 0, 1), pyz = km(0, 1, 1);
-    const float pn = fast_sqrt((pxx * pxx + pyy * pyy + pzz * pzz) + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz));
-    omega_shear = fast_rcp(0.5f * (tau0 + fast_sqrt(tau0 * tau0 + les_c * pn * fast_rcp(rho))));
-  }
-  const float os = fminf(omega_shear * (1.f + -0.16f * usq), 2.f);
-  const float bulk_neq = (km(2, 0, 0) + km(0, 2, 0) + km(0, 0, 2)) * (1.f / 3.f);
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int order = a + b + c;
-        const bool diag = order == 2 && (a == 2 || b == 2 || c == 2);
-        float& k = km(a, b, c);
-        if (order <= 1) k = 0.f;
-        else if (diag) k = -os * (k - bulk_neq) - bulk_neq;
-        else if (order == 2) k = -os * k;
-        else k = -k;
-      }
-  // backward: x (scalar), y, z (packed pairs + the c_x = 0 plane)
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cm_bwd(KP[j][k].x, K1[j][k], KP[j][k].y, ux);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    cm_bwd2(KP[0][k], KP[1][k], KP[2][k], uy2);
-    cm_bwd(K1[0][k], K1[1][k], K1[2][k], uy);
-  }
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    cm_bwd2(KP[j][0], KP[j][1], KP[j][2], uz2);
-    cm_bwd(K1[j][0], K1[j][1], K1[j][2], uz);
-  }
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      FP[j][k] = add2(FP[j][k], KP[j][k]);
-      F1[j][k] = F1[j][k] + K1[j][k];
+      FP[j][k] = fma2(bc2(wgt(nz + 1)), fma2(rho2, inner, drho2), GP[j][k]);
     }
 }
 

@@ -1,5 +1,6 @@
 // Two cells per thread AA collide-stream with packed fp32x2 arithmetic
-// (TRT / BGK, no uniform body force, fp32 | fp16 | bf16 storage).
+// (TRT / BGK or D3Q27 central moment, no uniform body force, fp32 | fp16 |
+// bf16 storage).
 //
 // Thread i owns the x-adjacent cells c = 2i and c + 1 (nx even, so a pair
 // never straddles a row and every plane offset q * plane + c is even).
@@ -26,6 +27,7 @@
 // accesses for that direction only. Cells inside IBM stencils are left to
 // hydro_cells_kernel; cells on a periodic face take the generic path.
 #pragma once
+#include <cuda_fp16.h>
 #include "hydro.cuh"
 
 namespace lbmb {
@@ -118,33 +120,27 @@ __device__ __forceinline__ float les_tau_pair(const float (&s)[6], float rho, fl
   return 0.5f * (tau0 + sqrt_fast(tau0 * tau0 + les_c * pn * inv_rho));
 }
 
-// TRT collision of two cells held in float2 lanes; returns rho (for the
-// moving-wall term).
+// TRT collision of two cells in float2 lanes in register-lean form: the
+// operator of trt_pair_collide (hydro_pair.cuh), with the pair sums
+// S = f_a + f_b and differences D = f_a - f_b recomputed where they are used
+// instead of being held for all pairs (the form of trt_lean_collide).
 template <int Q>
-__device__ __forceinline__ float2 trt_pair_collide(float2 (&f)[Q], const HydroParams<float>& p) {
+__device__ __forceinline__ float2 trt_pair_lean(float2 (&f)[Q], const HydroParams<float>& p) {
   using L = Lat<Q>;
   constexpr int NP = (Q - 1) / 2;
   static_assert(pair_heads_positive<Q>(), "pair head convention");
-  float2 S[NP], D[NP];
+  float2 drho = f[0], jx = bc2(0.f), jy = bc2(0.f), jz = bc2(0.f);
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    S[k] = add2(f[2 * k + 1], f[2 * k + 2]);
-    D[k] = sub2(f[2 * k + 1], f[2 * k + 2]);
-  }
-  float2 drho = add2(f[0], S[0]);
-#pragma unroll
-  for (int k = 1; k < NP; ++k) drho = add2(drho, S[k]);
-  // pairs 0, 1, 2 are the +x, +y, +z axis links
-  float2 jx = D[0], jy = D[1], jz = D[2];
-#pragma unroll
-  for (int k = 3; k < NP; ++k) {
-    const int a = 2 * k + 1;
-    if (L::cx(a) == 1) jx = add2(jx, D[k]);
-    if (L::cx(a) == -1) jx = sub2(jx, D[k]);
-    if (L::cy(a) == 1) jy = add2(jy, D[k]);
-    if (L::cy(a) == -1) jy = sub2(jy, D[k]);
-    if (L::cz(a) == 1) jz = add2(jz, D[k]);
-    if (L::cz(a) == -1) jz = sub2(jz, D[k]);
+    const int a = 2 * k + 1, b = a + 1;
+    drho = add2(drho, add2(f[a], f[b]));
+    const float2 d = sub2(f[a], f[b]);
+    if (L::cx(a) == 1) jx = add2(jx, d);
+    if (L::cx(a) == -1) jx = sub2(jx, d);
+    if (L::cy(a) == 1) jy = add2(jy, d);
+    if (L::cy(a) == -1) jy = sub2(jy, d);
+    if (L::cz(a) == 1) jz = add2(jz, d);
+    if (L::cz(a) == -1) jz = sub2(jz, d);
   }
   const float2 rho = add2(drho, bc2(1.f));
   const float2 inv = make_float2(rcp_fast(rho.x), rcp_fast(rho.y));
@@ -152,30 +148,25 @@ __device__ __forceinline__ float2 trt_pair_collide(float2 (&f)[Q], const HydroPa
   const float2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
   float2 op = bc2(p.omega_p), om = bc2(p.omega_m);
   if (p.les_c > 0.f) {
-    float s[2][6];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int i = 0; i < 6; ++i) s[h][i] = 0.f;
+    // second moments of the pair sums, both lanes at once
+    float2 s6[6] = {bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f)};
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       const int a = 2 * k + 1;
       const int cx = L::cx(a), cy = L::cy(a), cz = L::cz(a);
-      const float sv[2] = {S[k].x, S[k].y};
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (cx) s[h][0] += sv[h];
-        if (cy) s[h][1] += sv[h];
-        if (cz) s[h][2] += sv[h];
-        if (cx && cy) s[h][3] += float(cx * cy) * sv[h];
-        if (cx && cz) s[h][4] += float(cx * cz) * sv[h];
-        if (cy && cz) s[h][5] += float(cy * cz) * sv[h];
-      }
+      const float2 sv = add2(f[a], f[a + 1]);
+      if (cx) s6[0] = add2(s6[0], sv);
+      if (cy) s6[1] = add2(s6[1], sv);
+      if (cz) s6[2] = add2(s6[2], sv);
+      if (cx && cy) s6[3] = cx * cy > 0 ? add2(s6[3], sv) : sub2(s6[3], sv);
+      if (cx && cz) s6[4] = cx * cz > 0 ? add2(s6[4], sv) : sub2(s6[4], sv);
+      if (cy && cz) s6[5] = cy * cz > 0 ? add2(s6[5], sv) : sub2(s6[5], sv);
     }
-    const float te0 = les_tau_pair<Q>(s[0], rho.x, inv.x, ux.x, uy.x, uz.x, p.les_c, p.tau0);
-    const float te1 = les_tau_pair<Q>(s[1], rho.y, inv.y, ux.y, uy.y, uz.y, p.les_c, p.tau0);
+    const float sa[6] = {s6[0].x, s6[1].x, s6[2].x, s6[3].x, s6[4].x, s6[5].x};
+    const float sb[6] = {s6[0].y, s6[1].y, s6[2].y, s6[3].y, s6[4].y, s6[5].y};
+    const float te0 = les_tau_pair<Q>(sa, rho.x, inv.x, ux.x, uy.x, uz.x, p.les_c, p.tau0);
+    const float te1 = les_tau_pair<Q>(sb, rho.y, inv.y, ux.y, uy.y, uz.y, p.les_c, p.tau0);
     op = make_float2(rcp_fast(te0), rcp_fast(te1));
-    // omega- = 1 / (magic / (tau - 1/2) + 1/2) = (tau - 1/2) / (magic + (tau - 1/2) / 2)
     if (p.magic > 0.f) {
       const float l0 = te0 - 0.5f, l1 = te1 - 0.5f;
       om = make_float2(l0 * rcp_fast(p.magic + 0.5f * l0), l1 * rcp_fast(p.magic + 0.5f * l1));
@@ -183,55 +174,36 @@ __device__ __forceinline__ float2 trt_pair_collide(float2 (&f)[Q], const HydroPa
       om = op;
     }
   }
-  // base = drho - 1.5 rho u^2 (feq of the rest population is w0 * base)
   const float2 base = fma2(mul2(rho, bc2(-1.5f)), usq, drho);
   const float2 nhop = mul2(op, bc2(-0.5f)), hom = mul2(om, bc2(0.5f));
-  float2 oA[3], oB[3], nC[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const int a = k == 0 ? 1 : (k == 1 ? 7 : 19);
-    if (a >= Q) continue;
-    const float w = float(L::w(a));
-    oA[k] = mul2(mul2(op, bc2(w)), base);
-    oB[k] = mul2(mul2(op, bc2(4.5f * w)), rho);
-    nC[k] = mul2(mul2(om, bc2(-3.f * w)), rho);
-  }
   f[0] = fma2(sub2(bc2(1.f), op), f[0], mul2(mul2(op, bc2(float(L::w(0)))), base));
+  // the pairs come in weight classes (axis, face diagonal, corner) in
+  // direction order; a class's coefficients are formed where it starts
+  float2 oA = bc2(0.f), oB = bc2(0.f), nC = bc2(0.f);
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
     const int a = 2 * k + 1, b = a + 1;
-    const int cl = wclass<Q>(a);
+    if (k == 0 || wclass<Q>(a) != wclass<Q>(a - 2)) {
+      const float w = float(L::w(a));
+      oA = mul2(mul2(op, bc2(w)), base);
+      oB = mul2(mul2(op, bc2(4.5f * w)), rho);
+      nC = mul2(mul2(om, bc2(-3.f * w)), rho);
+    }
     float2 cu = L::cx(a) ? ux : (L::cy(a) ? uy : uz);
     if (L::cx(a) && L::cy(a)) cu = L::cy(a) > 0 ? add2(cu, uy) : sub2(cu, uy);
     if ((L::cx(a) || L::cy(a)) && L::cz(a)) cu = L::cz(a) > 0 ? add2(cu, uz) : sub2(cu, uz);
-    const float2 t = fma2(oB[cl], mul2(cu, cu), oA[cl]);
-    const float2 pn = fma2(nhop, S[k], t);            // -rp
-    const float2 m = fma2(nC[cl], cu, mul2(hom, D[k]));  // rm
+    const float2 t = fma2(oB, mul2(cu, cu), oA);
+    const float2 pn = fma2(nhop, add2(f[a], f[b]), t);          // -rp
+    const float2 m = fma2(nC, cu, mul2(hom, sub2(f[a], f[b])));  // rm
     f[a] = sub2(add2(f[a], pn), m);
     f[b] = add2(add2(f[b], pn), m);
   }
   return rho;
 }
 
-// Central-moment collision (kernels.rs:406-533, no force term) of two cells
-// in float2 lanes, in the form that keeps one set of 27 values live:
-//   K = f - feq;  K <- T K (factorised central-moment transform);
-//   K <- (I - R) K  (order <= 1 kept, order-2 deviatoric at 1 - w_s, trace
-//                    and order >= 3 to zero);
-//   f' = feq + T^-1 K
-// which is the same operator as f + T^-1[-R T(f - feq)] by linearity. The
-// exact-rest skip (kernels.rs:434-447) zeroes K of a lane whose populations
-// all equal w (rho - 1), so that lane comes back unchanged.
-__device__ __forceinline__ void cm_fwd2(float2& a, float2& b, float2& c, float2 u) {
-  const float2 k0 = add2(add2(a, b), c);
-  const float2 d = sub2(c, a);
-  const float2 s = add2(c, a);
-  const float2 k1 = fma2(mul2(u, bc2(-1.f)), k0, d);
-  const float2 k2 = fma2(mul2(u, u), k0, fma2(mul2(u, bc2(-2.f)), d, s));
-  a = k0;
-  b = k1;
-  c = k2;
-}
+// Backward central-moment transform of one line (the values at c = -1, 0,
+// +1 from the central moments of order 0, 1, 2 about u; cm_bwd of hydro.cuh)
+// on float2 lanes.
 __device__ __forceinline__ void cm_bwd2(float2& k0, float2& k1, float2& k2, float2 u) {
   const float2 m1 = fma2(u, k0, k1);
   const float2 m2 = fma2(mul2(u, u), k0, fma2(mul2(u, bc2(2.f)), k1, k2));
@@ -243,52 +215,44 @@ __device__ __forceinline__ void cm_bwd2(float2& k0, float2& k1, float2& k2, floa
   k2 = fp;
 }
 
+// D3Q27 central-moment collision (kernels.rs:406-533, no force) of two
+// cells in float2 lanes, in the regularized form of collide_cm_x2
+// (hydro_async.cuh): f' = feq + T^-1 K', where K' holds only the five
+// deviatoric order-2 central moments (1 - omega_s)(Pi - tr Pi / 3) of the
+// non-equilibrium stress Pi; the backward transform runs on that sparse
+// vector (x pass by fixed per-axis shape functions, then the y and z passes
+// of the factorised transform). A lane at exact rest (u = 0 and every
+// population w (rho - 1), kernels.rs:434-447) keeps its populations.
 template <int Q>
-__device__ __forceinline__ float2 cm_pair_collide(float2 (&f)[Q], const HydroParams<float>& p) {
+__device__ __forceinline__ float2 cm_pair_reg(float2 (&f)[Q], const HydroParams<float>& p) {
   static_assert(Q == 27, "central moments need the full D3Q27 tensor basis");
   using L = Lat<Q>;
   constexpr int NP = (Q - 1) / 2;
   float2 drho = f[0], jx = bc2(0.f), jy = bc2(0.f), jz = bc2(0.f);
-  float s6[2][6] = {{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+  float2 sxx = bc2(0.f), syy = bc2(0.f), szz = bc2(0.f), sxy = bc2(0.f), sxz = bc2(0.f), syz = bc2(0.f);
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
     const int a = 2 * k + 1, b = a + 1;
+    const int cx = L::cx(a), cy = L::cy(a), cz = L::cz(a);
     const float2 S = add2(f[a], f[b]), D = sub2(f[a], f[b]);
     drho = add2(drho, S);
-    if (L::cx(a) == 1) jx = add2(jx, D);
-    if (L::cx(a) == -1) jx = sub2(jx, D);
-    if (L::cy(a) == 1) jy = add2(jy, D);
-    if (L::cy(a) == -1) jy = sub2(jy, D);
-    if (L::cz(a) == 1) jz = add2(jz, D);
-    if (L::cz(a) == -1) jz = sub2(jz, D);
+    if (cx == 1) jx = add2(jx, D);
+    if (cx == -1) jx = sub2(jx, D);
+    if (cy == 1) jy = add2(jy, D);
+    if (cy == -1) jy = sub2(jy, D);
+    if (cz == 1) jz = add2(jz, D);
+    if (cz == -1) jz = sub2(jz, D);
+    if (cx) sxx = add2(sxx, S);
+    if (cy) syy = add2(syy, S);
+    if (cz) szz = add2(szz, S);
+    if (cx && cy) sxy = cx * cy > 0 ? add2(sxy, S) : sub2(sxy, S);
+    if (cx && cz) sxz = cx * cz > 0 ? add2(sxz, S) : sub2(sxz, S);
+    if (cy && cz) syz = cy * cz > 0 ? add2(syz, S) : sub2(syz, S);
   }
   const float2 rho = add2(drho, bc2(1.f));
   const float2 inv = make_float2(rcp_fast(rho.x), rcp_fast(rho.y));
   const float2 ux = mul2(jx, inv), uy = mul2(jy, inv), uz = mul2(jz, inv);
-  const float2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
-  float2 os = bc2(p.omega_shear);
-  if (p.les_c > 0.f) {
-#pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      const int a = 2 * k + 1;
-      const int cx = L::cx(a), cy = L::cy(a), cz = L::cz(a);
-      const float2 S = add2(f[a], f[a + 1]);
-      const float sv[2] = {S.x, S.y};
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (cx) s6[h][0] += sv[h];
-        if (cy) s6[h][1] += sv[h];
-        if (cz) s6[h][2] += sv[h];
-        if (cx && cy) s6[h][3] += float(cx * cy) * sv[h];
-        if (cx && cz) s6[h][4] += float(cx * cz) * sv[h];
-        if (cy && cz) s6[h][5] += float(cy * cz) * sv[h];
-      }
-    }
-    const float te0 = les_tau_pair<Q>(s6[0], rho.x, inv.x, ux.x, uy.x, uz.x, p.les_c, p.tau0);
-    const float te1 = les_tau_pair<Q>(s6[1], rho.y, inv.y, ux.y, uy.y, uz.y, p.les_c, p.tau0);
-    os = make_float2(rcp_fast(te0), rcp_fast(te1));
-  }
-  // exact rest (per lane): u == 0 and every population == w (rho - 1)
+  // exact rest (per lane)
   bool rest0 = ux.x == 0.f && uy.x == 0.f && uz.x == 0.f;
   bool rest1 = ux.y == 0.f && uy.y == 0.f && uz.y == 0.f;
   if (rest0 || rest1) {
@@ -299,70 +263,92 @@ __device__ __forceinline__ float2 cm_pair_collide(float2 (&f)[Q], const HydroPar
     }
     if (rest0 && rest1) return rho;
   }
-  auto feq = [&](int q) {
-    float2 cu = L::cx(q) ? (L::cx(q) > 0 ? ux : mul2(ux, bc2(-1.f))) : bc2(0.f);
-    if (L::cy(q)) cu = L::cy(q) > 0 ? add2(cu, uy) : sub2(cu, uy);
-    if (L::cz(q)) cu = L::cz(q) > 0 ? add2(cu, uz) : sub2(cu, uz);
-    // w (drho + rho (3 cu + 4.5 cu^2 - 1.5 u^2))
-    const float2 inner = fma2(cu, fma2(bc2(4.5f), cu, bc2(3.f)), mul2(bc2(-1.5f), usq));
-    return mul2(bc2(float(L::w(q))), fma2(rho, inner, drho));
+  const float2 d3 = mul2(drho, bc2(1.f / 3.f));
+  const float2 pxx = sub2(sub2(sxx, d3), mul2(mul2(rho, ux), ux));
+  const float2 pyy = sub2(sub2(syy, d3), mul2(mul2(rho, uy), uy));
+  const float2 pzz = sub2(sub2(szz, d3), mul2(mul2(rho, uz), uz));
+  const float2 pxy = sub2(sxy, mul2(mul2(rho, ux), uy));
+  const float2 pxz = sub2(sxz, mul2(mul2(rho, ux), uz));
+  const float2 pyz = sub2(syz, mul2(mul2(rho, uy), uz));
+  const float2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
+  float2 os = bc2(p.omega_shear);
+  if (p.les_c > 0.f) {
+    const float2 q2 = fma2(pxx, pxx, fma2(pyy, pyy, mul2(pzz, pzz)));
+    const float2 o2 = fma2(pxy, pxy, fma2(pxz, pxz, mul2(pyz, pyz)));
+    const float2 n2 = fma2(bc2(2.f), o2, q2);
+    const float t0 = p.tau0;
+    const float te0 = 0.5f * (t0 + sqrt_fast(t0 * t0 + p.les_c * sqrt_fast(n2.x) * inv.x));
+    const float te1 = 0.5f * (t0 + sqrt_fast(t0 * t0 + p.les_c * sqrt_fast(n2.y) * inv.y));
+    os = make_float2(rcp_fast(te0), rcp_fast(te1));
+  }
+  const float2 osc = fma2(os, mul2(usq, bc2(-0.16f)), os);
+  const float2 keep = sub2(bc2(1.f), make_float2(fminf(osc.x, 2.f), fminf(osc.y, 2.f)));
+  const float2 bulk = mul2(add2(add2(pxx, pyy), pzz), bc2(1.f / 3.f));
+  const float2 k200 = mul2(keep, sub2(pxx, bulk)), k020 = mul2(keep, sub2(pyy, bulk));
+  const float2 k002 = mul2(keep, sub2(pzz, bulk));
+  const float2 k110 = mul2(keep, pxy), k101 = mul2(keep, pxz), k011 = mul2(keep, pyz);
+  // x pass: G[a][b][c], a = c_x + 1, on the six order-2 lines (b, c)
+  const float2 ux2 = mul2(ux, ux);
+  const float2 s0m = mul2(bc2(0.5f), sub2(ux2, ux)), s0p = mul2(bc2(0.5f), add2(ux2, ux));
+  const float2 s00 = sub2(bc2(1.f), ux2);
+  const float2 s1m = sub2(ux, bc2(0.5f)), s1p = add2(ux, bc2(0.5f));
+  const float2 s10 = mul2(ux, bc2(-2.f));
+  float2 G[3][3][3];
+  auto line0 = [&](int b, int c, float2 k) {  // order 0 along x
+    G[0][b][c] = mul2(s0m, k);
+    G[1][b][c] = mul2(s00, k);
+    G[2][b][c] = mul2(s0p, k);
   };
-  float2 K[3][3][3];
+  auto line1 = [&](int b, int c, float2 k) {  // order 1 along x
+    G[0][b][c] = mul2(s1m, k);
+    G[1][b][c] = mul2(s10, k);
+    G[2][b][c] = mul2(s1p, k);
+  };
+  G[0][0][0] = mul2(bc2(0.5f), k200);  // order 2 along x
+  G[1][0][0] = mul2(bc2(-1.f), k200);
+  G[2][0][0] = G[0][0][0];
+  line0(2, 0, k020);
+  line0(0, 2, k002);
+  line0(1, 1, k011);
+  line1(1, 0, k110);
+  line1(0, 1, k101);
+  // y pass over b for each (a, c): c = 0 full, c = 1 without order 2,
+  // c = 2 order 0 only
+  const float2 uy2 = mul2(uy, uy);
+  const float2 t0m = mul2(bc2(0.5f), sub2(uy2, uy)), t0p = mul2(bc2(0.5f), add2(uy2, uy));
+  const float2 t00 = sub2(bc2(1.f), uy2);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = sub2(f[q], feq(q));
-  if (rest0 || rest1) {
-#pragma unroll
-    for (int i = 0; i < 27; ++i) {
-      float2& k = K[i / 9][(i / 3) % 3][i % 3];
-      if (rest0) k.x = 0.f;
-      if (rest1) k.y = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    cm_bwd2(G[a][0][0], G[a][1][0], G[a][2][0], uy);
+    {
+      const float2 k0 = G[a][0][1], k1 = G[a][1][1];
+      const float2 m1 = fma2(uy, k0, k1);
+      const float2 m2 = mul2(uy, fma2(uy, k0, mul2(bc2(2.f), k1)));
+      G[a][0][1] = mul2(bc2(0.5f), sub2(m2, m1));
+      G[a][1][1] = sub2(k0, m2);
+      G[a][2][1] = mul2(bc2(0.5f), add2(m2, m1));
+    }
+    {
+      const float2 k0 = G[a][0][2];
+      G[a][0][2] = mul2(t0m, k0);
+      G[a][1][2] = mul2(t00, k0);
+      G[a][2][2] = mul2(t0p, k0);
     }
   }
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) cm_fwd2(K[i][j][0], K[i][j][1], K[i][j][2], uz);
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cm_fwd2(K[i][0][k], K[i][1][k], K[i][2][k], uy);
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cm_fwd2(K[0][j][k], K[1][j][k], K[2][j][k], ux);
-  // deviatoric rate w_s (1 - 0.16 |u|^2) capped at 2
-  const float2 ws = make_float2(fminf(os.x * (1.f - 0.16f * usq.x), 2.f), fminf(os.y * (1.f - 0.16f * usq.y), 2.f));
-  const float2 keep = sub2(bc2(1.f), ws);
-  const float2 bulk = mul2(bc2(1.f / 3.f), add2(add2(K[2][0][0], K[0][2][0]), K[0][0][2]));
+  // z pass over c for each (a, b)
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int b = 0; b < 3; ++b)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int order = a + b + c;
-        const bool diag = order == 2 && (a == 2 || b == 2 || c == 2);
-        if (order <= 1) continue;
-        if (diag) K[a][b][c] = mul2(keep, sub2(K[a][b][c], bulk));
-        else if (order == 2) K[a][b][c] = mul2(keep, K[a][b][c]);
-        else K[a][b][c] = bc2(0.f);
-      }
-#pragma unroll
-  for (int j = 0; j < 3; ++j)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cm_bwd2(K[0][j][k], K[1][j][k], K[2][j][k], ux);
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cm_bwd2(K[i][0][k], K[i][1][k], K[i][2][k], uy);
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) cm_bwd2(K[i][j][0], K[i][j][1], K[i][j][2], uz);
+    for (int b = 0; b < 3; ++b) cm_bwd2(G[a][b][0], G[a][b][1], G[a][b][2], uz);
+  // f' = feq + G: w (drho + rho (3 cu + 4.5 cu^2 - 1.5 u^2))
+  const float2 nusq = mul2(bc2(-1.5f), usq);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    const float2 v = add2(feq(q), K[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1]);
-    // a lane at exact rest keeps its populations bit for bit
+    float2 cu = L::cx(q) ? (L::cx(q) > 0 ? ux : mul2(ux, bc2(-1.f))) : bc2(0.f);
+    if (L::cy(q)) cu = L::cy(q) > 0 ? add2(cu, uy) : sub2(cu, uy);
+    if (L::cz(q)) cu = L::cz(q) > 0 ? add2(cu, uz) : sub2(cu, uz);
+    const float2 inner = fma2(cu, fma2(bc2(4.5f), cu, bc2(3.f)), nusq);
+    const float2 v = fma2(bc2(float(L::w(q))), fma2(rho, inner, drho), G[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1]);
     f[q].x = rest0 ? f[q].x : v.x;
     f[q].y = rest1 ? f[q].y : v.y;
   }
@@ -372,23 +358,77 @@ __device__ __forceinline__ float2 cm_pair_collide(float2 (&f)[Q], const HydroPar
 // Collision of a pair in the chosen form.
 template <int Q, int COLL>
 __device__ __forceinline__ float2 pair_collide(float2 (&f)[Q], const HydroParams<float>& p) {
-  if constexpr (COLL == COLL_CM) return cm_pair_collide<Q>(f, p);
-  else return trt_pair_collide<Q>(f, p);
+  if constexpr (COLL == COLL_CM) return cm_pair_reg<Q>(f, p);
+  else return trt_pair_lean<Q>(f, p);
 }
 
-template <int Q, class S, bool ODD, int COLL = COLL_TRT>
-__global__ void __launch_bounds__(PAIR_BLOCK, COLL == COLL_CM ? 2 : 4) hydro_pair_kernel(HydroParams<float> p, uint32_t npairs) {
+// The two elements at e and e + 1 of a 16-bit array where e is odd: the two
+// aligned 4-byte words that hold them, merged (neighbouring threads load the
+// same words, so the second load hits L1).
+template <class S>
+__device__ __forceinline__ float2 ld2_odd(const S* p) {
+  if constexpr (sizeof(S) == 2) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(p - 1);
+    uint32_t v = __byte_perm(w[0], w[1], 0x5432);
+    if constexpr (std::is_same<S, __half>::value) return __half22float2(*reinterpret_cast<__half2*>(&v));
+    else return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162*>(&v));
+  } else {
+    return make_float2(PairIO<S>::ld1(p), PairIO<S>::ld1(p + 1));
+  }
+}
+
+// Pair sweep: two x-adjacent cells per thread, one warp per 64-cell tile of
+// a compacted list (tiles with a non-solid cell), direct accesses of at
+// least 4 bytes wherever the pair is aligned (TRT / BGK, or the central
+// moment on D3Q27; fp32 | fp16 | bf16 storage). With 2-byte storage, warps
+// of one-element accesses reach about 0.73 of the copy bandwidth even
+// without arithmetic, 4-byte pair accesses reach the copy bandwidth, and
+// the packed collisions (trt_pair_lean, cm_pair_reg) halve the arithmetic
+// instructions.
+//   even step: own slots, aligned pair loads and stores for every direction;
+//   odd step:  slot opp(q) of x - c_q and slot q of x + c_q; directions with
+//              c_x = 0 stay aligned, the others read the two aligned words
+//              around the pair and store two elements.
+// The population loads are issued together with the flag load (every
+// address is inside the allocation whatever the flags say), so a tile costs
+// one memory round trip; the solid-neighbour masks are loaded only by warps
+// with a wall cell (warp-uniform vote). Cells on a periodic face, under the
+// free-slip top or next to a moving wall take the generic path; IBM-forced
+// cells are left to hydro_cells_kernel.
+constexpr int PAIR_TILE = 64;
+
+template <int Q, class S, bool ODD, int MINB, int COLL>
+__global__ void __launch_bounds__(PAIR_BLOCK, MINB)
+    hydro_pair_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, uint32_t ncells) {
   using L = Lat<Q>;
   using IO = PairIO<S>;
-  const uint32_t pi = blockIdx.x * PAIR_BLOCK + threadIdx.x;
-  if (pi >= npairs) return;
-  const uint32_t c = 2 * pi;
-  const uint32_t fl2 = reinterpret_cast<const uint16_t*>(p.flags)[pi];
+  const int lane = threadIdx.x & 31;
+  const int w = int((blockIdx.x * PAIR_BLOCK + threadIdx.x) >> 5);
+  if (w >= ntiles) return;
+  const uint32_t c = uint32_t(__ldg(tiles + w)) * PAIR_TILE + 2 * uint32_t(lane);
+  const int nx = p.nx, nxy = p.nxy;
+  const int64_t pl = int64_t(p.plane);
+  // element offsets from the pair's first cell: own slot k, and slot k of
+  // the neighbour x + c_k (uniform across the grid)
+  auto P = [&](int k) { return int32_t(int64_t(k) * pl); };
+  auto T = [&](int k) { return int32_t(int64_t(k) * pl + (L::cx(k) + L::cy(k) * nx + L::cz(k) * nxy)); };
+  S* cb = static_cast<S*>(p.f) + c;
+  float2 f[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (!ODD) {
+      f[q] = IO::ld2(cb + P(q));
+    } else {
+      const S* src = cb + T(opp(q));
+      f[q] = (L::cx(q) & 1) ? ld2_odd(src) : IO::ld2(src);
+    }
+  }
+  const uint32_t fl2 = c < ncells ? uint32_t(reinterpret_cast<const uint16_t*>(p.flags)[c >> 1])
+                                  : uint32_t(F_SOLID | (F_SOLID << 8));
   const uint32_t fl0 = fl2 & 0xffu, fl1 = fl2 >> 8;
   const bool act0 = !(fl0 & (F_SOLID | F_FORCED)), act1 = !(fl1 & (F_SOLID | F_FORCED));
   if (!(act0 || act1)) return;
-  const int nx = p.nx, nxy = p.nxy;
-  if ((fl0 | fl1) & (F_WRAP | F_SLIP)) {
+  if ((fl0 | fl1) & (F_WRAP | F_SLIP | F_MOVING)) {
     const int z = int(c / uint32_t(nxy));
     const int r = int(c - uint32_t(z) * uint32_t(nxy));
     const int y = r / nx, x = r - y * nx;
@@ -396,69 +436,49 @@ __global__ void __launch_bounds__(PAIR_BLOCK, COLL == COLL_CM ? 2 : 4) hydro_pai
     if (act1) hydro_cell_generic<Q, S, COLL, ODD, false>(p, x + 1, y, z, c + 1, uint8_t(fl1));
     return;
   }
-  const uint32_t mk0 = (fl0 & F_BOUNDARY) ? p.nbr[c] : 0u;
-  const uint32_t mk1 = (fl1 & F_BOUNDARY) ? p.nbr[c + 1] : 0u;
-  const uint32_t mk = mk0 | mk1;
-  S* fb = static_cast<S*>(p.f);
-  const uint32_t pl = p.plane;
-  auto dq = [&](int q) { return L::cx(q) + L::cy(q) * nx + L::cz(q) * nxy; };
-  float2 f[Q];
+  const bool both = act0 && act1;
+  // odd step: a warp whose active cells have no solid neighbour takes the
+  // straight neighbour accesses; the others read the masks and select per link
+  const bool clear = !ODD || __all_sync(__activemask(), !((fl0 | fl1) & F_BOUNDARY) && both);
+  uint32_t mk0 = 0u, mk1 = 0u;
+  if (ODD && !clear) {
+    mk0 = (fl0 & F_BOUNDARY) ? p.nbr[c] : 0u;
+    mk1 = (fl1 & F_BOUNDARY) ? p.nbr[c + 1] : 0u;
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (!ODD) {
-      f[q] = IO::ld2(fb + (uint32_t(q) * pl + c));
-    } else {
+    for (int q = 0; q < Q; ++q) {
       const int o = opp(q);
-      // the neighbour window is always inside the allocation; a direction
-      // that bounces off a solid neighbour is then re-read from the own slot
-      const S* src = fb + int32_t(uint32_t(o) * pl + c - uint32_t(dq(q)));
-      if (L::cx(q) & 1) f[q] = make_float2(IO::ld1(src), IO::ld1(src + 1));
-      else f[q] = IO::ld2(src);
-      const S* own = fb + (uint32_t(q) * pl + c);
-      if ((mk0 >> o) & 1u) f[q].x = IO::ld1(own);
-      if ((mk1 >> o) & 1u) f[q].y = IO::ld1(own + 1);
+      if ((mk0 >> o) & 1u) f[q].x = IO::ld1(cb + P(q));
+      if ((mk1 >> o) & 1u) f[q].y = IO::ld1(cb + P(q) + 1);
     }
   }
-  const float2 rho = pair_collide<Q, COLL>(f, p);
-  const bool both = act0 && act1;
-  const bool moving = (fl0 | fl1) & F_MOVING;
+  pair_collide<Q, COLL>(f, p);
+  if (!ODD) {
+    // even step: a fresh copy of the base pointer keeps the compiler from
+    // holding the load addresses (the same offsets) live across the collision
+    asm volatile("" : "+l"(cb));
+  }
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int o = opp(q);
-    float2 v = f[q];
-    const bool w0 = (mk0 >> q) & 1u, w1 = (mk1 >> q) & 1u;
-    if (moving && (w0 || w1)) {
-      const float k6 = 6.f * float(L::w(o));
-      if (w0 && (fl0 & F_MOVING)) {
-        const Vec4<float> wu = p.wall_u[int32_t(c) + dq(q)];
-        v.x += (k6 * rho.x) * ((float(L::cx(o)) * wu.x + float(L::cy(o)) * wu.y) + float(L::cz(o)) * wu.z);
-      }
-      if (w1 && (fl1 & F_MOVING)) {
-        const Vec4<float> wu = p.wall_u[int32_t(c) + 1 + dq(q)];
-        v.y += (k6 * rho.y) * ((float(L::cx(o)) * wu.x + float(L::cy(o)) * wu.y) + float(L::cz(o)) * wu.z);
-      }
-    }
-    S* own = fb + (uint32_t(o) * pl + c);
+    const float2 v = f[q];
     if (!ODD) {
       if (both) {
-        IO::st2(own, v);
+        IO::st2(cb + P(o), v);
       } else {
-        if (act0) IO::st1(own, v.x);
-        if (act1) IO::st1(own + 1, v.y);
+        if (act0) IO::st1(cb + P(o), v.x);
+        if (act1) IO::st1(cb + P(o) + 1, v.y);
+      }
+    } else if (clear) {
+      if (L::cx(q) & 1) {
+        IO::st1(cb + T(q), v.x);
+        IO::st1(cb + T(q) + 1, v.y);
+      } else {
+        IO::st2(cb + T(q), v);
       }
     } else {
-      S* dst = fb + int32_t(uint32_t(q) * pl + c + uint32_t(dq(q)));
-      if (both && !((mk >> q) & 1u)) {
-        if (L::cx(q) & 1) {
-          IO::st1(dst, v.x);
-          IO::st1(dst + 1, v.y);
-        } else {
-          IO::st2(dst, v);
-        }
-      } else {
-        if (act0) IO::st1(w0 ? own : dst, v.x);
-        if (act1) IO::st1(w1 ? own + 1 : dst + 1, v.y);
-      }
+      const bool w0 = (mk0 >> q) & 1u, w1 = (mk1 >> q) & 1u;
+      if (act0) IO::st1(cb + (w0 ? P(o) : T(q)), v.x);
+      if (act1) IO::st1(cb + (w1 ? P(o) : T(q)) + 1, v.y);
     }
   }
 }

@@ -488,7 +488,7 @@ int lbmb_last_timing(lbmb_solver* h, double* total_ms, double* hydro_ms, int64_t
 int lbmb_set_sweep_kernel(lbmb_solver* h, int32_t kind) {
   return guarded([&] {
     NEED(h);
-    if (kind < LBMB_SWEEP_DIRECT || kind > LBMB_SWEEP_STAGED) lbmb::invalid("unknown sweep kernel kind");
+    if (kind < LBMB_SWEEP_DIRECT || kind > LBMB_SWEEP_WINDOW) lbmb::invalid("unknown sweep kernel kind");
     h->e->set_sweep_kernel(kind);
   });
 }

@@ -16,10 +16,10 @@ from cases import cavity
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("kind", ["bulk", "staged"])
-def test_bounded_wait_timeout_reports_error_and_context_survives(kind):
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_bounded_wait_timeout_reports_error_and_context_survives(storage):
+    kind = "bulk"
     dims, solid, wall_u, nu = cavity(16, re=20.0)
-    storage = "f16" if kind == "staged" else "f32"
     g = lb.Solver(dims, storage=storage, nu=nu, solid=solid, wall_u=wall_u)
     try:
         g.set_sweep_kernel(kind)
