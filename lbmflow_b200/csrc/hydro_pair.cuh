@@ -391,8 +391,9 @@ __device__ __forceinline__ float2 ld2_odd(const S* p) {
 //              around the pair and store two elements.
 // The population loads are issued together with the flag load (every
 // address is inside the allocation whatever the flags say), so a tile costs
-// one memory round trip; the solid-neighbour masks are loaded only by warps
-// with a wall cell (warp-uniform vote). Cells on a periodic face, under the
+// one memory round trip. A warp of 32 active pairs (and, on the odd step,
+// no wall cell) takes straight pair accesses (warp-uniform vote); the
+// others read the solid-neighbour masks and select per cell and link. Cells on a periodic face, under the
 // free-slip top or next to a moving wall take the generic path; IBM-forced
 // cells are left to hydro_cells_kernel.
 constexpr int PAIR_TILE = 64;
@@ -437,11 +438,27 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MINB)
     return;
   }
   const bool both = act0 && act1;
-  // odd step: a warp whose active cells have no solid neighbour takes the
-  // straight neighbour accesses; the others read the masks and select per link
-  const bool clear = !ODD || __all_sync(__activemask(), !((fl0 | fl1) & F_BOUNDARY) && both);
+  // A warp whose 64 cells are all active and (odd step) have no solid
+  // neighbour takes straight pair accesses with no per-link selects; the
+  // others select per cell and link.
+  if (__all_sync(__activemask(), both && !(ODD && ((fl0 | fl1) & F_BOUNDARY)))) {
+    pair_collide<Q, COLL>(f, p);
+    if (!ODD) asm volatile("" : "+l"(cb));
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (!ODD) {
+        IO::st2(cb + P(opp(q)), f[q]);
+      } else if (L::cx(q) & 1) {
+        IO::st1(cb + T(q), f[q].x);
+        IO::st1(cb + T(q) + 1, f[q].y);
+      } else {
+        IO::st2(cb + T(q), f[q]);
+      }
+    }
+    return;
+  }
   uint32_t mk0 = 0u, mk1 = 0u;
-  if (ODD && !clear) {
+  if (ODD) {
     mk0 = (fl0 & F_BOUNDARY) ? p.nbr[c] : 0u;
     mk1 = (fl1 & F_BOUNDARY) ? p.nbr[c + 1] : 0u;
 #pragma unroll
@@ -468,17 +485,14 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MINB)
         if (act0) IO::st1(cb + P(o), v.x);
         if (act1) IO::st1(cb + P(o) + 1, v.y);
       }
-    } else if (clear) {
-      if (L::cx(q) & 1) {
-        IO::st1(cb + T(q), v.x);
-        IO::st1(cb + T(q) + 1, v.y);
-      } else {
-        IO::st2(cb + T(q), v);
-      }
     } else {
       const bool w0 = (mk0 >> q) & 1u, w1 = (mk1 >> q) & 1u;
-      if (act0) IO::st1(cb + (w0 ? P(o) : T(q)), v.x);
-      if (act1) IO::st1(cb + (w1 ? P(o) : T(q)) + 1, v.y);
+      if (!(L::cx(q) & 1) && both && !(w0 || w1)) {
+        IO::st2(cb + T(q), v);
+      } else {
+        if (act0) IO::st1(cb + (w0 ? P(o) : T(q)), v.x);
+        if (act1) IO::st1(cb + (w1 ? P(o) : T(q)) + 1, v.y);
+      }
     }
   }
 }
