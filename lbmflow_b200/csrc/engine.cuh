@@ -746,21 +746,26 @@ struct Engine final : EngineBase {
   // (3 = 168 registers, 4 = 128, 5 = 96).
   int pair_minb[2] = {4, 4};
   template <bool ODD, int COLL, int MINB>
-  void launch_pair_mb(const HydroParams<A>& p, cudaStream_t s) {
+  void launch_pair_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
     if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
       if (n_pair_tiles == 0) return;
-      const unsigned blocks = unsigned(ceil_div(n_pair_tiles, PAIR_BLOCK / 32));
+      // one warp per tile; in the sweep of a runner step, where the IBM
+      // chain runs beside it, a persistent grid of every resident block slot
+      // less async_reserve
+      const int64_t need = ceil_div(n_pair_tiles, PAIR_BLOCK / 32);
+      const int64_t slots = int64_t(sm_count) * MINB - async_reserve;
+      const unsigned blocks = unsigned(std::max<int64_t>(1, concurrent ? std::min(need, slots) : need));
       hydro_pair_kernel<Q, S, ODD, MINB, COLL><<<blocks, PAIR_BLOCK, 0, s>>>(p, pair_list.p, n_pair_tiles,
                                                                              uint32_t(n));
       CK(cudaGetLastError());
     }
   }
   template <bool ODD, int COLL>
-  void launch_pair(const HydroParams<A>& p, cudaStream_t s) {
+  void launch_pair(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
     switch (pair_minb[ODD]) {
-      case 3: launch_pair_mb<ODD, COLL, 3>(p, s); return;
-      case 5: launch_pair_mb<ODD, COLL, 5>(p, s); return;
-      default: launch_pair_mb<ODD, COLL, 4>(p, s); return;
+      case 3: launch_pair_mb<ODD, COLL, 3>(p, s, concurrent); return;
+      case 5: launch_pair_mb<ODD, COLL, 5>(p, s, concurrent); return;
+      default: launch_pair_mb<ODD, COLL, 4>(p, s, concurrent); return;
     }
   }
 
@@ -768,7 +773,7 @@ struct Engine final : EngineBase {
   void launch_hydro_t(const HydroParams<A>& p, cudaStream_t s, bool main_grid, bool cells) {
     if (main_grid) {
       if (kernel_mode == LBMB_SWEEP_PAIR && pair_ok(p, COLL)) {
-        launch_pair<ODD, COLL>(p, s);
+        launch_pair<ODD, COLL>(p, s, !cells);
       } else if (kernel_mode == LBMB_SWEEP_WINDOW && window_ok() && !p.uniform_force) {
         launch_window<COLL, ODD>(p, s, !cells);
       } else if (kernel_mode == LBMB_SWEEP_TILE && pair_ok(p, COLL)) {
@@ -1038,9 +1043,23 @@ struct Engine final : EngineBase {
         pair_minb[0] = cd.ev;
         pair_minb[1] = cd.od;
       }
-      for (int i = 0; i < 2; ++i) launch_hydro(i);  // warm-up (first launches set up grids)
+      // each trial step runs as a plain step does: with force slots, the
+      // forced cells on the side stream beside the full-grid sweep
+      auto trial_step = [&](int par) {
+        if (nslots > 0 && !has_uniform_force()) {
+          CK(cudaEventRecord(ev_fork, st));
+          CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+          launch_hydro(par, st2, false, true);
+          launch_hydro(par, st, true, false);
+          CK(cudaEventRecord(ev_join, st2));
+          CK(cudaStreamWaitEvent(st, ev_join, 0));
+        } else {
+          launch_hydro(par);
+        }
+      };
+      for (int i = 0; i < 2; ++i) trial_step(i);  // warm-up (first launches set up grids)
       CK(cudaEventRecord(ev0, st));
-      for (int i = 0; i < steps; ++i) launch_hydro(i & 1);
+      for (int i = 0; i < steps; ++i) trial_step(i & 1);
       CK(cudaEventRecord(ev1, st));
       CK(cudaEventSynchronize(ev1));
       check_device_error();

@@ -398,15 +398,13 @@ __device__ __forceinline__ float2 ld2_odd(const S* p) {
 // cells are left to hydro_cells_kernel.
 constexpr int PAIR_TILE = 64;
 
-template <int Q, class S, bool ODD, int MINB, int COLL>
-__global__ void __launch_bounds__(PAIR_BLOCK, MINB)
-    hydro_pair_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, uint32_t ncells) {
+// One warp's tile (see hydro_pair_kernel).
+template <int Q, class S, bool ODD, int COLL>
+__device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t tile, uint32_t ncells) {
   using L = Lat<Q>;
   using IO = PairIO<S>;
   const int lane = threadIdx.x & 31;
-  const int w = int((blockIdx.x * PAIR_BLOCK + threadIdx.x) >> 5);
-  if (w >= ntiles) return;
-  const uint32_t c = uint32_t(__ldg(tiles + w)) * PAIR_TILE + 2 * uint32_t(lane);
+  const uint32_t c = tile * PAIR_TILE + 2 * uint32_t(lane);
   const int nx = p.nx, nxy = p.nxy;
   const int64_t pl = int64_t(p.plane);
   // element offsets from the pair's first cell: own slot k, and slot k of
@@ -494,6 +492,23 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MINB)
         if (act1) IO::st1(cb + (w1 ? P(o) : T(q)) + 1, v.y);
       }
     }
+  }
+}
+
+// Warps walk the tile list with a grid stride: one tile per warp when the
+// grid covers the list, persistent warps when a runner step sizes the grid
+// to leave block slots free for the IBM chain on the side stream.
+template <int Q, class S, bool ODD, int MINB, int COLL>
+__global__ void __launch_bounds__(PAIR_BLOCK, MINB)
+    hydro_pair_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, uint32_t ncells) {
+  const int nwarps = int(gridDim.x) * (PAIR_BLOCK / 32);
+  int w = int((blockIdx.x * PAIR_BLOCK + threadIdx.x) >> 5);
+  uint32_t tile = w < ntiles ? uint32_t(__ldg(tiles + w)) : 0u;
+  for (; w < ntiles; w += nwarps) {
+    const int wn = w + nwarps;
+    const uint32_t next = wn < ntiles ? uint32_t(__ldg(tiles + wn)) : 0u;  // one tile ahead
+    pair_tile<Q, S, ODD, COLL>(p, tile, ncells);
+    tile = next;
   }
 }
 
