@@ -217,7 +217,7 @@ struct Engine final : EngineBase {
   DevBuf<int32_t> tile_list;
   int n_tiles_active = 0;
   // pair sweep: 64-cell tiles holding a non-solid cell
-  DevBuf<int32_t> pair_list;
+  DevBuf<uint32_t> pair_list;
   int n_pair_tiles = 0;
   TileDirs tile_dirs[2];
   int tile_grid[2] = {0, 0};
@@ -280,9 +280,10 @@ struct Engine final : EngineBase {
     build_flags(wu);
     // Guard margin: shifted TMA windows of the odd step reach up to
     // nx*ny + nx + 1 cells (+ alignment slack and one tile) beyond a plane.
+    // Plane Q is the pair sweep's scratch plane (stores of inactive cells).
     margin = ceil_div(int64_t(nx) * ny + nx + 2 + 2 * TMA_TILE + 128, 64) * 64;
-    f_alloc.alloc(size_t(Q) * plane + 2 * size_t(margin));
-    CK(cudaMemsetAsync(f_alloc.p, 0, (size_t(Q) * plane + 2 * size_t(margin)) * sizeof(S), st));
+    f_alloc.alloc(size_t(Q + 1) * plane + 2 * size_t(margin));
+    CK(cudaMemsetAsync(f_alloc.p, 0, (size_t(Q + 1) * plane + 2 * size_t(margin)) * sizeof(S), st));
     fp = f_alloc.p + margin;
     fslot_h.assign(size_t(n), -1);
     fslot.alloc(size_t(n));
@@ -640,7 +641,8 @@ struct Engine final : EngineBase {
 
   // Whether the two-cells-per-thread kernel covers this sweep.
   bool pair_ok(const HydroParams<A>& p, int) const {
-    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0 && !omega_on;
+    return std::is_same<A, float>::value && !p.uniform_force && nx % 2 == 0 && !omega_on &&
+           int64_t(Q + 1) * plane < (int64_t(1) << 31);
   }
 
   // Tile list and window offsets of the tile-pipelined sweep.
@@ -654,19 +656,24 @@ struct Engine final : EngineBase {
       if (any) list.push_back(int32_t(t));
     }
     {
-      // 64-cell warp tiles of the pair sweep holding a non-solid cell
+      // 64-cell warp tiles of the pair sweep holding a non-solid cell,
+      // marked TILE_BND when one of them has a solid neighbour
       const int64_t np = ceil_div(n, PAIR_TILE);
-      std::vector<int32_t> pl_;
+      std::vector<uint32_t> pl_;
       for (int64_t t = 0; t < np; ++t) {
-        bool any = false;
-        for (int64_t c = t * PAIR_TILE; c < std::min<int64_t>(n, (t + 1) * PAIR_TILE) && !any; ++c)
-          any = !(flags_h[size_t(c)] & F_SOLID);
-        if (any) pl_.push_back(int32_t(t));
+        bool any = false, bnd = false;
+        for (int64_t c = t * PAIR_TILE; c < std::min<int64_t>(n, (t + 1) * PAIR_TILE); ++c) {
+          const uint8_t fl = flags_h[size_t(c)];
+          if (fl & F_SOLID) continue;
+          any = true;
+          bnd = bnd || (fl & F_BOUNDARY);
+        }
+        if (any) pl_.push_back(uint32_t(t) | (bnd ? TILE_BND : 0u));
       }
       n_pair_tiles = int(pl_.size());
       pair_list.alloc(pl_.size());
       if (!pl_.empty())
-        CK(cudaMemcpyAsync(pair_list.p, pl_.data(), pl_.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(pair_list.p, pl_.data(), pl_.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     }
     n_tiles_active = int(list.size());
     tile_list.alloc(list.size());
@@ -749,12 +756,11 @@ struct Engine final : EngineBase {
   void launch_pair_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
     if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
       if (n_pair_tiles == 0) return;
-      // one warp per tile; in the sweep of a runner step, where the IBM
-      // chain runs beside it, a persistent grid of every resident block slot
-      // less async_reserve
+      // persistent warps: every resident block slot, less async_reserve in
+      // the sweep of a runner step, where the IBM chain runs beside it
       const int64_t need = ceil_div(n_pair_tiles, PAIR_BLOCK / 32);
-      const int64_t slots = int64_t(sm_count) * MINB - async_reserve;
-      const unsigned blocks = unsigned(std::max<int64_t>(1, concurrent ? std::min(need, slots) : need));
+      const int64_t slots = int64_t(sm_count) * MINB - (concurrent ? async_reserve : 0);
+      const unsigned blocks = unsigned(std::max<int64_t>(1, std::min(need, slots)));
       hydro_pair_kernel<Q, S, ODD, MINB, COLL><<<blocks, PAIR_BLOCK, 0, s>>>(p, pair_list.p, n_pair_tiles,
                                                                              uint32_t(n));
       CK(cudaGetLastError());

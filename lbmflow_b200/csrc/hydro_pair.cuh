@@ -392,18 +392,35 @@ __device__ __forceinline__ float2 ld2_odd(const S* p) {
 // The population loads are issued together with the flag load (every
 // address is inside the allocation whatever the flags say), so a tile costs
 // one memory round trip. A warp of 32 active pairs (and, on the odd step,
-// no wall cell) takes straight pair accesses (warp-uniform vote); the
-// others read the solid-neighbour masks and select per cell and link. Cells on a periodic face, under the
-// free-slip top or next to a moving wall take the generic path; IBM-forced
-// cells are left to hydro_cells_kernel.
+// no wall cell) takes straight pair accesses (warp-uniform vote). The other
+// warps make every access per element and unconditionally, with the
+// address selected per cell and link instead of a predicated access (a
+// conditional load or store per link costs more than the access itself):
+//   odd-step loads: a link whose upstream cell is solid reads the cell's
+//     own slot (bounce-back); the tile list marks the tiles holding such
+//     cells (TILE_BND), and the warp loads their solid-neighbour masks one
+//     tile ahead, so the selection needs no extra round trip;
+//   stores: a link whose downstream cell is solid writes the cell's own
+//     slot (odd step), and an inactive cell of the pair (solid, or IBM-forced
+//     and updated by hydro_cells_kernel) writes its own word of the scratch
+//     plane Q, which nothing reads.
+// Cells on a periodic face, under the free-slip top or next to a moving
+// wall take the generic path.
 constexpr int PAIR_TILE = 64;
+constexpr uint32_t TILE_BND = 0x80000000u;  // tile-list bit: a fluid cell of the tile has a solid neighbour
 
-// One warp's tile (see hydro_pair_kernel).
+// One warp's tile (see hydro_pair_kernel). entry: tile index | TILE_BND;
+// mk0 / mk1: the solid-neighbour masks of the lane's two cells on the odd
+// step of a TILE_BND tile, else 0. The population buffer holds Q + 1 planes
+// (the last one the scratch plane).
 template <int Q, class S, bool ODD, int COLL>
-__device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t tile, uint32_t ncells) {
+__device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t entry, uint32_t mk0, uint32_t mk1,
+                                          uint32_t ncells) {
   using L = Lat<Q>;
   using IO = PairIO<S>;
   const int lane = threadIdx.x & 31;
+  const uint32_t tile = entry & ~TILE_BND;
+  const bool bnd_tile = ODD && (entry & TILE_BND);  // warp-uniform
   const uint32_t c = tile * PAIR_TILE + 2 * uint32_t(lane);
   const int nx = p.nx, nxy = p.nxy;
   const int64_t pl = int64_t(p.plane);
@@ -413,13 +430,23 @@ __device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t 
   auto T = [&](int k) { return int32_t(int64_t(k) * pl + (L::cx(k) + L::cy(k) * nx + L::cz(k) * nxy)); };
   S* cb = static_cast<S*>(p.f) + c;
   float2 f[Q];
+  if (bnd_tile) {
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (!ODD) {
-      f[q] = IO::ld2(cb + P(q));
-    } else {
-      const S* src = cb + T(opp(q));
-      f[q] = (L::cx(q) & 1) ? ld2_odd(src) : IO::ld2(src);
+    for (int q = 0; q < Q; ++q) {
+      const int o = opp(q);
+      const int32_t a0 = ((mk0 >> o) & 1u) ? P(q) : T(o);
+      const int32_t a1 = ((mk1 >> o) & 1u) ? P(q) : T(o);
+      f[q] = make_float2(IO::ld1(cb + a0), IO::ld1(cb + a1 + 1));
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (!ODD) {
+        f[q] = IO::ld2(cb + P(q));
+      } else {
+        const S* src = cb + T(opp(q));
+        f[q] = (L::cx(q) & 1) ? ld2_odd(src) : IO::ld2(src);
+      }
     }
   }
   const uint32_t fl2 = c < ncells ? uint32_t(reinterpret_cast<const uint16_t*>(p.flags)[c >> 1])
@@ -435,13 +462,13 @@ __device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t 
     if (act1) hydro_cell_generic<Q, S, COLL, ODD, false>(p, x + 1, y, z, c + 1, uint8_t(fl1));
     return;
   }
-  const bool both = act0 && act1;
-  // A warp whose 64 cells are all active and (odd step) have no solid
-  // neighbour takes straight pair accesses with no per-link selects; the
-  // others select per cell and link.
-  if (__all_sync(__activemask(), both && !(ODD && ((fl0 | fl1) & F_BOUNDARY)))) {
-    pair_collide<Q, COLL>(f, p);
-    if (!ODD) asm volatile("" : "+l"(cb));
+  const bool straight = __all_sync(__activemask(), act0 && act1) && !bnd_tile;
+  pair_collide<Q, COLL>(f, p);
+  // a fresh copy of the base pointer keeps the compiler from holding the
+  // load addresses (the same offsets on the even step) live across the
+  // collision
+  asm volatile("" : "+l"(cb));
+  if (straight) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (!ODD) {
@@ -455,60 +482,51 @@ __device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t 
     }
     return;
   }
-  uint32_t mk0 = 0u, mk1 = 0u;
-  if (ODD) {
-    mk0 = (fl0 & F_BOUNDARY) ? p.nbr[c] : 0u;
-    mk1 = (fl1 & F_BOUNDARY) ? p.nbr[c + 1] : 0u;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int o = opp(q);
-      if ((mk0 >> o) & 1u) f[q].x = IO::ld1(cb + P(q));
-      if ((mk1 >> o) & 1u) f[q].y = IO::ld1(cb + P(q) + 1);
-    }
-  }
-  pair_collide<Q, COLL>(f, p);
-  if (!ODD) {
-    // even step: a fresh copy of the base pointer keeps the compiler from
-    // holding the load addresses (the same offsets) live across the collision
-    asm volatile("" : "+l"(cb));
-  }
+  const int32_t scratch = P(Q);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int o = opp(q);
-    const float2 v = f[q];
-    if (!ODD) {
-      if (both) {
-        IO::st2(cb + P(o), v);
-      } else {
-        if (act0) IO::st1(cb + P(o), v.x);
-        if (act1) IO::st1(cb + P(o) + 1, v.y);
-      }
-    } else {
-      const bool w0 = (mk0 >> q) & 1u, w1 = (mk1 >> q) & 1u;
-      if (!(L::cx(q) & 1) && both && !(w0 || w1)) {
-        IO::st2(cb + T(q), v);
-      } else {
-        if (act0) IO::st1(cb + (w0 ? P(o) : T(q)), v.x);
-        if (act1) IO::st1(cb + (w1 ? P(o) : T(q)) + 1, v.y);
-      }
+    int32_t d0 = P(o), d1 = P(o);
+    if (ODD) {
+      d0 = ((mk0 >> q) & 1u) ? P(o) : T(q);
+      d1 = ((mk1 >> q) & 1u) ? P(o) : T(q);
     }
+    IO::st1(cb + (act0 ? d0 : scratch), f[q].x);
+    IO::st1(cb + (act1 ? d1 : scratch) + 1, f[q].y);
   }
 }
 
-// Warps walk the tile list with a grid stride: one tile per warp when the
-// grid covers the list, persistent warps when a runner step sizes the grid
-// to leave block slots free for the IBM chain on the side stream.
+// Persistent warps walk the tile list with a grid stride, the tile entries
+// two tiles ahead and (odd step, TILE_BND tiles) the solid-neighbour masks
+// one tile ahead. A runner step sizes the grid to leave block slots free
+// for the IBM chain on the side stream.
 template <int Q, class S, bool ODD, int MINB, int COLL>
 __global__ void __launch_bounds__(PAIR_BLOCK, MINB)
-    hydro_pair_kernel(HydroParams<float> p, const int32_t* tiles, int ntiles, uint32_t ncells) {
+    hydro_pair_kernel(HydroParams<float> p, const uint32_t* tiles, int ntiles, uint32_t ncells) {
   const int nwarps = int(gridDim.x) * (PAIR_BLOCK / 32);
+  const uint32_t lane2 = 2u * (threadIdx.x & 31u);
   int w = int((blockIdx.x * PAIR_BLOCK + threadIdx.x) >> 5);
-  uint32_t tile = w < ntiles ? uint32_t(__ldg(tiles + w)) : 0u;
+  // the masks of the lane's two cells (c is even, so the pair is one
+  // aligned 8-byte word of the mask array)
+  auto masks = [&](uint32_t e) {
+    uint2 m = make_uint2(0u, 0u);
+    if (ODD && (e & TILE_BND)) {
+      const uint32_t c = (e & ~TILE_BND) * PAIR_TILE + lane2;
+      if (c < ncells) m = __ldg(reinterpret_cast<const uint2*>(p.nbr) + (c >> 1));
+    }
+    return m;
+  };
+  uint32_t e0 = w < ntiles ? __ldg(tiles + w) : 0u;
+  uint32_t e1 = w + nwarps < ntiles ? __ldg(tiles + w + nwarps) : 0u;
+  uint2 m0 = masks(e0);
   for (; w < ntiles; w += nwarps) {
-    const int wn = w + nwarps;
-    const uint32_t next = wn < ntiles ? uint32_t(__ldg(tiles + wn)) : 0u;  // one tile ahead
-    pair_tile<Q, S, ODD, COLL>(p, tile, ncells);
-    tile = next;
+    const int w2 = w + 2 * nwarps;
+    const uint32_t e2 = w2 < ntiles ? __ldg(tiles + w2) : 0u;
+    const uint2 m1 = masks(e1);  // e1 = 0 past the end: no load
+    pair_tile<Q, S, ODD, COLL>(p, e0, m0.x, m0.y, ncells);
+    e0 = e1;
+    e1 = e2;
+    m0 = m1;
   }
 }
 
