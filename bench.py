@@ -45,7 +45,17 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum, mean of
 # one even and one odd launch) from an ncu full-set capture of the sweep kernel
 # the autotuner picks for the form, on the tank of the given diameter.
-NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 446.8e6}
+NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 448.2e6,
+               ("hydro_pair_kernel", 27, "cm", "f32", 128): 460.1e6,
+               ("hydro_pair_kernel", 19, "trt", "f32", 256): 2720.2e6,
+               ("hydro_pair_kernel", 19, "trt", "f16", 256): 1408.9e6,
+               ("hydro_pair_kernel", 19, "trt", "bf16", 256): 1403.9e6,
+               ("hydro_pair_kernel", 27, "cm", "f32", 256): 3916.6e6,
+               ("hydro_pair_kernel", 27, "cm", "f16", 256): 2006.1e6,
+               ("hydro_pair_kernel", 27, "cm", "bf16", 256): 2016.5e6}
+KERNEL_NAME = {"lean": "hydro_lean_kernel", "pair": "hydro_pair_kernel", "tile": "hydro_tile_kernel",
+               "window": "hydro_window_kernel", "async": "hydro_async_kernel", "direct": "hydro_aa_kernel",
+               "bulk": "hydro_tma_kernel"}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -162,14 +172,16 @@ def peak_hbm():
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle), bounded sample
 # ---------------------------------------------------------------------------
-def cpu_tank_sample(dims, solid, body, nu, q=27, collision="cm", bits=32, steps=3, warmup=1, cs=0.0):
+def cpu_tank_sample(dims, solid, body, nu, q=27, collision="cm", bits=32, steps=3, warmup=1, cs=0.0,
+                    store16=None):
     """The oracle's runner loop (OpenMP over the host cores) from rest:
     `warmup` untimed steps, then `steps` timed ones. Returns (MLUPS, seconds,
-    the torque series of all warmup + steps steps)."""
+    the torque series of all warmup + steps steps). store16: "f16" | "bf16"
+    rounds every stored population to that type (fp32 arithmetic)."""
     from oracle import oracle as o
     os_ = 1.0 / (3.0 * nu + 0.5)
     c = o.OracleSolver(dims, q=q, real_bits=bits, collision=collision, nu=nu, omega_shear=os_, solid=solid,
-                       smagorinsky_cs=cs, free_slip_top=FREE_SLIP_TOP)
+                       smagorinsky_cs=cs, free_slip_top=FREE_SLIP_TOP, store16=store16)
     r0 = c.run_tank(body.positions, body.weights, body.center, body.omega, warmup)
     t0 = time.perf_counter()
     r1 = c.run_tank(body.positions, body.weights, body.center, body.omega, steps)
@@ -496,8 +508,13 @@ def throughput_study(lb, args, local, peak):
             g.run_impeller(body, 8)
             g.run_impeller(body, args.big_steps)
             tms, _, _ = g.last_timing()
-            res[f"d3q{q}_{coll}_{st}"] = {"kernel": tune["kind"], "hydro_ms": per, "hydro_gbs": gbs,
-                                          "hydro_frac": gbs / peak,
+            traffic = NCU_TRAFFIC.get((KERNEL_NAME[tune["kind"]], q, coll, st, args.big_T))
+            res[f"d3q{q}_{coll}_{st}"] = {"kernel": tune["kind"],
+                                          "variant": [tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"]],
+                                          "hydro_ms": per, "hydro_gbs": gbs, "hydro_frac": gbs / peak,
+                                          "traffic": traffic,
+                                          "traffic_over_algorithmic": (traffic / (b_lu(q, st) * n_fluid)
+                                                                       if traffic else None),
                                           "runner_mlups": n_cells * args.big_steps / (tms * 1e-3) / 1e6}
             g.close()
     for q, coll in ((19, "trt"), (27, "cm")):
@@ -631,7 +648,11 @@ def run_b200(args, rank, world, local):
         # a fixed kernel (profiling runs: timings under a profiler would
         # mislead the autotuner)
         g.set_sweep_kernel(args.sweep_kernel)
-        tune = {"kind": args.sweep_kernel, "even_blocks_per_sm": 0, "odd_blocks_per_sm": 0,
+        ev, od = 0, 0
+        if args.sweep_variant:
+            ev, od = (int(v) for v in args.sweep_variant.split("/"))
+            g.set_sweep_variant(ev, od)
+        tune = {"kind": args.sweep_kernel, "even_blocks_per_sm": ev, "odd_blocks_per_sm": od,
                 "best_ms_per_step": None, "default_ms_per_step": None}
     else:
         # tune on a developed flow: on the quiescent start the central-moment
@@ -671,9 +692,7 @@ def run_b200(args, rank, world, local):
     e2e_steps = args.e2e_steps
     g2 = make_solver(lb, dims, solid, nu, q, coll, storage, args.les_cs, local)
     g2.set_sweep_kernel(tune["kind"])
-    if tune["kind"] == "lean":
-        g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
-    elif tune["kind"] == "async" and tune["even_blocks_per_sm"] and storage != "f64":
+    if tune["even_blocks_per_sm"] and tune["kind"] in ("lean", "pair", "window", "async") and storage != "f64":
         g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
     # the caller's marker arrays live in pinned host memory (copied to the
     # device by lbmb_ibm_set_body every step); the step's result is the IBM
@@ -722,9 +741,7 @@ def run_b200(args, rank, world, local):
         if args.mix_steps > 0:
             extra["mixing_precision"] = mixing_study(lb, args, local)
         extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
-    kname = {"lean": "hydro_lean_kernel", "pair": "hydro_pair_kernel", "tile": "hydro_tile_kernel",
-             "window": "hydro_window_kernel",
-             "async": "hydro_async_kernel", "direct": "hydro_aa_kernel", "bulk": "hydro_tma_kernel"}[tune["kind"]]
+    kname = KERNEL_NAME[tune["kind"]]
     coll_name = {"cm": "central_moment", "trt": "trt"}[coll]
     res = {
         "metric": f"MLUPS (stirred-tank runner step, D3Q{q} {coll_name}, {storage} populations)",
@@ -769,17 +786,34 @@ def run_b200(args, rank, world, local):
         warm = 3
         mlups, dt, tq_cpu = cpu_tank_sample(dims_o, solid_o, body_o, nu_o, q=q, collision=coll,
                                             steps=args.cpu_steps, warmup=warm, cs=args.les_cs)
-        g3 = make_solver(lb, dims, solid, nu, q, coll, storage, args.les_cs, local)
-        tq_gpu = g3.run_impeller(body, warm + args.cpu_steps)["torque_lu"]
-        g3.close()
         same_geo = bool(np.array_equal(solid_o, solid) and np.array_equal(body_o.positions, body.positions))
+        nsteps = warm + args.cpu_steps
+
+        def rel(a, b):
+            return float(np.abs(a - b).max() / np.abs(b).max())
+
+        # every storage precision of the device runner against the oracle
+        # run in the same precision (16-bit: the oracle's storage-rounding
+        # mode) and against the oracle in f64, over the same steps from rest
+        oracle_tq = {storage: tq_cpu}
+        for st, bits, s16 in (("f64", 64, None), ("f32", 32, None), ("f16", 32, "f16"), ("bf16", 32, "bf16")):
+            if st not in oracle_tq:
+                oracle_tq[st] = cpu_tank_sample(dims_o, solid_o, body_o, nu_o, q=q, collision=coll, bits=bits,
+                                                steps=nsteps - 1, warmup=1, cs=args.les_cs, store16=s16)[2]
+        per = {}
+        for st in ("f64", "f32", "f16", "bf16"):
+            g3 = make_solver(lb, dims, solid, nu, q, coll, st, args.les_cs, local)
+            tq_gpu = g3.run_impeller(body, nsteps)["torque_lu"]
+            g3.close()
+            per[st] = {"torque_max_rel_diff_vs_oracle_same_precision": rel(tq_gpu, oracle_tq[st]),
+                       "torque_max_rel_diff_vs_oracle_f64": rel(tq_gpu, oracle_tq["f64"])}
         res["cpu_baseline"] = {"value": mlups, "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
                                "sample": f"{args.cpu_steps} runner steps of the full tank after {warm} untimed, "
                                          f"{storage}, OpenMP ({dt:.1f} s)",
-                               "check": {"same_geometry_as_device": same_geo,
-                                         "steps_from_rest": warm + args.cpu_steps,
-                                         "torque_max_rel_diff_vs_device": float(
-                                             np.abs(tq_gpu - tq_cpu).max() / np.abs(tq_cpu).max())}}
+                               "check": {"same_geometry_as_device": same_geo, "steps_from_rest": nsteps,
+                                         "torque_max_rel_diff_vs_device": per[storage][
+                                             "torque_max_rel_diff_vs_oracle_same_precision"],
+                                         "per_storage": per}}
     return res
 
 
@@ -847,6 +881,8 @@ def main():
     ap.add_argument("--mix-D-fallback", type=float, default=1e-2,
                     help="diffusivity of the repeat when a run at --mix-D stops")
     ap.add_argument("--mix-steps", type=int, default=60000, help="step cap of the mixing study (0: skip)")
+    ap.add_argument("--sweep-variant", default="",
+                    help="with --sweep-kernel: resident blocks per SM, even/odd (e.g. 4/3)")
     ap.add_argument("--sweep-kernel", default=None, choices=["direct", "bulk", "async", "pair", "tile", "lean", "window"],
                     help="use this sweep kernel instead of the autotuner's choice")
     ap.add_argument("--lid", action="store_true", help="no-slip lid (the reference's tank) instead of a free-slip top")
