@@ -422,11 +422,11 @@ def mixing_study(lb, args, local):
     T = mix_T tank, D3Q27 central-moment form, every storage precision
     against the f64 path; CV probed every 200 steps, run until CV <= 0.01
     CV0 or mix_steps. The stated diffusivity (mix_D, 1e-3 lattice units,
-    grid Peclet u_tip / D = 50, tau_s = 4 D + 1/2 = 0.504) is tried first;
-    a precision whose run stops (non-finite CV or mass) is recorded with the
-    step it stopped at (none has: the runs stay bounded), and the study is
-    repeated at mix_D_fallback, where the pulse mixes within the step cap.
-    Each run reports the CV / CV0 it reached."""
+    grid Peclet u_tip / D = 50, tau_s = 4 D + 1/2 = 0.504) is run first; a
+    precision whose run stops (non-finite CV or mass) is recorded with the
+    step it stopped at (none has: the runs stay bounded and reach t99 within
+    about 150,000 steps), and the study is then repeated at 1e-2. mix_D2 > 0
+    adds a second diffusivity. Each run reports the CV / CV0 it reached."""
     from lbmflow_b200 import sweep
     c = sweep.TankCase(args.mix_T, 0.05, 2000.0)
     geo = sweep.tank_geometry(args.mix_T)
@@ -478,13 +478,16 @@ def mixing_study(lb, args, local):
 
     out = {"grid": list(dims), "sigma_cells": 4.0, "probe_every": probe, "step_cap": args.mix_steps,
            "revolution_steps": 2 * math.pi / c.omega, "form": "D3Q27 central moment + D3Q7 scalar"}
-    for D in (args.mix_D, args.mix_D_fallback):
+    Ds = [args.mix_D] + ([args.mix_D2] if args.mix_D2 > 0 else [])
+    for D in Ds:
         res, stops = run(D)
         out[f"D={D:g}"] = {"grid_peclet": 0.05 / D, "tau_s": 4.0 * D + 0.5,
                            "t95_steps": {k_: (v or {}).get("t95") for k_, v in res.items()},
                            "t99_steps": {k_: (v or {}).get("t99") for k_, v in res.items()},
                            "stopped_at_step": stops, "final": dict(finals),
                            "rel_err_vs_f64": errs(res)}
+        if D == args.mix_D and any(v is not None for v in stops.values()) and 1e-2 not in Ds:
+            Ds.append(1e-2)  # the loop picks it up
     return out
 
 
@@ -737,10 +740,12 @@ def run_b200(args, rank, world, local):
     if args.adj_steps > 0 and world == 1:
         extra["adjoint"] = adjoint_study(args, local)
     if args.variants and world == 1:
-        extra["qoi_precision"] = qoi_study(lb, args, local, dims, solid, body, nu, D, np_head)
+        if args.qoi_revs > 0:
+            extra["qoi_precision"] = qoi_study(lb, args, local, dims, solid, body, nu, D, np_head)
         if args.mix_steps > 0:
             extra["mixing_precision"] = mixing_study(lb, args, local)
-        extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
+        if args.big_steps > 0:
+            extra["throughput_T%d" % args.big_T] = throughput_study(lb, args, local, peak)
     kname = KERNEL_NAME[tune["kind"]]
     coll_name = {"cm": "central_moment", "trt": "trt"}[coll]
     res = {
@@ -867,10 +872,10 @@ def main():
     ap.add_argument("--ckpt", type=int, default=1, help="checkpoint save/restore study on the final state (0: skip)")
     ap.add_argument("--variants", type=int, default=1)
     ap.add_argument("--qoi-revs", type=float, default=4.0,
-                    help="impeller revolutions of the precision study (Np over the last half)")
+                    help="impeller revolutions of the precision study (Np over the last half; 0: skip)")
     ap.add_argument("--les-cs", type=float, default=0.1, help="Smagorinsky constant (0: reference operators)")
     ap.add_argument("--big-T", type=int, default=256, help="tank diameter of the throughput study")
-    ap.add_argument("--big-steps", type=int, default=100)
+    ap.add_argument("--big-steps", type=int, default=100, help="runner steps per form of the throughput study (0: skip)")
     ap.add_argument("--sweep-steps", type=int, default=5000, help="steps per case of the batched sweep (0: skip)")
     ap.add_argument("--adj-steps", type=int, default=2000, help="adjoint study steps (0: skip)")
     ap.add_argument("--adj-T", type=int, default=96)
@@ -878,9 +883,9 @@ def main():
     ap.add_argument("--adj-dirs", type=int, default=16)
     ap.add_argument("--mix-T", type=int, default=128, help="tank diameter of the mixing-time study")
     ap.add_argument("--mix-D", type=float, default=1e-3, help="scalar diffusivity of the mixing study (lattice)")
-    ap.add_argument("--mix-D-fallback", type=float, default=1e-2,
-                    help="diffusivity of the repeat when a run at --mix-D stops")
-    ap.add_argument("--mix-steps", type=int, default=60000, help="step cap of the mixing study (0: skip)")
+    ap.add_argument("--mix-D2", type=float, default=0.0,
+                    help="second diffusivity of the mixing study (0: none; 1e-2 is added when a run at --mix-D stops)")
+    ap.add_argument("--mix-steps", type=int, default=160000, help="step cap of the mixing study (0: skip)")
     ap.add_argument("--sweep-variant", default="",
                     help="with --sweep-kernel: resident blocks per SM, even/odd (e.g. 4/3)")
     ap.add_argument("--sweep-kernel", default=None, choices=["direct", "bulk", "async", "pair", "tile", "lean", "window"],

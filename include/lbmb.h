@@ -460,9 +460,14 @@ int lbmb_get_sweep_kernel(lbmb_solver* h, int32_t* kind);
  * step, where the IBM kernels run concurrently on a side stream. Window
  * kernel: resident 256-thread blocks per SM per parity, 2 (128 registers),
  * 3 (80) or 4 (64), with a tile ring of 3 where shared memory allows, else
- * 2; default 2 for the central moment, 3 for TRT/BGK. Pair kernel (TRT/BGK):
- * resident 128-thread blocks per SM per parity, 3 (168 registers), 4 (128,
- * the default) or 5 (96). */
+ * 2; default 2 for the central moment, 3 for TRT/BGK. Pair kernel (TRT/BGK,
+ * D3Q27 central moment): resident 128-thread blocks per SM per parity, 3 (168
+ * registers), 4 (128, the default) or 5 (96); 13, 14 or 15 name the same
+ * budgets with the populations of the next tile staged in shared memory by
+ * cp.async while the warp computes the current one (two stages of Q x 32
+ * 8-byte slots per warp; the grid holds as many blocks as shared memory
+ * allows, at most the budget's). The persistent pair grid leaves 32 block
+ * slots free in a runner step as the cp.async kernel does. */
 int lbmb_set_sweep_variant(lbmb_solver* h, int32_t even_blocks_per_sm, int32_t odd_blocks_per_sm);
 
 /* Sweep autotuner (no reference counterpart): times every sweep kernel kind

@@ -472,7 +472,8 @@ class Solver:
     def set_sweep_variant(self, even_blocks_per_sm, odd_blocks_per_sm):
         """Register budget of the current sweep kernel per parity, as resident
         blocks per SM: 6..10 for "lean", 4..6 for "async" (fp32 storage), 2..4
-        for "window" (256-thread blocks)."""
+        for "window" (256-thread blocks), 3..5 for "pair" (13..15: the same
+        with the next tile's populations staged by cp.async)."""
         _check(lib().lbmb_set_sweep_variant(self.h, int(even_blocks_per_sm), int(odd_blocks_per_sm)))
 
     def autotune_sweep(self, steps_per_trial=20):

@@ -583,11 +583,13 @@ struct Engine final : EngineBase {
       return;
     }
     if (kernel_mode == LBMB_SWEEP_PAIR) {
-      auto ok = [](int v) { return v >= 3 && v <= 5; };
+      auto ok = [](int v) { return (v >= 3 && v <= 5) || (v >= PAIR_STAGED + 3 && v <= PAIR_STAGED + 5); };
       if (!ok(even) || !ok(odd))
-        throw Error(LBMB_ERR_INVALID, "sweep variant: pair resident blocks per SM must be 3, 4 or 5");
+        throw Error(LBMB_ERR_INVALID,
+                    "sweep variant: pair resident blocks per SM must be 3, 4 or 5 (+10: cp.async-staged)");
       pair_minb[0] = even;
       pair_minb[1] = odd;
+      prepare_pair_variant();
       invalidate_graphs();
       return;
     }
@@ -749,30 +751,72 @@ struct Engine final : EngineBase {
     }
   }
 
-  // Resident 128-thread blocks per SM of the pair sweep, per parity
-  // (3 = 168 registers, 4 = 128, 5 = 96).
+  // Pair sweep launch variant per parity: resident 128-thread blocks per SM
+  // the registers are sized for (3 = 168 registers, 4 = 128, 5 = 96), plus
+  // PAIR_STAGED for the cp.async-staged form (its shared memory may allow
+  // fewer blocks).
+  static constexpr int PAIR_STAGED = 10;
   int pair_minb[2] = {4, 4};
+  // Resident blocks per SM of a staged pair kernel (shared memory attribute
+  // set on first use; called before any capture by set_sweep_variant and the
+  // autotuner's eager trials).
   template <bool ODD, int COLL, int MINB>
+  int pair_staged_per_sm() {
+    static int per_sm = -1;
+    if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
+      if (per_sm < 0) {
+        auto kern = hydro_pair_kernel<Q, S, ODD, MINB, COLL, true>;
+        const size_t smem = pair_staged_smem_bytes<Q>();
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int b = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, PAIR_BLOCK, smem));
+        per_sm = std::max(b, 1);
+      }
+    }
+    return per_sm;
+  }
+  template <bool ODD, int COLL, int MINB, bool STAGED>
   void launch_pair_mb(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
     if constexpr (std::is_same<A, float>::value && (COLL == COLL_TRT || Q == 27)) {
       if (n_pair_tiles == 0) return;
       // persistent warps: every resident block slot, less async_reserve in
       // the sweep of a runner step, where the IBM chain runs beside it
       const int64_t need = ceil_div(n_pair_tiles, PAIR_BLOCK / 32);
-      const int64_t slots = int64_t(sm_count) * MINB - (concurrent ? async_reserve : 0);
+      const int resident = STAGED ? std::min(MINB, pair_staged_per_sm<ODD, COLL, MINB>()) : MINB;
+      const int64_t slots = int64_t(sm_count) * resident - (concurrent ? async_reserve : 0);
       const unsigned blocks = unsigned(std::max<int64_t>(1, std::min(need, slots)));
-      hydro_pair_kernel<Q, S, ODD, MINB, COLL><<<blocks, PAIR_BLOCK, 0, s>>>(p, pair_list.p, n_pair_tiles,
-                                                                             uint32_t(n));
+      const size_t smem = STAGED ? pair_staged_smem_bytes<Q>() : 0;
+      hydro_pair_kernel<Q, S, ODD, MINB, COLL, STAGED><<<blocks, PAIR_BLOCK, smem, s>>>(p, pair_list.p, n_pair_tiles,
+                                                                                         uint32_t(n));
       CK(cudaGetLastError());
     }
   }
   template <bool ODD, int COLL>
   void launch_pair(const HydroParams<A>& p, cudaStream_t s, bool concurrent) {
     switch (pair_minb[ODD]) {
-      case 3: launch_pair_mb<ODD, COLL, 3>(p, s, concurrent); return;
-      case 5: launch_pair_mb<ODD, COLL, 5>(p, s, concurrent); return;
-      default: launch_pair_mb<ODD, COLL, 4>(p, s, concurrent); return;
+      case 3: launch_pair_mb<ODD, COLL, 3, false>(p, s, concurrent); return;
+      case 5: launch_pair_mb<ODD, COLL, 5, false>(p, s, concurrent); return;
+      case PAIR_STAGED + 3: launch_pair_mb<ODD, COLL, 3, true>(p, s, concurrent); return;
+      case PAIR_STAGED + 4: launch_pair_mb<ODD, COLL, 4, true>(p, s, concurrent); return;
+      case PAIR_STAGED + 5: launch_pair_mb<ODD, COLL, 5, true>(p, s, concurrent); return;
+      default: launch_pair_mb<ODD, COLL, 4, false>(p, s, concurrent); return;
     }
+  }
+  // Shared-memory setup of the staged pair kernels a variant names.
+  void prepare_pair_variant() {
+    auto one = [&](auto odd_tag, int v) {
+      constexpr bool ODD = decltype(odd_tag)::value;
+      auto per_coll = [&](auto coll_tag) {
+        constexpr int COLL = decltype(coll_tag)::value;
+        if (v == PAIR_STAGED + 3) pair_staged_per_sm<ODD, COLL, 3>();
+        if (v == PAIR_STAGED + 4) pair_staged_per_sm<ODD, COLL, 4>();
+        if (v == PAIR_STAGED + 5) pair_staged_per_sm<ODD, COLL, 5>();
+      };
+      if (coll == COLL_CM) per_coll(std::integral_constant<int, COLL_CM>{});
+      else per_coll(std::integral_constant<int, COLL_TRT>{});
+    };
+    one(std::false_type{}, pair_minb[0]);
+    one(std::true_type{}, pair_minb[1]);
   }
 
   template <int COLL, bool ODD>
@@ -1001,8 +1045,9 @@ struct Engine final : EngineBase {
     }
     if (!uf) cands.push_back({LBMB_SWEEP_BULK, 0, 0});
     if (is_f && nx % 2 == 0 && !uf && !omega_on) {
-      for (int ev = 3; ev <= 5; ++ev)
-        for (int od = 3; od <= 5; ++od) cands.push_back({LBMB_SWEEP_PAIR, ev, od});
+      for (int ev : {3, 4, 5, PAIR_STAGED + 3, PAIR_STAGED + 4, PAIR_STAGED + 5})
+        for (int od : {3, 4, 5, PAIR_STAGED + 3, PAIR_STAGED + 4, PAIR_STAGED + 5})
+          cands.push_back({LBMB_SWEEP_PAIR, ev, od});
       cands.push_back({LBMB_SWEEP_TILE, 0, 0});
     }
     if (window_ok()) {
@@ -1048,6 +1093,7 @@ struct Engine final : EngineBase {
       if (cd.kind == LBMB_SWEEP_PAIR) {
         pair_minb[0] = cd.ev;
         pair_minb[1] = cd.od;
+        prepare_pair_variant();
       }
       // each trial step runs as a plain step does: with force slots, the
       // forced cells on the side stream beside the full-grid sweep

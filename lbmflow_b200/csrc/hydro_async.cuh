@@ -182,12 +182,6 @@ __device__ __forceinline__ void cp_async_elem(S* dst_smem, const S* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // MINB: resident blocks per SM the register allocation is sized for (fp32:
 // 4 = 128 registers, 5 = 96 (102), 6 = 80 (85); the ring of STAGES x Q x 128

@@ -409,52 +409,152 @@ __device__ __forceinline__ float2 ld2_odd(const S* p) {
 constexpr int PAIR_TILE = 64;
 constexpr uint32_t TILE_BND = 0x80000000u;  // tile-list bit: a fluid cell of the tile has a solid neighbour
 
-// One warp's tile (see hydro_pair_kernel). entry: tile index | TILE_BND;
-// mk0 / mk1: the solid-neighbour masks of the lane's two cells on the odd
-// step of a TILE_BND tile, else 0. The population buffer holds Q + 1 planes
-// (the last one the scratch plane).
-template <int Q, class S, bool ODD, int COLL>
-__device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t entry, uint32_t mk0, uint32_t mk1,
-                                          uint32_t ncells) {
+// Per-tile addressing of a lane's pair: element offsets from the pair's
+// first cell (own slot k, and slot k of the neighbour x + c_k; uniform across
+// the grid).
+template <int Q>
+struct PairAddr {
+  int nx, nxy;
+  int64_t pl;
+  __device__ __forceinline__ int32_t P(int k) const { return int32_t(int64_t(k) * pl); }
+  __device__ __forceinline__ int32_t T(int k) const {
+    using L = Lat<Q>;
+    return int32_t(int64_t(k) * pl + (L::cx(k) + L::cy(k) * nx + L::cz(k) * nxy));
+  }
+};
+
+// Source of link q for element e of the lane's pair on a wall tile of the
+// odd step: the own slot when the upstream cell is solid, else the
+// neighbour's slot.
+template <int Q>
+__device__ __forceinline__ int32_t pair_src(const PairAddr<Q>& A, uint32_t mk, int q) {
+  const int o = opp(q);
+  return ((mk >> o) & 1u) ? A.P(q) : A.T(o);
+}
+
+// The lane's populations straight from global memory (see the access
+// rules above).
+template <int Q, class S, bool ODD>
+__device__ __forceinline__ void pair_load(const PairAddr<Q>& A, const S* cb, bool bnd_tile, uint32_t mk0,
+                                          uint32_t mk1, float2 (&f)[Q]) {
   using L = Lat<Q>;
   using IO = PairIO<S>;
-  const int lane = threadIdx.x & 31;
-  const uint32_t tile = entry & ~TILE_BND;
-  const bool bnd_tile = ODD && (entry & TILE_BND);  // warp-uniform
-  const uint32_t c = tile * PAIR_TILE + 2 * uint32_t(lane);
-  const int nx = p.nx, nxy = p.nxy;
-  const int64_t pl = int64_t(p.plane);
-  // element offsets from the pair's first cell: own slot k, and slot k of
-  // the neighbour x + c_k (uniform across the grid)
-  auto P = [&](int k) { return int32_t(int64_t(k) * pl); };
-  auto T = [&](int k) { return int32_t(int64_t(k) * pl + (L::cx(k) + L::cy(k) * nx + L::cz(k) * nxy)); };
-  S* cb = static_cast<S*>(p.f) + c;
-  float2 f[Q];
-  if (bnd_tile) {
+  if (ODD && bnd_tile) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int o = opp(q);
-      const int32_t a0 = ((mk0 >> o) & 1u) ? P(q) : T(o);
-      const int32_t a1 = ((mk1 >> o) & 1u) ? P(q) : T(o);
-      f[q] = make_float2(IO::ld1(cb + a0), IO::ld1(cb + a1 + 1));
-    }
+    for (int q = 0; q < Q; ++q) f[q] = make_float2(IO::ld1(cb + pair_src(A, mk0, q)), IO::ld1(cb + pair_src(A, mk1, q) + 1));
   } else {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (!ODD) {
-        f[q] = IO::ld2(cb + P(q));
+        f[q] = IO::ld2(cb + A.P(q));
       } else {
-        const S* src = cb + T(opp(q));
+        const S* src = cb + A.T(opp(q));
         f[q] = (L::cx(q) & 1) ? ld2_odd(src) : IO::ld2(src);
       }
     }
   }
-  const uint32_t fl2 = c < ncells ? uint32_t(reinterpret_cast<const uint16_t*>(p.flags)[c >> 1])
-                                  : uint32_t(F_SOLID | (F_SOLID << 8));
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+
+// Staged form of pair_load: the same bytes copied by cp.async into the
+// lane's staging slots (one 8-byte slot per link, slot q at byte offset
+// q * 256 + 8 * lane of the stage, so a warp's reads of one link are
+// conflict-free), then read back by pair_unstage once the copies landed.
+// A slot holds the pair (fp32: 8 bytes; 16-bit: the low 4 bytes), or the two
+// 4-byte pieces the pair is made of: two fp32 elements, or the two aligned
+// 16-bit words around an odd-offset pair or around each element of a wall
+// link.
+template <int Q, class S, bool ODD>
+__device__ __forceinline__ void pair_stage(const PairAddr<Q>& A, const S* cb, bool bnd_tile, uint32_t mk0,
+                                           uint32_t mk1, uint32_t slots) {
+  using L = Lat<Q>;
+  constexpr bool W16 = sizeof(S) == 2;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const uint32_t d = slots + uint32_t(q) * 256u;
+    if (ODD && bnd_tile) {
+      const S* s0 = cb + pair_src(A, mk0, q);
+      const S* s1 = cb + pair_src(A, mk1, q) + 1;
+      if (W16) {  // the aligned words holding each element
+        s0 = reinterpret_cast<const S*>(reinterpret_cast<uintptr_t>(s0) & ~uintptr_t(3));
+        s1 = reinterpret_cast<const S*>(reinterpret_cast<uintptr_t>(s1) & ~uintptr_t(3));
+      }
+      cp_async4(d, s0);
+      cp_async4(d + 4u, s1);
+    } else if (!ODD || !(L::cx(q) & 1)) {
+      const S* src = cb + (ODD ? A.T(opp(q)) : A.P(q));
+      if (W16) cp_async4(d, src);
+      else cp_async8(d, src);
+    } else {  // odd step, c_x odd: the pair starts at an odd element
+      const S* src = cb + A.T(opp(q));
+      if (W16) {
+        cp_async4(d, src - 1);
+        cp_async4(d + 4u, src + 1);
+      } else {
+        cp_async4(d, src);
+        cp_async4(d + 4u, src + 1);
+      }
+    }
+  }
+}
+
+template <class S>
+__device__ __forceinline__ float2 h2f2(uint32_t v) {
+  if constexpr (std::is_same<S, __half>::value) return __half22float2(*reinterpret_cast<__half2*>(&v));
+  else return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162*>(&v));
+}
+
+template <int Q, class S, bool ODD>
+__device__ __forceinline__ void pair_unstage(const PairAddr<Q>& A, bool bnd_tile, uint32_t mk0, uint32_t mk1,
+                                             const uint2* slots, float2 (&f)[Q]) {
+  using L = Lat<Q>;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const uint2 v = slots[q * 32];
+    if constexpr (sizeof(S) == 4) {
+      f[q] = make_float2(__uint_as_float(v.x), __uint_as_float(v.y));
+    } else if (ODD && bnd_tile) {
+      // element 0 sits in the high half of its word when its offset is odd
+      // (c is even; own slots are even, neighbour slots odd when c_x is)
+      const int o = opp(q);
+      const bool odd0 = !((mk0 >> o) & 1u) && (L::cx(o) & 1);
+      const bool odd1 = ((mk1 >> o) & 1u) || !(L::cx(o) & 1);
+      const uint32_t h = __byte_perm(v.x, v.y, (odd0 ? 0x32u : 0x10u) | (odd1 ? 0x7600u : 0x5400u));
+      f[q] = h2f2<S>(h);
+    } else if (!ODD || !(L::cx(q) & 1)) {
+      f[q] = h2f2<S>(v.x);
+    } else {
+      f[q] = h2f2<S>(__byte_perm(v.x, v.y, 0x5432));
+    }
+  }
+}
+
+// The rest of a lane's tile once its populations are in registers: flags
+// (fl2: the pair's two flag bytes), generic cells, collision, stores.
+template <int Q, class S, bool ODD, int COLL>
+__device__ __forceinline__ void pair_finish(const HydroParams<float>& p, const PairAddr<Q>& A, S* cb, uint32_t c,
+                                            bool bnd_tile, uint32_t mk0, uint32_t mk1, uint32_t fl2,
+                                            float2 (&f)[Q]) {
+  using L = Lat<Q>;
+  using IO = PairIO<S>;
   const uint32_t fl0 = fl2 & 0xffu, fl1 = fl2 >> 8;
   const bool act0 = !(fl0 & (F_SOLID | F_FORCED)), act1 = !(fl1 & (F_SOLID | F_FORCED));
   if (!(act0 || act1)) return;
   if ((fl0 | fl1) & (F_WRAP | F_SLIP | F_MOVING)) {
+    const int nx = A.nx, nxy = A.nxy;
     const int z = int(c / uint32_t(nxy));
     const int r = int(c - uint32_t(z) * uint32_t(nxy));
     const int y = r / nx, x = r - y * nx;
@@ -472,62 +572,130 @@ __device__ __forceinline__ void pair_tile(const HydroParams<float>& p, uint32_t 
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (!ODD) {
-        IO::st2(cb + P(opp(q)), f[q]);
+        IO::st2(cb + A.P(opp(q)), f[q]);
       } else if (L::cx(q) & 1) {
-        IO::st1(cb + T(q), f[q].x);
-        IO::st1(cb + T(q) + 1, f[q].y);
+        IO::st1(cb + A.T(q), f[q].x);
+        IO::st1(cb + A.T(q) + 1, f[q].y);
       } else {
-        IO::st2(cb + T(q), f[q]);
+        IO::st2(cb + A.T(q), f[q]);
       }
     }
     return;
   }
-  const int32_t scratch = P(Q);
+  const int32_t scratch = A.P(Q);
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int o = opp(q);
-    int32_t d0 = P(o), d1 = P(o);
+    int32_t d0 = A.P(o), d1 = A.P(o);
     if (ODD) {
-      d0 = ((mk0 >> q) & 1u) ? P(o) : T(q);
-      d1 = ((mk1 >> q) & 1u) ? P(o) : T(q);
+      d0 = ((mk0 >> q) & 1u) ? A.P(o) : A.T(q);
+      d1 = ((mk1 >> q) & 1u) ? A.P(o) : A.T(q);
     }
     IO::st1(cb + (act0 ? d0 : scratch), f[q].x);
     IO::st1(cb + (act1 ? d1 : scratch) + 1, f[q].y);
   }
 }
 
-// Persistent warps walk the tile list with a grid stride, the tile entries
-// two tiles ahead and (odd step, TILE_BND tiles) the solid-neighbour masks
-// one tile ahead. A runner step sizes the grid to leave block slots free
-// for the IBM chain on the side stream.
-template <int Q, class S, bool ODD, int MINB, int COLL>
+// The flag bytes of the lane's pair (both solid past the grid's end).
+__device__ __forceinline__ uint32_t pair_flags(const HydroParams<float>& p, uint32_t c, uint32_t ncells) {
+  return c < ncells ? uint32_t(reinterpret_cast<const uint16_t*>(p.flags)[c >> 1])
+                    : uint32_t(F_SOLID | (F_SOLID << 8));
+}
+
+// Warps walk the tile list with a grid stride (persistent: a runner step
+// sizes the grid to leave block slots free for the IBM chain on the side
+// stream), the tile entries ahead of the tile in hand and, on the odd step
+// of TILE_BND tiles, the solid-neighbour masks ahead of the populations.
+//   STAGED = false: the populations of a tile are loaded when the warp
+//     reaches it (entries two tiles ahead, masks one tile ahead);
+//   STAGED = true: they are copied by cp.async into the warp's staging
+//     slots one tile ahead (two stages of Q x 32 slots of 8 bytes per warp,
+//     dynamic shared memory), so their latency overlaps the collision of
+//     the tile in hand (entries three tiles ahead, masks two, flags one).
+template <int Q, class S, bool ODD, int MINB, int COLL, bool STAGED = false>
 __global__ void __launch_bounds__(PAIR_BLOCK, MINB)
     hydro_pair_kernel(HydroParams<float> p, const uint32_t* tiles, int ntiles, uint32_t ncells) {
   const int nwarps = int(gridDim.x) * (PAIR_BLOCK / 32);
-  const uint32_t lane2 = 2u * (threadIdx.x & 31u);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lane2 = 2u * lane;
   int w = int((blockIdx.x * PAIR_BLOCK + threadIdx.x) >> 5);
+  const PairAddr<Q> A{p.nx, p.nxy, int64_t(p.plane)};
+  S* const fb = static_cast<S*>(p.f);
+  auto cell0 = [&](uint32_t e) { return (e & ~TILE_BND) * PAIR_TILE + lane2; };
   // the masks of the lane's two cells (c is even, so the pair is one
   // aligned 8-byte word of the mask array)
   auto masks = [&](uint32_t e) {
     uint2 m = make_uint2(0u, 0u);
     if (ODD && (e & TILE_BND)) {
-      const uint32_t c = (e & ~TILE_BND) * PAIR_TILE + lane2;
+      const uint32_t c = cell0(e);
       if (c < ncells) m = __ldg(reinterpret_cast<const uint2*>(p.nbr) + (c >> 1));
     }
     return m;
   };
-  uint32_t e0 = w < ntiles ? __ldg(tiles + w) : 0u;
-  uint32_t e1 = w + nwarps < ntiles ? __ldg(tiles + w + nwarps) : 0u;
-  uint2 m0 = masks(e0);
-  for (; w < ntiles; w += nwarps) {
-    const int w2 = w + 2 * nwarps;
-    const uint32_t e2 = w2 < ntiles ? __ldg(tiles + w2) : 0u;
-    const uint2 m1 = masks(e1);  // e1 = 0 past the end: no load
-    pair_tile<Q, S, ODD, COLL>(p, e0, m0.x, m0.y, ncells);
-    e0 = e1;
-    e1 = e2;
-    m0 = m1;
+  auto entry = [&](int k) { return k < ntiles ? __ldg(tiles + k) : 0u; };
+  if constexpr (!STAGED) {
+    uint32_t e0 = entry(w);
+    uint32_t e1 = entry(w + nwarps);
+    uint2 m0 = masks(e0);
+    for (; w < ntiles; w += nwarps) {
+      const uint32_t e2 = entry(w + 2 * nwarps);
+      const uint2 m1 = masks(e1);  // e1 = 0 past the end: no load
+      const uint32_t c = cell0(e0);
+      S* cb = fb + c;
+      const bool bnd = ODD && (e0 & TILE_BND);  // warp-uniform
+      float2 f[Q];
+      pair_load<Q, S, ODD>(A, cb, bnd, m0.x, m0.y, f);
+      pair_finish<Q, S, ODD, COLL>(p, A, cb, c, bnd, m0.x, m0.y, pair_flags(p, c, ncells), f);
+      e0 = e1;
+      e1 = e2;
+      m0 = m1;
+    }
+  } else {
+    extern __shared__ uint2 pair_slots_smem[];
+    uint2* const wslots = pair_slots_smem + size_t(threadIdx.x >> 5) * (2 * Q * 32) + lane;
+    const uint32_t wsh = static_cast<uint32_t>(__cvta_generic_to_shared(wslots));
+    auto stage = [&](uint32_t e, uint2 m, int buf) {
+      const uint32_t c = cell0(e);
+      pair_stage<Q, S, ODD>(A, fb + c, ODD && (e & TILE_BND), m.x, m.y, wsh + uint32_t(buf) * (Q * 256u));
+    };
+    uint32_t e0 = entry(w);
+    uint32_t e1 = entry(w + nwarps);
+    uint32_t e2 = entry(w + 2 * nwarps);
+    uint2 m0 = masks(e0);
+    if (w < ntiles) stage(e0, m0, 0);
+    cp_async_commit();
+    uint32_t fl0 = pair_flags(p, cell0(e0), ncells);
+    uint2 m1 = masks(e1);
+    int buf = 0;
+    for (; w < ntiles; w += nwarps) {
+      const uint32_t e3 = entry(w + 3 * nwarps);
+      const bool more = w + nwarps < ntiles;
+      if (more) stage(e1, m1, buf ^ 1);
+      cp_async_commit();
+      const uint2 m2 = masks(e2);
+      const uint32_t fl1 = more ? pair_flags(p, cell0(e1), ncells) : 0u;
+      cp_async_wait<1>();  // this tile's copies (only the lane's own slots are read)
+      const uint32_t c = cell0(e0);
+      S* cb = fb + c;
+      const bool bnd = ODD && (e0 & TILE_BND);
+      float2 f[Q];
+      pair_unstage<Q, S, ODD>(A, bnd, m0.x, m0.y, wslots + size_t(buf) * (Q * 32), f);
+      pair_finish<Q, S, ODD, COLL>(p, A, cb, c, bnd, m0.x, m0.y, fl0, f);
+      e0 = e1;
+      e1 = e2;
+      e2 = e3;
+      m0 = m1;
+      m1 = m2;
+      fl0 = fl1;
+      buf ^= 1;
+    }
+    cp_async_wait<0>();
   }
+}
+
+template <int Q>
+constexpr size_t pair_staged_smem_bytes() {
+  return size_t(PAIR_BLOCK / 32) * 2 * Q * 32 * sizeof(uint2);
 }
 
 }  // namespace lbmb

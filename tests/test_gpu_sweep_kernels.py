@@ -230,3 +230,31 @@ def test_pair_register_budgets(budget, prec):
     ua, ub = a.read_moments()[1], b.read_moments()[1]
     tol = {"f32": 1e-5, "f16": 40 * 2.0 ** -10, "bf16": 40 * 2.0 ** -7}[prec]
     assert np.abs(ua - ub)[solid == 0].max() <= tol * max(np.abs(ua).max(), 1e-3)
+
+
+@pytest.mark.parametrize("budget", [(3, 3), (4, 4), (5, 5), (4, 3)])
+@pytest.mark.parametrize("q,coll,prec", [(19, "trt", "f32"), (19, "trt", "f16"), (19, "trt", "bf16"),
+                                         (27, "cm", "f32"), (27, "cm", "f16")])
+def test_pair_staged_matches_direct(budget, q, coll, prec):
+    # the cp.async-staged pair kernel reads the same bytes as the direct one
+    # (pairs, odd-offset pairs, wall links' own slots, 16-bit words split by
+    # element): the populations must agree bit for bit, on a walled cavity
+    # whose x extent leaves half-solid pairs at both ends of every row
+    dims, solid, wall_u, nu = cavity(19, u_lid=0.06, re=40.0)
+    dims = (dims[0] + 1, dims[1], dims[2])  # even nx: 20 cells, walls at x = 0 and 19
+    s3 = np.zeros((dims[2], dims[1], dims[0]), np.uint8)
+    s3[:, :, :19] = solid.reshape(dims[2], dims[1], 19)
+    s3[:, :, 19] = 1
+    solid = s3.ravel()
+    w3 = np.zeros((dims[2], dims[1], dims[0], 3))
+    w3[:, :, :19] = wall_u.reshape(dims[2], dims[1], 19, 3)
+    wall_u = w3.reshape(-1, 3)
+    runs = []
+    for staged in (False, True):
+        s = lb.Solver(dims, lattice=q, collision=coll, storage=prec, nu=nu, solid=solid, wall_u=wall_u)
+        s.set_sweep_kernel("pair")
+        s.set_sweep_variant(*(b + (10 if staged else 0) for b in budget))
+        s.run(23)
+        runs.append(s.stage_out())
+        s.close()
+    assert np.array_equal(runs[0], runs[1])
