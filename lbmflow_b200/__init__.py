@@ -479,7 +479,7 @@ class Solver:
     def autotune_sweep(self, steps_per_trial=20):
         """Time every applicable sweep kernel on this solver's grid and keep
         the fastest (state preserved). Returns the choice and the trials."""
-        cap = 64
+        cap = 256
         r = _AutotuneResult()
         desc = np.zeros(3 * cap, dtype=np.int32)
         ms = np.zeros(cap)
