@@ -698,8 +698,11 @@ def run_b200(args, rank, world, local):
     if tune["even_blocks_per_sm"] and tune["kind"] in ("lean", "pair", "window", "async") and storage != "f64":
         g2.set_sweep_variant(tune["even_blocks_per_sm"], tune["odd_blocks_per_sm"])
     # the caller's marker arrays live in pinned host memory (copied to the
-    # device by lbmb_ibm_set_body every step); the step's result is the IBM
-    # diagnostics record read back by lbmb_apply_rotating_ibm
+    # device every step); the step's result is the IBM diagnostics record
+    # read back to the host. Timed two ways: one lbmb_runner_step per step
+    # (the runner loop body in one call, the IBM beside the sweep), and the
+    # reference loop's four calls (clear field, upload markers, apply with
+    # the diagnostics, step).
     import torch
     pos_pin = torch.empty(body.positions.shape, dtype=torch.float64, pin_memory=True).numpy()
     w_pin = torch.empty(body.weights.shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -708,22 +711,30 @@ def run_b200(args, rank, world, local):
     body = lb.RotatingBody(body.center, body.omega, pos_pin, w_pin)
     h2d = body.positions.nbytes + body.weights.nbytes
     d2h = 128
-    for _ in range(3):
-        g2.clear_body_force_field()
-        g2.set_body(0, body)
-        g2.apply_rotating_ibm(body, cfg)
-        g2.run(1)
-    g2.sync()
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+
+    def calls_step():
         g2.clear_body_force_field()
         g2.set_body(0, body)  # host -> device upload of the marker set
         g2.apply_rotating_ibm(body, cfg)  # device -> host diagnostics
         g2.run(1)
-    g2.sync()
-    e2e_s = allmax(time.perf_counter() - t0, world)
+
+    def fused_step():
+        g2.runner_step(0, body, cfg)
+
+    e2e_per = {}
+    for name, fn in (("calls", calls_step), ("runner_step", fused_step)):
+        for _ in range(3):
+            fn()
+        g2.sync()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            fn()
+        g2.sync()
+        e2e_per[name] = allmax(time.perf_counter() - t0, world)
+    e2e_s = e2e_per["runner_step"]
     e2e_value = world * n_cells * e2e_steps / e2e_s / 1e6
+    e2e_calls_value = world * n_cells * e2e_steps / e2e_per["calls"] / 1e6
     g2.close()
     clk.__exit__()
     extra = {}
@@ -771,7 +782,11 @@ def run_b200(args, rank, world, local):
                    "l2": "inputs larger than L2 (populations %.0f MB)" % (q * 4 * n_cells / 1e6),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "path": "C ABI per step: ibm_set_body(host markers) + apply_rotating_ibm(diag to host) + step"},
+                "path": "C ABI per step: lbmb_runner_step (clear field, upload the host marker set, direct "
+                        "forcing beside the sweep, diagnostics to the host)",
+                "calls_value": e2e_calls_value,
+                "calls_path": "the same step as four C ABI calls: clear_body_force_field + ibm_set_body(host "
+                              "markers) + apply_rotating_ibm(diagnostics to host) + step"},
         "gpu_launches": int(13 * args.steps),
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -275,6 +275,19 @@ int lbmb_ibm_set_body(lbmb_solver* h, int32_t body, const double* pos, const dou
 int lbmb_apply_rotating_ibm(lbmb_solver* h, int32_t body, const lbmb_ibm_config* cfg,
                             lbmb_ibm_diag* diag);
 
+/* One iteration of the runner loop with the caller's marker set
+ * (crates/lbm-cli/src/runner.rs:1080-1085: clear_body_force_field, apply the
+ * impeller marker set, step): the same device work and results as
+ * lbmb_clear_body_force_field + lbmb_ibm_set_body + lbmb_apply_rotating_ibm
+ * + lbmb_step(h, 1), with the direct forcing and the IBM-forced cells on a
+ * side stream beside the full-grid sweep and one host synchronisation
+ * (the diagnostics are returned through a pinned staging copy). The marker
+ * arrays are copied every call (pinned host memory makes the copy
+ * asynchronous). diag may be NULL. Not with a uniform body force. */
+int lbmb_runner_step(lbmb_solver* h, int32_t body, const double* pos, const double* weight, int64_t n,
+                     const double center[3], const double omega[3], const lbmb_ibm_config* cfg,
+                     lbmb_ibm_diag* diag);
+
 /* Solver::enable_scalar_distribution (solver.rs:2856-2890): q = 7 (D3Q7,
  * cs^2 = 1/4) or the hydro lattice size (the reference's choice). */
 int lbmb_enable_scalar(lbmb_solver* h, int32_t q, double diffusivity, int32_t* index);

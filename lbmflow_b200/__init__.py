@@ -37,7 +37,7 @@ EXPORTS = (
     "lbmb_last_error", "lbmb_version", "lbmb_create", "lbmb_destroy", "lbmb_shape", "lbmb_init_fields",
     "lbmb_stage_in", "lbmb_stage_out", "lbmb_step", "lbmb_run_guarded", "lbmb_read_moments", "lbmb_reduce",
     "lbmb_total_mass", "lbmb_clear_body_force_field", "lbmb_get_force_field", "lbmb_ibm_set_body",
-    "lbmb_apply_rotating_ibm", "lbmb_enable_scalar", "lbmb_set_scalar_concentration",
+    "lbmb_apply_rotating_ibm", "lbmb_runner_step", "lbmb_enable_scalar", "lbmb_set_scalar_concentration",
     "lbmb_gather_scalar_concentration", "lbmb_scalar_cv", "lbmb_run_impeller", "lbmb_last_timing",
     "lbmb_build_wall_rims", "lbmb_build_stirred_tank", "lbmb_sync", "lbmb_reduce_populations_noalloc",
     "lbmb_set_sweep_kernel", "lbmb_get_sweep_kernel", "lbmb_set_sweep_variant", "lbmb_autotune_sweep",
@@ -263,6 +263,8 @@ def lib():
         L.lbmb_get_force_field.argtypes = [vp, _dp]
         L.lbmb_ibm_set_body.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int64, _dp, _dp]
         L.lbmb_apply_rotating_ibm.argtypes = [vp, C.c_int32, C.POINTER(_IbmConfig), C.POINTER(_IbmDiag)]
+        L.lbmb_runner_step.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int64, _dp, _dp, C.POINTER(_IbmConfig),
+                                       C.POINTER(_IbmDiag)]
         L.lbmb_enable_scalar.argtypes = [vp, C.c_int32, C.c_double, _i32p]
         L.lbmb_set_scalar_concentration.argtypes = [vp, C.c_int32, _dp]
         L.lbmb_gather_scalar_concentration.argtypes = [vp, C.c_int32, _dp]
@@ -648,6 +650,23 @@ class Solver:
         cfg = cfg or DirectForcingConfig()
         d = _IbmDiag()
         _check(lib().lbmb_apply_rotating_ibm(self.h, self._slot_for(body), C.byref(cfg._c()), C.byref(d)))
+        return IbmDiagnostics(d.iterations, d.slip_max, d.slip_rms, d.slip_max_rel, d.slip_rms_rel,
+                              np.array(d.torque[:]), np.array(d.fluid_force[:]), np.array(d.marker_force[:]),
+                              d.momentum_error_rel)
+
+    def runner_step(self, slot, body: RotatingBody, cfg: DirectForcingConfig = None) -> IbmDiagnostics:
+        """One iteration of the runner loop (runner.rs:1080-1085) with this
+        marker set in body slot `slot`: clear the force field, upload the
+        markers, apply the direct forcing, step; the IBM runs beside the
+        full-grid sweep and the call synchronises once."""
+        cfg = cfg or DirectForcingConfig()
+        pos = np.ascontiguousarray(body.positions, dtype=np.float64)
+        w = np.ascontiguousarray(body.weights, dtype=np.float64)
+        d = _IbmDiag()
+        _check(lib().lbmb_runner_step(self.h, int(slot), _d(pos), _d(w), int(w.size),
+                                      _d(np.asarray(body.center, dtype=np.float64)),
+                                      _d(np.asarray(body.omega, dtype=np.float64)), C.byref(cfg._c()), C.byref(d)))
+        self._bodies[int(slot)] = body
         return IbmDiagnostics(d.iterations, d.slip_max, d.slip_rms, d.slip_max_rel, d.slip_rms_rel,
                               np.array(d.torque[:]), np.array(d.fluid_force[:]), np.array(d.marker_force[:]),
                               d.momentum_error_rel)

@@ -126,6 +126,8 @@ struct EngineBase {
   virtual void ibm_set_body(int b, const double* pos, const double* w, int64_t n, const double* c,
                             const double* om) = 0;
   virtual void ibm_apply(int b, const lbmb_ibm_config& cfg, lbmb_ibm_diag* diag) = 0;
+  virtual void runner_step(int b, const double* pos, const double* w, int64_t n, const double* c,
+                           const double* om, const lbmb_ibm_config& cfg, lbmb_ibm_diag* diag) = 0;
   virtual int enable_scalar(int q, double d) = 0;
   virtual void set_scalar(int k, const double* c) = 0;
   virtual void get_scalar(int k, double* c) = 0;
@@ -312,12 +314,14 @@ struct Engine final : EngineBase {
   ~Engine() override {
     if (step_graph) cudaGraphExecDestroy(step_graph);
     for (auto& e : apply_cache) cudaGraphExecDestroy(e.exec);
+    for (auto& e : fused_cache) cudaGraphExecDestroy(e.exec);
     for (auto& g : run_graphs)
       if (g) cudaGraphExecDestroy(g);
     if (st) cudaStreamSynchronize(st);
     bodies.clear();
     scalars.clear();
     if (st2) cudaStreamSynchronize(st2);
+    if (h_diag) cudaFreeHost(h_diag);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -387,6 +391,7 @@ struct Engine final : EngineBase {
     }
     for (auto& e : apply_cache) CK(cudaGraphExecDestroy(e.exec));
     apply_cache.clear();
+    drop_fused_graphs();
     drop_run_graphs();
   }
 
@@ -1312,6 +1317,20 @@ struct Engine final : EngineBase {
     CK(cudaStreamSynchronize(st));
   }
 
+  // The device part of clear_force_field with no refresh pending: zero the
+  // current field, and the cached-moments field too when the cleared field
+  // was uniform.
+  void enqueue_clear_device() {
+    if (!nslots) return;
+    const unsigned g = unsigned(std::min<int64_t>(ceil_div(nslots, 256), int64_t(4) * sm_count));
+    CK(cudaMemsetAsync(d_flag.p, 0, sizeof(int), st));
+    field_uniform_kernel<A><<<g, 256, 0, st>>>(fcur.p, nslots, nslots == n ? 1 : 0, d_flag.p);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st));
+    field_zero_if_uniform_kernel<A><<<g, 256, 0, st>>>(fprev.p, nslots, d_flag.p);
+    CK(cudaGetLastError());
+  }
+
   // Solver::clear_body_force_field (solver.rs:2805-2822): a uniform field
   // (all cells equal) refreshes the cached moments without it; otherwise
   // the cached moments keep the old field until the next step.
@@ -1322,15 +1341,7 @@ struct Engine final : EngineBase {
       // field was uniform or not: the check and the conditional reset of
       // the cached-moments field run on the device, without a host sync.
       field_present = false;
-      if (nslots) {
-        const unsigned g = unsigned(std::min<int64_t>(ceil_div(nslots, 256), int64_t(4) * sm_count));
-        CK(cudaMemsetAsync(d_flag.p, 0, sizeof(int), st));
-        field_uniform_kernel<A><<<g, 256, 0, st>>>(fcur.p, nslots, nslots == n ? 1 : 0, d_flag.p);
-        CK(cudaGetLastError());
-        CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st));
-        field_zero_if_uniform_kernel<A><<<g, 256, 0, st>>>(fprev.p, nslots, d_flag.p);
-        CK(cudaGetLastError());
-      }
+      enqueue_clear_device();
       return;
     }
     bool uniform = true;
@@ -1648,21 +1659,27 @@ struct Engine final : EngineBase {
                     const double* om) override {
     if (b < 0 || b > 64) invalid("IBM body slot out of range");
     if (nm <= 0) invalid("IBM body must contain at least one marker");
-    for (int64_t m = 0; m < nm; ++m) {
-      for (int a = 0; a < 3; ++a)
-        if (!std::isfinite(pos[3 * m + a])) invalid("IBM marker must have finite position and positive finite weight");
-      if (!(std::isfinite(w[m]) && w[m] > 0.0))
-        invalid("IBM marker must have finite position and positive finite weight");
-    }
     for (int a = 0; a < 3; ++a)
       if (!std::isfinite(c[a]) || !std::isfinite(om[a])) invalid("IBM center and omega must be finite");
     if (int(bodies.size()) <= b) bodies.resize(size_t(b) + 1);
     // The runner passes the same marker set every step: when the markers are
-    // unchanged the stencils and device arrays stay; only the rotation
-    // (centre, angular velocity and the slip scale) is refreshed.
-    if (BodyState* old = bodies[size_t(b)].get()) {
-      if (old->nm == nm && std::memcmp(old->pos.data(), pos, size_t(3 * nm) * sizeof(double)) == 0 &&
-          std::memcmp(old->weight.data(), w, size_t(nm) * sizeof(double)) == 0) {
+    // unchanged (and so already checked) the stencils and device arrays
+    // stay; only the rotation (centre, angular velocity and the slip scale)
+    // is refreshed.
+    BodyState* old = bodies[size_t(b)].get();
+    const bool unchanged = old && old->nm == nm &&
+                           std::memcmp(old->pos.data(), pos, size_t(3 * nm) * sizeof(double)) == 0 &&
+                           std::memcmp(old->weight.data(), w, size_t(nm) * sizeof(double)) == 0;
+    if (!unchanged)
+      for (int64_t m = 0; m < nm; ++m) {
+        for (int a = 0; a < 3; ++a)
+          if (!std::isfinite(pos[3 * m + a]))
+            invalid("IBM marker must have finite position and positive finite weight");
+        if (!(std::isfinite(w[m]) && w[m] > 0.0))
+          invalid("IBM marker must have finite position and positive finite weight");
+      }
+    if (old) {
+      if (unchanged) {
         // the marker arrays are still copied, so the device always holds
         // what the caller passed (an asynchronous copy of the same bytes)
         CK(cudaMemcpyAsync(old->d_pos.p, pos, size_t(3 * nm) * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1916,8 +1933,9 @@ struct Engine final : EngineBase {
   std::vector<ApplyEntry> apply_cache;
   static constexpr size_t APPLY_CACHE = 8;
 
-  void ibm_apply(int b, const lbmb_ibm_config& c, lbmb_ibm_diag* out) override {
-    BodyState& B = body_for(b, c);
+  // The instantiated IBM graph of one apply (captured on the main stream at
+  // first use; launched on either stream).
+  cudaGraphExec_t apply_exec(BodyState& B, const lbmb_ibm_config& c) {
     ApplyKey k;
     std::memset(&k, 0, sizeof(k));
     k.a = ibm_args(B, c);
@@ -1944,12 +1962,116 @@ struct Engine final : EngineBase {
       CK(cudaGraphDestroy(g));
       apply_cache.push_back({k, exec});
     }
-    CK(cudaGraphLaunch(exec, st));
+    return exec;
+  }
+
+  void ibm_apply(int b, const lbmb_ibm_config& c, lbmb_ibm_diag* out) override {
+    BodyState& B = body_for(b, c);
+    CK(cudaGraphLaunch(apply_exec(B, c), st));
     field_present = true;
     fprev_stale = true;
     IbmDiagDev d;
     CK(cudaMemcpyAsync(&d, d_diag.p, sizeof(d), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    diag_out(d, out);
+  }
+
+  // Pinned host copy of the IBM diagnostics (runner_step).
+  IbmDiagDev* h_diag = nullptr;
+
+  // One iteration of the runner loop with the caller's marker set
+  // (runner.rs:1080-1085: clear_body_force_field, apply the marker set,
+  // step): the clear and the marker upload on the main stream, then the IBM
+  // apply, its diagnostics copy and the forced cells on the side stream
+  // beside the full-grid sweep (disjoint AA slots, as in run_impeller), one
+  // host sync. Same device operations and results as the four calls
+  // lbmb_clear_body_force_field, lbmb_ibm_set_body, lbmb_apply_rotating_ibm
+  // and lbmb_step(1).
+  // Instantiated device sequences of runner_step in the steady state (a
+  // field present, no refresh pending, no scalars), one per key (IBM
+  // arguments and AA parity): the clear, the fork, the sweep, the IBM, the
+  // diagnostics copy, the forced cells, the refresh and the join in one
+  // graph launch.
+  struct FusedEntry {
+    ApplyKey key;
+    cudaGraphExec_t exec;
+  };
+  std::vector<FusedEntry> fused_cache;
+
+  void drop_fused_graphs() {
+    for (auto& e : fused_cache) CK(cudaGraphExecDestroy(e.exec));
+    fused_cache.clear();
+  }
+
+  // The step's device work after the clear (the clear itself when
+  // with_clear): fork, full-grid sweep || IBM apply, diagnostics copy,
+  // forced cells and refresh, join.
+  void enqueue_runner_step(BodyState& B, const lbmb_ibm_config& c, bool with_clear) {
+    if (with_clear) enqueue_clear_device();
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+    launch_hydro(parity, st, true, false);
+    enqueue_ibm(B, c, nullptr, nullptr, nullptr, nullptr, false, st2);
+    CK(cudaMemcpyAsync(h_diag, d_diag.p, sizeof(IbmDiagDev), cudaMemcpyDeviceToHost, st2));
+    launch_hydro(parity, st2, false, true);
+    if (nslots) CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st2));
+    CK(cudaEventRecord(ev_join, st2));
+    CK(cudaStreamWaitEvent(st, ev_join, 0));
+  }
+
+  void runner_step(int b, const double* pos, const double* w, int64_t nm, const double* c, const double* om,
+                   const lbmb_ibm_config& cfg_ibm, lbmb_ibm_diag* out) override {
+    if (has_uniform_force()) throw Error(LBMB_ERR_UNSUPPORTED, "runner step: a uniform body force is set");
+    ibm_set_body(b, pos, w, nm, c, om);
+    BodyState& B = body_for(b, cfg_ibm);
+    if (!h_diag) CK(cudaMallocHost(&h_diag, sizeof(IbmDiagDev)));
+    const bool steady = field_present && !fprev_stale && scalars.empty();
+    if (steady) {
+      ApplyKey k;
+      std::memset(&k, 0, sizeof(k));
+      k.a = ibm_args(B, cfg_ibm);
+      k.f = fp;
+      k.slots = slot_cell.p;
+      k.field = fcur.p;
+      k.parity = parity;
+      k.sweeps = cfg_ibm.max_iterations;
+      cudaGraphExec_t exec = nullptr;
+      for (auto& e : fused_cache)
+        if (std::memcmp(&k, &e.key, sizeof(k)) == 0) exec = e.exec;
+      if (!exec) {
+        if (fused_cache.size() >= 4) {
+          CK(cudaGraphExecDestroy(fused_cache.front().exec));
+          fused_cache.erase(fused_cache.begin());
+        }
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue_runner_step(B, cfg_ibm, true);
+        CK(cudaStreamEndCapture(st, &g));
+        CK(cudaGraphInstantiate(&exec, g, 0));
+        CK(cudaGraphDestroy(g));
+        fused_cache.push_back({k, exec});
+      }
+      CK(cudaEventRecord(ev0, st));
+      CK(cudaGraphLaunch(exec, st));
+    } else {
+      clear_force_field();  // may synchronise (a refresh pending)
+      CK(cudaEventRecord(ev0, st));
+      enqueue_runner_step(B, cfg_ibm, false);
+    }
+    field_present = true;
+    fprev_stale = false;
+    parity ^= 1;
+    for (auto& sc : scalars) scalar_step(*sc);
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaStreamSynchronize(st));
+    pending_launches = 1;
+    timing_pending = true;
+    time += 1;
+    if (kernel_mode == LBMB_SWEEP_BULK) check_device_error();
+    diag_out(*h_diag, out);
+  }
+
+  static void diag_out(const IbmDiagDev& d, lbmb_ibm_diag* out) {
     if (out) {
       out->iterations = d.iterations;
       out->slip_max = d.slip_max;

@@ -401,6 +401,16 @@ int lbmb_apply_rotating_ibm(lbmb_solver* h, int32_t body, const lbmb_ibm_config*
   });
 }
 
+int lbmb_runner_step(lbmb_solver* h, int32_t body, const double* pos, const double* weight, int64_t n,
+                     const double center[3], const double omega[3], const lbmb_ibm_config* cfg,
+                     lbmb_ibm_diag* diag) {
+  return guarded([&] {
+    NEED(h);
+    if (!pos || !weight || !center || !omega || !cfg) throw Error(LBMB_ERR_INVALID, "null runner step argument");
+    h->e->runner_step(body, pos, weight, n, center, omega, *cfg, diag);
+  });
+}
+
 int lbmb_enable_scalar(lbmb_solver* h, int32_t q, double diffusivity, int32_t* index) {
   return guarded([&] {
     NEED(h);

@@ -90,3 +90,30 @@ def test_runner_timing_excludes_first_capture():
     t2 = g.last_timing()
     assert t1[2] == 32 and t2[2] == 32
     assert t2[0] > 0.0
+
+
+@pytest.mark.parametrize("storage,kind", [("f64", None), ("f32", "pair"), ("f16", "pair"), ("f32", "direct")])
+def test_runner_step_equals_the_four_calls(storage, kind):
+    # lbmb_runner_step overlaps the direct forcing with the full-grid sweep;
+    # it must give what the reference loop's calls give one after another
+    # (runner.rs:1080-1085): clear field, upload markers, apply, step
+    a, body, _, _ = _tank_solver(storage=storage, coll="cm", q=27)
+    b, _, _, _ = _tank_solver(storage=storage, coll="cm", q=27)
+    if kind:
+        a.set_sweep_kernel(kind)
+        b.set_sweep_kernel(kind)
+    cfg = lb.DirectForcingConfig()
+    for step in range(9):  # odd count: both parities, twice
+        a.clear_body_force_field()
+        a.set_body(0, body)
+        da = a.apply_rotating_ibm(body, cfg)
+        a.run(1)
+        db = b.runner_step(0, body, cfg)
+        assert da.iterations == db.iterations
+        assert np.array_equal(da.torque, db.torque) and np.array_equal(da.fluid_force, db.fluid_force)
+        assert da.slip_max == db.slip_max
+    assert np.array_equal(a.stage_out(), b.stage_out())
+    # and the device runner takes over from it without a seam
+    ra = a.run_impeller(body, 6)
+    rb = b.run_impeller(body, 6)
+    assert np.array_equal(ra["torque_lu"], rb["torque_lu"])
