@@ -280,10 +280,13 @@ int lbmb_apply_rotating_ibm(lbmb_solver* h, int32_t body, const lbmb_ibm_config*
  * impeller marker set, step): the same device work and results as
  * lbmb_clear_body_force_field + lbmb_ibm_set_body + lbmb_apply_rotating_ibm
  * + lbmb_step(h, 1), with the direct forcing and the IBM-forced cells on a
- * side stream beside the full-grid sweep and one host synchronisation
- * (the diagnostics are returned through a pinned staging copy). The marker
- * arrays are copied every call (pinned host memory makes the copy
- * asynchronous). diag may be NULL. Not with a uniform body force. */
+ * side stream beside the full-grid sweep. The call returns once the
+ * diagnostics are on the host (through a pinned staging copy); the step's
+ * sweep may still be running, as after lbmb_step, and later calls queue
+ * behind it (entry points that return data synchronise). The marker arrays
+ * are copied every call and may be changed once it returns (pinned host
+ * memory makes the copy asynchronous). diag may be NULL. Not with a uniform
+ * body force. */
 int lbmb_runner_step(lbmb_solver* h, int32_t body, const double* pos, const double* weight, int64_t n,
                      const double center[3], const double omega[3], const lbmb_ibm_config* cfg,
                      lbmb_ibm_diag* diag);

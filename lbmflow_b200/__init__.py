@@ -658,7 +658,8 @@ class Solver:
         """One iteration of the runner loop (runner.rs:1080-1085) with this
         marker set in body slot `slot`: clear the force field, upload the
         markers, apply the direct forcing, step; the IBM runs beside the
-        full-grid sweep and the call synchronises once."""
+        full-grid sweep, and the call returns once the diagnostics are on the
+        host (the sweep may still run, as after run())."""
         cfg = cfg or DirectForcingConfig()
         pos = np.ascontiguousarray(body.positions, dtype=np.float64)
         w = np.ascontiguousarray(body.weights, dtype=np.float64)

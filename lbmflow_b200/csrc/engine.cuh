@@ -273,6 +273,7 @@ struct Engine final : EngineBase {
     }
     CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_diag, cudaEventDisableTiming));
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
     solid_h.assign(size_t(n), 0);
@@ -326,6 +327,7 @@ struct Engine final : EngineBase {
     if (ev1) cudaEventDestroy(ev1);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_diag) cudaEventDestroy(ev_diag);
     if (st2) cudaStreamDestroy(st2);
     if (st) cudaStreamDestroy(st);
   }
@@ -1320,14 +1322,15 @@ struct Engine final : EngineBase {
   // The device part of clear_force_field with no refresh pending: zero the
   // current field, and the cached-moments field too when the cleared field
   // was uniform.
-  void enqueue_clear_device() {
+  void enqueue_clear_device(cudaStream_t s_ = nullptr) {
     if (!nslots) return;
+    cudaStream_t s = s_ ? s_ : st;
     const unsigned g = unsigned(std::min<int64_t>(ceil_div(nslots, 256), int64_t(4) * sm_count));
-    CK(cudaMemsetAsync(d_flag.p, 0, sizeof(int), st));
-    field_uniform_kernel<A><<<g, 256, 0, st>>>(fcur.p, nslots, nslots == n ? 1 : 0, d_flag.p);
+    CK(cudaMemsetAsync(d_flag.p, 0, sizeof(int), s));
+    field_uniform_kernel<A><<<g, 256, 0, s>>>(fcur.p, nslots, nslots == n ? 1 : 0, d_flag.p);
     CK(cudaGetLastError());
-    CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), st));
-    field_zero_if_uniform_kernel<A><<<g, 256, 0, st>>>(fprev.p, nslots, d_flag.p);
+    CK(cudaMemsetAsync(fcur.p, 0, size_t(nslots) * sizeof(Vec4<A>), s));
+    field_zero_if_uniform_kernel<A><<<g, 256, 0, s>>>(fprev.p, nslots, d_flag.p);
     CK(cudaGetLastError());
   }
 
@@ -1657,6 +1660,11 @@ struct Engine final : EngineBase {
   // ---- IBM -------------------------------------------------------------
   void ibm_set_body(int b, const double* pos, const double* w, int64_t nm, const double* c,
                     const double* om) override {
+    set_body(b, pos, w, nm, c, om, st);
+  }
+  // up: the stream of the marker upload when the marker set is unchanged.
+  void set_body(int b, const double* pos, const double* w, int64_t nm, const double* c, const double* om,
+                cudaStream_t up) {
     if (b < 0 || b > 64) invalid("IBM body slot out of range");
     if (nm <= 0) invalid("IBM body must contain at least one marker");
     for (int a = 0; a < 3; ++a)
@@ -1682,8 +1690,8 @@ struct Engine final : EngineBase {
       if (unchanged) {
         // the marker arrays are still copied, so the device always holds
         // what the caller passed (an asynchronous copy of the same bytes)
-        CK(cudaMemcpyAsync(old->d_pos.p, pos, size_t(3 * nm) * sizeof(double), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(old->d_weight.p, w, size_t(nm) * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(old->d_pos.p, pos, size_t(3 * nm) * sizeof(double), cudaMemcpyHostToDevice, up));
+        CK(cudaMemcpyAsync(old->d_weight.p, w, size_t(nm) * sizeof(double), cudaMemcpyHostToDevice, up));
         bool same = true;
         for (int a = 0; a < 3; ++a) same = same && old->center[a] == c[a] && old->omega[a] == om[a];
         if (same) return;
@@ -1976,17 +1984,19 @@ struct Engine final : EngineBase {
     diag_out(d, out);
   }
 
-  // Pinned host copy of the IBM diagnostics (runner_step).
+  // Pinned host copy of the IBM diagnostics (runner_step) and the event
+  // that marks its arrival.
   IbmDiagDev* h_diag = nullptr;
+  cudaEvent_t ev_diag = nullptr;
 
   // One iteration of the runner loop with the caller's marker set
   // (runner.rs:1080-1085: clear_body_force_field, apply the marker set,
-  // step): the clear and the marker upload on the main stream, then the IBM
+  // step): the marker upload and the clear on the main stream, then the IBM
   // apply, its diagnostics copy and the forced cells on the side stream
-  // beside the full-grid sweep (disjoint AA slots, as in run_impeller), one
-  // host sync. Same device operations and results as the four calls
-  // lbmb_clear_body_force_field, lbmb_ibm_set_body, lbmb_apply_rotating_ibm
-  // and lbmb_step(1).
+  // beside the full-grid sweep (disjoint AA slots, as in run_impeller); the
+  // host waits for the diagnostics only. Same device operations and results
+  // as the four calls lbmb_clear_body_force_field, lbmb_ibm_set_body,
+  // lbmb_apply_rotating_ibm and lbmb_step(1).
   // Instantiated device sequences of runner_step in the steady state (a
   // field present, no refresh pending, no scalars), one per key (IBM
   // arguments and AA parity): the clear, the fork, the sweep, the IBM, the
@@ -2003,16 +2013,20 @@ struct Engine final : EngineBase {
     fused_cache.clear();
   }
 
-  // The step's device work after the clear (the clear itself when
-  // with_clear): fork, full-grid sweep || IBM apply, diagnostics copy,
-  // forced cells and refresh, join.
-  void enqueue_runner_step(BodyState& B, const lbmb_ibm_config& c, bool with_clear) {
-    if (with_clear) enqueue_clear_device();
+  // The step's device work: the clear (captured form), fork, the full-grid
+  // sweep on the main stream and on the side stream the IBM apply, the
+  // diagnostics copy, the forced cells and the refresh; join. (Measured: the
+  // clear and the marker upload on the side stream instead made the
+  // per-call loop 6% slower.)
+  void enqueue_runner_step(BodyState& B, const lbmb_ibm_config& c, bool captured) {
+    if (captured) enqueue_clear_device();
     CK(cudaEventRecord(ev_fork, st));
     CK(cudaStreamWaitEvent(st2, ev_fork, 0));
     launch_hydro(parity, st, true, false);
     enqueue_ibm(B, c, nullptr, nullptr, nullptr, nullptr, false, st2);
     CK(cudaMemcpyAsync(h_diag, d_diag.p, sizeof(IbmDiagDev), cudaMemcpyDeviceToHost, st2));
+    // inside a graph, an external record node: the host waits on it
+    CK(cudaEventRecordWithFlags(ev_diag, st2, captured ? cudaEventRecordExternal : cudaEventRecordDefault));
     launch_hydro(parity, st2, false, true);
     if (nslots) CK(cudaMemcpyAsync(fprev.p, fcur.p, size_t(nslots) * sizeof(Vec4<A>), cudaMemcpyDeviceToDevice, st2));
     CK(cudaEventRecord(ev_join, st2));
@@ -2022,7 +2036,7 @@ struct Engine final : EngineBase {
   void runner_step(int b, const double* pos, const double* w, int64_t nm, const double* c, const double* om,
                    const lbmb_ibm_config& cfg_ibm, lbmb_ibm_diag* out) override {
     if (has_uniform_force()) throw Error(LBMB_ERR_UNSUPPORTED, "runner step: a uniform body force is set");
-    ibm_set_body(b, pos, w, nm, c, om);
+    set_body(b, pos, w, nm, c, om, st);
     BodyState& B = body_for(b, cfg_ibm);
     if (!h_diag) CK(cudaMallocHost(&h_diag, sizeof(IbmDiagDev)));
     const bool steady = field_present && !fprev_stale && scalars.empty();
@@ -2063,11 +2077,19 @@ struct Engine final : EngineBase {
     parity ^= 1;
     for (auto& sc : scalars) scalar_step(*sc);
     CK(cudaEventRecord(ev1, st));
-    CK(cudaStreamSynchronize(st));
     pending_launches = 1;
     timing_pending = true;
     time += 1;
-    if (kernel_mode == LBMB_SWEEP_BULK) check_device_error();
+    if (kernel_mode == LBMB_SWEEP_BULK) {
+      CK(cudaStreamSynchronize(st));
+      check_device_error();
+    } else {
+      // The call returns once the diagnostics are on the host, while the
+      // sweep may still run (as lbmb_step returns once its work is queued):
+      // the host's next call overlaps it. Entry points that return data
+      // synchronise the stream.
+      CK(cudaEventSynchronize(ev_diag));
+    }
     diag_out(*h_diag, out);
   }
 
