@@ -46,9 +46,9 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # one even and one odd launch) from an ncu full-set capture of the sweep kernel
 # the autotuner picks for the form, on the tank of the given diameter.
 NCU_TRAFFIC = {("hydro_async_kernel", 27, "cm", "f32", 128): 448.2e6,
-               ("hydro_pair_kernel", 27, "cm", "f32", 128): 460.1e6,
+               ("hydro_pair_kernel", 27, "cm", "f32", 128): 466.0e6,
                ("hydro_pair_kernel", 19, "trt", "f32", 256): 2720.2e6,
-               ("hydro_pair_kernel", 19, "trt", "f16", 256): 1408.9e6,
+               ("hydro_pair_kernel", 19, "trt", "f16", 256): 1406.1e6,
                ("hydro_pair_kernel", 19, "trt", "bf16", 256): 1403.9e6,
                ("hydro_pair_kernel", 27, "cm", "f32", 256): 3916.6e6,
                ("hydro_pair_kernel", 27, "cm", "f16", 256): 2006.1e6,
