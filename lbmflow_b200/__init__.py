@@ -424,6 +424,7 @@ class Solver:
                              _d(self._wall), C.byref(h)))
         self.h = h
         self._bodies = {}
+        self._runner_args = None
         self._lib = L  # kept for close() during interpreter shutdown
 
     def close(self):
@@ -661,12 +662,21 @@ class Solver:
         full-grid sweep, and the call returns once the diagnostics are on the
         host (the sweep may still run, as after run())."""
         cfg = cfg or DirectForcingConfig()
-        pos = np.ascontiguousarray(body.positions, dtype=np.float64)
-        w = np.ascontiguousarray(body.weights, dtype=np.float64)
-        d = _IbmDiag()
-        _check(lib().lbmb_runner_step(self.h, int(slot), _d(pos), _d(w), int(w.size),
-                                      _d(np.asarray(body.center, dtype=np.float64)),
-                                      _d(np.asarray(body.omega, dtype=np.float64)), C.byref(cfg._c()), C.byref(d)))
+        # the host arrays' pointers are kept while the caller passes the same
+        # arrays (a runner loop passes one marker set every step; their
+        # contents are read at each call)
+        arrays = (body.positions, body.weights, body.center, body.omega)
+        c = self._runner_args
+        if c is None or c[0] != int(slot) or any(a is not b for a, b in zip(c[1], arrays)):
+            pos = np.ascontiguousarray(body.positions, dtype=np.float64)
+            w = np.ascontiguousarray(body.weights, dtype=np.float64)
+            ctr = np.ascontiguousarray(body.center, dtype=np.float64)
+            om = np.ascontiguousarray(body.omega, dtype=np.float64)
+            c = (int(slot), arrays, (pos, w, ctr, om), (_d(pos), _d(w), int(w.size), _d(ctr), _d(om)), _IbmDiag())
+            self._runner_args = c
+        ptr, d = c[3], c[4]
+        _check(lib().lbmb_runner_step(self.h, int(slot), ptr[0], ptr[1], ptr[2], ptr[3], ptr[4], C.byref(cfg._c()),
+                                      C.byref(d)))
         self._bodies[int(slot)] = body
         return IbmDiagnostics(d.iterations, d.slip_max, d.slip_rms, d.slip_max_rel, d.slip_rms_rel,
                               np.array(d.torque[:]), np.array(d.fluid_force[:]), np.array(d.marker_force[:]),
